@@ -1,0 +1,162 @@
+/* treams_cuda.h — C ABI of the B200 (sm_100a) cluster multiple-scattering library.
+ *
+ * Every entry point replaces one Rust function of treams-core on the cluster hot path
+ * (cited per declaration as path:line inside the treams-rs tree). Complex numbers are
+ * two doubles (re, im), the layout of num_complex::Complex64; matrices are column-major,
+ * as nalgebra's DMatrix. Host-pointer entry points copy in and out; `_dev` entry points
+ * take device pointers and run on the context's stream.
+ *
+ * Errors: every call returns a tcu_status. The first six codes mirror treams-core's
+ * Error variants (lib.rs:384-411); the message of the last failure on the calling thread
+ * is tcu_last_error_message(). No call aborts or traps.
+ *
+ * Threading: a context owns one CUDA stream and its workspaces. Calls on one context are
+ * serialised by an internal mutex; distinct contexts may be used concurrently. Results
+ * do not depend on timing: every reduction runs in a fixed order.
+ */
+#ifndef TREAMS_CUDA_H
+#define TREAMS_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tcu_status {
+    TCU_OK = 0,
+    TCU_INVALID_INPUT = 1,      /* Error::InvalidInput */
+    TCU_SPECIAL_FUNCTION = 2,   /* Error::SpecialFunction */
+    TCU_NON_FINITE = 3,         /* Error::NonFinite */
+    TCU_NOT_CONVERGED = 4,      /* Error::NotConverged */
+    TCU_SINGULAR = 5,           /* Error::Singular */
+    TCU_OUT_OF_MEMORY = 6,      /* Error::OutOfMemory */
+    TCU_DEVICE_ERROR = 7,       /* CUDA runtime or kernel failure */
+    TCU_TIMEOUT = 8             /* a bounded device-side wait gave up */
+} tcu_status;
+
+typedef enum tcu_precision {
+    TCU_FP64 = 0,   /* complex128 LU, FP64 DMMA trailing updates */
+    TCU_MIXED = 1   /* complex64 LU, 3-pass split-TF32 tcgen05 updates, FP64 refinement */
+} tcu_precision;
+
+typedef enum tcu_preconditioner {
+    TCU_PRECOND_NONE = 0,          /* plain GMRES on I - T C */
+    TCU_PRECOND_BLOCK_JACOBI = 1,  /* neighbour-cluster block Jacobi */
+    TCU_PRECOND_LEARNED = 2        /* graph-network block-sparse approximate inverse */
+} tcu_preconditioner;
+
+typedef struct tcu_context tcu_context;
+typedef struct tcu_factor tcu_factor;
+
+/* Convergence certificate of one right-hand side (linalg/gmres.rs:86-93): the residual
+ * b - A x is recomputed in FP64 from the returned x. */
+typedef struct tcu_certificate {
+    int iterations;          /* GMRES iterations or refinement sweeps */
+    double residual_norm;    /* ||T b - (I - T C) x||_2 */
+    double rhs_norm;         /* ||T b||_2 */
+} tcu_certificate;
+
+/* GMRES options (linalg/gmres.rs:22-79). */
+typedef struct tcu_gmres_options {
+    double rtol;
+    double atol;
+    int restart;
+    int max_iterations;
+} tcu_gmres_options;
+
+/* ---- context ------------------------------------------------------------------------ */
+tcu_status tcu_context_create(int device, tcu_context** out);
+tcu_status tcu_context_destroy(tcu_context* ctx);
+/* The CUDA stream (cudaStream_t) the context runs on, for callers with device pointers. */
+void* tcu_context_stream(tcu_context* ctx);
+/* Thread-local message of the last failed call on this thread ("" if none). */
+const char* tcu_last_error_message(void);
+/* Number of kernel launches the context has issued (a counter for benchmarks). */
+long long tcu_context_launches(tcu_context* ctx);
+/* Per-stage device timing with CUDA events on the context stream (off by default).
+ * Stages: 0 assembly, 1 LU panel, 2 row swaps, 3 triangular block (TRSM), 4 trailing
+ * update GEMM, 5 operand packing, 6 triangular solves, 7 matrix-free operator, 8 Mie,
+ * 9 lattice sums, 10 batched small LU. Reading synchronises the stream. */
+tcu_status tcu_context_set_profiling(tcu_context* ctx, int enabled);
+tcu_status tcu_context_stage_time(tcu_context* ctx, int stage, long long* launches, double* total_ms);
+tcu_status tcu_context_reset_stage_times(tcu_context* ctx);
+
+/* ---- translation coefficients -------------------------------------------------------- */
+/* M x M block (M = 2 lmax (lmax + 2)) of vector spherical wave translation coefficients
+ * from a source to a destination at displacement disp = destination - source, helicity
+ * (helicity != 0) or parity modes, outgoing (singular != 0) or regular radial functions;
+ * column-major, source modes outer. Replaces TranslationPlan::evaluate (sw/plan.rs:282). */
+tcu_status tcu_translation_block(tcu_context* ctx, int lmax, double k, const double* disp, int singular,
+                                 int helicity, double* out);
+
+/* ---- Mie T and incident fields -------------------------------------------------------- */
+/* 2 x 2 Mie blocks in mode order, lmax per sphere, N spheres: out N * lmax * 4 complex,
+ * row-major per block (tmatrix/sphere.rs:43-80, coeffs/mie.rs:209). */
+tcu_status tcu_mie_blocks(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii, const double* eps,
+                          double* out);
+
+/* Regular expansion of p plane waves at the N sphere positions (pw/expand.rs:308-360):
+ * kvecs holds 3 complex per wave, pols 0/1 per wave (helicity); out n x p column-major. */
+tcu_status tcu_plane_wave_expansion(tcu_context* ctx, int lmax, size_t N, const double* positions, int p,
+                                    const double* kvecs, const int* pols, double* out);
+
+/* Scattering and extinction cross sections of p columns (python/treams_rs/_tmatrix.py:
+ * 413-441, flux 0.5): sca = Re(x^H O x) / k0^2 with O the regular coupling between all
+ * positions (applied matrix-free), ext = -Re(b^H x) / k0^2. */
+tcu_status tcu_cross_sections(tcu_context* ctx, int lmax, double k0, size_t N, const double* positions, int p,
+                              const double* x, const double* b, double* sca, double* ext);
+
+/* ---- dense cluster solve ------------------------------------------------------------- */
+/* Assemble I - T C for N spheres (eps: N complex, positions: 3 N doubles) and factor it
+ * in the given precision. Replaces cluster::sphere_cluster_factor (cluster/spheres.rs:85)
+ * = cluster_parts + InteractionFactor::from_blocks (cluster/interaction.rs:194). */
+tcu_status tcu_sphere_cluster_factor(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                     const double* eps, const double* positions, int precision, tcu_factor** out);
+/* Device-pointer variant: radii, eps, positions are device arrays. */
+tcu_status tcu_sphere_cluster_factor_dev(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                         const double* eps, const double* positions, int precision,
+                                         tcu_factor** out);
+/* Solve (I - T C) X = T B for p incident columns B (n x p), X out (n x p); certificates
+ * (p entries) may be NULL. Replaces InteractionFactor::solve (cluster/interaction.rs:214).
+ * Mixed factors refine in FP64 until ||r|| <= 1e-13 ||T b|| (at most 10 sweeps). */
+tcu_status tcu_factor_solve(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
+tcu_status tcu_factor_solve_dev(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
+/* Dimension n = N M of a factor. */
+size_t tcu_factor_dimension(const tcu_factor* f);
+tcu_status tcu_factor_destroy(tcu_factor* f);
+
+/* The assembled operator I - T C (n x n complex128, column-major, host), for inspection. */
+tcu_status tcu_cluster_operator(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                const double* eps, const double* positions, double* out);
+
+/* ---- matrix-free cluster ------------------------------------------------------------- */
+/* y = (I - T C) x for p columns without forming C (cluster/iterative.rs:225-232). */
+tcu_status tcu_cluster_apply(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii, const double* eps,
+                             const double* positions, int p, const double* x, double* y);
+/* Restarted GMRES on (I - T C) X = T B (cluster/iterative.rs:264-284, linalg/gmres.rs:119).
+ * The preconditioner, if any, is applied on the right; certificates report the true
+ * unpreconditioned residual. */
+tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                               const double* eps, const double* positions, const double* B, int p,
+                               const tcu_gmres_options* options, int preconditioner, double* X,
+                               tcu_certificate* certificates);
+
+/* ---- 2D lattice sums and periodic arrays --------------------------------------------- */
+/* Ewald lattice sums D_lm (lattice/mod.rs:11-15, 283; ewald.rs:39-270) of a 2D lattice
+ * for nk Bloch vectors, every degree l <= lmax_sum and order m (table index l*l+l+m):
+ * k real wavenumber, lattice 2 x 2 row vectors, kpars nk x 2, shift r[3] = 0 (one sphere
+ * per cell), eta (0 = automatic split, cell.rs:164-175). out nk x (lmax_sum+1)^2. */
+tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
+                              const double* kpars, double eta, double* out);
+/* Periodic array of one sphere per cell: X(kpar) = (I - T S(kpar))^-1 T for nk Bloch
+ * vectors (cluster/interaction.rs:292 with sw::lattice_expansion, sw/expansion.rs:418).
+ * out nk x M x M (column-major per kpar). */
+tcu_status tcu_array_solve_batch(tcu_context* ctx, int lmax, double k0, double radius, const double* eps,
+                                 const double* lattice, size_t nk, const double* kpars, double eta, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TREAMS_CUDA_H */

@@ -1,0 +1,235 @@
+"""CPU oracle — test infrastructure only.
+
+ctypes binding of ``oracle/liboracle.so``, the C++ restatement of the treams-rs FP64
+cluster path (``oracle.cpp``) and 2D Ewald lattice sums (``ewald.cpp``). Only the tests,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import this module,
+to check or time the CUDA library. The product never calls it.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+_LIB = None
+
+c_int = ctypes.c_int
+c_double = ctypes.c_double
+P = ctypes.c_void_p
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            build()
+        _LIB = ctypes.CDLL(str(path))
+        L = _LIB
+        L.orc_wigner3j.restype = c_double
+        L.orc_wigner3j.argtypes = [c_int] * 6
+        L.orc_degrees.restype = c_int
+        L.orc_degrees.argtypes = [c_int, c_int, c_int, c_int, c_int, P, c_int]
+        L.orc_spherical_hankels.argtypes = [c_int, c_double, P]
+        L.orc_spherical_j.argtypes = [c_int, c_double, c_double, P]
+        L.orc_spherical_h.argtypes = [c_int, c_double, c_double, P]
+        L.orc_solid_table.argtypes = [c_int, P, P]
+        L.orc_plan_terms.restype = c_int
+        L.orc_plan_terms.argtypes = [c_int]
+        L.orc_translation_block.argtypes = [c_int, c_double, P, c_int, c_int, P]
+        L.orc_mie_block.argtypes = [c_int, c_double, c_double, c_double, P]
+        L.orc_cluster_operator.argtypes = [c_int, c_double, c_int, P, P, P, P, P]
+        L.orc_plane_wave_expansion.argtypes = [c_int, c_int, P, c_int, P, P, P]
+        L.orc_dense_solve.restype = c_int
+        L.orc_dense_solve.argtypes = [c_int, c_int, P, P, P, c_int, P]
+        L.orc_lu_solve.restype = c_int
+        L.orc_lu_solve.argtypes = [c_int, P, P, c_int]
+        L.orc_cross_sections.argtypes = [c_int, c_double, c_int, P, P, P, P, P]
+        L.orc_iterative_apply.argtypes = [c_int, c_double, c_int, P, P, P, P, c_int, P]
+        L.orc_iterative_solve.restype = c_int
+        L.orc_iterative_solve.argtypes = [c_int, c_double, c_int, P, P, P, P, c_int, c_double, c_double,
+                                          c_int, c_int, P, P, P]
+        L.orc_gmres_dense.restype = c_int
+        L.orc_gmres_dense.argtypes = [c_int, P, P, c_double, c_int, c_int, P, P, P]
+        if hasattr(L, "orc_lsumsw2d"):
+            L.orc_lsumsw2d.restype = c_int
+            L.orc_lsumsw2d.argtypes = [c_int, c_int, c_double, c_double, P, P, P, c_double, c_double, P, P]
+        if hasattr(L, "orc_lsumsw2d_table"):
+            L.orc_lsumsw2d_table.restype = c_int
+            L.orc_lsumsw2d_table.argtypes = [c_int, c_double, c_double, P, P, P, c_double, c_double, P]
+        if hasattr(L, "orc_kambe"):
+            L.orc_kambe.restype = c_int
+            L.orc_kambe.argtypes = [c_int, c_double, c_double, c_double, c_double, P]
+        if hasattr(L, "orc_upper_gamma"):
+            L.orc_upper_gamma.restype = c_int
+            L.orc_upper_gamma.argtypes = [c_double, c_double, c_double, P]
+        if hasattr(L, "orc_array_solve"):
+            L.orc_array_solve.restype = c_int
+            L.orc_array_solve.argtypes = [c_int, c_double, c_double, c_double, P, P, c_double, c_double, c_int,
+                                          P, P]
+    return _LIB
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def modes(lmax: int) -> list[tuple[int, int, int]]:
+    return [(l, m, pol) for l in range(1, lmax + 1) for m in range(-l, l + 1) for pol in (1, 0)]
+
+
+def wigner3j(j1, j2, j3, m1, m2, m3) -> float:
+    return lib().orc_wigner3j(j1, j2, j3, m1, m2, m3)
+
+
+def degrees(l, m, lam, mu, cross) -> list[int]:
+    out = np.zeros(64, np.int32)
+    k = lib().orc_degrees(l, m, lam, mu, int(cross), _p(out), 64)
+    return [int(v) for v in out[:k]]
+
+
+def spherical_hankels(last: int, x: float) -> np.ndarray:
+    out = np.zeros(last + 1, np.complex128)
+    lib().orc_spherical_hankels(last, float(x), _p(out))
+    return out
+
+
+def spherical_j(last: int, z: complex) -> np.ndarray:
+    out = np.zeros(last + 1, np.complex128)
+    lib().orc_spherical_j(last, z.real, z.imag, _p(out))
+    return out
+
+
+def spherical_h(last: int, z: complex) -> np.ndarray:
+    out = np.zeros(last + 1, np.complex128)
+    lib().orc_spherical_h(last, z.real, z.imag, _p(out))
+    return out
+
+
+def solid_table(order: int, unit) -> np.ndarray:
+    u = np.ascontiguousarray(unit, np.float64)
+    out = np.zeros((order + 1) ** 2, np.complex128)
+    lib().orc_solid_table(order, _p(u), _p(out))
+    return out
+
+
+def plan_terms(lmax: int) -> int:
+    return lib().orc_plan_terms(lmax)
+
+
+def translation_block(lmax: int, k: float, disp, singular=True, helicity=True) -> np.ndarray:
+    M = 2 * lmax * (lmax + 2)
+    d = np.ascontiguousarray(disp, np.float64)
+    out = np.zeros(M * M, np.complex128)
+    lib().orc_translation_block(lmax, float(k), _p(d), int(singular), int(helicity), _p(out))
+    return out.reshape(M, M).T.copy()  # column-major storage -> (row, col)
+
+
+def mie_block(l: int, size: float, eps: complex) -> np.ndarray:
+    out = np.zeros(4, np.complex128)
+    lib().orc_mie_block(l, float(size), eps.real, eps.imag, _p(out))
+    return out.reshape(2, 2)
+
+
+def cluster_operator(lmax, k0, radii, eps, pos):
+    """A = I - T C as an (n, n) array plus the T blocks (N, lmax, 2, 2)."""
+    N = len(radii)
+    M = 2 * lmax * (lmax + 2)
+    n = N * M
+    r = np.ascontiguousarray(radii, np.float64)
+    e = np.ascontiguousarray(eps, np.complex128)
+    x = np.ascontiguousarray(pos, np.float64)
+    A = np.zeros((n, n), np.complex128, order="F")
+    tb = np.zeros((N, lmax, 2, 2), np.complex128)
+    lib().orc_cluster_operator(lmax, float(k0), N, _p(r), _p(e), _p(x), _p(A), _p(tb))
+    return A, tb
+
+
+def plane_wave_expansion(lmax, pos, kvecs, pols):
+    N = len(pos)
+    M = 2 * lmax * (lmax + 2)
+    x = np.ascontiguousarray(pos, np.float64)
+    kv = np.ascontiguousarray(kvecs, np.complex128)
+    pl = np.ascontiguousarray(pols, np.int32)
+    p = len(pl)
+    out = np.zeros((N * M, p), np.complex128, order="F")
+    lib().orc_plane_wave_expansion(lmax, N, _p(x), p, _p(kv), _p(pl), _p(out))
+    return out
+
+
+def dense_solve(lmax, A, tb, B):
+    """Solve (I - T C) X = T B with the restated LU."""
+    n, p = B.shape
+    N = tb.shape[0]
+    A = np.asfortranarray(A, np.complex128)
+    tb = np.ascontiguousarray(tb, np.complex128)
+    B = np.asfortranarray(B, np.complex128)
+    X = np.zeros((n, p), np.complex128, order="F")
+    st = lib().orc_dense_solve(lmax, N, _p(A), _p(tb), _p(B), p, _p(X))
+    if st:
+        raise RuntimeError(f"oracle dense solve failed with status {st}")
+    return X
+
+
+def lu_solve(A, B):
+    A = np.asfortranarray(A, np.complex128)
+    X = np.asfortranarray(B, np.complex128).copy(order="F")
+    st = lib().orc_lu_solve(A.shape[0], _p(A), _p(X), X.shape[1] if X.ndim == 2 else 1)
+    if st:
+        raise RuntimeError(f"oracle LU failed with status {st}")
+    return X
+
+
+def cross_sections(lmax, k0, pos, x, b):
+    xp = np.ascontiguousarray(pos, np.float64)
+    xx = np.ascontiguousarray(x, np.complex128)
+    bb = np.ascontiguousarray(b, np.complex128)
+    sca = c_double()
+    ext = c_double()
+    lib().orc_cross_sections(lmax, float(k0), len(pos), _p(xp), _p(xx), _p(bb), ctypes.byref(sca), ctypes.byref(ext))
+    return sca.value, ext.value
+
+
+def iterative_apply(lmax, k0, radii, eps, pos, X):
+    X = np.asfortranarray(X, np.complex128)
+    if X.ndim == 1:
+        X = X[:, None]
+    r = np.ascontiguousarray(radii, np.float64)
+    e = np.ascontiguousarray(eps, np.complex128)
+    x = np.ascontiguousarray(pos, np.float64)
+    Y = np.zeros_like(X, order="F")
+    lib().orc_iterative_apply(lmax, float(k0), len(r), _p(r), _p(e), _p(x), _p(X), X.shape[1], _p(Y))
+    return Y
+
+
+def iterative_solve(lmax, k0, radii, eps, pos, B, rtol=1e-10, atol=0.0, restart=30, max_iterations=300):
+    B = np.asfortranarray(B, np.complex128)
+    if B.ndim == 1:
+        B = B[:, None]
+    p = B.shape[1]
+    r = np.ascontiguousarray(radii, np.float64)
+    e = np.ascontiguousarray(eps, np.complex128)
+    x = np.ascontiguousarray(pos, np.float64)
+    X = np.zeros_like(B, order="F")
+    its = np.zeros(p, np.int32)
+    res = np.zeros(p, np.float64)
+    st = lib().orc_iterative_solve(lmax, float(k0), len(r), _p(r), _p(e), _p(x), _p(B), p, rtol, atol, restart,
+                                   max_iterations, _p(X), _p(its), _p(res))
+    return X, its, res, st
+
+
+def gmres_dense(A, b, rtol=1e-10, restart=30, max_iterations=300):
+    A = np.asfortranarray(A, np.complex128)
+    b = np.ascontiguousarray(b, np.complex128)
+    x = np.zeros_like(b)
+    its = np.zeros(1, np.int32)
+    res = np.zeros(1, np.float64)
+    st = lib().orc_gmres_dense(A.shape[0], _p(A), _p(b), rtol, restart, max_iterations, _p(x), _p(its), _p(res))
+    return x, int(its[0]), float(res[0]), st

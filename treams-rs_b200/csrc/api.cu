@@ -1,0 +1,844 @@
+// The C ABI (include/treams_cuda.h): contexts, validation mirroring treams-core, device
+// buffers, the dense factor + refinement driver and the GMRES driver.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/treams_cuda.h"
+#include "kernels.h"
+#include "plan.h"
+#include "precond.h"
+
+using namespace tcu;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+tcu_status fail(tcu_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+struct DevPlanStore {
+    HostPlan host;
+    DevPlan dev{};
+    void* mem = nullptr;
+};
+
+}  // namespace
+
+namespace tcu {
+thread_local Profiler* g_prof = nullptr;
+}
+
+struct tcu_context {
+    Profiler prof;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::recursive_mutex mu;
+    std::map<int, std::unique_ptr<DevPlanStore>> plans;
+    long long launches = 0;
+    double* d_partial = nullptr;  // reduction scratch (8 * 256 doubles)
+    cplx* d_cpartial = nullptr;   // complex reduction scratch (64 * 256)
+    double* d_small = nullptr;    // 64 doubles
+    cplx* d_csmall = nullptr;     // 64 complex
+    int* d_status = nullptr;
+    double* d_lfac = nullptr;     // sqrt((l-m)!/(l+m)!) table up to degree 16
+};
+
+struct tcu_factor {
+    tcu_context* ctx = nullptr;
+    int L = 0, N = 0;
+    size_t n = 0;
+    int precision = 0;
+    double k0 = 0;
+    double* d_pos = nullptr;
+    double* d_radii = nullptr;
+    cplx* d_eps = nullptr;
+    cplx* d_T = nullptr;
+    void* d_A = nullptr;
+    LuWork wk;
+};
+
+namespace {
+
+struct ProfGuard {
+    Profiler* prev;
+    explicit ProfGuard(tcu_context* ctx) : prev(g_prof) { g_prof = &ctx->prof; }
+    ~ProfGuard() { g_prof = prev; }
+};
+
+tcu_status cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return TCU_OK;
+    if (e == cudaErrorMemoryAllocation) return fail(TCU_OUT_OF_MEMORY, std::string(what) + ": " + cudaGetErrorString(e));
+    return fail(TCU_DEVICE_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(call, what)                              \
+    do {                                            \
+        tcu_status _s = cuda_check((call), (what)); \
+        if (_s != TCU_OK) return _s;                \
+    } while (0)
+
+bool finite_all(const double* p, size_t n) {
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+
+// cluster/spheres.rs:99-133
+tcu_status validate_spheres(int L, double k0, size_t N, const double* radii, const double* eps, const double* pos) {
+    if (L < 1 || L > 7) return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 7");
+    if (!std::isfinite(k0) || k0 <= 0.0 || N == 0 || !radii || !eps || !pos)
+        return fail(TCU_INVALID_INPUT,
+                    "require positive finite k0 and radii, and matching finite permittivities and positions");
+    for (size_t i = 0; i < N; ++i)
+        if (!std::isfinite(radii[i]) || radii[i] <= 0.0)
+            return fail(TCU_INVALID_INPUT,
+                        "require positive finite k0 and radii, and matching finite permittivities and positions");
+    if (!finite_all(eps, 2 * N) || !finite_all(pos, 3 * N))
+        return fail(TCU_INVALID_INPUT,
+                    "require positive finite k0 and radii, and matching finite permittivities and positions");
+    for (size_t i = 0; i < N; ++i)
+        for (size_t j = 0; j < i; ++j) {
+            double d = std::hypot(std::hypot(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1]),
+                                  pos[3 * i + 2] - pos[3 * j + 2]);
+            if (d <= radii[i] + radii[j] || !std::isfinite(d))
+                return fail(TCU_INVALID_INPUT,
+                            "spherical particles must have finite separation and must not touch or overlap");
+        }
+    return TCU_OK;
+}
+
+tcu_status get_plan(tcu_context* ctx, int L, const DevPlan** out) {
+    auto it = ctx->plans.find(L);
+    if (it == ctx->plans.end()) {
+        auto store = std::make_unique<DevPlanStore>();
+        store->host = build_plan(L);
+        HostPlan& h = store->host;
+        size_t ncombo = (size_t)h.nlm * h.nlm;
+        size_t nterm = h.idx.size();
+        size_t off_combo = 0, off_w = ncombo * 8, off_refl = off_w + nterm * 16,
+               off_idx = off_refl + h.reflection.size() * 8;
+        size_t total = off_idx + nterm + 16;
+        CK(cudaMalloc(&store->mem, total), "plan allocation");
+        char* base = (char*)store->mem;
+        CK(cudaMemcpy(base + off_combo, h.combo.data(), ncombo * 8, cudaMemcpyHostToDevice), "plan upload");
+        CK(cudaMemcpy(base + off_w, h.w.data(), nterm * 16, cudaMemcpyHostToDevice), "plan upload");
+        CK(cudaMemcpy(base + off_refl, h.reflection.data(), h.reflection.size() * 8, cudaMemcpyHostToDevice),
+           "plan upload");
+        CK(cudaMemcpy(base + off_idx, h.idx.data(), nterm, cudaMemcpyHostToDevice), "plan upload");
+        DevPlan& d = store->dev;
+        d.L = L;
+        d.nlm = h.nlm;
+        d.order = h.order;
+        d.tsize = (h.order + 1) * (h.order + 1);
+        d.combo = (const int2*)(base + off_combo);
+        d.w = (const double2*)(base + off_w);
+        d.reflection = (const double*)(base + off_refl);
+        d.idx = (const uint8_t*)(base + off_idx);
+        it = ctx->plans.emplace(L, std::move(store)).first;
+    }
+    *out = &it->second->dev;
+    return TCU_OK;
+}
+
+tcu_status sync_status(tcu_context* ctx, const char* what) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    return cuda_check(e, what);
+}
+
+tcu_status read_status(tcu_context* ctx, const char* what) {
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), what);
+    tcu_status s = sync_status(ctx, what);
+    if (s != TCU_OK) return s;
+    if (st == 5) return fail(TCU_SINGULAR, std::string(what) + ": numerically singular");
+    if (st == 8) return fail(TCU_TIMEOUT, std::string(what) + ": a device-side wait gave up");
+    if (st != 0) return fail(TCU_DEVICE_ERROR, std::string(what) + ": device status " + std::to_string(st));
+    return TCU_OK;
+}
+
+template <typename T>
+tcu_status dev_alloc(T** p, size_t count, const char* what) {
+    return cuda_check(cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T)), what);
+}
+
+struct DevBuf {
+    void* p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+// The y = zadd + alpha x + beta T C x operator in chunks of at most 8 columns.
+void apply_op(tcu_context* ctx, const DevPlan* P, int N, double k0, const double* d_pos, const cplx* d_T, const cplx* x,
+              size_t n, int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y) {
+    for (int c0 = 0; c0 < ncol; c0 += 8) {
+        int nc = std::min(8, ncol - c0);
+        launch_apply(*P, N, k0, d_pos, d_T, x + c0 * n, n, nc, zadd ? zadd + c0 * n : nullptr, alpha, beta, singular,
+                     y + c0 * n, ctx->stream);
+        ++ctx->launches;
+    }
+}
+
+tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const double* radii_h, const double* eps_h,
+                       const double* pos_h, const double* radii_d, const double* eps_d, const double* pos_d,
+                       int precision, tcu_factor** out) {
+    if (!out) return fail(TCU_INVALID_INPUT, "null output handle");
+    *out = nullptr;
+    if (precision != TCU_FP64 && precision != TCU_MIXED) return fail(TCU_INVALID_INPUT, "unknown precision");
+    tcu_status s = validate_spheres(L, k0, N, radii_h, eps_h, pos_h);
+    if (s) return s;
+    const DevPlan* P;
+    s = get_plan(ctx, L, &P);
+    if (s) return s;
+    size_t M = 2 * (size_t)L * (L + 2);
+    size_t n = N * M;
+    if (n > 28416) return fail(TCU_INVALID_INPUT, "dense cluster dimension above 28416; use the iterative solver");
+    auto f = std::make_unique<tcu_factor>();
+    f->ctx = ctx;
+    f->L = L;
+    f->N = (int)N;
+    f->n = n;
+    f->precision = precision;
+    f->k0 = k0;
+    auto cleanup = [&]() {
+        if (f->d_pos) cudaFree(f->d_pos);
+        if (f->d_radii) cudaFree(f->d_radii);
+        if (f->d_eps) cudaFree(f->d_eps);
+        if (f->d_T) cudaFree(f->d_T);
+        if (f->d_A) cudaFree(f->d_A);
+        if (f->wk.piv) cudaFree(f->wk.piv);
+    };
+    tcu_status e = TCU_OK;
+    do {
+        if ((e = dev_alloc(&f->d_pos, 3 * N, "positions"))) break;
+        if ((e = dev_alloc(&f->d_radii, N, "radii"))) break;
+        if ((e = dev_alloc(&f->d_eps, N, "permittivities"))) break;
+        if ((e = dev_alloc(&f->d_T, N * L * 4, "T blocks"))) break;
+        cudaMemcpyKind kind = pos_d ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+        if ((e = cuda_check(cudaMemcpyAsync(f->d_pos, pos_d ? pos_d : pos_h, 3 * N * 8, kind, ctx->stream), "copy"))) break;
+        if ((e = cuda_check(cudaMemcpyAsync(f->d_radii, radii_d ? radii_d : radii_h, N * 8, kind, ctx->stream), "copy")))
+            break;
+        if ((e = cuda_check(cudaMemcpyAsync(f->d_eps, eps_d ? eps_d : eps_h, N * 16, kind, ctx->stream), "copy"))) break;
+        size_t elem = precision == TCU_FP64 ? 16 : 8;
+        if ((e = cuda_check(cudaMalloc(&f->d_A, n * n * elem), "interaction matrix"))) break;
+        size_t ws = lu_workspace_bytes((int)n, precision == TCU_MIXED);
+        void* wmem = nullptr;
+        if ((e = cuda_check(cudaMalloc(&wmem, ws), "LU workspace"))) break;
+        f->wk.piv = (int*)wmem;
+        f->wk.perm = f->wk.piv + n;
+        f->wk.barrier = (unsigned*)(f->wk.perm + n);
+        f->wk.status = (int*)(f->wk.barrier + 4);
+        f->wk.cand = (void*)(((uintptr_t)(f->wk.status + 4) + 255) & ~(uintptr_t)255);
+        CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream), "status");
+        CK(cudaMemsetAsync(f->wk.status, 0, sizeof(int), ctx->stream), "status");
+        launch_mie(L, k0, (int)N, f->d_radii, f->d_eps, f->d_T, ctx->d_status, ctx->stream);
+        ++ctx->launches;
+        if ((e = read_status(ctx, "Mie coefficients"))) break;
+        launch_assemble(*P, (int)N, k0, f->d_pos, f->d_T, f->d_A, n, precision == TCU_MIXED, ctx->stream);
+        ++ctx->launches;
+        int rc;
+        if (precision == TCU_FP64)
+            rc = lu_factor_fp64((double2*)f->d_A, (int)n, f->wk, ctx->stream, &ctx->launches);
+        else
+            rc = lu_factor_fp32((float2*)f->d_A, (int)n, f->wk, ctx->stream, &ctx->launches, tf32_enabled());
+        if (rc) {
+            e = fail(TCU_DEVICE_ERROR, "LU panel launch failed (cooperative launch or shared memory)");
+            break;
+        }
+        int st = 0;
+        if ((e = cuda_check(cudaMemcpyAsync(&st, f->wk.status, 4, cudaMemcpyDeviceToHost, ctx->stream), "LU"))) break;
+        if ((e = sync_status(ctx, "LU factorization"))) break;
+        if (st == 5) {
+            e = fail(TCU_SINGULAR, "LU factorization: zero pivot");
+            break;
+        }
+        if (st == 8) {
+            e = fail(TCU_TIMEOUT, "LU factorization: a device-side wait gave up");
+            break;
+        }
+    } while (0);
+    if (e) {
+        cleanup();
+        return e;
+    }
+    *out = f.release();
+    return TCU_OK;
+}
+
+tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certs, bool device) {
+    if (!f || !B || !X || p <= 0) return fail(TCU_INVALID_INPUT, "require a factor and at least one column");
+    tcu_context* ctx = f->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    const DevPlan* P;
+    tcu_status s = get_plan(ctx, f->L, &P);
+    if (s) return s;
+    size_t n = f->n;
+    if (!device && !finite_all(B, 2 * n * p))
+        return fail(TCU_INVALID_INPUT,
+                    "require finite channel-by-illumination columns matching the factorization");
+    DevBuf bufs;
+    size_t per = n * p;
+    CK(cudaMalloc(&bufs.p, 5 * per * sizeof(cplx)), "solve buffers");
+    cplx* b = (cplx*)bufs.p;
+    cplx* tb = b + per;
+    cplx* x = tb + per;
+    cplx* r = x + per;
+    cplx* tmp = r + per;
+    CK(cudaMemcpyAsync(b, B, per * 16, device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream),
+       "copy rhs");
+    launch_apply_t(f->L, f->N, f->d_T, b, p, tb, ctx->stream);
+    ++ctx->launches;
+    std::vector<double> rn(p), bn(p);
+    vec_norms(tb, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(bn.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "norms");
+    int sweeps = 0;
+    auto lu_apply = [&](cplx* v) {
+        if (f->precision == TCU_FP64)
+            lu_solve_fp64((const double2*)f->d_A, (int)n, f->wk.perm, v, tmp, p, ctx->stream, &ctx->launches);
+        else
+            lu_solve_fp32((const float2*)f->d_A, (int)n, f->wk.perm, v, tmp, p, ctx->stream, &ctx->launches);
+    };
+    auto residual = [&]() -> tcu_status {
+        // r = T b - (x - T C x)
+        apply_op(ctx, P, f->N, f->k0, f->d_pos, f->d_T, x, n, p, tb, -1.0, 1.0, true, r);
+        vec_norms(r, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
+        ctx->launches += 2;
+        CK(cudaMemcpyAsync(rn.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "norms");
+        return sync_status(ctx, "residual");
+    };
+    CK(cudaMemcpyAsync(x, tb, per * 16, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    lu_apply(x);
+    sweeps = 1;
+    if ((s = residual())) return s;
+    if (f->precision == TCU_MIXED) {
+        const double tol = 1e-13;
+        double prev = INFINITY;
+        for (int it = 0; it < 10; ++it) {
+            double worst = 0.0;
+            for (int c = 0; c < p; ++c) worst = std::max(worst, bn[c] > 0 ? rn[c] / bn[c] : rn[c]);
+            if (worst <= tol || !(worst < 0.5 * prev)) break;
+            prev = worst;
+            lu_apply(r);
+            vec_axpy(x, r, n, p, ctx->stream);
+            ++ctx->launches;
+            ++sweeps;
+            if ((s = residual())) return s;
+        }
+    }
+    for (int c = 0; c < p; ++c)
+        if (!std::isfinite(rn[c])) return fail(TCU_SINGULAR, "non-finite solution: numerically singular operator");
+    CK(cudaMemcpyAsync(X, x, per * 16, device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream),
+       "copy solution");
+    if ((s = sync_status(ctx, "solve"))) return s;
+    if (certs)
+        for (int c = 0; c < p; ++c) {
+            certs[c].iterations = sweeps;
+            certs[c].residual_norm = rn[c];
+            certs[c].rhs_norm = bn[c];
+        }
+    return TCU_OK;
+}
+
+}  // namespace
+
+// =========================================================================================
+extern "C" {
+
+const char* tcu_last_error_message(void) { return g_last_error.c_str(); }
+
+tcu_status tcu_context_create(int device, tcu_context** out) {
+    if (!out) return fail(TCU_INVALID_INPUT, "null output handle");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        return fail(TCU_DEVICE_ERROR, "no CUDA device available: the library has no CPU path");
+    if (device < 0 || device >= count) return fail(TCU_INVALID_INPUT, "device index out of range");
+    CK(cudaSetDevice(device), "set device");
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device), "device properties");
+    if (prop.major != 10) return fail(TCU_DEVICE_ERROR, "the library is built for sm_100a (B200) only");
+    auto ctx = std::make_unique<tcu_context>();
+    ctx->device = device;
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+    CK(cudaMalloc(&ctx->d_partial, 8 * 256 * sizeof(double)), "scratch");
+    CK(cudaMalloc(&ctx->d_cpartial, 64 * 256 * sizeof(cplx)), "scratch");
+    CK(cudaMalloc(&ctx->d_small, 64 * sizeof(double)), "scratch");
+    CK(cudaMalloc(&ctx->d_csmall, 64 * sizeof(cplx)), "scratch");
+    CK(cudaMalloc(&ctx->d_status, 16), "scratch");
+    std::vector<double> lfac(17 * 17);
+    for (int l = 0; l <= 16; ++l)
+        for (int m = -l; m <= l; ++m)
+            lfac[l * l + l + m] = std::exp(0.5 * (std::lgamma(l - m + 1.0) - std::lgamma(l + m + 1.0)));
+    CK(cudaMalloc(&ctx->d_lfac, lfac.size() * 8), "scratch");
+    CK(cudaMemcpy(ctx->d_lfac, lfac.data(), lfac.size() * 8, cudaMemcpyHostToDevice), "upload");
+    lu_init_attributes();
+    pairs_init_attributes();
+    *out = ctx.release();
+    return TCU_OK;
+}
+
+tcu_status tcu_context_destroy(tcu_context* ctx) {
+    if (!ctx) return TCU_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->plans) cudaFree(kv.second->mem);
+    cudaFree(ctx->d_partial);
+    cudaFree(ctx->d_cpartial);
+    cudaFree(ctx->d_small);
+    cudaFree(ctx->d_csmall);
+    cudaFree(ctx->d_status);
+    cudaFree(ctx->d_lfac);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return TCU_OK;
+}
+
+void* tcu_context_stream(tcu_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+tcu_status tcu_context_set_profiling(tcu_context* ctx, int enabled) {
+    if (!ctx) return fail(TCU_INVALID_INPUT, "null context");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ctx->prof.on = enabled != 0;
+    return TCU_OK;
+}
+tcu_status tcu_context_stage_time(tcu_context* ctx, int stage, long long* launches, double* total_ms) {
+    if (!ctx || stage < 0 || stage >= ST_COUNT || !launches || !total_ms) return fail(TCU_INVALID_INPUT, "bad stage");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ctx->prof.collect();
+    *launches = ctx->prof.count[stage];
+    *total_ms = ctx->prof.total_ms[stage];
+    return TCU_OK;
+}
+tcu_status tcu_context_reset_stage_times(tcu_context* ctx) {
+    if (!ctx) return fail(TCU_INVALID_INPUT, "null context");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ctx->prof.collect();
+    for (int i = 0; i < ST_COUNT; ++i) {
+        ctx->prof.count[i] = 0;
+        ctx->prof.total_ms[i] = 0.0;
+    }
+    return TCU_OK;
+}
+long long tcu_context_launches(tcu_context* ctx) { return ctx ? ctx->launches : 0; }
+
+tcu_status tcu_translation_block(tcu_context* ctx, int lmax, double k, const double* disp, int singular, int helicity,
+                                 double* out) {
+    if (!ctx || !disp || !out) return fail(TCU_INVALID_INPUT, "null argument");
+    if (lmax < 1 || lmax > 7 || !std::isfinite(k) || k <= 0 || !finite_all(disp, 3))
+        return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 7, positive finite k and a finite displacement");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    if (singular && disp[0] == 0.0 && disp[1] == 0.0 && disp[2] == 0.0)
+        return fail(TCU_INVALID_INPUT, "outgoing spherical waves are singular at zero");
+    const DevPlan* P;
+    tcu_status s = get_plan(ctx, lmax, &P);
+    if (s) return s;
+    size_t M = 2 * (size_t)lmax * (lmax + 2);
+    DevBuf buf;
+    CK(cudaMalloc(&buf.p, M * M * 16), "block");
+    launch_block(*P, k, disp, singular != 0, helicity != 0, (cplx*)buf.p, ctx->stream);
+    ++ctx->launches;
+    CK(cudaMemcpyAsync(out, buf.p, M * M * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    return sync_status(ctx, "translation block");
+}
+
+tcu_status tcu_mie_blocks(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii, const double* eps,
+                          double* out) {
+    if (!ctx || !radii || !eps || !out || N == 0) return fail(TCU_INVALID_INPUT, "null argument");
+    if (lmax < 1 || lmax > 7 || !std::isfinite(k0) || k0 <= 0) return fail(TCU_INVALID_INPUT, "k0 must be finite and positive");
+    for (size_t i = 0; i < N; ++i)
+        if (!std::isfinite(radii[i]) || radii[i] <= 0) return fail(TCU_INVALID_INPUT, "radii must be finite and positive");
+    if (!finite_all(eps, 2 * N)) return fail(TCU_INVALID_INPUT, "permittivities must be finite");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    DevBuf buf;
+    CK(cudaMalloc(&buf.p, N * 8 + N * 16 + N * lmax * 64), "mie buffers");
+    double* r = (double*)buf.p;
+    cplx* e = (cplx*)(r + N);
+    cplx* T = e + N;
+    CK(cudaMemcpyAsync(r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
+    launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
+    ++ctx->launches;
+    tcu_status s = read_status(ctx, "Mie coefficients");
+    if (s) return s;
+    CK(cudaMemcpyAsync(out, T, N * lmax * 64, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    return sync_status(ctx, "Mie coefficients");
+}
+
+tcu_status tcu_plane_wave_expansion(tcu_context* ctx, int lmax, size_t N, const double* positions, int p,
+                                    const double* kvecs, const int* pols, double* out) {
+    if (!ctx || !positions || !kvecs || !pols || !out || N == 0 || p <= 0) return fail(TCU_INVALID_INPUT, "null argument");
+    if (lmax < 1 || lmax > 7) return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 7");
+    for (int c = 0; c < p; ++c)
+        if (pols[c] != 0 && pols[c] != 1) return fail(TCU_INVALID_INPUT, "polarization must be 0 or 1");
+    if (!finite_all(kvecs, 6 * p) || !finite_all(positions, 3 * N))
+        return fail(TCU_INVALID_INPUT, "wavevector must be finite");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M;
+    DevBuf buf;
+    CK(cudaMalloc(&buf.p, N * 24 + p * 48 + p * 4 + 16 + n * p * 16), "plane-wave buffers");
+    double* pos = (double*)buf.p;
+    cplx* kv = (cplx*)(pos + 3 * N);
+    cplx* o = kv + 3 * p;
+    int* pl = (int*)(o + n * p);
+    CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(kv, kvecs, p * 48, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(pl, pols, p * 4, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    launch_plane_wave(lmax, (int)N, pos, p, kv, pl, ctx->d_lfac, o, ctx->stream);
+    ++ctx->launches;
+    CK(cudaMemcpyAsync(out, o, n * p * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    return sync_status(ctx, "plane-wave expansion");
+}
+
+tcu_status tcu_cross_sections(tcu_context* ctx, int lmax, double k0, size_t N, const double* positions, int p,
+                              const double* x, const double* b, double* sca, double* ext) {
+    if (!ctx || !positions || !x || !b || !sca || !ext || N == 0 || p <= 0) return fail(TCU_INVALID_INPUT, "null argument");
+    if (lmax < 1 || lmax > 7 || !std::isfinite(k0) || k0 <= 0) return fail(TCU_INVALID_INPUT, "invalid lmax or k0");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    const DevPlan* P;
+    tcu_status s = get_plan(ctx, lmax, &P);
+    if (s) return s;
+    size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M, per = n * p;
+    DevBuf buf;
+    CK(cudaMalloc(&buf.p, N * 24 + 3 * per * 16), "cross-section buffers");
+    double* pos = (double*)buf.p;
+    cplx* dx = (cplx*)(pos + 3 * N);
+    cplx* db = dx + per;
+    cplx* ox = db + per;
+    CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(dx, x, per * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(db, b, per * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    apply_op(ctx, P, (int)N, k0, pos, nullptr, dx, n, p, nullptr, 1.0, 1.0, false, ox);
+    std::vector<double> s1(p), s2(p);
+    vec_real_dots(dx, ox, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
+    CK(cudaMemcpyAsync(s1.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    vec_real_dots(db, dx, n, p, ctx->d_small + 32, ctx->d_partial + 4 * 256, ctx->stream);
+    ctx->launches += 4;
+    CK(cudaMemcpyAsync(s2.data(), ctx->d_small + 32, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    s = sync_status(ctx, "cross sections");
+    if (s) return s;
+    for (int c = 0; c < p; ++c) {
+        sca[c] = s1[c] / (k0 * k0);
+        ext[c] = -s2[c] / (k0 * k0);
+    }
+    return TCU_OK;
+}
+
+tcu_status tcu_sphere_cluster_factor(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                     const double* eps, const double* positions, int precision, tcu_factor** out) {
+    if (!ctx) return fail(TCU_INVALID_INPUT, "null context");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    return factor_impl(ctx, lmax, k0, N, radii, eps, positions, nullptr, nullptr, nullptr, precision, out);
+}
+
+tcu_status tcu_sphere_cluster_factor_dev(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                         const double* eps, const double* positions, int precision,
+                                         tcu_factor** out) {
+    if (!ctx || !radii || !eps || !positions) return fail(TCU_INVALID_INPUT, "null argument");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    // validation reads the (small) geometry back to the host
+    std::vector<double> r(N), e(2 * N), p(3 * N);
+    CK(cudaMemcpyAsync(r.data(), radii, N * 8, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(e.data(), eps, N * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(p.data(), positions, N * 24, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    tcu_status s = sync_status(ctx, "copy");
+    if (s) return s;
+    return factor_impl(ctx, lmax, k0, N, r.data(), e.data(), p.data(), radii, eps, positions, precision, out);
+}
+
+tcu_status tcu_factor_solve(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates) {
+    return solve_impl(f, B, p, X, certificates, false);
+}
+tcu_status tcu_factor_solve_dev(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates) {
+    return solve_impl(f, B, p, X, certificates, true);
+}
+size_t tcu_factor_dimension(const tcu_factor* f) { return f ? f->n : 0; }
+
+tcu_status tcu_factor_destroy(tcu_factor* f) {
+    if (!f) return TCU_OK;
+    cudaSetDevice(f->ctx->device);
+    cudaStreamSynchronize(f->ctx->stream);
+    cudaFree(f->d_pos);
+    cudaFree(f->d_radii);
+    cudaFree(f->d_eps);
+    cudaFree(f->d_T);
+    cudaFree(f->d_A);
+    cudaFree(f->wk.piv);
+    if (f->wk.pack) cudaFree(f->wk.pack);
+    delete f;
+    return TCU_OK;
+}
+
+tcu_status tcu_cluster_operator(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                const double* eps, const double* positions, double* out) {
+    if (!ctx || !out) return fail(TCU_INVALID_INPUT, "null argument");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    tcu_status s = validate_spheres(lmax, k0, N, radii, eps, positions);
+    if (s) return s;
+    const DevPlan* P;
+    if ((s = get_plan(ctx, lmax, &P))) return s;
+    size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M;
+    DevBuf buf;
+    CK(cudaMalloc(&buf.p, N * 24 + N * 8 + N * 16 + N * lmax * 64 + n * n * 16), "operator buffers");
+    double* pos = (double*)buf.p;
+    double* r = pos + 3 * N;
+    cplx* e = (cplx*)(r + N);
+    cplx* T = e + N;
+    cplx* A = T + N * lmax * 4;
+    CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
+    launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
+    if ((s = read_status(ctx, "Mie coefficients"))) return s;
+    launch_assemble(*P, (int)N, k0, pos, T, A, n, false, ctx->stream);
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(out, A, n * n * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    return sync_status(ctx, "cluster operator");
+}
+
+tcu_status tcu_cluster_apply(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii, const double* eps,
+                             const double* positions, int p, const double* x, double* y) {
+    if (!ctx || !x || !y || p <= 0) return fail(TCU_INVALID_INPUT, "null argument");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    tcu_status s = validate_spheres(lmax, k0, N, radii, eps, positions);
+    if (s) return s;
+    const DevPlan* P;
+    if ((s = get_plan(ctx, lmax, &P))) return s;
+    size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M, per = n * p;
+    DevBuf buf;
+    CK(cudaMalloc(&buf.p, N * 24 + N * 8 + N * 16 + N * lmax * 64 + 2 * per * 16), "apply buffers");
+    double* pos = (double*)buf.p;
+    double* r = pos + 3 * N;
+    cplx* e = (cplx*)(r + N);
+    cplx* T = e + N;
+    cplx* dx = T + N * lmax * 4;
+    cplx* dy = dx + per;
+    CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(dx, x, per * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
+    launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
+    ++ctx->launches;
+    if ((s = read_status(ctx, "Mie coefficients"))) return s;
+    apply_op(ctx, P, (int)N, k0, pos, T, dx, n, p, nullptr, 1.0, -1.0, true, dy);
+    CK(cudaMemcpyAsync(y, dy, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    return sync_status(ctx, "cluster apply");
+}
+
+}  // extern "C"
+
+// ---- GMRES --------------------------------------------------------------------------------
+namespace tcu {
+
+// Restarted GMRES of linalg/gmres.rs:119-347 on device vectors: Arnoldi with two classical
+// Gram-Schmidt passes (each a fixed-order batched dot product), Givens rotations and the
+// Hessenberg solve on the host, true residual b - A x at every restart. With a right
+// preconditioner M the Krylov space is built for A M and x = M y.
+tcu_status gmres_device(tcu_context* ctx, const DevPlan* P, int N, double k0, const double* d_pos, const cplx* d_T,
+                        const cplx* rhs, size_t n, const tcu_gmres_options& opt, Preconditioner* pre, cplx* x,
+                        cplx* work, tcu_certificate* cert) {
+    int restart = (int)std::min<long long>(std::min<long long>(opt.restart, (long long)n), opt.max_iterations);
+    cplx* V = work;                       // (restart + 1) * n
+    cplx* w = V + (size_t)(restart + 1) * n;
+    cplx* r = w + n;
+    cplx* z = r + n;                      // preconditioned vector
+    cplx* Z = z + n;                      // preconditioned basis (restart * n) when pre
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemsetAsync(x, 0, n * 16, st), "zero");
+    CK(cudaMemcpyAsync(r, rhs, n * 16, cudaMemcpyDeviceToDevice, st), "copy");
+    double bnorm = 0, rnorm = 0;
+    vec_norms(rhs, n, 1, ctx->d_small, ctx->d_partial, st);
+    CK(cudaMemcpyAsync(&bnorm, ctx->d_small, 8, cudaMemcpyDeviceToHost, st), "norm");
+    tcu_status s = sync_status(ctx, "gmres");
+    if (s) return s;
+    rnorm = bnorm;
+    double tol = std::max(opt.atol, opt.rtol * bnorm);
+    int iterations = 0;
+    std::vector<std::complex<double>> h((size_t)(restart + 1) * restart), g(restart + 1);
+    std::vector<std::pair<double, std::complex<double>>> rot;
+    std::vector<std::complex<double>> hp(restart + 1);
+    while (true) {
+        cert->iterations = iterations;
+        cert->residual_norm = rnorm;
+        cert->rhs_norm = bnorm;
+        if (std::isfinite(rnorm) && rnorm <= tol) return TCU_OK;
+        if (!std::isfinite(rnorm) || iterations >= opt.max_iterations) {
+            char msg[256];
+            snprintf(msg, sizeof msg, "GMRES did not converge after %d iterations: residual %e, tolerance %e", iterations,
+                     rnorm, tol);
+            return fail(TCU_NOT_CONVERGED, msg);
+        }
+        vec_scale_copy(V, r, n, 1.0 / rnorm, st);
+        std::fill(h.begin(), h.end(), 0.0);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = rnorm;
+        rot.clear();
+        int used = 0;
+        for (int j = 0; j < restart; ++j) {
+            const cplx* vin = V + (size_t)j * n;
+            if (pre) {
+                pre->apply(vin, Z + (size_t)j * n, st);
+                vin = Z + (size_t)j * n;
+            }
+            launch_apply(*P, N, k0, d_pos, d_T, vin, n, 1, nullptr, 1.0, -1.0, true, w, st);
+            ctx->launches += 2;
+            for (int pass = 0; pass < 2; ++pass) {
+                vec_dots(V, n, j + 1, w, n, ctx->d_csmall, ctx->d_cpartial, st);
+                vec_gemv_sub(w, V, n, j + 1, ctx->d_csmall, n, st);
+                CK(cudaMemcpyAsync(hp.data(), ctx->d_csmall, (j + 1) * 16, cudaMemcpyDeviceToHost, st), "dots");
+                if ((s = sync_status(ctx, "gmres"))) return s;
+                for (int i = 0; i <= j; ++i) h[(size_t)j * (restart + 1) + i] += hp[i];
+                ctx->launches += 3;
+            }
+            double next = 0;
+            vec_norms(w, n, 1, ctx->d_small, ctx->d_partial, st);
+            CK(cudaMemcpyAsync(&next, ctx->d_small, 8, cudaMemcpyDeviceToHost, st), "norm");
+            if ((s = sync_status(ctx, "gmres"))) return s;
+            ctx->launches += 2;
+            h[(size_t)j * (restart + 1) + j + 1] = next;
+            for (size_t i = 0; i < rot.size(); ++i) {
+                size_t off = (size_t)j * (restart + 1) + i;
+                auto a = h[off], b = h[off + 1];
+                h[off] = rot[i].first * a + rot[i].second * b;
+                h[off + 1] = -std::conj(rot[i].second) * a + rot[i].first * b;
+            }
+            size_t dg = (size_t)j * (restart + 1) + j;
+            auto a = h[dg], b = h[dg + 1];
+            double length = std::hypot(std::abs(a), std::abs(b));
+            if (!std::isfinite(length) || length == 0.0)
+                return fail(TCU_NOT_CONVERGED, "GMRES Arnoldi breakdown before convergence");
+            std::complex<double> phase = std::abs(a) == 0.0 ? 1.0 : a / std::abs(a);
+            double c = std::abs(a) / length;
+            auto sn = phase * std::conj(b) / length;
+            h[dg] = phase * length;
+            h[dg + 1] = 0.0;
+            rot.push_back({c, sn});
+            g[j + 1] = -std::conj(sn) * g[j];
+            g[j] *= c;
+            used = j + 1;
+            iterations += 1;
+            if (std::abs(g[j + 1]) <= tol || next == 0.0 || iterations == opt.max_iterations) break;
+            vec_scale_copy(V + (size_t)(j + 1) * n, w, n, 1.0 / next, st);
+            ++ctx->launches;
+        }
+        for (int i = used - 1; i >= 0; --i) {
+            std::complex<double> tail = 0.0;
+            for (int jj = i + 1; jj < used; ++jj) tail += h[(size_t)jj * (restart + 1) + i] * g[jj];
+            g[i] = (g[i] - tail) / h[(size_t)i * (restart + 1) + i];
+        }
+        CK(cudaMemcpyAsync(ctx->d_csmall, g.data(), used * 16, cudaMemcpyHostToDevice, st), "coefficients");
+        vec_lincomb(x, pre ? Z : V, n, used, ctx->d_csmall, n, st);
+        // true residual r = rhs - A x
+        launch_apply(*P, N, k0, d_pos, d_T, x, n, 1, rhs, -1.0, 1.0, true, r, st);
+        vec_norms(r, n, 1, ctx->d_small, ctx->d_partial, st);
+        CK(cudaMemcpyAsync(&rnorm, ctx->d_small, 8, cudaMemcpyDeviceToHost, st), "norm");
+        if ((s = sync_status(ctx, "gmres"))) return s;
+        ctx->launches += 4;
+    }
+}
+
+}  // namespace tcu
+
+extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                          const double* eps, const double* positions, const double* B, int p,
+                                          const tcu_gmres_options* options, int preconditioner, double* X,
+                                          tcu_certificate* certificates) {
+    if (!ctx || !B || !X || p <= 0) return fail(TCU_INVALID_INPUT, "null argument");
+    tcu_gmres_options opt = options ? *options : tcu_gmres_options{1e-10, 0.0, 30, 300};
+    if (!std::isfinite(opt.rtol) || !std::isfinite(opt.atol) || opt.rtol < 0 || opt.atol < 0 ||
+        opt.rtol + opt.atol == 0.0 || opt.restart <= 0 || opt.max_iterations <= 0)
+        return fail(TCU_INVALID_INPUT,
+                    "GMRES needs finite nonnegative tolerances, a positive tolerance, restart and iteration limit");
+    if (preconditioner < 0 || preconditioner > 2) return fail(TCU_INVALID_INPUT, "unknown preconditioner");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    tcu_status s = validate_spheres(lmax, k0, N, radii, eps, positions);
+    if (s) return s;
+    const DevPlan* P;
+    if ((s = get_plan(ctx, lmax, &P))) return s;
+    size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M, per = n * p;
+    if (!finite_all(B, 2 * per))
+        return fail(TCU_INVALID_INPUT,
+                    "incident coefficients must be finite, with one row per local multipole and at least one column");
+    int restart = std::min(opt.restart, opt.max_iterations);
+    if ((size_t)restart > n) restart = (int)n;
+    DevBuf buf;
+    size_t work = (size_t)(2 * restart + 4) * n;
+    CK(cudaMalloc(&buf.p, N * 24 + N * 8 + N * 16 + N * lmax * 64 + (3 * per + work) * 16), "GMRES buffers");
+    double* pos = (double*)buf.p;
+    double* r = pos + 3 * N;
+    cplx* e = (cplx*)(r + N);
+    cplx* T = e + N;
+    cplx* b = T + N * lmax * 4;
+    cplx* tb = b + per;
+    cplx* x = tb + per;
+    cplx* wk = x + per;
+    CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(b, B, per * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
+    launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
+    ++ctx->launches;
+    if ((s = read_status(ctx, "Mie coefficients"))) return s;
+    launch_apply_t(lmax, (int)N, T, b, p, tb, ctx->stream);
+    ++ctx->launches;
+    std::unique_ptr<Preconditioner> pre;
+    if (preconditioner != TCU_PRECOND_NONE) {
+        s = make_preconditioner(ctx->stream, preconditioner, *P, lmax, (int)N, k0, pos, T, &pre, &ctx->launches);
+        if (s) return s;
+    }
+    tcu_status worst = TCU_OK;
+    std::string msg;
+    for (int c = 0; c < p; ++c) {
+        tcu_certificate cert{};
+        s = gmres_device(ctx, P, (int)N, k0, pos, T, tb + c * n, n, opt, pre.get(), x + c * n, wk, &cert);
+        if (certificates) certificates[c] = cert;
+        if (s && !worst) {
+            worst = s;
+            msg = g_last_error;
+        }
+    }
+    CK(cudaMemcpyAsync(X, x, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    s = sync_status(ctx, "GMRES");
+    if (s) return s;
+    if (worst) return fail(worst, msg);
+    return TCU_OK;
+}

@@ -1,0 +1,124 @@
+// Host-side launchers of the device kernels (one header for the C ABI layer).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "plan.h"
+
+#include <vector>
+
+namespace tcu {
+
+typedef double2 cplx;
+
+// Per-stage CUDA-event timing (tcu_context_set_profiling). The API layer installs the
+// context's profiler as the calling thread's current one for the duration of a call; the
+// launch sites bracket their kernels with a StageScope.
+enum Stage { ST_ASSEMBLE = 0, ST_PANEL, ST_SWAP, ST_TRSM, ST_GEMM, ST_PACK, ST_SOLVE, ST_APPLY, ST_MIE, ST_LATTICE,
+             ST_SMALL_LU, ST_COUNT };
+struct Profiler {
+    bool on = false;
+    struct Rec {
+        int stage;
+        cudaEvent_t a, b;
+    };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    double total_ms[ST_COUNT] = {};
+    long long count[ST_COUNT] = {};
+    cudaEvent_t take() {
+        if (!pool.empty()) {
+            cudaEvent_t e = pool.back();
+            pool.pop_back();
+            return e;
+        }
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        return e;
+    }
+    void collect() {
+        for (auto& r : recs) {
+            cudaEventSynchronize(r.b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, r.a, r.b);
+            total_ms[r.stage] += ms;
+            count[r.stage] += 1;
+            pool.push_back(r.a);
+            pool.push_back(r.b);
+        }
+        recs.clear();
+    }
+    ~Profiler() {
+        collect();
+        for (auto e : pool) cudaEventDestroy(e);
+    }
+};
+extern thread_local Profiler* g_prof;
+struct StageScope {
+    Profiler* p;
+    int stage;
+    cudaStream_t st;
+    cudaEvent_t a = nullptr;
+    StageScope(int stage_, cudaStream_t st_) : p(g_prof), stage(stage_), st(st_) {
+        if (p && p->on) {
+            a = p->take();
+            cudaEventRecord(a, st);
+        }
+    }
+    ~StageScope() {
+        if (a) {
+            cudaEvent_t b = p->take();
+            cudaEventRecord(b, st);
+            p->recs.push_back({stage, a, b});
+        }
+    }
+};
+
+// pairs.cu
+void launch_assemble(const DevPlan& P, int N, double k, const double* pos, const cplx* T, void* out, size_t ld,
+                     bool fp32, cudaStream_t st);
+void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
+                  int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st);
+size_t apply_smem_bytes(const DevPlan& P, int ncol);
+void launch_block(const DevPlan& P, double k, const double* d, bool singular, bool helicity, cplx* out,
+                  cudaStream_t st);
+void launch_mie(int L, double k0, int N, const double* radii, const cplx* eps, cplx* T, int* status, cudaStream_t st);
+void launch_plane_wave(int L, int N, const double* pos, int ncol, const cplx* kvecs, const int* pols,
+                       const double* lfac, cplx* out, cudaStream_t st);
+void launch_apply_t(int L, int N, const cplx* T, const cplx* x, int ncol, cplx* y, cudaStream_t st);
+void pairs_init_attributes();
+
+// lu.cu — dense LU of an n x n column-major complex matrix (lda = n) in FP64 (double2)
+// or FP32 (float2) storage, row permutation kept as perm (row i of P A is row perm[i]).
+struct LuWork {
+    int* piv = nullptr;        // n
+    int* perm = nullptr;       // n
+    unsigned* barrier = nullptr;
+    int* status = nullptr;     // device status word
+    void* cand = nullptr;      // candidate values/rows, double-buffered
+    void* pack = nullptr;      // packed GEMM operands (mixed path)
+    size_t pack_bytes = 0;
+};
+int lu_factor_fp64(double2* A, int n, LuWork& w, cudaStream_t st, long long* launches);
+int lu_factor_fp32(float2* A, int n, LuWork& w, cudaStream_t st, long long* launches, bool tensor_cores);
+// x (n x ncol, FP64) <- A^-1 x using the factors (storage FP64 or FP32)
+void lu_solve_fp64(const double2* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
+                   long long* launches);
+void lu_solve_fp32(const float2* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
+                   long long* launches);
+size_t lu_workspace_bytes(int n, bool fp32);
+void lu_init_attributes();
+
+// blas.cu — fixed-order reductions and vector updates on FP64 complex vectors
+void vec_norms(const cplx* x, size_t n, int ncol, double* out_dev, double* partial, cudaStream_t st);
+void vec_axpy(cplx* y, const cplx* x, size_t n, int ncol, cudaStream_t st);
+void vec_sub(cplx* out, const cplx* a, const cplx* b, size_t n, int ncol, cudaStream_t st);
+void vec_dots(const cplx* V, size_t ldv, int nv, const cplx* w, size_t n, cplx* out_dev, cplx* partial,
+              cudaStream_t st);
+void vec_gemv_sub(cplx* w, const cplx* V, size_t ldv, int nv, const cplx* h_dev, size_t n, cudaStream_t st);
+void vec_scale_copy(cplx* out, const cplx* x, size_t n, double s, cudaStream_t st);
+void vec_lincomb(cplx* x, const cplx* V, size_t ldv, int nv, const cplx* g_dev, size_t n, cudaStream_t st);
+void vec_real_dots(const cplx* a, const cplx* b, size_t n, int ncol, double* out_dev, double* partial,
+                   cudaStream_t st);
+
+}  // namespace tcu

@@ -1,0 +1,786 @@
+// Dense right-looking blocked LU with partial pivoting of a complex n x n column-major
+// matrix, FP64 (double2) or FP32 (float2) storage, and the triangular solves.
+//
+// Per panel of width w (64 complex columns in FP64, 128 in FP32):
+//  1. panel_kernel (cooperative, one CTA per SM): every CTA holds a slab of the panel rows
+//     in shared memory; per column one grid barrier publishes each CTA's pivot candidate
+//     (largest |a|, ties to the lower row) with its row and the current diagonal row, so
+//     every CTA picks the same pivot, swaps locally and applies the rank-1 update.
+//  2. laswp_kernel: the panel's row swaps on the columns outside it (skips identities).
+//  3. trsm_kernel: U12 = L11^-1 A12, one warp per column.
+//  4. trailing update A22 -= L21 U12: FP64 DMMA (mma.sync m8n8k4 f64) complex GEMM, or in
+//     the mixed path the 3-pass split-TF32 tcgen05 GEMM of gemm_tf32.cu.
+// The solves gather x = P b, then run blocked forward/backward substitutions.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace tcu {
+
+template <typename R>
+struct Cx;
+template <>
+struct Cx<double> {
+    typedef double2 T;
+};
+template <>
+struct Cx<float> {
+    typedef float2 T;
+};
+
+template <typename C>
+__device__ __forceinline__ C cx_make(double r, double i);
+template <>
+__device__ __forceinline__ double2 cx_make<double2>(double r, double i) {
+    return make_double2(r, i);
+}
+template <>
+__device__ __forceinline__ float2 cx_make<float2>(double r, double i) {
+    return make_float2((float)r, (float)i);
+}
+
+struct Cand {
+    double val;
+    int row;
+    int pad;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier for co-resident CTAs (cooperative launch). Every wait is bounded: after
+// 4 s, or once another CTA has raised an error, it records TIMEOUT (8) in *status and
+// returns false so the kernel can leave.
+__device__ bool grid_sync(unsigned* bar, unsigned nblocks, int* status) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        unsigned gen = ld_acquire_u32(&bar[1]);
+        __threadfence();
+        unsigned arrived = atomicAdd(&bar[0], 1u);
+        if (arrived == nblocks - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            unsigned long long t0 = global_ns();
+            unsigned spins = 0;
+            while (ld_acquire_u32(&bar[1]) == gen) {
+                if ((++spins & 255u) == 0) {
+                    if (*(volatile int*)status == 8) {
+                        ok = 0;
+                        break;
+                    }
+                    if (global_ns() - t0 > 4000000000ull) {
+                        atomicExch(status, 8);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <typename R>
+__device__ __forceinline__ double cx_abs2(typename Cx<R>::T a) {
+    return (double)a.x * (double)a.x + (double)a.y * (double)a.y;
+}
+
+// ---- panel factorization ------------------------------------------------------------------
+template <typename R, int NB>
+__global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t lda, int k0, int n, int w,
+                                                    int chunk, int* piv, int* perm, Cand* cand,
+                                                    typename Cx<R>::T* crow, typename Cx<R>::T* drow, unsigned* bar,
+                                                    int* status) {
+    typedef typename Cx<R>::T C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* tile = (C*)smem_raw;                      // chunk x (NB + 1)
+    C* prow = tile + (size_t)chunk * (NB + 1);   // NB
+    __shared__ double s_val[8];
+    __shared__ int s_row[8];
+    __shared__ double s_bval;
+    __shared__ int s_brow, s_bcta;
+    const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int rows = n - k0;
+    const int row0 = k0 + b * chunk;
+    const int myrows = max(0, min(chunk, rows - b * chunk));
+    const int LD = NB + 1;
+    for (int idx = tid; idx < myrows * w; idx += blockDim.x) {
+        int r = idx % myrows, c = idx / myrows;
+        tile[(size_t)r * LD + c] = A[(size_t)(k0 + c) * lda + row0 + r];
+    }
+    __syncthreads();
+    for (int j = 0; j < w; ++j) {
+        const int gj = k0 + j;
+        const int buf = j & 1;
+        // local candidate
+        double bv = -1.0;
+        int br = 0x7fffffff;
+        for (int r = tid; r < myrows; r += blockDim.x) {
+            int g = row0 + r;
+            if (g < gj) continue;
+            double v = cx_abs2<R>(tile[(size_t)r * LD + j]);
+            if (v > bv || (v == bv && g < br)) {
+                bv = v;
+                br = g;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            int orr = __shfl_xor_sync(0xffffffffu, br, o);
+            if (ov > bv || (ov == bv && orr < br)) {
+                bv = ov;
+                br = orr;
+            }
+        }
+        if (lane == 0) {
+            s_val[warp] = bv;
+            s_row[warp] = br;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double v = s_val[0];
+            int rr = s_row[0];
+            for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
+                if (s_val[q] > v || (s_val[q] == v && s_row[q] < rr)) {
+                    v = s_val[q];
+                    rr = s_row[q];
+                }
+            s_bval = v;
+            s_brow = rr;
+            Cand cd;
+            cd.val = v;
+            cd.row = rr;
+            cd.pad = 0;
+            cand[buf * P + b] = cd;
+        }
+        __syncthreads();
+        if (s_bval >= 0.0) {
+            int lr = s_brow - row0;
+            for (int c = tid; c < w; c += blockDim.x) __stcg(&crow[((size_t)buf * P + b) * NB + c], tile[(size_t)lr * LD + c]);
+        }
+        if (gj >= row0 && gj < row0 + myrows) {
+            int lr = gj - row0;
+            for (int c = tid; c < w; c += blockDim.x) __stcg(&drow[(size_t)buf * NB + c], tile[(size_t)lr * LD + c]);
+        }
+        if (!grid_sync(bar, P, status)) return;
+        // winner
+        if (warp == 0) {
+            double v = -1.0;
+            int rr = 0x7fffffff, cb = 0;
+            for (int q = lane; q < P; q += 32) {
+                double cv = __ldcg(&cand[buf * P + q].val);
+                int crr = __ldcg(&cand[buf * P + q].row);
+                if (cv > v || (cv == v && crr < rr)) {
+                    v = cv;
+                    rr = crr;
+                    cb = q;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                int orr = __shfl_xor_sync(0xffffffffu, rr, o);
+                int ocb = __shfl_xor_sync(0xffffffffu, cb, o);
+                if (ov > v || (ov == v && orr < rr)) {
+                    v = ov;
+                    rr = orr;
+                    cb = ocb;
+                }
+            }
+            if (lane == 0) {
+                s_bval = v;
+                s_brow = rr;
+                s_bcta = cb;
+            }
+        }
+        __syncthreads();
+        const int pr = s_brow;
+        const double pv = s_bval;
+        for (int c = tid; c < w; c += blockDim.x) prow[c] = __ldcg(&crow[((size_t)buf * P + s_bcta) * NB + c]);
+        __syncthreads();
+        if (pr != gj) {
+            if (pr >= row0 && pr < row0 + myrows) {
+                int lr = pr - row0;
+                for (int c = tid; c < w; c += blockDim.x) tile[(size_t)lr * LD + c] = __ldcg(&drow[(size_t)buf * NB + c]);
+            }
+            if (gj >= row0 && gj < row0 + myrows) {
+                int lr = gj - row0;
+                for (int c = tid; c < w; c += blockDim.x) tile[(size_t)lr * LD + c] = prow[c];
+            }
+        }
+        if (b == 0 && tid == 0) {
+            piv[gj] = pr;
+            if (pr != gj) {
+                int a = perm[gj];
+                perm[gj] = perm[pr];
+                perm[pr] = a;
+            }
+            if (!(pv > 0.0)) atomicCAS(status, 0, 5);
+        }
+        __syncthreads();
+        // rank-1 update of the rows below the pivot
+        C pivot = prow[j];
+        double den = (double)pivot.x * pivot.x + (double)pivot.y * pivot.y;
+        if (den > 0.0) {
+            double ir = pivot.x / den, ii = -pivot.y / den;  // 1 / pivot
+            for (int r = tid; r < myrows; r += blockDim.x) {
+                int g = row0 + r;
+                if (g <= gj) continue;
+                C a = tile[(size_t)r * LD + j];
+                R lr_ = (R)(a.x * ir - a.y * ii), li_ = (R)(a.x * ii + a.y * ir);
+                C l;
+                l.x = lr_;
+                l.y = li_;
+                tile[(size_t)r * LD + j] = l;
+                for (int c = j + 1; c < w; ++c) {
+                    C u = prow[c];
+                    C& t = tile[(size_t)r * LD + c];
+                    t.x = t.x - (l.x * u.x - l.y * u.y);
+                    t.y = t.y - (l.x * u.y + l.y * u.x);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < myrows * w; idx += blockDim.x) {
+        int r = idx % myrows, c = idx / myrows;
+        A[(size_t)(k0 + c) * lda + row0 + r] = tile[(size_t)r * LD + c];
+    }
+}
+
+// ---- row swaps outside the panel ------------------------------------------------------------
+template <typename C>
+__global__ void laswp_kernel(C* A, size_t lda, int n, int k0, int w, const int* __restrict__ piv) {
+    __shared__ int sp[128];
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    for (int j = threadIdx.x; j < w; j += blockDim.x) {
+        sp[j] = piv[k0 + j];
+        if (sp[j] != k0 + j) any = 1;
+    }
+    __syncthreads();
+    if (!any) return;
+    int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= n || (col >= k0 && col < k0 + w)) return;
+    C* a = A + (size_t)col * lda;
+    for (int j = 0; j < w; ++j) {
+        int p = sp[j];
+        if (p != k0 + j) {
+            C t = a[k0 + j];
+            a[k0 + j] = a[p];
+            a[p] = t;
+        }
+    }
+}
+
+// ---- U12 = L11^-1 A12 ---------------------------------------------------------------------
+template <typename R, int NB>
+__global__ void __launch_bounds__(256) trsm_kernel(typename Cx<R>::T* A, size_t lda, int k0, int w, int n,
+                                                   int cols_per_cta) {
+    typedef typename Cx<R>::T C;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* Ls = (C*)smem_raw;  // Ls[k * NB + i] = L[i][k]
+    for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+        int i = idx % w, k = idx / w;
+        Ls[k * NB + i] = A[(size_t)(k0 + k) * lda + k0 + i];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int S = NB / 32;
+    int cbeg = k0 + w + blockIdx.x * cols_per_cta;
+    int cend = min(n, cbeg + cols_per_cta);
+    for (int col = cbeg + warp; col < cend; col += blockDim.x >> 5) {
+        C* a = A + (size_t)col * lda + k0;
+        R xr[S], xi[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            int i = lane + 32 * s;
+            C v = (i < w) ? a[i] : cx_make<C>(0.0, 0.0);
+            xr[s] = v.x;
+            xi[s] = v.y;
+        }
+#pragma unroll
+        for (int kb = 0; kb < S; ++kb) {
+            for (int kk = 0; kk < 32; ++kk) {
+                int k = kb * 32 + kk;
+                if (k >= w) break;
+                R br = __shfl_sync(0xffffffffu, xr[kb], kk);
+                R bi = __shfl_sync(0xffffffffu, xi[kb], kk);
+#pragma unroll
+                for (int s = kb; s < S; ++s) {
+                    int i = lane + 32 * s;
+                    if (i > k && i < w) {
+                        C l = Ls[k * NB + i];
+                        xr[s] -= l.x * br - l.y * bi;
+                        xi[s] -= l.x * bi + l.y * br;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            int i = lane + 32 * s;
+            if (i < w) {
+                C v;
+                v.x = xr[s];
+                v.y = xi[s];
+                a[i] = v;
+            }
+        }
+    }
+}
+
+// ---- FP64 complex GEMM on DMMA: A22 -= L21 U12 -------------------------------------------
+// CTA tile 64 x 64 complex; K = w complex in chunks of 16 staged by cp.async (2 stages).
+// The complex product runs as a real GEMM of the 2x2-embedded L21 (rows re/im interleaved)
+// with U12 read as interleaved reals: D[2mu+c][nu] = sum_k Lemb[2mu+c][2k+c'] U[2k+c'][nu].
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+constexpr int ZG_T = 64;   // tile rows/cols (complex)
+constexpr int ZG_KC = 16;  // K chunk (complex)
+constexpr size_t ZG_SMEM = 4 * ZG_KC * ZG_T * sizeof(double2);
+
+__global__ void __launch_bounds__(256) zgemm_dmma_kernel(double2* A, size_t lda, int k0, int w, int r0, int n) {
+    extern __shared__ __align__(16) unsigned char zg_smem[];
+    double2 (*Ls)[ZG_KC][ZG_T] = (double2 (*)[ZG_KC][ZG_T])zg_smem;                       // [stage][k][row]
+    double2 (*Us)[ZG_KC][ZG_T] = (double2 (*)[ZG_KC][ZG_T])(zg_smem + 2 * ZG_KC * ZG_T * 16);  // [stage][k][col]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tr = r0 + blockIdx.x * ZG_T, tc = r0 + blockIdx.y * ZG_T;
+    const int wr = (warp & 1) * 32, wc = (warp >> 1) * 16;  // warp tile: 32 complex rows x 16 cols
+    double acc[8][2][2];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    const int nchunks = (w + ZG_KC - 1) / ZG_KC;
+    auto load = [&](int stage, int ch) {
+        int kc = ch * ZG_KC;
+        for (int idx = tid; idx < ZG_KC * ZG_T; idx += 256) {
+            int r = idx % ZG_T, k = idx / ZG_T;
+            int row = tr + r, kk = kc + k;
+            bool ok = row < n && kk < w;
+            cp_async16(&Ls[stage][k][r], A + (size_t)(k0 + (ok ? kk : 0)) * lda + (ok ? row : 0), ok);
+        }
+        for (int idx = tid; idx < ZG_KC * ZG_T; idx += 256) {
+            int k = idx % ZG_KC, c = idx / ZG_KC;
+            int col = tc + c, kk = kc + k;
+            bool ok = col < n && kk < w;
+            cp_async16(&Us[stage][k][c], A + (size_t)(ok ? col : 0) * lda + k0 + (ok ? kk : 0), ok);
+        }
+        cp_async_commit();
+    };
+    load(0, 0);
+    for (int ch = 0; ch < nchunks; ++ch) {
+        int st = ch & 1;
+        if (ch + 1 < nchunks) {
+            load(st ^ 1, ch + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < 2 * ZG_KC / 4; ++ks) {  // real k steps of 4
+            int kr = ks * 4 + (lane & 3);
+            int kc = kr >> 1, kp = kr & 1;
+            double bfrag[2];
+#pragma unroll
+            for (int cb = 0; cb < 2; ++cb) {
+                double2 u = Us[st][kc][wc + cb * 8 + (lane >> 2)];
+                bfrag[cb] = kp ? u.y : u.x;
+            }
+#pragma unroll
+            for (int rb = 0; rb < 8; ++rb) {
+                int rr = rb * 8 + (lane >> 2);  // real row within the warp's 64
+                int mu = wr + (rr >> 1), rp = rr & 1;
+                double2 l = Ls[st][kc][mu];
+                double a = (rp == kp) ? l.x : (rp == 0 ? -l.y : l.y);
+#pragma unroll
+                for (int cb = 0; cb < 2; ++cb) {
+                    asm volatile(
+                        "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                        : "+d"(acc[rb][cb][0]), "+d"(acc[rb][cb][1])
+                        : "d"(a), "d"(bfrag[cb]));
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // epilogue: lanes (l, l^4) hold the re/im rows of one complex row
+    const bool even = ((lane >> 2) & 1) == 0;
+#pragma unroll
+    for (int rb = 0; rb < 8; ++rb) {
+        int rr = rb * 8 + (lane >> 2);
+        int mu = wr + (rr >> 1);
+#pragma unroll
+        for (int cb = 0; cb < 2; ++cb) {
+            double d0 = acc[rb][cb][0], d1 = acc[rb][cb][1];
+            double p0 = __shfl_xor_sync(0xffffffffu, d0, 4), p1 = __shfl_xor_sync(0xffffffffu, d1, 4);
+            int col = wc + cb * 8 + 2 * (lane & 3) + (even ? 0 : 1);
+            double re = even ? d0 : p1, im = even ? p0 : d1;
+            int grow = tr + mu, gcol = tc + col;
+            if (grow < n && gcol < n) {
+                double2* c = A + (size_t)gcol * lda + grow;
+                double2 v = *c;
+                v.x -= re;
+                v.y -= im;
+                *c = v;
+            }
+        }
+    }
+}
+
+// ---- FP32 complex GEMM on CUDA cores (fallback when tcgen05 is disabled) -----------------
+__global__ void __launch_bounds__(256) cgemm_simt_kernel(float2* A, size_t lda, int k0, int w, int r0, int n) {
+    __shared__ float2 Ls[ZG_KC][ZG_T + 1];
+    __shared__ float2 Us[ZG_KC][ZG_T + 1];
+    const int tid = threadIdx.x;
+    const int tr = r0 + blockIdx.x * ZG_T, tc = r0 + blockIdx.y * ZG_T;
+    const int ty = tid / 16, tx = tid % 16;  // 16 x 16 threads, 4 x 4 complex each
+    float accr[4][4], acci[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) accr[a][b] = acci[a][b] = 0.f;
+    for (int kc = 0; kc < w; kc += ZG_KC) {
+        for (int idx = tid; idx < ZG_KC * ZG_T; idx += 256) {
+            int r = idx % ZG_T, k = idx / ZG_T;
+            int row = tr + r, kk = kc + k;
+            Ls[k][r] = (row < n && kk < w) ? A[(size_t)(k0 + kk) * lda + row] : make_float2(0.f, 0.f);
+            int kq = idx % ZG_KC, c = idx / ZG_KC;
+            int col = tc + c, kk2 = kc + kq;
+            Us[kq][c] = (col < n && kk2 < w) ? A[(size_t)col * lda + k0 + kk2] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < ZG_KC; ++k) {
+            float2 lv[4], uv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) lv[a] = Ls[k][ty + 16 * a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) uv[b] = Us[k][tx + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    accr[a][b] = fmaf(lv[a].x, uv[b].x, fmaf(-lv[a].y, uv[b].y, accr[a][b]));
+                    acci[a][b] = fmaf(lv[a].x, uv[b].y, fmaf(lv[a].y, uv[b].x, acci[a][b]));
+                }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            int row = tr + ty + 16 * a, col = tc + tx + 16 * b;
+            if (row < n && col < n) {
+                float2* c = A + (size_t)col * lda + row;
+                float2 v = *c;
+                v.x -= accr[a][b];
+                v.y -= acci[a][b];
+                *c = v;
+            }
+        }
+}
+
+// ---- host driver --------------------------------------------------------------------------
+static int g_num_sms = 0;
+static void solve_init_attributes();
+
+template <typename R, int NB>
+static size_t panel_smem(int chunk) {
+    typedef typename Cx<R>::T C;
+    return (size_t)chunk * (NB + 1) * sizeof(C) + NB * sizeof(C);
+}
+
+void lu_init_attributes() {
+    if (g_num_sms) return;
+    int dev;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(panel_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(panel_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(trsm_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(trsm_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZG_SMEM);
+    solve_init_attributes();
+}
+
+size_t lu_workspace_bytes(int n, bool fp32) {
+    (void)fp32;
+    size_t P = 160;
+    return (size_t)n * 2 * sizeof(int) + 64 + 2 * P * sizeof(Cand) + 2 * P * 128 * sizeof(double2) +
+           2 * 128 * sizeof(double2) + 1024;
+}
+
+template <typename R, int NB>
+static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cudaStream_t st) {
+    typedef typename Cx<R>::T C;
+    int rows = n - k0;
+    int P = std::min(g_num_sms, std::max(1, (rows + 31) / 32));
+    int chunk = (rows + P - 1) / P;
+    size_t smem = panel_smem<R, NB>(chunk);
+    if (smem > 220 * 1024) return 1;
+    Cand* cand = (Cand*)wk.cand;
+    C* crow = (C*)(cand + 2 * 160);
+    C* drow = crow + 2 * 160 * NB;
+    cudaMemsetAsync(wk.barrier, 0, 2 * sizeof(unsigned), st);
+    size_t lda = (size_t)n;
+    void* args[] = {&A, &lda, &k0, &n, &w, &chunk, &wk.piv, &wk.perm, &cand, &crow, &drow, &wk.barrier, &wk.status};
+    cudaError_t e = cudaLaunchCooperativeKernel((void*)panel_kernel<R, NB>, dim3(P), dim3(256), args, smem, st);
+    return e == cudaSuccess ? 0 : 2;
+}
+
+__global__ void iota_kernel(int* p, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = i;
+}
+
+void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches);
+
+template <typename R, int NB>
+static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t st, long long* launches,
+                          bool tensor_cores) {
+    typedef typename Cx<R>::T C;
+    lu_init_attributes();
+    iota_kernel<<<(n + 255) / 256, 256, 0, st>>>(wk.perm, n);
+    ++*launches;
+    size_t lda = n;
+    for (int k0 = 0; k0 < n; k0 += NB) {
+        int w = std::min(NB, n - k0);
+        int rc;
+        {
+            StageScope sc(ST_PANEL, st);
+            rc = run_panel<R, NB>(A, n, k0, w, wk, st);
+        }
+        ++*launches;
+        if (rc) return rc;
+        {
+            StageScope sc(ST_SWAP, st);
+            laswp_kernel<C><<<(n + 255) / 256, 256, 0, st>>>(A, lda, n, k0, w, wk.piv);
+        }
+        ++*launches;
+        int r0 = k0 + w;
+        if (r0 >= n) break;
+        int cols = n - r0;
+        int cpc = 64;
+        size_t smem = (size_t)NB * NB * sizeof(C);
+        {
+            StageScope sc(ST_TRSM, st);
+            trsm_kernel<R, NB><<<(cols + cpc - 1) / cpc, 256, smem, st>>>(A, lda, k0, w, n, cpc);
+        }
+        ++*launches;
+        dim3 grid((cols + ZG_T - 1) / ZG_T, (cols + ZG_T - 1) / ZG_T);
+        if constexpr (sizeof(R) == 8) {
+            StageScope sc(ST_GEMM, st);
+            zgemm_dmma_kernel<<<grid, 256, ZG_SMEM, st>>>((double2*)A, lda, k0, w, r0, n);
+            ++*launches;
+        } else {
+            if (tensor_cores) {
+                launch_tf32_update((float2*)A, n, k0, w, wk, st, launches);
+            } else {
+                StageScope sc(ST_GEMM, st);
+                cgemm_simt_kernel<<<grid, 256, 0, st>>>((float2*)A, lda, k0, w, r0, n);
+                ++*launches;
+            }
+        }
+    }
+    return 0;
+}
+
+int lu_factor_fp64(double2* A, int n, LuWork& w, cudaStream_t st, long long* launches) {
+    return lu_factor_impl<double, 64>(A, n, w, st, launches, false);
+}
+int lu_factor_fp32(float2* A, int n, LuWork& w, cudaStream_t st, long long* launches, bool tensor_cores) {
+    return lu_factor_impl<float, 128>(A, n, w, st, launches, tensor_cores);
+}
+
+// ---- solves -------------------------------------------------------------------------------
+// x <- P x (gather through perm), then L y = x (unit lower), U x = y (upper), blockwise:
+// each launch solves one diagonal block redundantly per CTA and updates the remaining rows
+// of its chunk with the block column (read once, coalesced over rows).
+constexpr int SB = 64;  // solve block
+constexpr int SMAXC = 8;
+constexpr size_t TV_SMEM = (size_t)SB * (SB + 1) * sizeof(double2);
+
+__global__ void gather_kernel(const double2* __restrict__ x, double2* __restrict__ y, const int* __restrict__ perm,
+                              int n, int ncol) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)n * ncol) return;
+    int c = (int)(t / n), i = (int)(t % n);
+    y[t] = x[(size_t)c * n + perm[i]];
+}
+
+template <typename C, bool LOWER>
+__global__ void __launch_bounds__(256) trsv_step_kernel(const C* __restrict__ A, size_t lda, int n, int b0, int bw,
+                                                        double2* __restrict__ x, int ncol) {
+    __shared__ double2 xb[SMAXC][SB];
+    extern __shared__ __align__(16) unsigned char tv_smem[];
+    double2 (*Db)[SB + 1] = (double2 (*)[SB + 1])tv_smem;  // diagonal block, Db[i][k]
+    // diagonal block and the current right-hand side block
+    for (int idx = threadIdx.x; idx < bw * bw; idx += blockDim.x) {
+        int i = idx % bw, k = idx / bw;
+        C v = A[(size_t)(b0 + k) * lda + b0 + i];
+        Db[i][k] = make_double2(v.x, v.y);
+    }
+    for (int idx = threadIdx.x; idx < bw * ncol; idx += blockDim.x) {
+        int i = idx % bw, c = idx / bw;
+        xb[c][i] = x[(size_t)c * n + b0 + i];
+    }
+    __syncthreads();
+    // small triangular solve: one warp per column
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp < ncol) {
+        int c = warp;
+        double2 v0 = lane < bw ? xb[c][lane] : make_double2(0, 0);
+        double2 v1 = lane + 32 < bw ? xb[c][lane + 32] : make_double2(0, 0);
+        if (LOWER) {
+            for (int k = 0; k < bw; ++k) {
+                double2 xk;
+                xk.x = __shfl_sync(0xffffffffu, k < 32 ? v0.x : v1.x, k & 31);
+                xk.y = __shfl_sync(0xffffffffu, k < 32 ? v0.y : v1.y, k & 31);
+                if (lane > k && lane < bw) {
+                    double2 l = Db[lane][k];
+                    v0.x -= l.x * xk.x - l.y * xk.y;
+                    v0.y -= l.x * xk.y + l.y * xk.x;
+                }
+                if (lane + 32 > k && lane + 32 < bw) {
+                    double2 l = Db[lane + 32][k];
+                    v1.x -= l.x * xk.x - l.y * xk.y;
+                    v1.y -= l.x * xk.y + l.y * xk.x;
+                }
+            }
+        } else {
+            for (int k = bw - 1; k >= 0; --k) {
+                // x_k = v_k / U_kk, owner lane computes, then broadcast
+                double2 own = k < 32 ? v0 : v1;
+                double2 d = Db[k][k];
+                double den = d.x * d.x + d.y * d.y;
+                double2 q = make_double2((own.x * d.x + own.y * d.y) / den, (own.y * d.x - own.x * d.y) / den);
+                double2 xk;
+                xk.x = __shfl_sync(0xffffffffu, q.x, k & 31);
+                xk.y = __shfl_sync(0xffffffffu, q.y, k & 31);
+                if (lane == (k & 31)) {
+                    if (k < 32)
+                        v0 = xk;
+                    else
+                        v1 = xk;
+                }
+                if (lane < k) {
+                    double2 u = Db[lane][k];
+                    v0.x -= u.x * xk.x - u.y * xk.y;
+                    v0.y -= u.x * xk.y + u.y * xk.x;
+                }
+                if (lane + 32 < k) {
+                    double2 u = Db[lane + 32][k];
+                    v1.x -= u.x * xk.x - u.y * xk.y;
+                    v1.y -= u.x * xk.y + u.y * xk.x;
+                }
+            }
+        }
+        if (lane < bw) xb[c][lane] = v0;
+        if (lane + 32 < bw) xb[c][lane + 32] = v1;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0)
+        for (int idx = threadIdx.x; idx < bw * ncol; idx += blockDim.x) {
+            int i = idx % bw, c = idx / bw;
+            x[(size_t)c * n + b0 + i] = xb[c][i];
+        }
+    // update the other rows: lower -> rows below the block; upper -> rows above
+    int lo = LOWER ? b0 + bw : 0, hi = LOWER ? n : b0;
+    for (int r = lo + blockIdx.x * blockDim.x + threadIdx.x; r < hi; r += gridDim.x * blockDim.x) {
+        double2 acc[SMAXC];
+        for (int c = 0; c < ncol; ++c) acc[c] = make_double2(0, 0);
+        for (int k = 0; k < bw; ++k) {
+            C v = A[(size_t)(b0 + k) * lda + r];
+            double lr = v.x, li = v.y;
+            for (int c = 0; c < ncol; ++c) {
+                double2 xk = xb[c][k];
+                acc[c].x += lr * xk.x - li * xk.y;
+                acc[c].y += lr * xk.y + li * xk.x;
+            }
+        }
+        for (int c = 0; c < ncol; ++c) {
+            double2* p = x + (size_t)c * n + r;
+            double2 v = *p;
+            v.x -= acc[c].x;
+            v.y -= acc[c].y;
+            *p = v;
+        }
+    }
+}
+
+template <typename C>
+static void lu_solve_impl(const C* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
+                          long long* launches) {
+    lu_init_attributes();
+    StageScope sc(ST_SOLVE, st);
+    for (int c0 = 0; c0 < ncol; c0 += SMAXC) {
+        int nc = std::min(SMAXC, ncol - c0);
+        double2* xc = x + (size_t)c0 * n;
+        size_t tot = (size_t)n * nc;
+        gather_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(xc, tmp, perm, n, nc);
+        ++*launches;
+        int grid = g_num_sms;
+        for (int b0 = 0; b0 < n; b0 += SB) {
+            int bw = std::min(SB, n - b0);
+            trsv_step_kernel<C, true><<<grid, 256, TV_SMEM, st>>>(A, n, n, b0, bw, tmp, nc);
+            ++*launches;
+        }
+        int last = ((n - 1) / SB) * SB;
+        for (int b0 = last; b0 >= 0; b0 -= SB) {
+            int bw = std::min(SB, n - b0);
+            trsv_step_kernel<C, false><<<grid, 256, TV_SMEM, st>>>(A, n, n, b0, bw, tmp, nc);
+            ++*launches;
+        }
+        cudaMemcpyAsync(xc, tmp, tot * sizeof(double2), cudaMemcpyDeviceToDevice, st);
+    }
+}
+
+static void solve_init_attributes() {
+    cudaFuncSetAttribute(trsv_step_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV_SMEM);
+    cudaFuncSetAttribute(trsv_step_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV_SMEM);
+    cudaFuncSetAttribute(trsv_step_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV_SMEM);
+    cudaFuncSetAttribute(trsv_step_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV_SMEM);
+}
+
+void lu_solve_fp64(const double2* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
+                   long long* launches) {
+    lu_solve_impl<double2>(A, n, perm, x, tmp, ncol, st, launches);
+}
+void lu_solve_fp32(const float2* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
+                   long long* launches) {
+    lu_solve_impl<float2>(A, n, perm, x, tmp, ncol, st, launches);
+}
+
+}  // namespace tcu

@@ -1,0 +1,31 @@
+"""2D Ewald lattice sums (treams_rs.lattice.lsumsw2d) and periodic arrays."""
+from __future__ import annotations
+
+import numpy as np
+
+from ._lib import _check, _p, default_context, lib
+
+
+def lsumsw2d_batch(lmax_sum: int, k: float, lattice, kpars, eta: float = 0.0, ctx=None) -> np.ndarray:
+    """D_lm for every l <= lmax_sum (table index l*l+l+m) and every Bloch vector (nk, 2),
+    one sphere per cell (shift 0)."""
+    ctx = ctx or default_context()
+    a = np.ascontiguousarray(lattice, np.float64).reshape(2, 2)
+    kp = np.ascontiguousarray(kpars, np.float64).reshape(-1, 2)
+    out = np.zeros((kp.shape[0], (lmax_sum + 1) ** 2), np.complex128)
+    _check(lib().tcu_lsumsw2d_batch(ctx.handle, lmax_sum, float(k), _p(a), kp.shape[0], _p(kp), float(eta), _p(out)))
+    return out
+
+
+def array_solve_batch(lmax: int, k0: float, radius: float, eps: complex, lattice, kpars, eta: float = 0.0,
+                      ctx=None) -> np.ndarray:
+    """X(kpar) = (I - T S(kpar))^-1 T for each Bloch vector: (nk, M, M)."""
+    ctx = ctx or default_context()
+    a = np.ascontiguousarray(lattice, np.float64).reshape(2, 2)
+    kp = np.ascontiguousarray(kpars, np.float64).reshape(-1, 2)
+    e = np.array([complex(eps)], np.complex128)
+    M = 2 * lmax * (lmax + 2)
+    out = np.zeros((kp.shape[0], M, M), np.complex128)
+    _check(lib().tcu_array_solve_batch(ctx.handle, lmax, float(k0), float(radius), _p(e), _p(a), kp.shape[0], _p(kp),
+                                       float(eta), _p(out)))
+    return np.ascontiguousarray(np.transpose(out, (0, 2, 1)))
