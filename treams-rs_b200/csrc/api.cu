@@ -127,8 +127,10 @@ tcu_status get_plan(tcu_context* ctx, int L, const DevPlan** out) {
         HostPlan& h = store->host;
         size_t ncombo = (size_t)h.nlm * h.nlm;
         size_t nterm = h.idx.size();
-        size_t off_combo = 0, off_w = ncombo * 8, off_refl = off_w + nterm * 16,
-               off_idx = off_refl + h.reflection.size() * 8;
+        // every array starts on a 256-byte boundary (the weights are read as 16-byte double2)
+        auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+        size_t off_combo = 0, off_w = up(ncombo * 8), off_refl = up(off_w + nterm * 16),
+               off_idx = up(off_refl + h.reflection.size() * 8);
         size_t total = off_idx + nterm + 16;
         CK(cudaMalloc(&store->mem, total), "plan allocation");
         char* base = (char*)store->mem;
@@ -178,6 +180,22 @@ struct DevBuf {
     void* p = nullptr;
     ~DevBuf() {
         if (p) cudaFree(p);
+    }
+};
+
+// Sub-buffers of one allocation, each on a 256-byte boundary.
+struct Arena {
+    std::vector<size_t> offs;
+    size_t total = 0;
+    size_t add(size_t bytes) {
+        size_t o = total;
+        offs.push_back(o);
+        total = (total + bytes + 255) & ~(size_t)255;
+        return o;
+    }
+    template <typename T>
+    T* at(void* base, size_t off) const {
+        return (T*)((char*)base + off);
     }
 };
 
@@ -472,10 +490,12 @@ tcu_status tcu_mie_blocks(tcu_context* ctx, int lmax, double k0, size_t N, const
     ProfGuard pg(ctx);
     CK(cudaSetDevice(ctx->device), "device");
     DevBuf buf;
-    CK(cudaMalloc(&buf.p, N * 8 + N * 16 + N * lmax * 64), "mie buffers");
-    double* r = (double*)buf.p;
-    cplx* e = (cplx*)(r + N);
-    cplx* T = e + N;
+    Arena ar;
+    size_t o_r = ar.add(N * 8), o_e = ar.add(N * 16), o_t = ar.add(N * lmax * 64);
+    CK(cudaMalloc(&buf.p, ar.total), "mie buffers");
+    double* r = ar.at<double>(buf.p, o_r);
+    cplx* e = ar.at<cplx>(buf.p, o_e);
+    cplx* T = ar.at<cplx>(buf.p, o_t);
     CK(cudaMemcpyAsync(r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemcpyAsync(e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
@@ -500,11 +520,13 @@ tcu_status tcu_plane_wave_expansion(tcu_context* ctx, int lmax, size_t N, const 
     CK(cudaSetDevice(ctx->device), "device");
     size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M;
     DevBuf buf;
-    CK(cudaMalloc(&buf.p, N * 24 + p * 48 + p * 4 + 16 + n * p * 16), "plane-wave buffers");
-    double* pos = (double*)buf.p;
-    cplx* kv = (cplx*)(pos + 3 * N);
-    cplx* o = kv + 3 * p;
-    int* pl = (int*)(o + n * p);
+    Arena ar;
+    size_t o_pos = ar.add(N * 24), o_kv = ar.add(p * 48), o_o = ar.add(n * p * 16), o_pl = ar.add(p * 4);
+    CK(cudaMalloc(&buf.p, ar.total), "plane-wave buffers");
+    double* pos = ar.at<double>(buf.p, o_pos);
+    cplx* kv = ar.at<cplx>(buf.p, o_kv);
+    cplx* o = ar.at<cplx>(buf.p, o_o);
+    int* pl = ar.at<int>(buf.p, o_pl);
     CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemcpyAsync(kv, kvecs, p * 48, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemcpyAsync(pl, pols, p * 4, cudaMemcpyHostToDevice, ctx->stream), "copy");
@@ -526,9 +548,11 @@ tcu_status tcu_cross_sections(tcu_context* ctx, int lmax, double k0, size_t N, c
     if (s) return s;
     size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M, per = n * p;
     DevBuf buf;
-    CK(cudaMalloc(&buf.p, N * 24 + 3 * per * 16), "cross-section buffers");
-    double* pos = (double*)buf.p;
-    cplx* dx = (cplx*)(pos + 3 * N);
+    Arena ar;
+    size_t o_pos = ar.add(N * 24), o_x = ar.add(3 * per * 16);
+    CK(cudaMalloc(&buf.p, ar.total), "cross-section buffers");
+    double* pos = ar.at<double>(buf.p, o_pos);
+    cplx* dx = ar.at<cplx>(buf.p, o_x);
     cplx* db = dx + per;
     cplx* ox = db + per;
     CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
