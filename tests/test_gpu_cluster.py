@@ -108,6 +108,8 @@ def test_dense_solve_lmax4_subset(ctx, precision):
     assert rel(X, Xo) <= 1e-10
     for c in certs:
         assert c.residual_norm <= 1e-12 * c.rhs_norm
+        # an FP32-accurate factor reaches 1e-13 in a handful of FP64 refinement sweeps
+        assert c.iterations <= (1 if precision == "fp64" else 5)
 
 
 def test_lossless_energy_balance_on_gpu(ctx):

@@ -67,6 +67,7 @@ struct tcu_factor {
     cplx* d_eps = nullptr;
     cplx* d_T = nullptr;
     void* d_A = nullptr;
+    double2* d_inv = nullptr;  // inverses of the diagonal blocks of L and U
     LuWork wk;
 };
 
@@ -237,7 +238,9 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
         if (f->d_eps) cudaFree(f->d_eps);
         if (f->d_T) cudaFree(f->d_T);
         if (f->d_A) cudaFree(f->d_A);
+        if (f->d_inv) cudaFree(f->d_inv);
         if (f->wk.piv) cudaFree(f->wk.piv);
+        if (f->wk.pack) cudaFree(f->wk.pack);
     };
     tcu_status e = TCU_OK;
     do {
@@ -287,6 +290,20 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
             e = fail(TCU_TIMEOUT, "LU factorization: a device-side wait gave up");
             break;
         }
+        if (st == 6) {
+            e = fail(TCU_OUT_OF_MEMORY, "LU factorization: no memory for the packed tensor-core operands");
+            break;
+        }
+        if (st != 0) {
+            e = fail(TCU_DEVICE_ERROR, "LU factorization: device status " + std::to_string(st));
+            break;
+        }
+        if ((e = cuda_check(cudaMalloc(&f->d_inv, lu_inverse_bytes((int)n)), "block inverses"))) break;
+        if (precision == TCU_FP64)
+            lu_block_inverses_fp64((const double2*)f->d_A, (int)n, f->d_inv, ctx->stream, &ctx->launches);
+        else
+            lu_block_inverses_fp32((const float2*)f->d_A, (int)n, f->d_inv, ctx->stream, &ctx->launches);
+        if ((e = sync_status(ctx, "block inverses"))) break;
     } while (0);
     if (e) {
         cleanup();
@@ -311,12 +328,12 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
                     "require finite channel-by-illumination columns matching the factorization");
     DevBuf bufs;
     size_t per = n * p;
-    CK(cudaMalloc(&bufs.p, 5 * per * sizeof(cplx)), "solve buffers");
+    CK(cudaMalloc(&bufs.p, 6 * per * sizeof(cplx)), "solve buffers");
     cplx* b = (cplx*)bufs.p;
     cplx* tb = b + per;
     cplx* x = tb + per;
     cplx* r = x + per;
-    cplx* tmp = r + per;
+    cplx* tmp = r + per;  // 2 per
     CK(cudaMemcpyAsync(b, B, per * 16, device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream),
        "copy rhs");
     launch_apply_t(f->L, f->N, f->d_T, b, p, tb, ctx->stream);
@@ -328,9 +345,11 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
     int sweeps = 0;
     auto lu_apply = [&](cplx* v) {
         if (f->precision == TCU_FP64)
-            lu_solve_fp64((const double2*)f->d_A, (int)n, f->wk.perm, v, tmp, p, ctx->stream, &ctx->launches);
+            lu_solve_fp64((const double2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, p, ctx->stream,
+                          &ctx->launches);
         else
-            lu_solve_fp32((const float2*)f->d_A, (int)n, f->wk.perm, v, tmp, p, ctx->stream, &ctx->launches);
+            lu_solve_fp32((const float2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, p, ctx->stream,
+                          &ctx->launches);
     };
     auto residual = [&]() -> tcu_status {
         // r = T b - (x - T C x)
@@ -617,6 +636,7 @@ tcu_status tcu_factor_destroy(tcu_factor* f) {
     cudaFree(f->d_eps);
     cudaFree(f->d_T);
     cudaFree(f->d_A);
+    cudaFree(f->d_inv);
     cudaFree(f->wk.piv);
     if (f->wk.pack) cudaFree(f->wk.pack);
     delete f;

@@ -1,13 +1,553 @@
-// Trailing update of the mixed-precision LU on the tcgen05 tensor cores (placeholder).
+// Trailing update of the mixed-precision LU on the 5th-generation tensor cores:
+//   A22 -= L21 U12   (complex64, column-major, in place)
+// as one real GEMM D = Lemb * U^T with
+//   Lemb[2mu+c][2k+c'] = { Re L, -Im L ; Im L, Re L }   (2m x 2w, K-major)
+//   U[nu][2k+c']       = interleaved (Re, Im) of column nu of U12   (n' x 2w, K-major)
+// so that D[2mu+c][nu] is part c of (L21 U12)[mu][nu] and the 2m x n' result maps onto
+// the interleaved storage of A22 (real leading dimension 2n).
+//
+// Precision: every operand is split x = hi + lo with hi = tf32(x), lo = tf32(x - hi), and
+// three tcgen05.mma kind::tf32 passes hi*hi + hi*lo + lo*hi accumulate in FP32 in TMEM
+// (the lo*lo term is below FP32 rounding).
+//
+// Kernel layout (persistent, one CTA per SM, 192 threads):
+//   warp 0     TMA producer: 128-byte-swizzled boxes of the four packed operands into a
+//              2-stage shared-memory ring (96 KB per stage), mbarrier complete_tx;
+//   warp 1     TMEM allocator and MMA issuer (one thread): 4 K-steps x 3 passes per stage
+//              into a 128 x 256 FP32 accumulator, double-buffered in TMEM (512 columns);
+//   warps 2-5  epilogue: tcgen05.ld 32 columns at a time, A22 -= D with coalesced stores.
+// Every mbarrier wait is bounded; on timeout the kernel records status 8, drains its TMA
+// loads, frees TMEM and returns.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cstdlib>
 
 #include "kernels.h"
 #include "precond.h"
 
 namespace tcu {
 
-bool tf32_enabled() { return false; }
+constexpr int TB_M = 128;       // real rows per tile (64 complex rows)
+constexpr int TB_N = 256;       // columns per tile
+constexpr int TB_K = 16;        // floats per K chunk (one 64-byte swizzle row)
+constexpr int TB_STAGES = 4;
+constexpr int A_BYTES = TB_M * TB_K * 4;   // 8 KB
+constexpr int B_BYTES = TB_N * TB_K * 4;   // 16 KB
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 48 KB
+constexpr int TMEM_COLS = 2 * TB_N;        // two accumulators
+constexpr size_t TF32_SMEM = (size_t)TB_STAGES * STAGE_BYTES + 1024 + 256;
 
-void launch_tf32_update(float2*, int, int, int, LuWork&, cudaStream_t, long long*) {}
+// ---- device helpers ---------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false after 2 s or when another role has aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    if (mbar_try(bar, parity)) return true;
+    unsigned long long t0 = gtimer();
+    for (unsigned it = 1;; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 63u) == 0) {
+            if (*abort_flag) return false;
+            if (gtimer() - t0 > 2000000000ull) {
+                *abort_flag = 1;
+                return false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// K-major, 64-byte swizzled operand tile: rows of 16 floats, 8-row groups 512 bytes apart.
+__device__ __forceinline__ uint64_t swz_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;             // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(512 >> 4) << 32;    // stride byte offset: next 8-row group
+    d |= (uint64_t)1 << 46;             // descriptor version (sm_100)
+    d |= (uint64_t)4 << 61;             // SWIZZLE_64B
+    return d;
+}
+
+// Tile t of the persistent loop: groups of 16 M-tiles sweep all N-tiles, so the CTAs in
+// flight share a few A and B tiles in L2.
+constexpr int TILE_GROUP = 16;
+__device__ __forceinline__ void tile_coords(int t, int tiles_m, int tiles_n, int& tm, int& tn) {
+    int per_group = TILE_GROUP * tiles_n;
+    int g = t / per_group;
+    int first = g * TILE_GROUP;
+    int gm = min(TILE_GROUP, tiles_m - first);
+    int local = t - g * per_group;
+    tm = first + local % gm;
+    tn = local / gm;
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---- the GEMM ---------------------------------------------------------------------------
+struct Tf32Args {
+    float* C;        // A viewed as floats
+    size_t ldc;      // 2n (floats per column)
+    int row0;        // 2 r0: first real row of A22
+    int col0;        // r0
+    int m2;          // real rows of A22 (2m)
+    int ncols;       // columns of A22
+    int kchunks;     // K / TB_K
+    int tiles_m, tiles_n, tiles;
+    int* status;
+};
+
+__global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_constant__ CUtensorMap mAhi,
+                                                             const __grid_constant__ CUtensorMap mAlo,
+                                                             const __grid_constant__ CUtensorMap mBhi,
+                                                             const __grid_constant__ CUtensorMap mBlo, Tf32Args args) {
+    extern __shared__ uint8_t smem_raw[];
+    uint32_t base = smem_u32(smem_raw);
+    uint32_t tiles_smem = (base + 1023u) & ~1023u;  // 1024-byte aligned stage ring
+    uint8_t* ctrl = smem_raw + (tiles_smem - base) + TB_STAGES * STAGE_BYTES;
+    // barriers: full[S], empty[S], tmem_full[2], tmem_empty[2]
+    uint64_t* bars = (uint64_t*)ctrl;
+    uint32_t* tmem_slot = (uint32_t*)(ctrl + 8 * (2 * TB_STAGES + 4));
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto bar = [&](int i) { return smem_u32(&bars[i]); };
+    constexpr int EMPTY = TB_STAGES, TFULL = 2 * TB_STAGES, TEMPTY = 2 * TB_STAGES + 2;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TB_STAGES; ++s) {
+            mbar_init(bar(s), 1);
+            mbar_init(bar(EMPTY + s), 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(bar(TFULL + a), 1);
+            mbar_init(bar(TEMPTY + a), 128);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int step = 0;
+            for (int t = blockIdx.x; t < args.tiles && !*abort_flag; t += gridDim.x) {
+                int tm, tn;
+                tile_coords(t, args.tiles_m, args.tiles_n, tm, tn);
+                for (int kb = 0; kb < args.kchunks; ++kb, ++step) {
+                    int s = step % TB_STAGES;
+                    uint32_t ph = (step / TB_STAGES) & 1;
+                    if (!mbar_wait(bar(EMPTY + s), ph ^ 1, abort_flag)) break;
+                    uint32_t st = tiles_smem + s * STAGE_BYTES;
+                    mbar_expect_tx(bar(s), STAGE_BYTES);
+                    tma_load_2d(st, &mAhi, kb * TB_K, tm * TB_M, bar(s));
+                    tma_load_2d(st + A_BYTES, &mAlo, kb * TB_K, tm * TB_M, bar(s));
+                    tma_load_2d(st + 2 * A_BYTES, &mBhi, kb * TB_K, tn * TB_N, bar(s));
+                    tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBlo, kb * TB_K, tn * TB_N, bar(s));
+                }
+            }
+            if (*abort_flag) {
+                // drain: wait (bounded) for the loads of every stage still in flight
+                volatile int never = 0;
+                for (int s = 0; s < TB_STAGES; ++s) {
+                    int last = step - 1 - ((step - 1 - s) % TB_STAGES + TB_STAGES) % TB_STAGES;
+                    if (last >= 0) mbar_wait(bar(s), (last / TB_STAGES) & 1, &never);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TB_N >> 3) << 17) |
+                                   ((uint32_t)(TB_M >> 4) << 24);
+            int step = 0, it = 0;
+            for (int t = blockIdx.x; t < args.tiles && !*abort_flag; t += gridDim.x, ++it) {
+                int acc = it & 1;
+                uint32_t aph = (it >> 1) & 1;
+                if (!mbar_wait(bar(TEMPTY + acc), aph ^ 1, abort_flag)) break;
+                fence_after();
+                uint32_t d = tmem_base + (uint32_t)(acc * TB_N);
+                bool ok = true;
+                for (int kb = 0; kb < args.kchunks; ++kb, ++step) {
+                    int s = step % TB_STAGES;
+                    uint32_t ph = (step / TB_STAGES) & 1;
+                    if (!mbar_wait(bar(s), ph, abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    fence_after();
+                    uint32_t st = tiles_smem + s * STAGE_BYTES;
+#pragma unroll
+                    for (int ks = 0; ks < TB_K / 8; ++ks) {
+                        uint64_t ahi = swz_desc(st + ks * 32), alo = swz_desc(st + A_BYTES + ks * 32);
+                        uint64_t bhi = swz_desc(st + 2 * A_BYTES + ks * 32);
+                        uint64_t blo = swz_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
+                        uint32_t first = (kb == 0 && ks == 0) ? 0u : 1u;
+                        mma_tf32(d, ahi, bhi, idesc, first);
+                        mma_tf32(d, ahi, blo, idesc, 1u);
+                        mma_tf32(d, alo, bhi, idesc, 1u);
+                    }
+                    mma_commit(bar(EMPTY + s));
+                }
+                if (!ok) break;
+                mma_commit(bar(TFULL + acc));
+            }
+        }
+    } else {
+        const int q = warp & 3;  // TMEM lane quarter of this warp
+        int it = 0;
+        for (int t = blockIdx.x; t < args.tiles && !*abort_flag; t += gridDim.x, ++it) {
+            int acc = it & 1;
+            uint32_t aph = (it >> 1) & 1;
+            if (!mbar_wait(bar(TFULL + acc), aph, abort_flag)) break;
+            fence_after();
+            int tm, tn;
+            tile_coords(t, args.tiles_m, args.tiles_n, tm, tn);
+            int R = tm * TB_M + q * 32 + lane;
+            bool row_ok = R < args.m2;
+            float* crow = args.C + (size_t)(args.row0 + R);
+            for (int cb = 0; cb < TB_N / 32; ++cb) {
+                float v[32];
+                uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TB_N + cb * 32);
+                tmem_ld32(taddr, v);
+                int c0 = tn * TB_N + cb * 32;
+                if (row_ok) {
+                    // all 32 loads first, then the stores: keeps 32 loads in flight per thread
+                    float old[32];
+                    float* p0 = crow + (size_t)(args.col0 + c0) * args.ldc;
+                    int ncol = min(32, args.ncols - c0);
+                    if (ncol == 32) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) old[j] = __ldcs(p0 + (size_t)j * args.ldc);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) __stcs(p0 + (size_t)j * args.ldc, old[j] - v[j]);
+                    } else {
+                        for (int j = 0; j < ncol; ++j) old[j] = __ldcs(p0 + (size_t)j * args.ldc);
+                        for (int j = 0; j < ncol; ++j) __stcs(p0 + (size_t)j * args.ldc, old[j] - v[j]);
+                    }
+                }
+            }
+            fence_before();
+            mbar_arrive(bar(TEMPTY + acc));
+        }
+    }
+    __syncthreads();
+    if (*abort_flag && threadIdx.x == 0) atomicExch(args.status, 8);
+    if (warp == 1) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+}
+
+// ---- operand packing ----------------------------------------------------------------------
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+__device__ __forceinline__ void split(float x, float& hi, float& lo) {
+    hi = tf32_rna(x);
+    lo = tf32_rna(x - hi);
+}
+
+// Lemb hi/lo (2m x kp floats, row-major): a 32 x 32 complex tile through shared memory.
+__global__ void pack_l_kernel(const float2* __restrict__ A, size_t lda, int r0, int k0, int m, int w, int kp,
+                              float* __restrict__ hi, float* __restrict__ lo) {
+    __shared__ float2 tile[32][33];
+    int mu0 = blockIdx.x * 32, k00 = blockIdx.y * 32;
+    int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (int r = ty; r < 32; r += 8) {
+        int kk = k00 + r, mu = mu0 + tx;
+        tile[r][tx] = (kk < w && mu < m) ? A[(size_t)(k0 + kk) * lda + r0 + mu] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        int mu = mu0 + r, kk = k00 + tx;
+        if (mu >= m || 2 * kk >= kp) continue;
+        float2 l = tile[tx][r];
+        float rh, rl, ih, il;
+        split(l.x, rh, rl);
+        split(l.y, ih, il);
+        size_t o0 = (size_t)(2 * mu) * kp + 2 * kk, o1 = o0 + kp;
+        *(float2*)(hi + o0) = make_float2(rh, -ih);
+        *(float2*)(hi + o1) = make_float2(ih, rh);
+        *(float2*)(lo + o0) = make_float2(rl, -il);
+        *(float2*)(lo + o1) = make_float2(il, rl);
+    }
+}
+
+// U hi/lo (n' x kp floats, row-major): row nu = interleaved column nu of U12.
+__global__ void pack_u_kernel(const float2* __restrict__ A, size_t lda, int r0, int k0, int ncols, int w, int kp,
+                              float* __restrict__ hi, float* __restrict__ lo) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int half = kp / 2;
+    if (t >= (size_t)ncols * half) return;
+    int nu = (int)(t / half), kk = (int)(t % half);
+    float2 u = kk < w ? A[(size_t)(r0 + nu) * lda + k0 + kk] : make_float2(0.f, 0.f);
+    float rh, rl, ih, il;
+    split(u.x, rh, rl);
+    split(u.y, ih, il);
+    size_t o = (size_t)nu * kp + 2 * kk;
+    *(float2*)(hi + o) = make_float2(rh, ih);
+    *(float2*)(lo + o) = make_float2(rl, il);
+}
+
+// x <- -x over hi and lo halves (2 count floats starting at p, contiguous)
+__global__ void negate_kernel(float* __restrict__ p, size_t count) {
+    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) p[t] = -p[t];
+}
+
+// ---- host -------------------------------------------------------------------------------
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiled encoder() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiled)p;
+    }
+    return fn;
+}
+
+static bool make_map(CUtensorMap* map, float* base, int rows, int kp, int box_rows) {
+    EncodeTiled enc = encoder();
+    if (!enc) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kp * 4};
+    cuuint32_t box[2] = {(cuuint32_t)TB_K, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool tf32_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("TCU_DISABLE_TCGEN05");
+        on = (e && e[0] == '1') ? 0 : 1;
+        if (on) {
+            cudaFuncSetAttribute(tf32_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
+            if (!encoder()) on = 0;
+        }
+    }
+    return on == 1;
+}
+
+// N = L11^-1 - I for the unit lower w x w diagonal block of the panel (FP32, in place in
+// shared memory, columns right to left: X[i][j] = -sum_{k=j+1..i} X[i][k] L[k][j]), stored
+// column-major w x w. U12 = L11^-1 A12 = A12 + N A12 then runs as a tensor-core update.
+__global__ void __launch_bounds__(256) tri_inverse_l_kernel(const float2* __restrict__ A, size_t lda, int k0, int w,
+                                                            float2* __restrict__ N) {
+    extern __shared__ float2 ti_smem[];
+    const int LD = 129;
+    float2* M = ti_smem;            // M[i * LD + k]
+    float2* col = ti_smem + 128 * LD;
+    for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+        int i = idx % w, k = idx / w;
+        M[i * LD + k] = (i > k) ? A[(size_t)(k0 + k) * lda + k0 + i] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int i = threadIdx.x;
+    for (int j = w - 2; j >= 0; --j) {
+        if (i < w) col[i] = M[i * LD + j];
+        __syncthreads();
+        if (i < w && i > j) {
+            float sr = col[i].x, si = col[i].y;  // k = i term: X[i][i] = 1
+            for (int k = j + 1; k < i; ++k) {
+                float2 x = M[i * LD + k], l = col[k];
+                sr += x.x * l.x - x.y * l.y;
+                si += x.x * l.y + x.y * l.x;
+            }
+            M[i * LD + j] = make_float2(-sr, -si);
+        }
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+        int ii = idx % w, k = idx / w;
+        N[(size_t)k * w + ii] = M[ii * LD + k];
+    }
+}
+constexpr size_t TI_SMEM = (size_t)(128 * 129 + 128) * sizeof(float2);
+
+size_t tf32_pack_bytes(int n) {
+    size_t kp = 256;
+    return ((size_t)2 * n * kp + (size_t)n * kp) * 2 * 4 + (size_t)128 * 128 * 8 + 8192;
+}
+
+static int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return sms;
+}
+
+static bool ensure_pack(LuWork& wk, size_t need, int n, cudaStream_t st) {
+    if (wk.pack && wk.pack_bytes >= need) return true;
+    if (wk.pack) cudaFree(wk.pack);
+    size_t want = std::max(need, tf32_pack_bytes(n));
+    if (cudaMalloc(&wk.pack, want) != cudaSuccess) {
+        wk.pack = nullptr;
+        wk.pack_bytes = 0;
+        cudaMemsetAsync(wk.status, 6, 1, st);
+        return false;
+    }
+    wk.pack_bytes = want;
+    return true;
+}
+
+// C[row0 .. row0+m2) x [col0 .. col0+ncols) -= Apack (m2 x kp) * Bpack (ncols x kp)^T
+static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, int kp, float* ahi, float* alo,
+                     float* bhi, float* blo, LuWork& wk, cudaStream_t st, long long* launches) {
+    CUtensorMap mAhi, mAlo, mBhi, mBlo;
+    bool ok = make_map(&mAhi, ahi, m2, kp, TB_M) && make_map(&mAlo, alo, m2, kp, TB_M) &&
+              make_map(&mBhi, bhi, ncols, kp, TB_N) && make_map(&mBlo, blo, ncols, kp, TB_N);
+    if (!ok) {
+        cudaMemsetAsync(wk.status, 7, 1, st);
+        return;
+    }
+    Tf32Args a;
+    a.C = (float*)A;
+    a.ldc = (size_t)2 * n;
+    a.row0 = row0;
+    a.col0 = col0;
+    a.m2 = m2;
+    a.ncols = ncols;
+    a.kchunks = kp / TB_K;
+    a.tiles_m = (m2 + TB_M - 1) / TB_M;
+    a.tiles_n = (ncols + TB_N - 1) / TB_N;
+    a.tiles = a.tiles_m * a.tiles_n;
+    a.status = wk.status;
+    int grid = std::min(num_sms(), a.tiles);
+    tf32_update_kernel<<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, a);
+    *launches += 1;
+}
+
+// U12 = L11^-1 A12 on the tensor cores: invert L11, then A12 -= (-(L11^-1 - I)) A12 with the
+// operands packed (A12 is read from its packed copy, so the in-place update is race free).
+void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches) {
+    int r0 = k0 + w, ncols = n - r0;
+    int kp = ((2 * w + TB_K - 1) / TB_K) * TB_K;
+    size_t need = ((size_t)2 * w * kp + (size_t)ncols * kp) * 2 * 4 + (size_t)w * w * 8 + 8192;
+    if (!ensure_pack(wk, need, n, st)) return;
+    float* ahi = (float*)wk.pack;
+    float* alo = ahi + (size_t)2 * w * kp;
+    float* bhi = alo + (size_t)2 * w * kp;
+    float* blo = bhi + (size_t)ncols * kp;
+    float2* Nm = (float2*)(((uintptr_t)(blo + (size_t)ncols * kp) + 255) & ~(uintptr_t)255);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(tri_inverse_l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TI_SMEM);
+        attr = true;
+    }
+    {
+        StageScope sc(ST_TRSM, st);
+        tri_inverse_l_kernel<<<1, 256, TI_SMEM, st>>>(A, (size_t)n, k0, w, Nm);
+        // A operand: -N embedded, so that the update C -= (-N) A12 adds N A12
+        dim3 g1((w + 31) / 32, (kp / 2 + 31) / 32);
+        pack_l_kernel<<<g1, 256, 0, st>>>(Nm, (size_t)w, 0, 0, w, w, kp, ahi, alo);
+        size_t tot = (size_t)ncols * (kp / 2);
+        pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
+        negate_kernel<<<(unsigned)(((size_t)4 * w * kp + 255) / 256), 256, 0, st>>>(ahi, (size_t)4 * w * kp);
+        run_gemm(A, n, 2 * k0, r0, 2 * w, ncols, kp, ahi, alo, bhi, blo, wk, st, launches);
+        *launches += 4;
+    }
+}
+
+void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches) {
+    int r0 = k0 + w, m = n - r0, ncols = n - r0;
+    int kp = ((2 * w + TB_K - 1) / TB_K) * TB_K;
+    size_t need = ((size_t)2 * m * kp + (size_t)ncols * kp) * 2 * 4 + 4096;
+    if (!ensure_pack(wk, need, n, st)) return;
+    float* ahi = (float*)wk.pack;
+    float* alo = ahi + (size_t)2 * m * kp;
+    float* bhi = alo + (size_t)2 * m * kp;
+    float* blo = bhi + (size_t)ncols * kp;
+    {
+        StageScope sc(ST_PACK, st);
+        dim3 g1((m + 31) / 32, (kp / 2 + 31) / 32);
+        pack_l_kernel<<<g1, 256, 0, st>>>(A, (size_t)n, r0, k0, m, w, kp, ahi, alo);
+        size_t tot = (size_t)ncols * (kp / 2);
+        pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
+        *launches += 2;
+    }
+    StageScope sc(ST_GEMM, st);
+    run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, ahi, alo, bhi, blo, wk, st, launches);
+}
 
 }  // namespace tcu

@@ -101,11 +101,15 @@ struct LuWork {
 };
 int lu_factor_fp64(double2* A, int n, LuWork& w, cudaStream_t st, long long* launches);
 int lu_factor_fp32(float2* A, int n, LuWork& w, cudaStream_t st, long long* launches, bool tensor_cores);
-// x (n x ncol, FP64) <- A^-1 x using the factors (storage FP64 or FP32)
-void lu_solve_fp64(const double2* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
-                   long long* launches);
-void lu_solve_fp32(const float2* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
-                   long long* launches);
+// solve.cu — inverses of the 64 x 64 diagonal blocks of L and U (FP64, lu_inverse_bytes),
+// then x (n x ncol, FP64) <- A^-1 x; tmp holds 2 n min(ncol, 8) complex.
+size_t lu_inverse_bytes(int n);
+void lu_block_inverses_fp64(const double2* A, int n, double2* inv, cudaStream_t st, long long* launches);
+void lu_block_inverses_fp32(const float2* A, int n, double2* inv, cudaStream_t st, long long* launches);
+void lu_solve_fp64(const double2* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp, int ncol,
+                   cudaStream_t st, long long* launches);
+void lu_solve_fp32(const float2* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp, int ncol,
+                   cudaStream_t st, long long* launches);
 size_t lu_workspace_bytes(int n, bool fp32);
 void lu_init_attributes();
 

@@ -63,22 +63,20 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // Grid barrier for co-resident CTAs (cooperative launch). Every wait is bounded: after
 // 4 s, or once another CTA has raised an error, it records TIMEOUT (8) in *status and
 // returns false so the kernel can leave.
+// The arrival counter only grows (reset per launch): barrier instance g completes when the
+// counter reaches (g + 1) * nblocks, so one release-add and acquire polls suffice.
 __device__ bool grid_sync(unsigned* bar, unsigned nblocks, int* status) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
-        unsigned gen = ld_acquire_u32(&bar[1]);
-        __threadfence();
-        unsigned arrived = atomicAdd(&bar[0], 1u);
-        if (arrived == nblocks - 1) {
-            atomicExch(&bar[0], 0u);
-            __threadfence();
-            atomicAdd(&bar[1], 1u);
-        } else {
+        unsigned old;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
+        unsigned target = (old / nblocks + 1) * nblocks;
+        if (old + 1 != target) {
             unsigned long long t0 = global_ns();
             unsigned spins = 0;
-            while (ld_acquire_u32(&bar[1]) == gen) {
+            while ((int)(ld_acquire_u32(bar) - target) < 0) {
                 if ((++spins & 255u) == 0) {
                     if (*(volatile int*)status == 8) {
                         ok = 0;
@@ -117,6 +115,7 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
     __shared__ int s_row[8];
     __shared__ double s_bval;
     __shared__ int s_brow, s_bcta;
+    unsigned long long* keys = (unsigned long long*)cand;  // 3 pivot keys, cycled per column
     const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int rows = n - k0;
@@ -131,20 +130,21 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
     for (int j = 0; j < w; ++j) {
         const int gj = k0 + j;
         const int buf = j & 1;
-        // local candidate
-        double bv = -1.0;
+        // Local candidate: the largest |a|^2 (as FP32 bits; ties to the lower row), packed as
+        // (bits << 32) | ~row so that one 64-bit atomicMax across the CTAs picks the pivot.
+        float bv = -1.f;
         int br = 0x7fffffff;
         for (int r = tid; r < myrows; r += blockDim.x) {
             int g = row0 + r;
             if (g < gj) continue;
-            double v = cx_abs2<R>(tile[(size_t)r * LD + j]);
+            float v = (float)cx_abs2<R>(tile[(size_t)r * LD + j]);
             if (v > bv || (v == bv && g < br)) {
                 bv = v;
                 br = g;
             }
         }
         for (int o = 16; o > 0; o >>= 1) {
-            double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            float ov = __shfl_xor_sync(0xffffffffu, bv, o);
             int orr = __shfl_xor_sync(0xffffffffu, br, o);
             if (ov > bv || (ov == bv && orr < br)) {
                 bv = ov;
@@ -157,64 +157,37 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
         }
         __syncthreads();
         if (tid == 0) {
-            double v = s_val[0];
+            float v = (float)s_val[0];
             int rr = s_row[0];
             for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
-                if (s_val[q] > v || (s_val[q] == v && s_row[q] < rr)) {
-                    v = s_val[q];
+                if ((float)s_val[q] > v || ((float)s_val[q] == v && s_row[q] < rr)) {
+                    v = (float)s_val[q];
                     rr = s_row[q];
                 }
             s_bval = v;
             s_brow = rr;
-            Cand cd;
-            cd.val = v;
-            cd.row = rr;
-            cd.pad = 0;
-            cand[buf * P + b] = cd;
         }
         __syncthreads();
         if (s_bval >= 0.0) {
             int lr = s_brow - row0;
             for (int c = tid; c < w; c += blockDim.x) __stcg(&crow[((size_t)buf * P + b) * NB + c], tile[(size_t)lr * LD + c]);
+            if (tid == 0) {
+                unsigned long long key = ((unsigned long long)__float_as_uint((float)s_bval) << 32) |
+                                         (unsigned long long)(0xFFFFFFFFu - (unsigned)s_brow);
+                atomicMax(&keys[j % 3], key);
+            }
         }
         if (gj >= row0 && gj < row0 + myrows) {
             int lr = gj - row0;
             for (int c = tid; c < w; c += blockDim.x) __stcg(&drow[(size_t)buf * NB + c], tile[(size_t)lr * LD + c]);
         }
         if (!grid_sync(bar, P, status)) return;
-        // winner
-        if (warp == 0) {
-            double v = -1.0;
-            int rr = 0x7fffffff, cb = 0;
-            for (int q = lane; q < P; q += 32) {
-                double cv = __ldcg(&cand[buf * P + q].val);
-                int crr = __ldcg(&cand[buf * P + q].row);
-                if (cv > v || (cv == v && crr < rr)) {
-                    v = cv;
-                    rr = crr;
-                    cb = q;
-                }
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                double ov = __shfl_xor_sync(0xffffffffu, v, o);
-                int orr = __shfl_xor_sync(0xffffffffu, rr, o);
-                int ocb = __shfl_xor_sync(0xffffffffu, cb, o);
-                if (ov > v || (ov == v && orr < rr)) {
-                    v = ov;
-                    rr = orr;
-                    cb = ocb;
-                }
-            }
-            if (lane == 0) {
-                s_bval = v;
-                s_brow = rr;
-                s_bcta = cb;
-            }
-        }
-        __syncthreads();
-        const int pr = s_brow;
-        const double pv = s_bval;
-        for (int c = tid; c < w; c += blockDim.x) prow[c] = __ldcg(&crow[((size_t)buf * P + s_bcta) * NB + c]);
+        // every thread reads the winning key and its share of the pivot row
+        const unsigned long long key = __ldcg(&keys[j % 3]);
+        const int pr = (int)(0xFFFFFFFFu - (unsigned)(key & 0xFFFFFFFFull));
+        const int owner = (pr - k0) / chunk;
+        for (int c = tid; c < w; c += blockDim.x) prow[c] = __ldcg(&crow[((size_t)buf * P + owner) * NB + c]);
+        if (b == 0 && tid == 0) atomicExch(&keys[(j + 2) % 3], 0ull);  // slot of column j-1, read before this barrier
         __syncthreads();
         if (pr != gj) {
             if (pr >= row0 && pr < row0 + myrows) {
@@ -233,7 +206,8 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
                 perm[gj] = perm[pr];
                 perm[pr] = a;
             }
-            if (!(pv > 0.0)) atomicCAS(status, 0, 5);
+            C pvt = prow[j];
+            if (!((double)pvt.x * pvt.x + (double)pvt.y * pvt.y > 0.0)) atomicCAS(status, 0, 5);
         }
         __syncthreads();
         // rank-1 update of the rows below the pivot
@@ -368,7 +342,7 @@ constexpr int ZG_T = 64;   // tile rows/cols (complex)
 constexpr int ZG_KC = 16;  // K chunk (complex)
 constexpr size_t ZG_SMEM = 4 * ZG_KC * ZG_T * sizeof(double2);
 
-__global__ void __launch_bounds__(256) zgemm_dmma_kernel(double2* A, size_t lda, int k0, int w, int r0, int n) {
+__global__ void __launch_bounds__(256, 2) zgemm_dmma_kernel(double2* A, size_t lda, int k0, int w, int r0, int n) {
     extern __shared__ __align__(16) unsigned char zg_smem[];
     double2 (*Ls)[ZG_KC][ZG_T] = (double2 (*)[ZG_KC][ZG_T])zg_smem;                       // [stage][k][row]
     double2 (*Us)[ZG_KC][ZG_T] = (double2 (*)[ZG_KC][ZG_T])(zg_smem + 2 * ZG_KC * ZG_T * 16);  // [stage][k][col]
@@ -436,23 +410,31 @@ __global__ void __launch_bounds__(256) zgemm_dmma_kernel(double2* A, size_t lda,
     }
     // epilogue: lanes (l, l^4) hold the re/im rows of one complex row
     const bool even = ((lane >> 2) & 1) == 0;
+    const int csel = 2 * (lane & 3) + (even ? 0 : 1);
+    // two halves of 8 read-modify-writes, each with all its loads in flight before its stores
 #pragma unroll
-    for (int rb = 0; rb < 8; ++rb) {
-        int rr = rb * 8 + (lane >> 2);
-        int mu = wr + (rr >> 1);
+    for (int half = 0; half < 2; ++half) {
+        double2 upd[4][2], old[4][2];
 #pragma unroll
-        for (int cb = 0; cb < 2; ++cb) {
-            double d0 = acc[rb][cb][0], d1 = acc[rb][cb][1];
-            double p0 = __shfl_xor_sync(0xffffffffu, d0, 4), p1 = __shfl_xor_sync(0xffffffffu, d1, 4);
-            int col = wc + cb * 8 + 2 * (lane & 3) + (even ? 0 : 1);
-            double re = even ? d0 : p1, im = even ? p0 : d1;
-            int grow = tr + mu, gcol = tc + col;
-            if (grow < n && gcol < n) {
-                double2* c = A + (size_t)gcol * lda + grow;
-                double2 v = *c;
-                v.x -= re;
-                v.y -= im;
-                *c = v;
+        for (int q = 0; q < 4; ++q) {
+            int rb = half * 4 + q;
+#pragma unroll
+            for (int cb = 0; cb < 2; ++cb) {
+                double d0 = acc[rb][cb][0], d1 = acc[rb][cb][1];
+                double p0 = __shfl_xor_sync(0xffffffffu, d0, 4), p1 = __shfl_xor_sync(0xffffffffu, d1, 4);
+                upd[q][cb] = make_double2(even ? d0 : p1, even ? p0 : d1);
+                int grow = tr + wr + ((rb * 8 + (lane >> 2)) >> 1), gcol = tc + wc + cb * 8 + csel;
+                old[q][cb] = (grow < n && gcol < n) ? A[(size_t)gcol * lda + grow] : make_double2(0.0, 0.0);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            int rb = half * 4 + q;
+#pragma unroll
+            for (int cb = 0; cb < 2; ++cb) {
+                int grow = tr + wr + ((rb * 8 + (lane >> 2)) >> 1), gcol = tc + wc + cb * 8 + csel;
+                if (grow < n && gcol < n)
+                    A[(size_t)gcol * lda + grow] = make_double2(old[q][cb].x - upd[q][cb].x, old[q][cb].y - upd[q][cb].y);
             }
         }
     }
@@ -514,7 +496,6 @@ __global__ void __launch_bounds__(256) cgemm_simt_kernel(float2* A, size_t lda, 
 
 // ---- host driver --------------------------------------------------------------------------
 static int g_num_sms = 0;
-static void solve_init_attributes();
 
 template <typename R, int NB>
 static size_t panel_smem(int chunk) {
@@ -532,7 +513,6 @@ void lu_init_attributes() {
     cudaFuncSetAttribute(trsm_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(trsm_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZG_SMEM);
-    solve_init_attributes();
 }
 
 size_t lu_workspace_bytes(int n, bool fp32) {
@@ -554,6 +534,7 @@ static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cud
     C* crow = (C*)(cand + 2 * 160);
     C* drow = crow + 2 * 160 * NB;
     cudaMemsetAsync(wk.barrier, 0, 2 * sizeof(unsigned), st);
+    cudaMemsetAsync(cand, 0, 3 * sizeof(unsigned long long), st);
     size_t lda = (size_t)n;
     void* args[] = {&A, &lda, &k0, &n, &w, &chunk, &wk.piv, &wk.perm, &cand, &crow, &drow, &wk.barrier, &wk.status};
     cudaError_t e = cudaLaunchCooperativeKernel((void*)panel_kernel<R, NB>, dim3(P), dim3(256), args, smem, st);
@@ -566,6 +547,7 @@ __global__ void iota_kernel(int* p, int n) {
 }
 
 void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches);
+void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches);
 
 template <typename R, int NB>
 static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t st, long long* launches,
@@ -594,11 +576,13 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
         int cols = n - r0;
         int cpc = 64;
         size_t smem = (size_t)NB * NB * sizeof(C);
-        {
+        if (sizeof(R) == 4 && tensor_cores) {
+            launch_tf32_trsm((float2*)A, n, k0, w, wk, st, launches);
+        } else {
             StageScope sc(ST_TRSM, st);
             trsm_kernel<R, NB><<<(cols + cpc - 1) / cpc, 256, smem, st>>>(A, lda, k0, w, n, cpc);
+            ++*launches;
         }
-        ++*launches;
         dim3 grid((cols + ZG_T - 1) / ZG_T, (cols + ZG_T - 1) / ZG_T);
         if constexpr (sizeof(R) == 8) {
             StageScope sc(ST_GEMM, st);
@@ -622,165 +606,6 @@ int lu_factor_fp64(double2* A, int n, LuWork& w, cudaStream_t st, long long* lau
 }
 int lu_factor_fp32(float2* A, int n, LuWork& w, cudaStream_t st, long long* launches, bool tensor_cores) {
     return lu_factor_impl<float, 128>(A, n, w, st, launches, tensor_cores);
-}
-
-// ---- solves -------------------------------------------------------------------------------
-// x <- P x (gather through perm), then L y = x (unit lower), U x = y (upper), blockwise:
-// each launch solves one diagonal block redundantly per CTA and updates the remaining rows
-// of its chunk with the block column (read once, coalesced over rows).
-constexpr int SB = 64;  // solve block
-constexpr int SMAXC = 8;
-constexpr size_t TV_SMEM = (size_t)SB * (SB + 1) * sizeof(double2);
-
-__global__ void gather_kernel(const double2* __restrict__ x, double2* __restrict__ y, const int* __restrict__ perm,
-                              int n, int ncol) {
-    size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (size_t)n * ncol) return;
-    int c = (int)(t / n), i = (int)(t % n);
-    y[t] = x[(size_t)c * n + perm[i]];
-}
-
-template <typename C, bool LOWER>
-__global__ void __launch_bounds__(256) trsv_step_kernel(const C* __restrict__ A, size_t lda, int n, int b0, int bw,
-                                                        double2* __restrict__ x, int ncol) {
-    __shared__ double2 xb[SMAXC][SB];
-    extern __shared__ __align__(16) unsigned char tv_smem[];
-    double2 (*Db)[SB + 1] = (double2 (*)[SB + 1])tv_smem;  // diagonal block, Db[i][k]
-    // diagonal block and the current right-hand side block
-    for (int idx = threadIdx.x; idx < bw * bw; idx += blockDim.x) {
-        int i = idx % bw, k = idx / bw;
-        C v = A[(size_t)(b0 + k) * lda + b0 + i];
-        Db[i][k] = make_double2(v.x, v.y);
-    }
-    for (int idx = threadIdx.x; idx < bw * ncol; idx += blockDim.x) {
-        int i = idx % bw, c = idx / bw;
-        xb[c][i] = x[(size_t)c * n + b0 + i];
-    }
-    __syncthreads();
-    // small triangular solve: one warp per column
-    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp < ncol) {
-        int c = warp;
-        double2 v0 = lane < bw ? xb[c][lane] : make_double2(0, 0);
-        double2 v1 = lane + 32 < bw ? xb[c][lane + 32] : make_double2(0, 0);
-        if (LOWER) {
-            for (int k = 0; k < bw; ++k) {
-                double2 xk;
-                xk.x = __shfl_sync(0xffffffffu, k < 32 ? v0.x : v1.x, k & 31);
-                xk.y = __shfl_sync(0xffffffffu, k < 32 ? v0.y : v1.y, k & 31);
-                if (lane > k && lane < bw) {
-                    double2 l = Db[lane][k];
-                    v0.x -= l.x * xk.x - l.y * xk.y;
-                    v0.y -= l.x * xk.y + l.y * xk.x;
-                }
-                if (lane + 32 > k && lane + 32 < bw) {
-                    double2 l = Db[lane + 32][k];
-                    v1.x -= l.x * xk.x - l.y * xk.y;
-                    v1.y -= l.x * xk.y + l.y * xk.x;
-                }
-            }
-        } else {
-            for (int k = bw - 1; k >= 0; --k) {
-                // x_k = v_k / U_kk, owner lane computes, then broadcast
-                double2 own = k < 32 ? v0 : v1;
-                double2 d = Db[k][k];
-                double den = d.x * d.x + d.y * d.y;
-                double2 q = make_double2((own.x * d.x + own.y * d.y) / den, (own.y * d.x - own.x * d.y) / den);
-                double2 xk;
-                xk.x = __shfl_sync(0xffffffffu, q.x, k & 31);
-                xk.y = __shfl_sync(0xffffffffu, q.y, k & 31);
-                if (lane == (k & 31)) {
-                    if (k < 32)
-                        v0 = xk;
-                    else
-                        v1 = xk;
-                }
-                if (lane < k) {
-                    double2 u = Db[lane][k];
-                    v0.x -= u.x * xk.x - u.y * xk.y;
-                    v0.y -= u.x * xk.y + u.y * xk.x;
-                }
-                if (lane + 32 < k) {
-                    double2 u = Db[lane + 32][k];
-                    v1.x -= u.x * xk.x - u.y * xk.y;
-                    v1.y -= u.x * xk.y + u.y * xk.x;
-                }
-            }
-        }
-        if (lane < bw) xb[c][lane] = v0;
-        if (lane + 32 < bw) xb[c][lane + 32] = v1;
-    }
-    __syncthreads();
-    if (blockIdx.x == 0)
-        for (int idx = threadIdx.x; idx < bw * ncol; idx += blockDim.x) {
-            int i = idx % bw, c = idx / bw;
-            x[(size_t)c * n + b0 + i] = xb[c][i];
-        }
-    // update the other rows: lower -> rows below the block; upper -> rows above
-    int lo = LOWER ? b0 + bw : 0, hi = LOWER ? n : b0;
-    for (int r = lo + blockIdx.x * blockDim.x + threadIdx.x; r < hi; r += gridDim.x * blockDim.x) {
-        double2 acc[SMAXC];
-        for (int c = 0; c < ncol; ++c) acc[c] = make_double2(0, 0);
-        for (int k = 0; k < bw; ++k) {
-            C v = A[(size_t)(b0 + k) * lda + r];
-            double lr = v.x, li = v.y;
-            for (int c = 0; c < ncol; ++c) {
-                double2 xk = xb[c][k];
-                acc[c].x += lr * xk.x - li * xk.y;
-                acc[c].y += lr * xk.y + li * xk.x;
-            }
-        }
-        for (int c = 0; c < ncol; ++c) {
-            double2* p = x + (size_t)c * n + r;
-            double2 v = *p;
-            v.x -= acc[c].x;
-            v.y -= acc[c].y;
-            *p = v;
-        }
-    }
-}
-
-template <typename C>
-static void lu_solve_impl(const C* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
-                          long long* launches) {
-    lu_init_attributes();
-    StageScope sc(ST_SOLVE, st);
-    for (int c0 = 0; c0 < ncol; c0 += SMAXC) {
-        int nc = std::min(SMAXC, ncol - c0);
-        double2* xc = x + (size_t)c0 * n;
-        size_t tot = (size_t)n * nc;
-        gather_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(xc, tmp, perm, n, nc);
-        ++*launches;
-        int grid = g_num_sms;
-        for (int b0 = 0; b0 < n; b0 += SB) {
-            int bw = std::min(SB, n - b0);
-            trsv_step_kernel<C, true><<<grid, 256, TV_SMEM, st>>>(A, n, n, b0, bw, tmp, nc);
-            ++*launches;
-        }
-        int last = ((n - 1) / SB) * SB;
-        for (int b0 = last; b0 >= 0; b0 -= SB) {
-            int bw = std::min(SB, n - b0);
-            trsv_step_kernel<C, false><<<grid, 256, TV_SMEM, st>>>(A, n, n, b0, bw, tmp, nc);
-            ++*launches;
-        }
-        cudaMemcpyAsync(xc, tmp, tot * sizeof(double2), cudaMemcpyDeviceToDevice, st);
-    }
-}
-
-static void solve_init_attributes() {
-    cudaFuncSetAttribute(trsv_step_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV_SMEM);
-    cudaFuncSetAttribute(trsv_step_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV_SMEM);
-    cudaFuncSetAttribute(trsv_step_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV_SMEM);
-    cudaFuncSetAttribute(trsv_step_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TV_SMEM);
-}
-
-void lu_solve_fp64(const double2* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
-                   long long* launches) {
-    lu_solve_impl<double2>(A, n, perm, x, tmp, ncol, st, launches);
-}
-void lu_solve_fp32(const float2* A, int n, const int* perm, double2* x, double2* tmp, int ncol, cudaStream_t st,
-                   long long* launches) {
-    lu_solve_impl<float2>(A, n, perm, x, tmp, ncol, st, launches);
 }
 
 }  // namespace tcu
