@@ -29,6 +29,45 @@ tcu_status fail(tcu_status st, const std::string& msg) {
     return st;
 }
 
+// Caching device allocator of a context: blocks freed by factors and per-call buffers are
+// kept for reuse (stream-ordered on the context's stream), so repeated factorizations do
+// not pay cudaMalloc/cudaFree of multi-GB matrices. Pooled blocks are released on
+// allocation failure and when the context is destroyed.
+struct DevicePool {
+    std::multimap<size_t, void*> free_;
+    std::map<void*, size_t> sizes_;
+    cudaError_t alloc(void** p, size_t bytes) {
+        bytes = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+        auto it = free_.lower_bound(bytes);
+        if (it != free_.end() && it->first <= 2 * bytes + ((size_t)1 << 20)) {
+            *p = it->second;
+            free_.erase(it);
+            return cudaSuccess;
+        }
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            release();
+            e = cudaMalloc(p, bytes);
+        }
+        if (e == cudaSuccess) sizes_[*p] = bytes;
+        return e;
+    }
+    void free(void* p) {
+        if (!p) return;
+        auto it = sizes_.find(p);
+        if (it == sizes_.end()) return;
+        free_.emplace(it->second, p);
+    }
+    void release() {
+        for (auto& kv : free_) {
+            cudaFree(kv.second);
+            sizes_.erase(kv.second);
+        }
+        free_.clear();
+    }
+};
+
 struct DevPlanStore {
     HostPlan host;
     DevPlan dev{};
@@ -43,6 +82,7 @@ thread_local Profiler* g_prof = nullptr;
 
 struct tcu_context {
     Profiler prof;
+    DevicePool pool;
     int device = 0;
     cudaStream_t stream = nullptr;
     std::recursive_mutex mu;
@@ -173,14 +213,18 @@ tcu_status read_status(tcu_context* ctx, const char* what) {
 }
 
 template <typename T>
-tcu_status dev_alloc(T** p, size_t count, const char* what) {
-    return cuda_check(cudaMalloc((void**)p, std::max<size_t>(count, 1) * sizeof(T)), what);
+tcu_status dev_alloc(tcu_context* ctx, T** p, size_t count, const char* what) {
+    return cuda_check(ctx->pool.alloc((void**)p, std::max<size_t>(count, 1) * sizeof(T)), what);
 }
 
+// A per-call device buffer from the context pool.
 struct DevBuf {
+    tcu_context* ctx;
     void* p = nullptr;
+    explicit DevBuf(tcu_context* c) : ctx(c) {}
+    cudaError_t alloc(size_t bytes) { return ctx->pool.alloc(&p, bytes); }
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p) ctx->pool.free(p);
     }
 };
 
@@ -233,31 +277,30 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
     f->precision = precision;
     f->k0 = k0;
     auto cleanup = [&]() {
-        if (f->d_pos) cudaFree(f->d_pos);
-        if (f->d_radii) cudaFree(f->d_radii);
-        if (f->d_eps) cudaFree(f->d_eps);
-        if (f->d_T) cudaFree(f->d_T);
-        if (f->d_A) cudaFree(f->d_A);
-        if (f->d_inv) cudaFree(f->d_inv);
-        if (f->wk.piv) cudaFree(f->wk.piv);
-        if (f->wk.pack) cudaFree(f->wk.pack);
+        for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
+                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack})
+            ctx->pool.free(q);
     };
     tcu_status e = TCU_OK;
     do {
-        if ((e = dev_alloc(&f->d_pos, 3 * N, "positions"))) break;
-        if ((e = dev_alloc(&f->d_radii, N, "radii"))) break;
-        if ((e = dev_alloc(&f->d_eps, N, "permittivities"))) break;
-        if ((e = dev_alloc(&f->d_T, N * L * 4, "T blocks"))) break;
+        if ((e = dev_alloc(ctx, &f->d_pos, 3 * N, "positions"))) break;
+        if ((e = dev_alloc(ctx, &f->d_radii, N, "radii"))) break;
+        if ((e = dev_alloc(ctx, &f->d_eps, N, "permittivities"))) break;
+        if ((e = dev_alloc(ctx, &f->d_T, N * L * 4, "T blocks"))) break;
         cudaMemcpyKind kind = pos_d ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
         if ((e = cuda_check(cudaMemcpyAsync(f->d_pos, pos_d ? pos_d : pos_h, 3 * N * 8, kind, ctx->stream), "copy"))) break;
         if ((e = cuda_check(cudaMemcpyAsync(f->d_radii, radii_d ? radii_d : radii_h, N * 8, kind, ctx->stream), "copy")))
             break;
         if ((e = cuda_check(cudaMemcpyAsync(f->d_eps, eps_d ? eps_d : eps_h, N * 16, kind, ctx->stream), "copy"))) break;
         size_t elem = precision == TCU_FP64 ? 16 : 8;
-        if ((e = cuda_check(cudaMalloc(&f->d_A, n * n * elem), "interaction matrix"))) break;
+        if ((e = cuda_check(ctx->pool.alloc(&f->d_A, n * n * elem), "interaction matrix"))) break;
+        if (precision == TCU_MIXED && tf32_enabled()) {
+            f->wk.pack_bytes = tf32_pack_bytes((int)n);
+            if ((e = cuda_check(ctx->pool.alloc(&f->wk.pack, f->wk.pack_bytes), "tensor-core operands"))) break;
+        }
         size_t ws = lu_workspace_bytes((int)n, precision == TCU_MIXED);
         void* wmem = nullptr;
-        if ((e = cuda_check(cudaMalloc(&wmem, ws), "LU workspace"))) break;
+        if ((e = cuda_check(ctx->pool.alloc(&wmem, ws), "LU workspace"))) break;
         f->wk.piv = (int*)wmem;
         f->wk.perm = f->wk.piv + n;
         f->wk.barrier = (unsigned*)(f->wk.perm + n);
@@ -298,7 +341,7 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
             e = fail(TCU_DEVICE_ERROR, "LU factorization: device status " + std::to_string(st));
             break;
         }
-        if ((e = cuda_check(cudaMalloc(&f->d_inv, lu_inverse_bytes((int)n)), "block inverses"))) break;
+        if ((e = cuda_check(ctx->pool.alloc((void**)&f->d_inv, lu_inverse_bytes((int)n)), "block inverses"))) break;
         if (precision == TCU_FP64)
             lu_block_inverses_fp64((const double2*)f->d_A, (int)n, f->d_inv, ctx->stream, &ctx->launches);
         else
@@ -326,9 +369,9 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
     if (!device && !finite_all(B, 2 * n * p))
         return fail(TCU_INVALID_INPUT,
                     "require finite channel-by-illumination columns matching the factorization");
-    DevBuf bufs;
+    DevBuf bufs(ctx);
     size_t per = n * p;
-    CK(cudaMalloc(&bufs.p, 6 * per * sizeof(cplx)), "solve buffers");
+    CK(bufs.alloc(6 * per * sizeof(cplx)), "solve buffers");
     cplx* b = (cplx*)bufs.p;
     cplx* tb = b + per;
     cplx* x = tb + per;
@@ -435,6 +478,7 @@ tcu_status tcu_context_destroy(tcu_context* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     for (auto& kv : ctx->plans) cudaFree(kv.second->mem);
+    ctx->pool.release();
     cudaFree(ctx->d_partial);
     cudaFree(ctx->d_cpartial);
     cudaFree(ctx->d_small);
@@ -490,8 +534,8 @@ tcu_status tcu_translation_block(tcu_context* ctx, int lmax, double k, const dou
     tcu_status s = get_plan(ctx, lmax, &P);
     if (s) return s;
     size_t M = 2 * (size_t)lmax * (lmax + 2);
-    DevBuf buf;
-    CK(cudaMalloc(&buf.p, M * M * 16), "block");
+    DevBuf buf(ctx);
+    CK(buf.alloc(M * M * 16), "block");
     launch_block(*P, k, disp, singular != 0, helicity != 0, (cplx*)buf.p, ctx->stream);
     ++ctx->launches;
     CK(cudaMemcpyAsync(out, buf.p, M * M * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
@@ -508,10 +552,10 @@ tcu_status tcu_mie_blocks(tcu_context* ctx, int lmax, double k0, size_t N, const
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
     CK(cudaSetDevice(ctx->device), "device");
-    DevBuf buf;
+    DevBuf buf(ctx);
     Arena ar;
     size_t o_r = ar.add(N * 8), o_e = ar.add(N * 16), o_t = ar.add(N * lmax * 64);
-    CK(cudaMalloc(&buf.p, ar.total), "mie buffers");
+    CK(buf.alloc(ar.total), "mie buffers");
     double* r = ar.at<double>(buf.p, o_r);
     cplx* e = ar.at<cplx>(buf.p, o_e);
     cplx* T = ar.at<cplx>(buf.p, o_t);
@@ -538,10 +582,10 @@ tcu_status tcu_plane_wave_expansion(tcu_context* ctx, int lmax, size_t N, const 
     ProfGuard pg(ctx);
     CK(cudaSetDevice(ctx->device), "device");
     size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M;
-    DevBuf buf;
+    DevBuf buf(ctx);
     Arena ar;
     size_t o_pos = ar.add(N * 24), o_kv = ar.add(p * 48), o_o = ar.add(n * p * 16), o_pl = ar.add(p * 4);
-    CK(cudaMalloc(&buf.p, ar.total), "plane-wave buffers");
+    CK(buf.alloc(ar.total), "plane-wave buffers");
     double* pos = ar.at<double>(buf.p, o_pos);
     cplx* kv = ar.at<cplx>(buf.p, o_kv);
     cplx* o = ar.at<cplx>(buf.p, o_o);
@@ -566,10 +610,10 @@ tcu_status tcu_cross_sections(tcu_context* ctx, int lmax, double k0, size_t N, c
     tcu_status s = get_plan(ctx, lmax, &P);
     if (s) return s;
     size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M, per = n * p;
-    DevBuf buf;
+    DevBuf buf(ctx);
     Arena ar;
     size_t o_pos = ar.add(N * 24), o_x = ar.add(3 * per * 16);
-    CK(cudaMalloc(&buf.p, ar.total), "cross-section buffers");
+    CK(buf.alloc(ar.total), "cross-section buffers");
     double* pos = ar.at<double>(buf.p, o_pos);
     cplx* dx = ar.at<cplx>(buf.p, o_x);
     cplx* db = dx + per;
@@ -631,14 +675,12 @@ tcu_status tcu_factor_destroy(tcu_factor* f) {
     if (!f) return TCU_OK;
     cudaSetDevice(f->ctx->device);
     cudaStreamSynchronize(f->ctx->stream);
-    cudaFree(f->d_pos);
-    cudaFree(f->d_radii);
-    cudaFree(f->d_eps);
-    cudaFree(f->d_T);
-    cudaFree(f->d_A);
-    cudaFree(f->d_inv);
-    cudaFree(f->wk.piv);
-    if (f->wk.pack) cudaFree(f->wk.pack);
+    {
+        std::lock_guard<std::recursive_mutex> lock(f->ctx->mu);
+        for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
+                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack})
+            f->ctx->pool.free(q);
+    }
     delete f;
     return TCU_OK;
 }
@@ -654,8 +696,8 @@ tcu_status tcu_cluster_operator(tcu_context* ctx, int lmax, double k0, size_t N,
     const DevPlan* P;
     if ((s = get_plan(ctx, lmax, &P))) return s;
     size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M;
-    DevBuf buf;
-    CK(cudaMalloc(&buf.p, N * 24 + N * 8 + N * 16 + N * lmax * 64 + n * n * 16), "operator buffers");
+    DevBuf buf(ctx);
+    CK(buf.alloc(N * 24 + N * 8 + N * 16 + N * lmax * 64 + n * n * 16), "operator buffers");
     double* pos = (double*)buf.p;
     double* r = pos + 3 * N;
     cplx* e = (cplx*)(r + N);
@@ -684,8 +726,8 @@ tcu_status tcu_cluster_apply(tcu_context* ctx, int lmax, double k0, size_t N, co
     const DevPlan* P;
     if ((s = get_plan(ctx, lmax, &P))) return s;
     size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M, per = n * p;
-    DevBuf buf;
-    CK(cudaMalloc(&buf.p, N * 24 + N * 8 + N * 16 + N * lmax * 64 + 2 * per * 16), "apply buffers");
+    DevBuf buf(ctx);
+    CK(buf.alloc(N * 24 + N * 8 + N * 16 + N * lmax * 64 + 2 * per * 16), "apply buffers");
     double* pos = (double*)buf.p;
     double* r = pos + 3 * N;
     cplx* e = (cplx*)(r + N);
@@ -843,9 +885,9 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
                     "incident coefficients must be finite, with one row per local multipole and at least one column");
     int restart = std::min(opt.restart, opt.max_iterations);
     if ((size_t)restart > n) restart = (int)n;
-    DevBuf buf;
+    DevBuf buf(ctx);
     size_t work = (size_t)(2 * restart + 4) * n;
-    CK(cudaMalloc(&buf.p, N * 24 + N * 8 + N * 16 + N * lmax * 64 + (3 * per + work) * 16), "GMRES buffers");
+    CK(buf.alloc(N * 24 + N * 8 + N * 16 + N * lmax * 64 + (3 * per + work) * 16), "GMRES buffers");
     double* pos = (double*)buf.p;
     double* r = pos + 3 * N;
     cplx* e = (cplx*)(r + N);

@@ -33,12 +33,14 @@ namespace tcu {
 constexpr int TB_M = 128;       // real rows per tile (64 complex rows)
 constexpr int TB_N = 256;       // columns per tile
 constexpr int TB_K = 16;        // floats per K chunk (one 64-byte swizzle row)
-constexpr int TB_STAGES = 4;
+constexpr int TB_STAGES = 3;
 constexpr int A_BYTES = TB_M * TB_K * 4;   // 8 KB
 constexpr int B_BYTES = TB_N * TB_K * 4;   // 16 KB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 48 KB
 constexpr int TMEM_COLS = 2 * TB_N;        // two accumulators
-constexpr size_t TF32_SMEM = (size_t)TB_STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int EPI_COLS = 64;                         // columns per epilogue staging buffer
+constexpr int EPI_BYTES = TB_M * EPI_COLS * 4;         // 32 KB
+constexpr size_t TF32_SMEM = (size_t)TB_STAGES * STAGE_BYTES + 2 * EPI_BYTES + 1024 + 256;
 
 // ---- device helpers ---------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -162,11 +164,14 @@ struct Tf32Args {
 __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_constant__ CUtensorMap mAhi,
                                                              const __grid_constant__ CUtensorMap mAlo,
                                                              const __grid_constant__ CUtensorMap mBhi,
-                                                             const __grid_constant__ CUtensorMap mBlo, Tf32Args args) {
+                                                             const __grid_constant__ CUtensorMap mBlo,
+                                                             const __grid_constant__ CUtensorMap mC, Tf32Args args) {
     extern __shared__ uint8_t smem_raw[];
     uint32_t base = smem_u32(smem_raw);
     uint32_t tiles_smem = (base + 1023u) & ~1023u;  // 1024-byte aligned stage ring
-    uint8_t* ctrl = smem_raw + (tiles_smem - base) + TB_STAGES * STAGE_BYTES;
+    const uint32_t epi_smem = tiles_smem + TB_STAGES * STAGE_BYTES;  // 2 staging buffers
+    float* epi = (float*)(smem_raw + (epi_smem - base));
+    uint8_t* ctrl = smem_raw + (tiles_smem - base) + TB_STAGES * STAGE_BYTES + 2 * EPI_BYTES;
     // barriers: full[S], empty[S], tmem_full[2], tmem_empty[2]
     uint64_t* bars = (uint64_t*)ctrl;
     uint32_t* tmem_slot = (uint32_t*)(ctrl + 8 * (2 * TB_STAGES + 4));
@@ -260,42 +265,54 @@ __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_consta
             }
         }
     } else {
+        // Epilogue: -D goes through a shared-memory staging buffer ([64 columns][128 rows])
+        // and a TMA reduce-add into A22 in L2, so no thread waits on a load of A22.
         const int q = warp & 3;  // TMEM lane quarter of this warp
-        int it = 0;
-        for (int t = blockIdx.x; t < args.tiles && !*abort_flag; t += gridDim.x, ++it) {
+        const int R = q * 32 + lane;
+        const bool issuer = (warp == 2 && lane == 0);
+        volatile int* s_go = abort_flag + 1;  // the issuer's wait result, shared by the 4 warps
+        int it = 0, e = 0;
+        for (int t = blockIdx.x; t < args.tiles; t += gridDim.x, ++it) {
             int acc = it & 1;
             uint32_t aph = (it >> 1) & 1;
-            if (!mbar_wait(bar(TFULL + acc), aph, abort_flag)) break;
+            // one thread waits (bounded) and the four warps take its decision together, so a
+            // time-out cannot leave some of them at the named barrier
+            if (issuer) *s_go = (!*abort_flag && mbar_wait(bar(TFULL + acc), aph, abort_flag)) ? 1 : 0;
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (!*s_go) break;
             fence_after();
             int tm, tn;
             tile_coords(t, args.tiles_m, args.tiles_n, tm, tn);
-            int R = tm * TB_M + q * 32 + lane;
-            bool row_ok = R < args.m2;
-            float* crow = args.C + (size_t)(args.row0 + R);
-            for (int cb = 0; cb < TB_N / 32; ++cb) {
-                float v[32];
-                uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * TB_N + cb * 32);
-                tmem_ld32(taddr, v);
-                int c0 = tn * TB_N + cb * 32;
-                if (row_ok) {
-                    // all 32 loads first, then the stores: keeps 32 loads in flight per thread
-                    float old[32];
-                    float* p0 = crow + (size_t)(args.col0 + c0) * args.ldc;
-                    int ncol = min(32, args.ncols - c0);
-                    if (ncol == 32) {
+            for (int sub = 0; sub < TB_N / EPI_COLS; ++sub, ++e) {
+                const int buf = e & 1;
+                if (issuer) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+                float* stage = epi + buf * (TB_M * EPI_COLS);
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) old[j] = __ldcs(p0 + (size_t)j * args.ldc);
+                for (int cb = 0; cb < EPI_COLS / 32; ++cb) {
+                    float v[32];
+                    uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) +
+                                     (uint32_t)(acc * TB_N + sub * EPI_COLS + cb * 32);
+                    tmem_ld32(taddr, v);
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) __stcs(p0 + (size_t)j * args.ldc, old[j] - v[j]);
-                    } else {
-                        for (int j = 0; j < ncol; ++j) old[j] = __ldcs(p0 + (size_t)j * args.ldc);
-                        for (int j = 0; j < ncol; ++j) __stcs(p0 + (size_t)j * args.ldc, old[j] - v[j]);
-                    }
+                    for (int jj = 0; jj < 32; ++jj) stage[(cb * 32 + jj) * TB_M + R] = -v[jj];
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+                if (issuer) {
+                    int x = args.row0 + tm * TB_M, y = args.col0 + tn * TB_N + sub * EPI_COLS;
+                    asm volatile(
+                        "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                            (uint64_t)&mC),
+                        "r"(x), "r"(y), "r"(epi_smem + buf * EPI_BYTES)
+                        : "memory");
+                    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
                 }
             }
             fence_before();
             mbar_arrive(bar(TEMPTY + acc));
         }
+        if (issuer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
     }
     __syncthreads();
     if (*abort_flag && threadIdx.x == 0) atomicExch(args.status, 8);
@@ -406,41 +423,84 @@ bool tf32_enabled() {
     return on == 1;
 }
 
-// N = L11^-1 - I for the unit lower w x w diagonal block of the panel (FP32, in place in
-// shared memory, columns right to left: X[i][j] = -sum_{k=j+1..i} X[i][k] L[k][j]), stored
-// column-major w x w. U12 = L11^-1 A12 = A12 + N A12 then runs as a tensor-core update.
+// N = L11^-1 - I for the unit lower w x w (w <= 128) diagonal block of the panel, in FP32
+// in shared memory, by recursive doubling: the eight 16 x 16 diagonal blocks are inverted
+// by one warp each (columns right to left), then pairs of inverted blocks [A 0; B C] are
+// joined level by level (s = 16, 32, 64) with the lower-left block -C^-1 B A^-1 formed as
+// two small dense products. M holds the strictly lower part; unit diagonals are implicit.
+// Stored column-major w x w. U12 = L11^-1 A12 = A12 + N A12 then runs on the tensor cores.
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
 __global__ void __launch_bounds__(256) tri_inverse_l_kernel(const float2* __restrict__ A, size_t lda, int k0, int w,
                                                             float2* __restrict__ N) {
     extern __shared__ float2 ti_smem[];
     const int LD = 129;
-    float2* M = ti_smem;            // M[i * LD + k]
-    float2* col = ti_smem + 128 * LD;
-    for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
-        int i = idx % w, k = idx / w;
-        M[i * LD + k] = (i > k) ? A[(size_t)(k0 + k) * lda + k0 + i] : make_float2(0.f, 0.f);
+    float2* M = ti_smem;             // M[i * LD + k], 128 x 128
+    float2* T = ti_smem + 128 * LD;  // 64 x 64 scratch
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int idx = tid; idx < 128 * 128; idx += blockDim.x) {
+        int i = idx % 128, k = idx / 128;
+        M[i * LD + k] = (i > k && i < w && k < w) ? A[(size_t)(k0 + k) * lda + k0 + i] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    const int i = threadIdx.x;
-    for (int j = w - 2; j >= 0; --j) {
-        if (i < w) col[i] = M[i * LD + j];
-        __syncthreads();
-        if (i < w && i > j) {
-            float sr = col[i].x, si = col[i].y;  // k = i term: X[i][i] = 1
-            for (int k = j + 1; k < i; ++k) {
-                float2 x = M[i * LD + k], l = col[k];
-                sr += x.x * l.x - x.y * l.y;
-                si += x.x * l.y + x.y * l.x;
+    // 16 x 16 diagonal blocks: X[i][j] = -sum_{k=j+1..i} X[i][k] L[k][j], X[i][i] = 1
+    {
+        __shared__ float2 colbuf[8][16];
+        const int o = warp * 16;
+        for (int j = 14; j >= 0; --j) {
+            if (lane < 16) colbuf[warp][lane] = M[(o + lane) * LD + o + j];
+            __syncwarp();
+            if (lane < 16 && lane > j) {
+                int i = lane;
+                float2 sum = colbuf[warp][i];  // k = i term
+                for (int k = j + 1; k < i; ++k) {
+                    float2 l = colbuf[warp][k], x = M[(o + i) * LD + o + k];
+                    sum.x += x.x * l.x - x.y * l.y;
+                    sum.y += x.x * l.y + x.y * l.x;
+                }
+                M[(o + i) * LD + o + j] = make_float2(-sum.x, -sum.y);
             }
-            M[i * LD + j] = make_float2(-sr, -si);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // join pairs: [A 0; B C]^-1 lower-left = -Cinv (B Ainv)
+    for (int s = 16; s < 128; s *= 2) {
+        const int pairs = 128 / (2 * s);
+        // T = B Ainv for every pair (pair p stores at T + p * s * s)
+        for (int idx = tid; idx < pairs * s * s; idx += blockDim.x) {
+            int p = idx / (s * s), e = idx % (s * s), i = e / s, k = e % s;
+            int a0 = p * 2 * s, c0 = a0 + s;
+            float2 sum = M[(c0 + i) * LD + a0 + k];  // m = k, Ainv diagonal 1
+            for (int m = k + 1; m < s; ++m) {
+                float2 b = M[(c0 + i) * LD + a0 + m], x = M[(a0 + m) * LD + a0 + k];
+                sum.x += b.x * x.x - b.y * x.y;
+                sum.y += b.x * x.y + b.y * x.x;
+            }
+            T[p * s * s + i * s + k] = sum;
+        }
+        __syncthreads();
+        // lower-left = -(Cinv T)
+        for (int idx = tid; idx < pairs * s * s; idx += blockDim.x) {
+            int p = idx / (s * s), e = idx % (s * s), i = e / s, k = e % s;
+            int a0 = p * 2 * s, c0 = a0 + s;
+            float2 sum = T[p * s * s + i * s + k];  // m = i, Cinv diagonal 1
+            for (int m = 0; m < i; ++m) {
+                float2 c = M[(c0 + i) * LD + c0 + m], t = T[p * s * s + m * s + k];
+                sum.x += c.x * t.x - c.y * t.y;
+                sum.y += c.x * t.y + c.y * t.x;
+            }
+            M[(c0 + i) * LD + a0 + k] = make_float2(-sum.x, -sum.y);
         }
         __syncthreads();
     }
-    for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+    for (int idx = tid; idx < w * w; idx += blockDim.x) {
         int ii = idx % w, k = idx / w;
         N[(size_t)k * w + ii] = M[ii * LD + k];
     }
 }
-constexpr size_t TI_SMEM = (size_t)(128 * 129 + 128) * sizeof(float2);
+constexpr size_t TI_SMEM = (size_t)(128 * 129 + 64 * 64) * sizeof(float2);
 
 size_t tf32_pack_bytes(int n) {
     size_t kp = 256;
@@ -477,6 +537,18 @@ static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, in
     CUtensorMap mAhi, mAlo, mBhi, mBlo;
     bool ok = make_map(&mAhi, ahi, m2, kp, TB_M) && make_map(&mAlo, alo, m2, kp, TB_M) &&
               make_map(&mBhi, bhi, ncols, kp, TB_N) && make_map(&mBlo, blo, ncols, kp, TB_N);
+    // A viewed as a 2n x n float matrix (column-major): box of 128 real rows x 64 columns
+    CUtensorMap mC;
+    {
+        EncodeTiled enc = encoder();
+        cuuint64_t dims[2] = {(cuuint64_t)2 * n, (cuuint64_t)n};
+        cuuint64_t strides[1] = {(cuuint64_t)2 * n * 4};
+        cuuint32_t box[2] = {(cuuint32_t)TB_M, (cuuint32_t)EPI_COLS};
+        cuuint32_t estr[2] = {1, 1};
+        ok = ok && enc && enc(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)A, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    }
     if (!ok) {
         cudaMemsetAsync(wk.status, 7, 1, st);
         return;
@@ -494,7 +566,7 @@ static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, in
     a.tiles = a.tiles_m * a.tiles_n;
     a.status = wk.status;
     int grid = std::min(num_sms(), a.tiles);
-    tf32_update_kernel<<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, a);
+    tf32_update_kernel<<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
     *launches += 1;
 }
 

@@ -111,6 +111,7 @@ void lu_solve_fp64(const double2* A, int n, const int* perm, const double2* inv,
 void lu_solve_fp32(const float2* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp, int ncol,
                    cudaStream_t st, long long* launches);
 size_t lu_workspace_bytes(int n, bool fp32);
+size_t tf32_pack_bytes(int n);  // packed tensor-core operands of the mixed LU
 void lu_init_attributes();
 
 // blas.cu — fixed-order reductions and vector updates on FP64 complex vectors

@@ -102,20 +102,57 @@ __device__ __forceinline__ double cx_abs2(typename Cx<R>::T a) {
 }
 
 // ---- panel factorization ------------------------------------------------------------------
+// Per column every CTA publishes its best local candidate row, folds its candidate key
+//   [|a|^2 as FP32 bits : 32][0xFFFFFFFF - row : 32]
+// into one 64-bit atomicMax word (three words cycle over the columns), and arrives at a grid
+// barrier (fire-and-forget release add on a counter that only grows; relaxed polls with a
+// short back-off keep the counter's L2 line lightly loaded). After the barrier every CTA
+// reads the winning key and the pivot row: the largest |a| with ties to the lower row.
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ bool column_barrier(unsigned* bar, unsigned target, int* status) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        __threadfence();
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
+        if (ld_relaxed_u32(bar) < target) {
+            unsigned long long t0 = global_ns();
+            unsigned spins = 0;
+            while (ld_relaxed_u32(bar) < target) {
+                __nanosleep(20);
+                if ((++spins & 255u) == 0) {
+                    if (*(volatile int*)status == 8 || global_ns() - t0 > 4000000000ull) {
+                        atomicExch(status, 8);
+                        ok = 0;
+                        break;
+                    }
+                }
+            }
+        }
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 template <typename R, int NB>
 __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t lda, int k0, int n, int w,
-                                                    int chunk, int* piv, int* perm, Cand* cand,
+                                                    int chunk, int* piv, int* perm, unsigned long long* keys,
                                                     typename Cx<R>::T* crow, typename Cx<R>::T* drow, unsigned* bar,
                                                     int* status) {
     typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tile = (C*)smem_raw;                      // chunk x (NB + 1)
     C* prow = tile + (size_t)chunk * (NB + 1);   // NB
-    __shared__ double s_val[8];
+    __shared__ float s_val[8];
     __shared__ int s_row[8];
-    __shared__ double s_bval;
-    __shared__ int s_brow, s_bcta;
-    unsigned long long* keys = (unsigned long long*)cand;  // 3 pivot keys, cycled per column
+    __shared__ unsigned long long s_win;
     const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int rows = n - k0;
@@ -127,22 +164,19 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
         tile[(size_t)r * LD + c] = A[(size_t)(k0 + c) * lda + row0 + r];
     }
     __syncthreads();
+    // candidate of this thread's rows for column 0
+    float bv = -1.f;
+    int br = 0x7fffffff;
+    for (int r = tid; r < myrows; r += blockDim.x) {
+        float v = (float)cx_abs2<R>(tile[(size_t)r * LD]);
+        if (v > bv) {
+            bv = v;
+            br = row0 + r;
+        }
+    }
     for (int j = 0; j < w; ++j) {
         const int gj = k0 + j;
         const int buf = j & 1;
-        // Local candidate: the largest |a|^2 (as FP32 bits; ties to the lower row), packed as
-        // (bits << 32) | ~row so that one 64-bit atomicMax across the CTAs picks the pivot.
-        float bv = -1.f;
-        int br = 0x7fffffff;
-        for (int r = tid; r < myrows; r += blockDim.x) {
-            int g = row0 + r;
-            if (g < gj) continue;
-            float v = (float)cx_abs2<R>(tile[(size_t)r * LD + j]);
-            if (v > bv || (v == bv && g < br)) {
-                bv = v;
-                br = g;
-            }
-        }
         for (int o = 16; o > 0; o >>= 1) {
             float ov = __shfl_xor_sync(0xffffffffu, bv, o);
             int orr = __shfl_xor_sync(0xffffffffu, br, o);
@@ -156,43 +190,47 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
             s_row[warp] = br;
         }
         __syncthreads();
-        if (tid == 0) {
-            float v = (float)s_val[0];
-            int rr = s_row[0];
-            for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
-                if ((float)s_val[q] > v || ((float)s_val[q] == v && s_row[q] < rr)) {
-                    v = (float)s_val[q];
-                    rr = s_row[q];
-                }
-            s_bval = v;
-            s_brow = rr;
-        }
-        __syncthreads();
-        if (s_bval >= 0.0) {
-            int lr = s_brow - row0;
-            for (int c = tid; c < w; c += blockDim.x) __stcg(&crow[((size_t)buf * P + b) * NB + c], tile[(size_t)lr * LD + c]);
-            if (tid == 0) {
-                unsigned long long key = ((unsigned long long)__float_as_uint((float)s_bval) << 32) |
-                                         (unsigned long long)(0xFFFFFFFFu - (unsigned)s_brow);
-                atomicMax(&keys[j % 3], key);
+        float cv = s_val[0];
+        int crr = s_row[0];
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
+            if (s_val[q] > cv || (s_val[q] == cv && s_row[q] < crr)) {
+                cv = s_val[q];
+                crr = s_row[q];
             }
+        const bool has = cv >= 0.f;
+        if (has) {
+            int lr = crr - row0;
+            for (int c = tid; c < w; c += blockDim.x) __stcg(&crow[((size_t)buf * P + b) * NB + c], tile[(size_t)lr * LD + c]);
         }
         if (gj >= row0 && gj < row0 + myrows) {
             int lr = gj - row0;
             for (int c = tid; c < w; c += blockDim.x) __stcg(&drow[(size_t)buf * NB + c], tile[(size_t)lr * LD + c]);
         }
-        if (!grid_sync(bar, P, status)) return;
-        // every thread reads the winning key and its share of the pivot row
+        if (tid == 0 && has) {
+            unsigned long long kv = ((unsigned long long)__float_as_uint(cv) << 32) |
+                                    (unsigned long long)(0xFFFFFFFFu - (unsigned)crr);
+            asm volatile("red.relaxed.gpu.global.max.u64 [%0], %1;" ::"l"(&keys[j % 3]), "l"(kv) : "memory");
+        }
+        if (!column_barrier(bar, (unsigned)(j + 1) * (unsigned)P, status)) return;
+        // The winning key and, speculatively, the diagonal row in one round trip: when the
+        // pivot is the diagonal row (no interchange) the pivot row is already here.
         const unsigned long long key = __ldcg(&keys[j % 3]);
+        C dv;
+        dv.x = 0;
+        dv.y = 0;
+        if (tid < w) dv = __ldcg(&drow[(size_t)buf * NB + tid]);
+        if (b == 0 && tid == 0) {
+            // the word of column j-1, read by every CTA before this barrier
+            *(volatile unsigned long long*)&keys[(j + 2) % 3] = 0ull;
+        }
         const int pr = (int)(0xFFFFFFFFu - (unsigned)(key & 0xFFFFFFFFull));
         const int owner = (pr - k0) / chunk;
-        for (int c = tid; c < w; c += blockDim.x) prow[c] = __ldcg(&crow[((size_t)buf * P + owner) * NB + c]);
-        if (b == 0 && tid == 0) atomicExch(&keys[(j + 2) % 3], 0ull);  // slot of column j-1, read before this barrier
+        if (tid < w) prow[tid] = (pr == gj) ? dv : __ldcg(&crow[((size_t)buf * P + owner) * NB + tid]);
         __syncthreads();
         if (pr != gj) {
             if (pr >= row0 && pr < row0 + myrows) {
                 int lr = pr - row0;
-                for (int c = tid; c < w; c += blockDim.x) tile[(size_t)lr * LD + c] = __ldcg(&drow[(size_t)buf * NB + c]);
+                if (tid < w) tile[(size_t)lr * LD + tid] = dv;
             }
             if (gj >= row0 && gj < row0 + myrows) {
                 int lr = gj - row0;
@@ -200,38 +238,56 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
             }
         }
         if (b == 0 && tid == 0) {
-            piv[gj] = pr;
-            if (pr != gj) {
-                int a = perm[gj];
-                perm[gj] = perm[pr];
-                perm[pr] = a;
-            }
+            piv[gj] = pr;  // the row permutation is composed from piv after the factorization
             C pvt = prow[j];
             if (!((double)pvt.x * pvt.x + (double)pvt.y * pvt.y > 0.0)) atomicCAS(status, 0, 5);
         }
         __syncthreads();
-        // rank-1 update of the rows below the pivot
+        // rank-1 update of the rows below the pivot; each thread keeps its next candidate
         C pivot = prow[j];
         double den = (double)pivot.x * pivot.x + (double)pivot.y * pivot.y;
-        if (den > 0.0) {
-            double ir = pivot.x / den, ii = -pivot.y / den;  // 1 / pivot
-            for (int r = tid; r < myrows; r += blockDim.x) {
-                int g = row0 + r;
-                if (g <= gj) continue;
-                C a = tile[(size_t)r * LD + j];
-                R lr_ = (R)(a.x * ir - a.y * ii), li_ = (R)(a.x * ii + a.y * ir);
-                C l;
-                l.x = lr_;
-                l.y = li_;
-                tile[(size_t)r * LD + j] = l;
-                for (int c = j + 1; c < w; ++c) {
-                    C u = prow[c];
-                    C& t = tile[(size_t)r * LD + c];
-                    t.x = t.x - (l.x * u.x - l.y * u.y);
-                    t.y = t.y - (l.x * u.y + l.y * u.x);
+        double ir = den > 0.0 ? pivot.x / den : 0.0, ii = den > 0.0 ? -pivot.y / den : 0.0;
+        // Multipliers first (one thread per row), then the update as independent (row, 32-column
+        // chunk) items so every thread has a run of independent shared-memory updates; the item
+        // holding column j+1 tracks the next column's candidate.
+        bv = -1.f;
+        br = 0x7fffffff;
+        const int first = max(0, gj + 1 - row0);  // first local row below the pivot
+        for (int r = first + tid; r < myrows; r += blockDim.x) {
+            C a = tile[(size_t)r * LD + j];
+            C l;
+            l.x = (R)(a.x * ir - a.y * ii);
+            l.y = (R)(a.x * ii + a.y * ir);
+            if (den > 0.0) tile[(size_t)r * LD + j] = l;
+        }
+        __syncthreads();
+        const int act = myrows - first;
+        const int q0 = (j + 1) >> 5, nq = ((w + 31) >> 5) - q0;
+        if (act > 0 && j + 1 < w)
+            for (int item = tid; item < act * nq; item += blockDim.x) {
+                int r = first + item % act, q = q0 + item / act;
+                C* trow = tile + (size_t)r * LD;
+                int c0 = max(j + 1, q * 32), c1 = min(w, q * 32 + 32);
+                if (den > 0.0) {
+                    C l = trow[j];
+#pragma unroll 8
+                    for (int c = c0; c < c1; ++c) {
+                        C u = prow[c];
+                        C t = trow[c];
+                        t.x = t.x - (l.x * u.x - l.y * u.y);
+                        t.y = t.y - (l.x * u.y + l.y * u.x);
+                        trow[c] = t;
+                    }
+                }
+                if (q == q0) {
+                    float v = (float)cx_abs2<R>(trow[j + 1]);
+                    int g = row0 + r;
+                    if (v > bv || (v == bv && g < br)) {
+                        bv = v;
+                        br = g;
+                    }
                 }
             }
-        }
         __syncthreads();
     }
     for (int idx = tid; idx < myrows * w; idx += blockDim.x) {
@@ -530,20 +586,34 @@ static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cud
     int chunk = (rows + P - 1) / P;
     size_t smem = panel_smem<R, NB>(chunk);
     if (smem > 220 * 1024) return 1;
-    Cand* cand = (Cand*)wk.cand;
-    C* crow = (C*)(cand + 2 * 160);
+    unsigned long long* keys = (unsigned long long*)wk.cand;  // 3 pivot words
+    C* crow = (C*)(keys + 2 * 160);
     C* drow = crow + 2 * 160 * NB;
+    cudaMemsetAsync(keys, 0, 4 * sizeof(unsigned long long), st);
     cudaMemsetAsync(wk.barrier, 0, 2 * sizeof(unsigned), st);
-    cudaMemsetAsync(cand, 0, 3 * sizeof(unsigned long long), st);
     size_t lda = (size_t)n;
-    void* args[] = {&A, &lda, &k0, &n, &w, &chunk, &wk.piv, &wk.perm, &cand, &crow, &drow, &wk.barrier, &wk.status};
+    void* args[] = {&A, &lda, &k0, &n, &w, &chunk, &wk.piv, &wk.perm, &keys, &crow, &drow, &wk.barrier, &wk.status};
     cudaError_t e = cudaLaunchCooperativeKernel((void*)panel_kernel<R, NB>, dim3(P), dim3(256), args, smem, st);
     return e == cudaSuccess ? 0 : 2;
 }
 
-__global__ void iota_kernel(int* p, int n) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = i;
+// perm from the interchanges: perm = iota, then swap perm[k] <-> perm[piv[k]] for k = 0..n-1
+// in shared memory (one CTA; row i of P A is row perm[i] of A).
+__global__ void perm_from_piv_kernel(const int* __restrict__ piv, int* __restrict__ perm, int n) {
+    extern __shared__ int pm[];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) pm[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < n; ++k) {
+            int p = piv[k];
+            if (p != k) {
+                int t = pm[k];
+                pm[k] = pm[p];
+                pm[p] = t;
+            }
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = pm[i];
 }
 
 void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches);
@@ -554,8 +624,6 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
                           bool tensor_cores) {
     typedef typename Cx<R>::T C;
     lu_init_attributes();
-    iota_kernel<<<(n + 255) / 256, 256, 0, st>>>(wk.perm, n);
-    ++*launches;
     size_t lda = n;
     for (int k0 = 0; k0 < n; k0 += NB) {
         int w = std::min(NB, n - k0);
@@ -597,6 +665,16 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
                 ++*launches;
             }
         }
+    }
+    {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(perm_from_piv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            attr = true;
+        }
+        StageScope sc(ST_SWAP, st);
+        perm_from_piv_kernel<<<1, 1024, (size_t)n * sizeof(int), st>>>(wk.piv, wk.perm, n);
+        ++*launches;
     }
     return 0;
 }

@@ -101,72 +101,94 @@ __global__ void gather_kernel(const double2* __restrict__ x, double2* __restrict
 }
 
 // One block step: sol_b = Dinv_b r_b; r[other rows] -= A[other rows, block] sol_b.
+// Every load that does not depend on the block solution (the Dinv quarter of each thread,
+// the right-hand side block, the first half of the thread's row of the block column) is
+// issued up front, so a step costs about two memory round trips.
 template <typename C, bool LOWER, int NC>
 __global__ void __launch_bounds__(256) trsv_inv_step_kernel(const C* __restrict__ A, size_t lda, int n, int b0, int bw,
                                                             const double2* __restrict__ dinv, double2* __restrict__ r,
                                                             double2* __restrict__ sol) {
     __shared__ double2 rb[NC][SB];
+    __shared__ double2 part[4][NC][SB];
     __shared__ double2 xb[NC][SB];
-    for (int idx = threadIdx.x; idx < SB * NC; idx += blockDim.x) {
-        int i = idx % SB, c = idx / SB;
-        rb[c][i] = i < bw ? r[(size_t)c * n + b0 + i] : make_double2(0.0, 0.0);
+    constexpr int KH = 16;  // preloaded first chunk of the block column
+    const int tid = threadIdx.x;
+    const int i = tid % SB, kq = tid / SB;  // Dinv row and K quarter
+    double2 d[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) d[u] = dinv[(size_t)(kq * 16 + u) * SB + i];
+    const int lo = LOWER ? b0 + bw : 0, hi = LOWER ? n : b0;
+    const int row = lo + blockIdx.x * blockDim.x + tid;
+    const bool has_row = row < hi;
+    C av[KH];
+#pragma unroll
+    for (int u = 0; u < KH; ++u) {
+        if (has_row && u < bw)
+            av[u] = A[(size_t)(b0 + u) * lda + row];
+        else {
+            av[u].x = 0;
+            av[u].y = 0;
+        }
+    }
+    for (int idx = tid; idx < SB * NC; idx += blockDim.x) {
+        int ii = idx % SB, c = idx / SB;
+        rb[c][ii] = ii < bw ? r[(size_t)c * n + b0 + ii] : make_double2(0.0, 0.0);
     }
     __syncthreads();
-    // x_b = Dinv r_b: thread (row i, column group g) over the 64 columns of Dinv
-    {
-        const int i = threadIdx.x % SB, g = threadIdx.x / SB;  // 4 groups
-        double2 acc[(NC + 3) / 4];
 #pragma unroll
-        for (int q = 0; q < (NC + 3) / 4; ++q) acc[q] = make_double2(0.0, 0.0);
-#pragma unroll 8
-        for (int k = 0; k < SB; ++k) {
-            double2 d = dinv[(size_t)k * SB + i];
+    for (int c = 0; c < NC; ++c) {
+        double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-            for (int q = 0; q < (NC + 3) / 4; ++q) {
-                int c = g + 4 * q;
-                if (c < NC) {
-                    double2 v = rb[c][k];
-                    acc[q].x += d.x * v.x - d.y * v.y;
-                    acc[q].y += d.x * v.y + d.y * v.x;
-                }
-            }
+        for (int u = 0; u < 16; ++u) {
+            double2 v = rb[c][kq * 16 + u];
+            acc.x += d[u].x * v.x - d[u].y * v.y;
+            acc.y += d[u].x * v.y + d[u].y * v.x;
         }
+        part[kq][c][i] = acc;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < SB * NC; idx += blockDim.x) {
+        int ii = idx % SB, c = idx / SB;
+        double2 s = part[0][c][ii];
 #pragma unroll
-        for (int q = 0; q < (NC + 3) / 4; ++q) {
-            int c = g + 4 * q;
-            if (c < NC) xb[c][i] = acc[q];
+        for (int q = 1; q < 4; ++q) {
+            s.x += part[q][c][ii].x;
+            s.y += part[q][c][ii].y;
         }
+        xb[c][ii] = s;
     }
     __syncthreads();
     if (blockIdx.x == 0)
-        for (int idx = threadIdx.x; idx < bw * NC; idx += blockDim.x) {
-            int i = idx % bw, c = idx / bw;
-            sol[(size_t)c * n + b0 + i] = xb[c][i];
+        for (int idx = tid; idx < bw * NC; idx += blockDim.x) {
+            int ii = idx % bw, c = idx / bw;
+            sol[(size_t)c * n + b0 + ii] = xb[c][ii];
         }
-    int lo = LOWER ? b0 + bw : 0, hi = LOWER ? n : b0;
-    constexpr int KU = 16;
-    for (int row = lo + blockIdx.x * blockDim.x + threadIdx.x; row < hi; row += gridDim.x * blockDim.x) {
+    // rows beyond the first pass of the grid (n > 148 * 256) load their first chunk here too
+    for (int rr = row; rr < hi; rr += gridDim.x * blockDim.x) {
+        const bool first = rr == row;
         double2 acc[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) acc[c] = make_double2(0, 0);
-        for (int k0 = 0; k0 < bw; k0 += KU) {
-            C v[KU];
+#pragma unroll 1
+        for (int kc = 0; kc < SB; kc += KH) {
+            C v[KH];
 #pragma unroll
-            for (int u = 0; u < KU; ++u) {
-                if (k0 + u < bw)
-                    v[u] = A[(size_t)(b0 + k0 + u) * lda + row];
+            for (int u = 0; u < KH; ++u) {
+                if (kc == 0 && first)
+                    v[u] = av[u];
+                else if (kc + u < bw)
+                    v[u] = A[(size_t)(b0 + kc + u) * lda + rr];
                 else {
                     v[u].x = 0;
                     v[u].y = 0;
                 }
             }
 #pragma unroll
-            for (int u = 0; u < KU; ++u) {
+            for (int u = 0; u < KH; ++u) {
                 double lr = v[u].x, li = v[u].y;
-                int k = min(k0 + u, SB - 1);
 #pragma unroll
                 for (int c = 0; c < NC; ++c) {
-                    double2 x = xb[c][k];
+                    double2 x = xb[c][kc + u];
                     acc[c].x += lr * x.x - li * x.y;
                     acc[c].y += lr * x.y + li * x.x;
                 }
@@ -174,7 +196,7 @@ __global__ void __launch_bounds__(256) trsv_inv_step_kernel(const C* __restrict_
         }
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-            double2* p = r + (size_t)c * n + row;
+            double2* p = r + (size_t)c * n + rr;
             double2 v = *p;
             v.x -= acc[c].x;
             v.y -= acc[c].y;
