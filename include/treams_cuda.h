@@ -134,6 +134,17 @@ tcu_status tcu_cluster_operator(tcu_context* ctx, int lmax, double k0, size_t N,
 /* y = (I - T C) x for p columns without forming C (cluster/iterative.rs:225-232). */
 tcu_status tcu_cluster_apply(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii, const double* eps,
                              const double* positions, int p, const double* x, double* y);
+/* Allocation-free y = (I - T C) x (no counterpart in the reference; for callers that cannot
+ * allocate device memory, e.g. inside another framework's memory plan). Every pointer is a
+ * device pointer (radii N doubles, eps N complex, positions 3 N doubles, x and y n x p
+ * complex); the call runs on `stream` (a cudaStream_t, may be NULL) and needs no context.
+ * Scratch (plan tables, Mie blocks, a status word) lives in one 8 MiB static device array
+ * per GPU: the plan plus N * lmax * 64 bytes must fit, larger clusters are rejected with
+ * TCU_INVALID_INPUT. The first call on a device looks up that array's address; make it
+ * before any stream capture. Calls that overlap on the GPU race on the shared array. The
+ * call synchronises `stream` (geometry check and status read). Errors: tcu_last_error_message(). */
+tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k0, size_t N, const double* radii,
+                                     const double* eps, const double* positions, int p, const double* x, double* y);
 /* Restarted GMRES on (I - T C) X = T B (cluster/iterative.rs:264-284, linalg/gmres.rs:119).
  * The preconditioner, if any, is applied on the right; certificates report the true
  * unpreconditioned residual. */

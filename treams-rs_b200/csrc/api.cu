@@ -78,6 +78,7 @@ struct DevPlanStore {
 
 namespace tcu {
 thread_local Profiler* g_prof = nullptr;
+void set_error_message(const char* msg) { g_last_error = msg; }
 }
 
 struct tcu_context {

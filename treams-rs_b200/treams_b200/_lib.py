@@ -55,6 +55,7 @@ SIGNATURES = {
     "tcu_factor_destroy": (c_int, [P]),
     "tcu_cluster_operator": (c_int, [P, c_int, c_double, c_size, P, P, P, P]),
     "tcu_cluster_apply": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, P]),
+    "tcu_cluster_apply_noalloc": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, P]),
     "tcu_iterative_solve": (c_int, [P, c_int, c_double, c_size, P, P, P, P, c_int, P, c_int, P, P]),
     "tcu_lsumsw2d_batch": (c_int, [P, c_int, c_double, P, c_size, P, c_double, P]),
     "tcu_array_solve_batch": (c_int, [P, c_int, c_double, c_double, P, P, c_size, P, c_double, P]),
