@@ -3,9 +3,11 @@
 Workload: the 512-sphere, lmax-4 precision cluster (n = 24,576 unknowns, three plane-wave
 incidences), seeded synthetic geometry. One step = assemble I - T C, factor it and solve
 the three columns to an FP64 residual <= 1e-13 |T b| (relative error well below 1e-10):
-`tcu_sphere_cluster_factor_dev` + `tcu_factor_solve_dev`. The default is the mixed
-path (complex64 LU with split-TF32 tensor-core trailing updates + FP64 refinement);
-`--precision fp64` times the plain FP64 drop-in.
+`tcu_sphere_cluster_factor_dev` + `tcu_factor_solve_dev`. The headline is the mixed
+path (complex64 LU with split-TF32 tensor-core trailing updates + FP64 refinement); the
+same run then times the plain FP64 drop-in on the same inputs (`fp64` and
+`speedup_vs_fp64` in the JSON line, `--no-compare` skips it). `--precision fp64` makes
+the FP64 path the headline.
 
 value: solves/s with inputs resident in HBM, device-timed with CUDA events on the library
 stream (max over ranks). e2e: the same through the host-buffer C ABI with host<->device
@@ -33,6 +35,26 @@ import numpy as np  # noqa: E402
 
 METRIC = "cluster-solve/s, 512 spheres lmax 4: mixed+learned vs plain FP64 @1e-10 err"
 UNIT = "solves/s"
+
+
+FP64_TENSOR_PEAK = 40.0  # TFLOP/s, nominal B200 FP64 tensor-core rate
+
+# DRAM traffic of the trailing-update kernel relative to its algorithmic bytes (the
+# complex64 C block read and written once, 16 m^2 bytes), from an ncu capture of the
+# m = 11,776 launch of a 256-sphere solve: 2.395 GB measured for 2.219 GB algorithmic.
+# Traffic grows with m^2 like the algorithmic bytes, so the bench scales this ratio to the
+# average launch of the measured workload.
+TF32_TRAFFIC = {"ratio": 2.395 / 2.219,
+                "note": "dram__bytes_read.sum + dram__bytes_write.sum of tf32_update_kernel per launch: "
+                        "ncu ratio to algorithmic bytes (1.08, m=11776 launch of a 256-sphere solve) "
+                        "x the average algorithmic bytes 16 m^2 of this workload's launches"}
+
+
+def update_launch_bytes(n: int, nb: int) -> float:
+    """Average algorithmic bytes (complex64 C read + write) per trailing-update launch."""
+    sizes = [n - k0 - min(nb, n - k0) for k0 in range(0, n, nb)]
+    sizes = [m for m in sizes if m > 0]
+    return sum(16.0 * m * m for m in sizes) / len(sizes)
 
 
 def peaks():
@@ -149,6 +171,10 @@ def main() -> None:
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--spheres", type=int, default=512)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", dest="compare", action="store_false",
+                    help="skip the plain FP64 comparison arm of the mixed headline")
+    ap.add_argument("--compare-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -172,8 +198,6 @@ def main() -> None:
             dist.destroy_process_group()
         return
 
-    import ctypes
-
     import torch
     import treams_b200 as t
     from treams_b200 import _lib, workloads
@@ -183,8 +207,54 @@ def main() -> None:
     lib = _lib.lib()
     stream = torch.cuda.ExternalStream(ctx.stream)
     w = workloads.precision_cluster(count=args.spheres)
-    prec = t.MIXED if args.precision == "mixed" else t.FP64
     dev = torch.device("cuda", local)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def reduce_max(vals):
+        if not dist:
+            return vals
+        tt = torch.tensor(vals, dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return [float(v) for v in tt]
+
+    def measure(precision, steps, warmup, with_e2e):
+        return _measure_impl(args, precision, steps, warmup, with_e2e, ctx=ctx, lib=lib, stream=stream, w=w,
+                             dev=dev, world=world, local=local, dist=dist, barrier=barrier, reduce_max=reduce_max)
+
+    head = measure(args.precision, args.steps, args.warmup, not args.no_e2e)
+    other = None
+    if args.compare and args.precision == "mixed":
+        other = measure("fp64", min(args.steps, args.compare_steps), 1, False)
+    if rank == 0:
+        line = head["line"]
+        if other is not None:
+            o = other["line"]
+            line["fp64"] = {"value": o["value"], "ms_per_step": o["ms_per_step"], "steps": o["steps"],
+                            "warmup": o["warmup"], "max_rel_residual": o["max_rel_residual"],
+                            "roofline": o["roofline"], "stages_ms_per_step": o["stages_ms_per_step"],
+                            "gpu_launches": o["gpu_launches"]}
+            line["speedup_vs_fp64"] = line["value"] / o["value"]
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_reference(1, os.cpu_count() or 1)
+            line["cpu_baseline"].pop("seconds_per_solve_full_size", None)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def _measure_impl(args, precision, steps, warmup, with_e2e, *, ctx, lib, stream, w, dev, world, local, dist,
+                  barrier, reduce_max):
+    import ctypes
+
+    import torch
+    import treams_b200 as t
+    from treams_b200 import _lib
+
+    prec = t.MIXED if precision == "mixed" else t.FP64
     r_d = torch.tensor(w.radii, dtype=torch.float64, device=dev)
     e_d = torch.view_as_real(torch.tensor(w.eps, dtype=torch.complex128, device=dev)).contiguous()
     x_d = torch.tensor(w.positions, dtype=torch.float64, device=dev).contiguous()
@@ -218,13 +288,9 @@ def main() -> None:
         _lib._check(lib.tcu_factor_solve(h, B_pin.data_ptr(), p, X_pin.data_ptr(), certs))
         lib.tcu_factor_destroy(h)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step_device()
     torch.cuda.synchronize()
-
-    def barrier():
-        if dist:
-            dist.barrier()
 
     # device-resident timing with stage events
     ctx.reset_stage_times()
@@ -235,7 +301,7 @@ def main() -> None:
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         step_device()
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -248,63 +314,58 @@ def main() -> None:
     worst = max(c.residual_norm / c.rhs_norm for c in certs)
 
     # end-to-end through the host-buffer ABI
-    step_host()
-    torch.cuda.synchronize()
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
+    ms_e2e = None
+    if with_e2e:
         step_host()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    ms_e2e = e0.elapsed_time(e1)
-
-    if dist:
-        tt = torch.tensor([ms, ms_e2e], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, ms_e2e = float(tt[0]), float(tt[1])
-    value = world * args.steps / (ms / 1e3)
-    e2e = world * args.steps / (ms_e2e / 1e3)
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step_host()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_e2e = e0.elapsed_time(e1)
+    ms, ms_e2e = reduce_max([ms, ms_e2e if ms_e2e is not None else 0.0])
+    value = world * steps / (ms / 1e3)
 
     pk = peaks()
     nb = 128 if prec == t.MIXED else 64
-    flops = lu_update_flops(n, nb) * args.steps
+    flops = lu_update_flops(n, nb) * steps
     gemm = stages.get("gemm", (0, 0.0))
     if prec == t.MIXED:
         tensor_peak = pk.get("bf16_tflops", 1590.0) / 2.0  # TF32 dense = half of bf16 dense
         executed = 3.0 * flops
         achieved = executed / (gemm[1] / 1e3) / 1e12 if gemm[1] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": tensor_peak, "unit": "TFLOP/s",
-                "frac": achieved / tensor_peak if achieved else None, "traffic": None,
-                "kernel": "split-TF32 tcgen05 trailing update (3 passes executed)",
+                "frac": achieved / tensor_peak if achieved else None,
+                "traffic": TF32_TRAFFIC["ratio"] * update_launch_bytes(n, nb),
+                "traffic_note": TF32_TRAFFIC["note"],
+                "kernel": "tf32_update_kernel: split-TF32 tcgen05 trailing update (3 passes executed)",
                 "useful_tflops": flops / (gemm[1] / 1e3) / 1e12 if gemm[1] else None,
                 "peak_note": "TF32 dense peak = half the measured bf16 burst (of measured)"}
     else:
-        fp64_peak = 40.0
+        fp64_peak = FP64_TENSOR_PEAK
         achieved = flops / (gemm[1] / 1e3) / 1e12 if gemm[1] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": achieved / fp64_peak if achieved else None, "traffic": None,
-                "kernel": "FP64 DMMA trailing update", "peak_note": "nominal FP64 tensor peak (not measured)"}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "kernel": "zgemm_dmma_kernel: FP64 DMMA trailing update",
+                "peak_note": "nominal FP64 tensor peak (no measured FP64 figure on this pool)"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64+c128 refine" if prec == t.MIXED else "c128", "data": "synthetic",
             "config": {"workload": f"precision cluster: {args.spheres} spheres lmax 4 (n={n}), 3 plane waves",
-                       "precision": args.precision, "l2": "inputs larger than L2 (matrix 4.8-9.7 GB)",
+                       "precision": precision, "l2": "inputs larger than L2 (matrix 4.8-9.7 GB), no flush",
                        "parallelism": f"replicas x{world}"},
             "max_rel_residual": worst, "roofline": roof,
-            "stages_ms_per_step": {k: v[1] / args.steps for k, v in stages.items()},
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "stages_ms_per_step": {k: v[1] / steps for k, v in stages.items()},
             "gpu_launches": int(launches), "clocks": clk}
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference(1, os.cpu_count() or 1)
-        line["cpu_baseline"].pop("seconds_per_solve_full_size", None)
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    ctx.close()
-    if dist:
-        dist.destroy_process_group()
+    if with_e2e:
+        line["e2e"] = {"value": world * steps / (ms_e2e / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                       "d2h_bytes_per_step": int(d2h)}
+    return {"line": line}
 
 
 if __name__ == "__main__":

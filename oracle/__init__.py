@@ -58,22 +58,17 @@ def lib() -> ctypes.CDLL:
                                           c_int, c_int, P, P, P]
         L.orc_gmres_dense.restype = c_int
         L.orc_gmres_dense.argtypes = [c_int, P, P, c_double, c_int, c_int, P, P, P]
-        if hasattr(L, "orc_lsumsw2d"):
-            L.orc_lsumsw2d.restype = c_int
-            L.orc_lsumsw2d.argtypes = [c_int, c_int, c_double, c_double, P, P, P, c_double, c_double, P, P]
-        if hasattr(L, "orc_lsumsw2d_table"):
-            L.orc_lsumsw2d_table.restype = c_int
-            L.orc_lsumsw2d_table.argtypes = [c_int, c_double, c_double, P, P, P, c_double, c_double, P]
-        if hasattr(L, "orc_kambe"):
-            L.orc_kambe.restype = c_int
-            L.orc_kambe.argtypes = [c_int, c_double, c_double, c_double, c_double, P]
-        if hasattr(L, "orc_upper_gamma"):
-            L.orc_upper_gamma.restype = c_int
-            L.orc_upper_gamma.argtypes = [c_double, c_double, c_double, P]
+        L.orc_upper_gamma.restype = c_int
+        L.orc_upper_gamma.argtypes = [c_double, c_double, c_double, P]
+        L.orc_kambe.restype = c_int
+        L.orc_kambe.argtypes = [c_int, c_double, c_double, c_double, c_double, P]
+        L.orc_lsumsw2d.restype = c_int
+        L.orc_lsumsw2d.argtypes = [c_int, c_int, c_double, c_double, P, P, P, c_double, c_double, c_int, P]
+        L.orc_lsumsw2d_table.restype = c_int
+        L.orc_lsumsw2d_table.argtypes = [c_int, c_double, c_double, P, P, P, c_double, c_double, P]
         if hasattr(L, "orc_array_solve"):
             L.orc_array_solve.restype = c_int
-            L.orc_array_solve.argtypes = [c_int, c_double, c_double, c_double, P, P, c_double, c_double, c_int,
-                                          P, P]
+            L.orc_array_solve.argtypes = [c_int, c_double, c_double, c_double, c_double, P, P, c_double, P]
     return _LIB
 
 
@@ -233,3 +228,45 @@ def gmres_dense(A, b, rtol=1e-10, restart=30, max_iterations=300):
     res = np.zeros(1, np.float64)
     st = lib().orc_gmres_dense(A.shape[0], _p(A), _p(b), rtol, restart, max_iterations, _p(x), _p(its), _p(res))
     return x, int(its[0]), float(res[0]), st
+
+
+def upper_gamma(a: float, z: complex) -> complex:
+    """Gamma(a, z), principal branch; a zero imaginary part picks the side by its sign."""
+    out = np.zeros(2)
+    lib().orc_upper_gamma(float(a), z.real, z.imag, _p(out))
+    return complex(out[0], out[1])
+
+
+def kambe(n: int, z: complex, eta: complex) -> complex:
+    out = np.zeros(2)
+    lib().orc_kambe(int(n), z.real, z.imag, eta.real, eta.imag, _p(out))
+    return complex(out[0], out[1])
+
+
+_PARTS = {"full": 0, "real": 1, "reciprocal": 2}
+
+
+def lsumsw2d(l: int, m: int, k: complex, lattice, kpar, r, eta: complex = 0.0, part: str = "full") -> complex:
+    """One 2D spherical lattice sum D_lm (lattice/mod.rs:11-15) or one of its Ewald parts."""
+    a = np.ascontiguousarray(lattice, np.float64).reshape(4)
+    kp = np.ascontiguousarray(kpar, np.float64).reshape(2)
+    rr = np.ascontiguousarray(r, np.float64).reshape(3)
+    out = np.zeros(2)
+    k, eta = complex(k), complex(eta)
+    st = lib().orc_lsumsw2d(l, m, k.real, k.imag, _p(a), _p(kp), _p(rr), eta.real, eta.imag, _PARTS[part], _p(out))
+    if st:
+        raise ValueError(f"oracle lattice sum failed with status {st}")
+    return complex(out[0], out[1])
+
+
+def lsumsw2d_table(lmax: int, k: complex, lattice, kpar, r=(0.0, 0.0, 0.0), eta: complex = 0.0) -> np.ndarray:
+    """Every D_lm with l <= lmax, table index l*l+l+m."""
+    a = np.ascontiguousarray(lattice, np.float64).reshape(4)
+    kp = np.ascontiguousarray(kpar, np.float64).reshape(2)
+    rr = np.ascontiguousarray(r, np.float64).reshape(3)
+    out = np.zeros((lmax + 1) ** 2, np.complex128)
+    k, eta = complex(k), complex(eta)
+    st = lib().orc_lsumsw2d_table(lmax, k.real, k.imag, _p(a), _p(kp), _p(rr), eta.real, eta.imag, _p(out))
+    if st:
+        raise ValueError(f"oracle lattice sum failed with status {st}")
+    return out
