@@ -66,9 +66,8 @@ def lib() -> ctypes.CDLL:
         L.orc_lsumsw2d.argtypes = [c_int, c_int, c_double, c_double, P, P, P, c_double, c_double, c_int, P]
         L.orc_lsumsw2d_table.restype = c_int
         L.orc_lsumsw2d_table.argtypes = [c_int, c_double, c_double, P, P, P, c_double, c_double, P]
-        if hasattr(L, "orc_array_solve"):
-            L.orc_array_solve.restype = c_int
-            L.orc_array_solve.argtypes = [c_int, c_double, c_double, c_double, c_double, P, P, c_double, P]
+        L.orc_array_solve.restype = c_int
+        L.orc_array_solve.argtypes = [c_int, c_double, c_double, c_double, c_double, P, P, c_double, P]
     return _LIB
 
 
@@ -270,3 +269,16 @@ def lsumsw2d_table(lmax: int, k: complex, lattice, kpar, r=(0.0, 0.0, 0.0), eta:
     if st:
         raise ValueError(f"oracle lattice sum failed with status {st}")
     return out
+
+
+def array_solve(lmax: int, k0: float, radius: float, eps: complex, lattice, kpar, eta: float = 0.0) -> np.ndarray:
+    """X = (I - T S(kpar))^-1 T of a periodic array of one sphere per cell, (M, M)."""
+    a = np.ascontiguousarray(lattice, np.float64).reshape(4)
+    kp = np.ascontiguousarray(kpar, np.float64).reshape(2)
+    M = 2 * lmax * (lmax + 2)
+    out = np.zeros(M * M, np.complex128)
+    eps = complex(eps)
+    st = lib().orc_array_solve(lmax, k0, radius, eps.real, eps.imag, _p(a), _p(kp), float(eta), _p(out))
+    if st:
+        raise ValueError(f"oracle array solve failed with status {st}")
+    return out.reshape(M, M, order="F")

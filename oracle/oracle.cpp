@@ -832,6 +832,9 @@ static int gmres_solve(size_t n, const cd* rhs, cd* answer, double rtol, double 
 
 // =======================================================================================
 // C interface for the tests (ctypes). Complex arrays are interleaved re, im doubles.
+int ewald_table(int lmax, std::complex<double> k, const double* lattice, const double* kpar, const double* r,
+                std::complex<double> eta, std::complex<double>* out);
+
 extern "C" {
 
 int orc_version() { return 1; }
@@ -951,6 +954,51 @@ int orc_dense_solve(int lmax, int N, const double* Aop, const double* tb, const 
                 x[o + 1] = t[2] * b[o] + t[3] * b[o + 1];
             }
     lu_solve(f, x, p);
+    return 0;
+}
+
+// Periodic array of one sphere per cell (cluster/interaction.rs:292-315 with
+// sw/expansion.rs:418-454 and sw/plan.rs:383-413): S = evaluate_table(D_pm / N_pm) with the
+// lattice sums at shift 0 (ewald.cpp), X = (I - T S)^-1 T, M x M column-major.
+int orc_array_solve(int lmax, double k0, double radius, double eps_re, double eps_im, const double* lattice,
+                    const double* kpar, double eta, double* out) {
+    Plan plan = plan_between(lmax, true);
+    int M = plan.M, order = plan.lmax;
+    int T = (order + 1) * (order + 1);
+    std::vector<cd> D(T), S((size_t)M * M);
+    double r0[3] = {0.0, 0.0, 0.0};
+    int st = ewald_table(order, cd(k0, 0.0), lattice, kpar, r0, cd(eta, 0.0), D.data());
+    if (st) return st;
+    for (int p = 0; p <= order; ++p)
+        for (int m = -p; m <= p; ++m) {
+            double nrm = std::sqrt((2 * p + 1) / (4 * M_PI)) * std::exp(0.5 * (log_factorial(p - m) - log_factorial(p + m)));
+            D[p * p + p + m] /= nrm;
+        }
+    plan_evaluate_table(plan, D.data(), S.data());
+    std::vector<Mode> md = modes(lmax);
+    std::vector<cd> Tb((size_t)lmax * 4);
+    for (int l = 1; l <= lmax; ++l) mie_block_mode_order(l, k0 * radius, cd(eps_re, eps_im), &Tb[(l - 1) * 4]);
+    LuFactor f;
+    f.n = M;
+    f.a.assign((size_t)M * M, cd(0, 0));
+    std::vector<cd> X((size_t)M * M, cd(0, 0));
+    for (int c = 0; c < M; ++c)
+        for (int r = 0; r < M; r += 2) {
+            const cd* t = &Tb[(md[r].l - 1) * 4];
+            cd s0 = S[(size_t)c * M + r], s1 = S[(size_t)c * M + r + 1];
+            f.a[(size_t)c * M + r] = (r == c ? 1.0 : 0.0) - (t[0] * s0 + t[1] * s1);
+            f.a[(size_t)c * M + r + 1] = (r + 1 == c ? 1.0 : 0.0) - (t[2] * s0 + t[3] * s1);
+        }
+    for (int c = 0; c < M; c += 2) {
+        const cd* t = &Tb[(md[c].l - 1) * 4];
+        X[(size_t)c * M + c] = t[0];
+        X[(size_t)c * M + c + 1] = t[2];
+        X[(size_t)(c + 1) * M + c] = t[1];
+        X[(size_t)(c + 1) * M + c + 1] = t[3];
+    }
+    if ((st = lu_factor(f))) return st;
+    lu_solve(f, X.data(), M);
+    std::memcpy(out, X.data(), X.size() * sizeof(cd));
     return 0;
 }
 

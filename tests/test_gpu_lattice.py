@@ -1,0 +1,102 @@
+"""GPU 2D lattice sums and the batched periodic-array solve against the binary128 oracle.
+
+Tolerances: lattice sums to 1e-11 * max(|D|, 1) over the whole table (the reference checks its
+own sums to 2.5e-13 * max(|S|, 1) of 30-digit values; the device path works in FP64 with
+series and continued fractions whose rounding we bound at ~1e-13 per term, and the largest
+tables reach |D| ~ 1e7 at l = 12); array solves to 1e-10 * max(|X|).
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from treams_b200 import lattice as tl
+from treams_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_table(D, lsum, k, lat, kps, eta=0.0, tol=1e-11):
+    for i, kp in enumerate(kps):
+        ref = oracle.lsumsw2d_table(lsum, k, lat, kp, eta=eta)
+        scale = max(1.0, np.max(np.abs(ref)))
+        err = np.max(np.abs(D[i] - ref)) / scale
+        assert err <= tol, (i, kp, err)
+
+
+@pytest.mark.parametrize("draw", [0, 3])
+def test_lattice_sums_periodic_workload(ctx, draw):
+    # the 4096-Bloch-vector square-lattice workload (k0 = 4, degrees <= 12), checked on a subset
+    w = workloads.periodic_array(draw=draw)
+    kps = w.kpars[:24]
+    D = tl.lsumsw2d_batch(12, w.k0, w.lattice, kps, ctx=ctx)
+    assert D.shape == (24, 169)
+    _check_table(D[::4], 12, w.k0, w.lattice, kps[::4])
+
+
+def test_lattice_sums_hexagonal_and_explicit_split(ctx):
+    lat = np.array([[1.0, 0.0], [0.5, math.sqrt(3) / 2]])
+    kps = np.array([[0.3, -0.2], [1.1, 0.4], [-2.0, 0.7]])
+    for eta in (0.0, 0.6):
+        D = tl.lsumsw2d_batch(9, 2.7, lat, kps, eta=eta, ctx=ctx)
+        _check_table(D, 9, 2.7, lat, kps, eta=eta)
+
+
+def test_lattice_sums_oblique_large_kl(ctx):
+    # |k L| > 8 selects the larger automatic split (cell.rs:164-175)
+    lat = np.array([[1.4, 0.0], [0.5, 1.6]])
+    kps = np.array([[0.4, -0.7], [0.0, 0.0]])
+    D = tl.lsumsw2d_batch(6, 7.3, lat, kps, ctx=ctx)
+    _check_table(D, 6, 7.3, lat, kps)
+
+
+def test_lattice_sums_are_bloch_periodic_on_device(ctx):
+    w = workloads.periodic_array()
+    g = 2 * math.pi / w.period
+    kp = np.array([w.kpars[7], w.kpars[7] + np.array([-g, g])])
+    D = tl.lsumsw2d_batch(12, w.k0, w.lattice, kp, ctx=ctx)
+    assert np.max(np.abs(D[1] - D[0])) <= 1e-11 * max(1.0, np.max(np.abs(D[0])))
+
+
+def test_lattice_sum_at_a_diffraction_threshold_is_rejected(ctx):
+    # |kpar + G| = k for G = 0 (lattice/mod.rs failure table)
+    with pytest.raises(ValueError, match="diffraction threshold"):
+        tl.lsumsw2d_batch(4, 2.0, np.eye(2), np.array([[2.0, 0.0]]), ctx=ctx)
+
+
+def test_lattice_sum_invalid_inputs(ctx):
+    with pytest.raises(ValueError):
+        tl.lsumsw2d_batch(4, -1.0, np.eye(2), np.array([[0.1, 0.0]]), ctx=ctx)
+    with pytest.raises(ValueError):
+        tl.lsumsw2d_batch(4, 1.0, np.array([[1.0, 0.0], [2.0, 0.0]]), np.array([[0.1, 0.0]]), ctx=ctx)
+    with pytest.raises(ValueError):
+        tl.lsumsw2d_batch(15, 1.0, np.eye(2), np.array([[0.1, 0.0]]), ctx=ctx)
+    with pytest.raises(ValueError, match="split"):
+        tl.lsumsw2d_batch(4, 1.0, np.eye(2), np.array([[0.1, 0.0]]), eta=0.1, ctx=ctx)
+
+
+@pytest.mark.parametrize("draw", [0, 5])
+def test_array_solve_matches_oracle(ctx, draw):
+    w = workloads.periodic_array(draw=draw)
+    kps = w.kpars[:6]
+    X = tl.array_solve_batch(w.lmax, w.k0, w.radius, w.eps, w.lattice, kps, ctx=ctx)
+    assert X.shape == (6, 96, 96)
+    for i in (0, 3, 5):
+        ref = oracle.array_solve(w.lmax, w.k0, w.radius, w.eps, w.lattice, kps[i])
+        err = np.max(np.abs(X[i] - ref)) / np.max(np.abs(ref))
+        assert err <= 1e-10, (i, err)
+
+
+def test_array_solve_small_lmax_lossy(ctx):
+    lat = np.array([[0.9, 0.0], [0.3, 0.8]])
+    kps = np.array([[0.5, 0.1], [-1.2, 2.0]])
+    X = tl.array_solve_batch(3, 2.5, 0.25, 3.0 + 0.4j, lat, kps, ctx=ctx)
+    for i in range(2):
+        ref = oracle.array_solve(3, 2.5, 0.25, 3.0 + 0.4j, lat, kps[i])
+        assert np.max(np.abs(X[i] - ref)) <= 1e-10 * np.max(np.abs(ref))
+
+
+def test_array_solve_rejects_touching_spheres(ctx):
+    with pytest.raises(ValueError, match="overlap"):
+        tl.array_solve_batch(2, 2.0, 0.6, 4.0, np.eye(2), np.array([[0.1, 0.2]]), ctx=ctx)

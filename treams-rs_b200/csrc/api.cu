@@ -929,3 +929,255 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
     if (worst) return fail(worst, msg);
     return TCU_OK;
 }
+
+// =========================================================================================
+// 2D lattice sums at shift 0 and the batched periodic-array solve.
+namespace {
+
+double log_fact(int n) { return std::lgamma((double)n + 1.0); }
+
+// Host-side set-up of one batch of lattice sums: split, lattice points within the real-space
+// cutoff, reciprocal vectors within the reciprocal cutoff, and the per-(l, m) constants.
+struct LatticeSetup {
+    double eta = 0, area = 0;
+    std::vector<double2> R, G;
+    std::vector<double> norm, reflection, coef;
+    std::vector<double2> pref;
+    double2 self0{0, 0};
+};
+
+tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const double* kpars, double eta_in,
+                         LatticeSetup& S) {
+    if (lsum < 0 || lsum > LS_MAXL) return fail(TCU_INVALID_INPUT, "require 0 <= lmax_sum <= 14");
+    if (!std::isfinite(k) || k <= 0.0)
+        return fail(TCU_INVALID_INPUT, "the device lattice sums take a positive real wavenumber");
+    if (!lat || !finite_all(lat, 4) || nk == 0 || !kpars || !finite_all(kpars, 2 * nk))
+        return fail(TCU_INVALID_INPUT, "lattice must be a finite 2 x 2 matrix with finite Bloch vectors");
+    const double a1x = lat[0], a1y = lat[1], a2x = lat[2], a2y = lat[3];
+    const double det = a1x * a2y - a1y * a2x;
+    S.area = std::fabs(det);
+    if (!(S.area > 0.0) || !std::isfinite(S.area)) return fail(TCU_INVALID_INPUT, "lattice is numerically singular");
+    double eta = eta_in;
+    if (!std::isfinite(eta) || eta < 0.0) return fail(TCU_INVALID_INPUT, "the device lattice sums take a real split >= 0");
+    if (eta == 0.0) {  // lattice/cell.rs:164-175
+        double kl = k * std::sqrt(S.area);
+        eta = std::sqrt(2.0 * M_PI) / kl * std::max(kl / 8.0, 1.0);
+    }
+    const double c = 0.5 / (eta * eta);
+    if (c > 8.0)
+        return fail(TCU_INVALID_INPUT,
+                    "Ewald split too small for the device lattice sums (require 1/(2 eta^2) <= 8); eta = 0 selects one");
+    S.eta = eta;
+    const double ke = k * eta;
+    // real space: Gaussian factor e^{-(k eta)^2 R^2/2 + c} below e^-46 times the polynomial growth
+    double Rc = std::sqrt(2.0 * (46.0 + c) / (ke * ke));
+    for (int it = 0; it < 30; ++it)
+        Rc = std::sqrt(2.0 * (46.0 + c + lsum * std::log(std::max(1.0, k * Rc)) +
+                              (2 * lsum + 1) * std::log(std::max(1.0, eta))) /
+                       (ke * ke));
+    const double len1 = std::hypot(a1x, a1y), len2 = std::hypot(a2x, a2y);
+    const double hdir = S.area / std::max(len1, len2);
+    long Nd = (long)std::ceil(Rc / hdir) + 1;
+    if (Nd > 64) return fail(TCU_INVALID_INPUT, "lattice too elongated for the device lattice sums");
+    for (long s = 1; s <= Nd; ++s)  // cube shells, fixed order
+        for (long n1 = -s; n1 <= s; ++n1)
+            for (long n2 = -s; n2 <= s; ++n2) {
+                if (std::max(std::labs(n1), std::labs(n2)) != s) continue;
+                double x = n1 * a1x + n2 * a2x, y = n1 * a1y + n2 * a2y;
+                if (std::hypot(x, y) <= Rc) S.R.push_back(make_double2(x, y));
+            }
+    // reciprocal: e^{-v} (q/k)^lsum (2 eta^2)^n below e^-46
+    const double b1x = 2 * M_PI * a2y / det, b1y = -2 * M_PI * a2x / det;
+    const double b2x = -2 * M_PI * a1y / det, b2y = 2 * M_PI * a1x / det;
+    double x2 = 1.0 + 2.0 * eta * eta * 46.0;
+    for (int it = 0; it < 30; ++it)
+        x2 = 1.0 + 2.0 * eta * eta *
+                       (46.0 + 0.5 * lsum * std::log(std::max(1.0, x2)) +
+                        (lsum / 2) * std::log(std::max(1.0, 2.0 * eta * eta)) + std::log(std::max(1.0, 1.0 / eta)));
+    double kmax = 0.0;
+    for (size_t i = 0; i < nk; ++i) kmax = std::max(kmax, std::hypot(kpars[2 * i], kpars[2 * i + 1]));
+    const double qc = k * std::sqrt(x2) + kmax;
+    const double blen1 = std::hypot(b1x, b1y), blen2 = std::hypot(b2x, b2y);
+    const double hrec = (4 * M_PI * M_PI / S.area) / std::max(blen1, blen2);
+    long Nr = (long)std::ceil(qc / hrec) + 1;
+    if (Nr > 64) return fail(TCU_INVALID_INPUT, "lattice or Bloch vectors out of range for the device lattice sums");
+    for (long s = 0; s <= Nr; ++s)
+        for (long n1 = -s; n1 <= s; ++n1)
+            for (long n2 = -s; n2 <= s; ++n2) {
+                if (std::max(std::labs(n1), std::labs(n2)) != s) continue;
+                double x = n1 * b1x + n2 * b2x, y = n1 * b1y + n2 * b2y;
+                if (std::hypot(x, y) <= qc) S.G.push_back(make_double2(x, y));
+            }
+    const int T = (lsum + 1) * (lsum + 1);
+    S.norm.assign(T, 0.0);
+    S.reflection.assign(T, 0.0);
+    S.coef.assign((size_t)T * LS_NMAX, 0.0);
+    S.pref.assign(T, make_double2(0, 0));
+    for (int l = 0; l <= lsum; ++l)
+        for (int m = -l; m <= l; ++m) {
+            int lm = l * l + l + m, am = std::abs(m);
+            S.norm[lm] = std::sqrt((2 * l + 1) / (4 * M_PI)) * std::exp(0.5 * (log_fact(l - m) - log_fact(l + m)));
+            S.reflection[lm] = ((am % 2) ? -1.0 : 1.0) * std::exp(log_fact(l - am) - log_fact(l + am));
+            if ((l - am) % 2 == 0)
+                for (int n = 0; n <= (l - am) / 2; ++n)
+                    S.coef[(size_t)lm * LS_NMAX + n] =
+                        std::exp(-log_fact(n) - log_fact((l + am - 2 * n) / 2) - log_fact((l - am - 2 * n) / 2));
+            // sqrt(2l+1) (-i)^m sqrt((l+m)!(l-m)!) / (A k^2 (-2)^l)   (reciprocal.rs:320-330)
+            double mag = std::sqrt(2.0 * l + 1.0) * std::exp(0.5 * (log_fact(l + m) + log_fact(l - m))) /
+                         (S.area * k * k * std::pow(-2.0, l));
+            int ph = ((m % 4) + 4) % 4;  // (-i)^m
+            double re = ph == 0 ? 1 : ph == 2 ? -1 : 0, im = ph == 1 ? -1 : ph == 3 ? 1 : 0;
+            S.pref[lm] = make_double2(mag * re, mag * im);
+        }
+    // self term (reciprocal.rs:467-487) at l = 0: Y_00 / (2 sqrt pi) Gamma(-1/2, -1/(2 eta^2) - 0i);
+    // Gamma(-1/2, -y - 0i) = Gamma(-1/2) - i y^(-1/2) sum_k y^k / (k! (k - 1/2))
+    {
+        double y = c, s = 0.0, term = 1.0;
+        for (int kk = 0; kk < 400; ++kk) {
+            if (kk > 0) term *= y / kk;
+            double add = term / (kk - 0.5);
+            s += add;
+            if (kk > y && std::fabs(add) < 1e-18 * std::fabs(s)) break;
+        }
+        double gre = -2.0 * std::sqrt(M_PI), gim = -s / std::sqrt(y);
+        double f = S.norm[0] * 0.5 / std::sqrt(M_PI);
+        S.self0 = make_double2(f * gre, f * gim);
+    }
+    return TCU_OK;
+}
+
+// D (device, nk x T) for device Bloch vectors; shares one LatticeSetup
+tcu_status lattice_sums_device(tcu_context* ctx, int lsum, double k, const LatticeSetup& S, size_t nk,
+                               const double2* d_kpar, double2* d_out, Arena* scratch_arena, DevBuf& scratch) {
+    (void)scratch_arena;
+    const int T = (lsum + 1) * (lsum + 1);
+    if (lattice_sum_smem(lsum, (int)S.R.size()) > 200 * 1024 || S.G.size() > (1u << 20))
+        return fail(TCU_INVALID_INPUT, "lattice too elongated for the device lattice sums");
+    Arena ar;
+    size_t oR = ar.add(S.R.size() * 16), oG = ar.add(S.G.size() * 16), oN = ar.add(T * 8), oRf = ar.add(T * 8),
+           oC = ar.add((size_t)T * LS_NMAX * 8), oP = ar.add(T * 16), oTab = ar.add(S.R.size() * T * 16);
+    CK(scratch.alloc(ar.total), "lattice scratch");
+    void* b = scratch.p;
+    CK(cudaMemcpyAsync(ar.at<void>(b, oR), S.R.data(), S.R.size() * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oG), S.G.data(), S.G.size() * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oN), S.norm.data(), T * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oRf), S.reflection.data(), T * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oC), S.coef.data(), (size_t)T * LS_NMAX * 8, cudaMemcpyHostToDevice, ctx->stream),
+       "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oP), S.pref.data(), T * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
+    double2* tab = ar.at<double2>(b, oTab);
+    launch_real_table(lsum, k, S.eta, (int)S.R.size(), ar.at<double2>(b, oR), ar.at<double>(b, oN),
+                      ar.at<double>(b, oRf), tab, ctx->stream);
+    ++ctx->launches;
+    LatticeSumArgs a;
+    a.lsum = lsum;
+    a.k = k;
+    a.eta = S.eta;
+    a.NR = (int)S.R.size();
+    a.R = ar.at<double2>(b, oR);
+    a.realtab = tab;
+    a.NG = (int)S.G.size();
+    a.G = ar.at<double2>(b, oG);
+    a.coef = ar.at<double>(b, oC);
+    a.pref = ar.at<double2>(b, oP);
+    a.self0 = S.self0;
+    a.nk = (int)nk;
+    a.kpar = d_kpar;
+    a.out = d_out;
+    a.ldo = T;
+    a.status = ctx->d_status;
+    int grid = (int)std::min<size_t>(nk, 148 * 8);
+    launch_lattice_sum(a, grid, ctx->stream);
+    ++ctx->launches;
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "status");
+    tcu_status s = sync_status(ctx, "lattice sums");
+    if (s) return s;
+    if (st == 9)
+        return fail(TCU_INVALID_INPUT, "lattice sum is at a diffraction threshold; supply a limiting complex wavenumber");
+    if (st) return fail(TCU_DEVICE_ERROR, "lattice sums: device status " + std::to_string(st));
+    return TCU_OK;
+}
+
+tcu_status array_solve_device(tcu_context* ctx, int lmax, double k0, double radius, const double* eps,
+                              const double* lattice, size_t nk, const double2* d_kpar, double eta,
+                              const double* kpars_host, double2* d_X) {
+    if (lmax < 1 || lmax > 6) return fail(TCU_INVALID_INPUT, "the batched array solve takes 1 <= lmax <= 6");
+    if (!std::isfinite(radius) || radius <= 0.0 || !eps || !finite_all(eps, 2))
+        return fail(TCU_INVALID_INPUT, "require a positive finite radius and a finite permittivity");
+    LatticeSetup S;
+    tcu_status s = lattice_setup(2 * lmax, k0, lattice, nk, kpars_host, eta, S);
+    if (s) return s;
+    double rmin = 1e300;
+    for (auto& R : S.R) rmin = std::min(rmin, std::hypot(R.x, R.y));
+    if (!(2.0 * radius < rmin))
+        return fail(TCU_INVALID_INPUT, "spherical particles must not touch or overlap their lattice images");
+    const DevPlan* P = nullptr;
+    if ((s = get_plan(ctx, lmax, &P))) return s;
+    const int T = (2 * lmax + 1) * (2 * lmax + 1);
+    Arena ar;
+    size_t oD = ar.add(nk * T * 16), oT = ar.add(lmax * 4 * 16), oE = ar.add(16), oRad = ar.add(8), oN = ar.add(T * 8);
+    DevBuf work(ctx), scratch(ctx);
+    CK(work.alloc(ar.total), "array-solve workspace");
+    void* b = work.p;
+    double2* D = ar.at<double2>(b, oD);
+    CK(cudaMemcpyAsync(ar.at<void>(b, oE), eps, 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oRad), &radius, 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oN), S.norm.data(), T * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    if ((s = lattice_sums_device(ctx, 2 * lmax, k0, S, nk, d_kpar, D, nullptr, scratch))) return s;
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
+    double2* Tm = ar.at<double2>(b, oT);
+    launch_mie(lmax, k0, 1, ar.at<double>(b, oRad), ar.at<cplx>(b, oE), Tm, ctx->d_status, ctx->stream);
+    ++ctx->launches;
+    if ((s = read_status(ctx, "Mie coefficients"))) return s;
+    int grid = (int)std::min<size_t>(nk, 148 * 4);
+    launch_array_solve(*P, D, T, ar.at<double>(b, oN), Tm, (int)nk, d_X, ctx->d_status, grid, ctx->stream);
+    ++ctx->launches;
+    return read_status(ctx, "periodic array solve");
+}
+
+}  // namespace
+
+extern "C" tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
+                                         const double* kpars, double eta, double* out) {
+    if (!ctx || !out) return fail(TCU_INVALID_INPUT, "null context or output");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ProfGuard pg(ctx);
+    LatticeSetup S;
+    tcu_status s = lattice_setup(lmax_sum, k, lattice, nk, kpars, eta, S);
+    if (s) return s;
+    const int T = (lmax_sum + 1) * (lmax_sum + 1);
+    Arena ar;
+    size_t oK = ar.add(nk * 16), oO = ar.add(nk * T * 16);
+    DevBuf io(ctx), scratch(ctx);
+    CK(io.alloc(ar.total), "lattice-sum buffers");
+    CK(cudaMemcpyAsync(ar.at<void>(io.p, oK), kpars, nk * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    if ((s = lattice_sums_device(ctx, lmax_sum, k, S, nk, ar.at<double2>(io.p, oK), ar.at<double2>(io.p, oO), nullptr,
+                                 scratch)))
+        return s;
+    CK(cudaMemcpyAsync(out, ar.at<void>(io.p, oO), nk * T * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    return sync_status(ctx, "lattice sums");
+}
+
+extern "C" tcu_status tcu_array_solve_batch(tcu_context* ctx, int lmax, double k0, double radius, const double* eps,
+                                            const double* lattice, size_t nk, const double* kpars, double eta,
+                                            double* out) {
+    if (!ctx || !out || !kpars || nk == 0) return fail(TCU_INVALID_INPUT, "null context, Bloch vectors or output");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ProfGuard pg(ctx);
+    if (lmax < 1 || lmax > 6) return fail(TCU_INVALID_INPUT, "the batched array solve takes 1 <= lmax <= 6");
+    const size_t M = 2 * (size_t)lmax * (lmax + 2);
+    Arena ar;
+    size_t oK = ar.add(nk * 16), oX = ar.add(nk * M * M * 16);
+    DevBuf io(ctx);
+    CK(io.alloc(ar.total), "array-solve buffers");
+    CK(cudaMemcpyAsync(ar.at<void>(io.p, oK), kpars, nk * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    tcu_status s = array_solve_device(ctx, lmax, k0, radius, eps, lattice, nk, ar.at<double2>(io.p, oK), eta, kpars,
+                                      ar.at<double2>(io.p, oX));
+    if (s) return s;
+    CK(cudaMemcpyAsync(out, ar.at<void>(io.p, oX), nk * M * M * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    return sync_status(ctx, "periodic array solve");
+}

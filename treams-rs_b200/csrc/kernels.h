@@ -88,6 +88,34 @@ void launch_plane_wave(int L, int N, const double* pos, int ncol, const cplx* kv
 void launch_apply_t(int L, int N, const cplx* T, const cplx* x, int ncol, cplx* y, cudaStream_t st);
 void pairs_init_attributes();
 
+// lattice.cu — 2D lattice sums at shift 0 and the batched periodic-array solve
+constexpr int LS_MAXL = 14;                // largest degree of a lattice sum
+constexpr int LS_NMAX = LS_MAXL / 2 + 1;   // reciprocal orders n per (l, m) in the plane
+struct LatticeSumArgs {
+    int lsum = 0;                          // degrees l <= lsum, T = (lsum+1)^2 outputs
+    double k = 0, eta = 0;
+    int NR = 0;                            // real-space lattice points (R != 0)
+    const double2* R = nullptr;
+    const double2* realtab = nullptr;      // NR x T real-space terms
+    int NG = 0;                            // reciprocal lattice vectors
+    const double2* G = nullptr;
+    const double* coef = nullptr;          // T x LS_NMAX in-plane polynomial coefficients
+    const double2* pref = nullptr;         // T reciprocal prefactors
+    double2 self0{0, 0};                   // self term of l = 0
+    int nk = 0;
+    const double2* kpar = nullptr;
+    double2* out = nullptr;                // out[kp * ldo + l*l+l+m]
+    size_t ldo = 0;
+    int* status = nullptr;                 // 9: a diffraction order on its threshold
+};
+void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, const double* norm,
+                       const double* reflection, double2* tab, cudaStream_t st);
+size_t lattice_sum_smem(int lsum, int NR);
+void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st);
+size_t array_solve_smem(int L);
+void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const double* norm, const double2* Tm, int nk,
+                        double2* X, int* status, int grid, cudaStream_t st);
+
 // lu.cu — dense LU of an n x n column-major complex matrix (lda = n) in FP64 (double2)
 // or FP32 (float2) storage, row permutation kept as perm (row i of P A is row perm[i]).
 struct LuWork {

@@ -1,11 +1,424 @@
-// 2D Ewald lattice sums and the batched periodic-array solve (placeholder).
-#include "../../include/treams_cuda.h"
+// 2D Ewald lattice sums of outgoing spherical waves for one sphere per cell (shift 0, real
+// wavenumber, real split) and the batched periodic-array solve X = (I - T S)^-1 T.
+//
+// D_lm(k, kpar, 0) = sum'_R h_l(k|R|) Y_lm(-R) e^{i kpar.R} (lattice/mod.rs:11-15) is split
+// at eta (lattice/ewald.rs:39-270) into
+//   real space  sum_R e^{i kpar.R} Treal_lm(R),  Treal_lm(R) = -i sqrt(2/pi) k^l |R|^l
+//               Y_lm(-R/|R|) I_2l(k|R|, eta)                         (lattice/real.rs:149-187)
+//   reciprocal  sum_G pref_lm az^|m| sum_n (2 eta^2)^n/(sqrt2 eta) F_(1/2-n)(v, 0) S_lmn(beta^2)
+//               with q = kpar + G, beta^2 = q.q/k^2, v = (beta^2 - 1)/(2 eta^2),
+//               az = (q_x +- i q_y)/k                                (lattice/reciprocal.rs:288-334)
+//   self term   at l = 0                                             (lattice/reciprocal.rs:467-487)
+// In the lattice plane only the n with s = 2n of S_lmn survive, so l - |m| odd sums vanish and
+// n runs to (l - |m|)/2 (reciprocal.rs:22-60).
+//
+// Device layout: the real-space terms do not depend on the Bloch vector, so one launch
+// tabulates Treal (NR x T complex, T = (lsum+1)^2) for the lattice points within the cutoff,
+// and one CTA per Bloch vector then forms sum_R e^{i kpar.R} Treal_lm(R) (threads over lm,
+// fixed order over R) plus the reciprocal sum over G in chunks of 256 points (threads over G
+// evaluate F_n into shared memory, then threads over lm add the chunk in a fixed order).
+// Results do not depend on the launch geometry or on timing.
+//
+// Special functions, all FP64 (each from a published method, checked against the binary128
+// oracle to ~1e-14):
+//   I_2l(z, eta) = eta^(2l+1)/2 sum_j c^j/j! R(l + 1/2 - j), c = 1/(2 eta^2), a = (z eta)^2/2,
+//     R(d) = Gamma(d, a)/a^d (Kambe series, special/integrals/kambe.rs:36-120). R(d) for d >= 1/2
+//     by the upward recurrence R(d+1) = (d R(d) + e^-a)/a from R(1/2) = sqrt(pi) erfc(sqrt a)/sqrt a
+//     (all terms positive); for d < 1/2 by the power series (DLMF 8.7.3) where a < 2, else by
+//     Legendre's continued fraction (DLMF 8.9.2, modified Lentz).
+//   F_(1/2-n)(v, 0) = Gamma(1/2-n, v)/(-v)^(1/2-n) on the lower side of the cut
+//     (lattice/reduced.rs:18-100): for v > 0, -i (-1)^n R(1/2-n, v); for v < 0 (propagating
+//     orders, y = -v), Gamma(b)/y^b + i (-1)^n sum_k y^k/(k! (b+k)).
+#include <cuda_runtime.h>
 
-extern "C" tcu_status tcu_lsumsw2d_batch(tcu_context*, int, double, const double*, size_t, const double*, double,
-                                         double*) {
-    return TCU_INVALID_INPUT;
+#include "common.cuh"
+#include "kernels.h"
+
+namespace tcu {
+
+namespace {
+
+constexpr int LS_JMAX = 64;                  // Kambe series terms
+constexpr int LS_LADDER = LS_MAXL + 1 + LS_JMAX;
+constexpr int LS_CHUNK = 256;                // reciprocal points per chunk
+
+// Gamma(d, a)/a^d for real a > 0 and half-integer d < 1/2
+__device__ double scaled_gamma_low(double d, double a) {
+    if (a < 2.0) {
+        // Gamma(d)/a^d - sum_k (-a)^k / (k! (d + k))
+        double s = 1.0 / d, term = 1.0;
+        for (int k = 1; k < 200; ++k) {
+            term *= -a / k;
+            double add = term / (d + k);
+            s += add;
+            if (k > a && fabs(add) < 1e-17 * fabs(s)) break;
+        }
+        return tgamma(d) * pow(a, -d) - s;
+    }
+    // e^-a / (a + 1 - d - 1(1-d)/(a + 3 - d - 2(2-d)/(a + 5 - d - ...)))
+    const double tiny = 1e-300;
+    double b = a + 1.0 - d, c = 1.0 / tiny, dd = 1.0 / b, h = dd;
+    for (int i = 1; i < 400; ++i) {
+        double an = -i * (i - d);
+        b += 2.0;
+        dd = an * dd + b;
+        if (fabs(dd) < tiny) dd = tiny;
+        c = b + an / c;
+        if (fabs(c) < tiny) c = tiny;
+        dd = 1.0 / dd;
+        double del = dd * c;
+        h *= del;
+        if (fabs(del - 1.0) < 1e-16) break;
+    }
+    return exp(-a) * h;
 }
-extern "C" tcu_status tcu_array_solve_batch(tcu_context*, int, double, double, const double*, const double*, size_t,
-                                            const double*, double, double*) {
-    return TCU_INVALID_INPUT;
+
+// One warp per lattice point: Treal_lm(R) for every l <= lsum, |m| <= l.
+__global__ void __launch_bounds__(128) real_table_kernel(int lsum, double k, double eta, int NR,
+                                                         const double2* __restrict__ R,
+                                                         const double* __restrict__ norm,
+                                                         const double* __restrict__ reflection,
+                                                         double2* __restrict__ tab) {
+    __shared__ double ladder[4][LS_LADDER];
+    __shared__ double kam[4][LS_MAXL + 1];
+    __shared__ cplx Y[4][(LS_MAXL + 1) * (LS_MAXL + 1)];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r = blockIdx.x * 4 + warp;
+    if (r >= NR) return;
+    const int T = (lsum + 1) * (lsum + 1);
+    const double2 p = R[r];
+    double dist, u[3];
+    unit_direction(-p.x, -p.y, 0.0, dist, u);
+    const double a = 0.5 * (k * dist * eta) * (k * dist * eta), c = 0.5 / (eta * eta);
+    // ladder[i] = R(lsum + 1/2 - i)
+    const int nlad = lsum + 1 + LS_JMAX;
+    if (lane == 0) {
+        double sa = sqrt(a), ea = exp(-a);
+        double rr = 1.7724538509055160273 * erfc(sa) / sa;  // R(1/2)
+        ladder[warp][lsum] = rr;
+        double d = 0.5;
+        for (int i = lsum - 1; i >= 0; --i) {
+            rr = (d * rr + ea) / a;
+            d += 1.0;
+            ladder[warp][i] = rr;
+        }
+    }
+    for (int i = lsum + 1 + lane; i < nlad; i += 32) ladder[warp][i] = scaled_gamma_low(lsum + 0.5 - i, a);
+    if (lane <= lsum) solid_column(lsum, lane, u, reflection, Y[warp]);
+    __syncwarp();
+    if (lane <= lsum) {
+        const int l = lane;
+        double sum = 0.0, coef = 1.0;
+        for (int j = 0; j < LS_JMAX; ++j) {
+            if (j > 0) coef *= c / j;
+            double term = coef * ladder[warp][lsum - l + j];
+            sum += term;
+            if (j > c + 3.0 && term <= 1e-17 * sum) break;
+        }
+        kam[warp][l] = 0.5 * pow(eta, 2 * l + 1) * sum;
+    }
+    __syncwarp();
+    const double s2p = 0.79788456080286535588;  // sqrt(2/pi)
+    for (int lm = lane; lm < T; lm += 32) {
+        int l = (int)sqrt((double)lm);
+        while (l * l > lm) --l;
+        while ((l + 1) * (l + 1) <= lm) ++l;
+        double f = s2p * pow(k * dist, (double)l) * norm[lm] * kam[warp][l];
+        cplx y = Y[warp][lm];
+        // -i f y
+        tab[(size_t)r * T + lm] = mk(f * y.y, -f * y.x);
+    }
 }
+
+// F'_n = (2 eta^2)^n / (sqrt 2 eta) F_(1/2-n)(v, 0), n = 0..nmax, real v != 0 (lower side)
+__device__ void reduced_limits(int nmax, double v, double eta, cplx* out) {
+    double factor = 1.0 / (1.4142135623730950488 * eta), step = 2.0 * eta * eta;
+    if (v < 0.0) {
+        double y = -v;
+        for (int n = 0; n <= nmax; ++n) {
+            double b = 0.5 - n;
+            double s = 0.0, term = 1.0;
+            for (int kk = 0; kk < 200; ++kk) {
+                if (kk > 0) term *= y / kk;
+                double add = term / (b + kk);
+                s += add;
+                if (kk > y && fabs(add) < 1e-18 * fabs(s)) break;
+            }
+            double re = tgamma(b) * pow(y, -b);
+            double im = (n & 1) ? -s : s;
+            out[n] = mk(factor * re, factor * im);
+            factor *= step;
+        }
+    } else {
+        for (int n = 0; n <= nmax; ++n) {
+            double rr = scaled_gamma_low(0.5 - n, v);
+            if (n == 0 && v >= 2.0) rr = 1.7724538509055160273 * erfc(sqrt(v)) / sqrt(v);
+            // -i (-1)^n R
+            double im = (n & 1) ? rr : -rr;
+            out[n] = mk(0.0, factor * im);
+            factor *= step;
+        }
+    }
+}
+
+// One CTA per Bloch vector. smem: phases NR double2, chunk arrays.
+__global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
+    extern __shared__ double2 ls_smem[];
+    double2* ph = ls_smem;                               // NR
+    double2* gF = ph + A.NR;                             // LS_CHUNK * (nmax + 1)
+    double2* gaz = gF + LS_CHUNK * (A.lsum / 2 + 1);     // LS_CHUNK
+    double* gb2 = (double*)(gaz + LS_CHUNK);             // LS_CHUNK
+    const int T = (A.lsum + 1) * (A.lsum + 1), nmax = A.lsum / 2;
+    const int tid = threadIdx.x;
+    for (int kp = blockIdx.x; kp < A.nk; kp += gridDim.x) {
+        const double2 kpar = A.kpar[kp];
+        for (int r = tid; r < A.NR; r += blockDim.x) {
+            double2 R = A.R[r];
+            double s, c;
+            sincos(kpar.x * R.x + kpar.y * R.y, &s, &c);
+            ph[r] = mk(c, s);
+        }
+        __syncthreads();
+        int lm = tid, l = 0, m = 0;
+        bool active = lm < T;
+        if (active) {
+            while ((l + 1) * (l + 1) <= lm) ++l;
+            m = lm - l * l - l;
+        }
+        const int am = m < 0 ? -m : m;
+        const bool even = ((l - am) & 1) == 0;
+        cplx acc = mk(0.0, 0.0);
+        if (active)
+            for (int r = 0; r < A.NR; ++r) cfma(acc, __ldg(&A.realtab[(size_t)r * T + lm]), ph[r]);
+        cplx rec = mk(0.0, 0.0);
+        for (int g0 = 0; g0 < A.NG; g0 += LS_CHUNK) {
+            __syncthreads();
+            int g = g0 + tid;
+            if (tid < LS_CHUNK && g < A.NG) {
+                double2 G = A.G[g];
+                double qx = kpar.x + G.x, qy = kpar.y + G.y;
+                double b2 = (qx * qx + qy * qy) / (A.k * A.k);
+                double v = (b2 - 1.0) / (2.0 * A.eta * A.eta);
+                if (fabs(v) <= 1e-14) {
+                    atomicExch(A.status, 9);  // on a diffraction threshold (reciprocal.rs:236-241)
+                    for (int n = 0; n <= nmax; ++n) gF[tid * (nmax + 1) + n] = mk(0.0, 0.0);
+                } else {
+                    reduced_limits(nmax, v, A.eta, gF + tid * (nmax + 1));
+                }
+                gb2[tid] = b2;
+                gaz[tid] = mk(qx / A.k, qy / A.k);
+            }
+            __syncthreads();
+            if (active && even) {
+                const int nm = (l - am) / 2;
+                const double* coef = A.coef + (size_t)lm * LS_NMAX;
+                const int cnt = min(LS_CHUNK, A.NG - g0);
+                for (int t = 0; t < cnt; ++t) {
+                    const double b2 = gb2[t];
+                    const double2* F = gF + t * (nmax + 1);
+                    cplx s = mk(0.0, 0.0);
+                    for (int n = 0; n <= nm; ++n) {  // Horner in beta^2
+                        s = cscale(s, b2);
+                        cfma(s, mk(coef[n], 0.0), F[n]);
+                    }
+                    cplx az = gaz[t];
+                    if (m < 0) az.y = -az.y;
+                    cplx azm = mk(1.0, 0.0);
+                    for (int q = 0; q < am; ++q) azm = cmul(azm, az);
+                    cfma(rec, s, azm);
+                }
+            }
+        }
+        if (active) {
+            cplx v = cadd(acc, cmul(A.pref[lm], rec));
+            if (lm == 0) v = cadd(v, A.self0);
+            A.out[(size_t)kp * A.ldo + lm] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// ---- batched periodic-array solve ----------------------------------------------------------
+// One CTA per Bloch vector: Z = D/N (harmonic table), A = I - T S in shared memory (S from the
+// translation plan, cluster/interaction.rs:292-315 with sw/plan.rs:383-413 evaluate_periodic),
+// partial-pivot LU in shared memory, then X = A^-1 T in panels of 48 right-hand-side columns.
+constexpr int AS_PANEL = 48;
+
+__global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const double2* __restrict__ D, size_t ldd,
+                                                          const double* __restrict__ norm,
+                                                          const double2* __restrict__ Tm, int nk,
+                                                          double2* __restrict__ X, int* __restrict__ status) {
+    extern __shared__ double2 as_smem[];
+    const int M = 2 * P.nlm;
+    double2* A = as_smem;                  // M x M column-major
+    double2* B = A + M * M;                // M x AS_PANEL column-major; the harmonic table aliases it
+    __shared__ int piv[128];
+    __shared__ int sing;
+    const int tid = threadIdx.x, nth = blockDim.x;
+    for (int kp = blockIdx.x; kp < nk; kp += gridDim.x) {
+        double2* Z = B;
+        for (int t = tid; t < P.tsize; t += nth) {
+            double2 d = D[(size_t)kp * ldd + t];
+            Z[t] = cscale(d, 1.0 / norm[t]);
+        }
+        if (tid == 0) sing = 0;
+        __syncthreads();
+        // A = I - T S: item (s, d) writes rows 2d, 2d+1 of columns 2s, 2s+1
+        for (int it = tid; it < P.nlm * P.nlm; it += nth) {
+            int s = it / P.nlm, d = it - s * P.nlm;
+            int lam = 1;
+            while ((lam + 1) * (lam + 1) - 1 <= d) ++lam;
+            const double2* t4 = Tm + (lam - 1) * 4;
+            cplx Aa, Bb;
+            plan_combo_sums(P, s * P.nlm + d, Z, Aa, Bb);
+            cplx cp = cadd(Aa, Bb), cn = csub(Aa, Bb);
+            double one = s == d ? 1.0 : 0.0;
+            cplx a00 = cmul(t4[0], cp), a10 = cmul(t4[2], cp), a01 = cmul(t4[1], cn), a11 = cmul(t4[3], cn);
+            A[(2 * s) * M + 2 * d] = mk(one - a00.x, -a00.y);
+            A[(2 * s) * M + 2 * d + 1] = cneg(a10);
+            A[(2 * s + 1) * M + 2 * d] = cneg(a01);
+            A[(2 * s + 1) * M + 2 * d + 1] = mk(one - a11.x, -a11.y);
+        }
+        __syncthreads();
+        // LU with partial pivoting (largest modulus, first index on ties)
+        for (int kc = 0; kc < M; ++kc) {
+            if (tid < 32) {
+                double best = -1.0;
+                int bi = kc;
+                for (int i = kc + tid; i < M; i += 32) {
+                    double v = cabs2(A[kc * M + i]);
+                    if (v > best) {
+                        best = v;
+                        bi = i;
+                    }
+                }
+                for (int off = 16; off > 0; off >>= 1) {
+                    double ov = __shfl_down_sync(0xffffffffu, best, off);
+                    int oi = __shfl_down_sync(0xffffffffu, bi, off);
+                    if (ov > best || (ov == best && oi < bi)) {
+                        best = ov;
+                        bi = oi;
+                    }
+                }
+                if (tid == 0) {
+                    piv[kc] = bi;
+                    if (!(best > 0.0)) sing = 1;
+                }
+            }
+            __syncthreads();
+            const int pr = piv[kc];
+            if (pr != kc)
+                for (int j = tid; j < M; j += nth) {
+                    double2 t = A[j * M + kc];
+                    A[j * M + kc] = A[j * M + pr];
+                    A[j * M + pr] = t;
+                }
+            __syncthreads();
+            if (sing) break;
+            const cplx inv = cinv(A[kc * M + kc]);
+            for (int i = kc + 1 + tid; i < M; i += nth) A[kc * M + i] = cmul(A[kc * M + i], inv);
+            __syncthreads();
+            const int rem = M - kc - 1;
+            for (int it = tid; it < rem * rem; it += nth) {
+                int j = kc + 1 + it / rem, i = kc + 1 + it % rem;
+                cplx v = A[j * M + i];
+                cfma(v, cneg(A[kc * M + i]), A[j * M + kc]);
+                A[j * M + i] = v;
+            }
+            __syncthreads();
+        }
+        if (sing) {
+            if (tid == 0) atomicExch(status, 5);
+            __syncthreads();
+            continue;
+        }
+        // X = U^-1 L^-1 P T, panels of AS_PANEL columns
+        double2* Xk = X + (size_t)kp * M * M;
+        for (int c0 = 0; c0 < M; c0 += AS_PANEL) {
+            const int nc = min(AS_PANEL, M - c0);
+            // B = T (block diagonal: columns 2i, 2i+1 of mode pair i carry t[.][0], t[.][1])
+            for (int it = tid; it < M * nc; it += nth) {
+                int jj = it / M, i = it - jj * M, col = c0 + jj;
+                cplx v = mk(0.0, 0.0);
+                if ((i >> 1) == (col >> 1)) {
+                    int lm = col >> 1, lam = 1;
+                    while ((lam + 1) * (lam + 1) - 1 <= lm) ++lam;
+                    v = Tm[(lam - 1) * 4 + (i & 1) * 2 + (col & 1)];
+                }
+                B[jj * M + i] = v;
+            }
+            __syncthreads();
+            for (int kc = 0; kc < M; ++kc) {  // row interchanges in factorization order
+                const int pr = piv[kc];
+                if (pr != kc)
+                    for (int jj = tid; jj < nc; jj += nth) {
+                        double2 t = B[jj * M + kc];
+                        B[jj * M + kc] = B[jj * M + pr];
+                        B[jj * M + pr] = t;
+                    }
+                __syncthreads();
+            }
+            for (int kc = 0; kc < M - 1; ++kc) {  // unit lower
+                const int rem = M - kc - 1;
+                for (int it = tid; it < rem * nc; it += nth) {
+                    int jj = it / rem, i = kc + 1 + it % rem;
+                    cplx v = B[jj * M + i];
+                    cfma(v, cneg(A[kc * M + i]), B[jj * M + kc]);
+                    B[jj * M + i] = v;
+                }
+                __syncthreads();
+            }
+            for (int kc = M - 1; kc >= 0; --kc) {  // upper
+                const cplx inv = cinv(A[kc * M + kc]);
+                for (int jj = tid; jj < nc; jj += nth) B[jj * M + kc] = cmul(B[jj * M + kc], inv);
+                __syncthreads();
+                for (int it = tid; it < kc * nc; it += nth) {
+                    int jj = it / kc, i = it % kc;
+                    cplx v = B[jj * M + i];
+                    cfma(v, cneg(A[kc * M + i]), B[jj * M + kc]);
+                    B[jj * M + i] = v;
+                }
+                __syncthreads();
+            }
+            for (int it = tid; it < M * nc; it += nth) {
+                int jj = it / M, i = it - jj * M;
+                Xk[(size_t)(c0 + jj) * M + i] = B[jj * M + i];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace
+
+void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, const double* norm,
+                       const double* reflection, double2* tab, cudaStream_t st) {
+    StageScope sc(ST_LATTICE, st);
+    real_table_kernel<<<(NR + 3) / 4, 128, 0, st>>>(lsum, k, eta, NR, R, norm, reflection, tab);
+}
+
+size_t lattice_sum_smem(int lsum, int NR) {
+    return (size_t)NR * 16 + (size_t)LS_CHUNK * (lsum / 2 + 1) * 16 + LS_CHUNK * 16 + LS_CHUNK * 8;
+}
+
+void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st) {
+    StageScope sc(ST_LATTICE, st);
+    size_t smem = lattice_sum_smem(a.lsum, a.NR);
+    cudaFuncSetAttribute(lattice_sum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    lattice_sum_kernel<<<grid, 256, smem, st>>>(a);
+}
+
+size_t array_solve_smem(int L) {
+    int M = 2 * L * (L + 2);
+    return (size_t)M * M * 16 + (size_t)M * AS_PANEL * 16;
+}
+
+void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const double* norm, const double2* Tm, int nk,
+                        double2* X, int* status, int grid, cudaStream_t st) {
+    StageScope sc(ST_SMALL_LU, st);
+    size_t smem = array_solve_smem(P.L);
+    cudaFuncSetAttribute(array_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    array_solve_kernel<<<grid, 512, smem, st>>>(P, D, ldd, norm, Tm, nk, X, status);
+}
+
+}  // namespace tcu

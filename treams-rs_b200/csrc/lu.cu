@@ -152,7 +152,6 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
     C* prow = tile + (size_t)chunk * (NB + 1);   // NB
     __shared__ float s_val[8];
     __shared__ int s_row[8];
-    __shared__ unsigned long long s_win;
     const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int rows = n - k0;

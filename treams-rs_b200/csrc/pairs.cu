@@ -64,12 +64,7 @@ __device__ __forceinline__ void pair_table(const DevPlan& P, double k, double dx
 
 // A and B term sums of combo c against table Z
 __device__ __forceinline__ void combo_sums(const DevPlan& P, int c, const cplx* Z, cplx& A, cplx& B) {
-    int2 cb = __ldg(&P.combo[c]);
-    int t = cb.x, na = cb.y & 0xffff, nb = cb.y >> 16;
-    A = mk(0.0, 0.0);
-    B = mk(0.0, 0.0);
-    for (int e = 0; e < na; ++e, ++t) cfma(A, __ldg(&P.w[t]), Z[__ldg(&P.idx[t])]);
-    for (int e = 0; e < nb; ++e, ++t) cfma(B, __ldg(&P.w[t]), Z[__ldg(&P.idx[t])]);
+    plan_combo_sums(P, c, Z, A, B);
 }
 
 __device__ __forceinline__ int degree_of(int lm) {  // lm = l*l - 1 + l + m

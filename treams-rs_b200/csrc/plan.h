@@ -30,4 +30,24 @@ struct DevPlan {
     const double* reflection;
 };
 
+#ifdef __CUDACC__
+// A (same-helicity) and B (cross) term sums of combo c = s * nlm + d against a harmonic table Z
+__device__ __forceinline__ void plan_combo_sums(const DevPlan& P, int c, const double2* Z, double2& A, double2& B) {
+    int2 cb = __ldg(&P.combo[c]);
+    int t = cb.x, na = cb.y & 0xffff, nb = cb.y >> 16;
+    A = make_double2(0.0, 0.0);
+    B = make_double2(0.0, 0.0);
+    for (int e = 0; e < na; ++e, ++t) {
+        double2 w = __ldg(&P.w[t]), z = Z[__ldg(&P.idx[t])];
+        A.x = fma(w.x, z.x, fma(-w.y, z.y, A.x));
+        A.y = fma(w.x, z.y, fma(w.y, z.x, A.y));
+    }
+    for (int e = 0; e < nb; ++e, ++t) {
+        double2 w = __ldg(&P.w[t]), z = Z[__ldg(&P.idx[t])];
+        B.x = fma(w.x, z.x, fma(-w.y, z.y, B.x));
+        B.y = fma(w.x, z.y, fma(w.y, z.x, B.y));
+    }
+}
+#endif
+
 }  // namespace tcu
