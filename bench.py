@@ -115,14 +115,15 @@ def lu_update_flops(n: int, nb: int) -> float:
     return total
 
 
-def cpu_reference(samples: int, threads: int) -> dict:
-    """Time the CPU path on a bounded sample: 128 spheres of the same distribution
-    (n = 6144), oracle assembly of I - T C + LAPACK LU solve of the three columns.
-    Extrapolation to 512 spheres: assembly x (512/128)^2, LU x (512/128)^3."""
+def cpu_reference(samples: int, threads: int, count: int = 128, full: int = 512) -> dict:
+    """Time the CPU path on a bounded sample: `count` spheres of the same distribution
+    (n = 48 count), oracle assembly of I - T C + LAPACK LU solve of the three columns.
+    Extrapolation to `full` spheres: assembly x (full/count)^2, LU x (full/count)^3."""
     import oracle
     from treams_b200 import workloads
 
-    w = workloads.precision_cluster(count=128)
+    w = workloads.precision_cluster(count=count)
+    f2, f3 = (full / count) ** 2, (full / count) ** 3
     best = None
     for _ in range(samples):
         t0 = time.perf_counter()
@@ -131,11 +132,12 @@ def cpu_reference(samples: int, threads: int) -> dict:
         B = oracle.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols)
         np.linalg.solve(A, B)
         t2 = time.perf_counter()
-        est = (t1 - t0) * 16.0 + (t2 - t1) * 64.0
+        est = (t1 - t0) * f2 + (t2 - t1) * f3
         best = est if best is None else min(best, est)
     return {"value": 1.0 / best, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "128 spheres (n=6144) of the 512-sphere lmax-4 distribution: C++ restatement assembly "
-                      "+ LAPACK zgesv (numpy), extrapolated x16 (assembly) and x64 (LU) to n=24576",
+            "sample": f"{count} spheres (n={48 * count}) of the {full}-sphere lmax-4 distribution: C++ restatement "
+                      f"assembly + LAPACK zgesv (numpy), extrapolated x{f2:g} (assembly) and x{f3:g} (LU) to "
+                      f"n={48 * full}",
             "seconds_per_solve_full_size": best}
 
 
@@ -145,19 +147,20 @@ def run_reference(args, rank: int, world: int) -> None:
     threads = os.cpu_count() or 1
     samples = []
     for _ in range(args.warmup):
-        cpu_reference(1, threads)
+        cpu_reference(1, threads, args.cpu_sample_spheres, args.spheres)
     for _ in range(args.steps):
-        samples.append(cpu_reference(1, threads)["seconds_per_solve_full_size"])
+        samples.append(cpu_reference(1, threads, args.cpu_sample_spheres, args.spheres)["seconds_per_solve_full_size"])
     sec = float(np.mean(samples))
     v = 1.0 / sec
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": "precision cluster: 512 spheres lmax 4 (n=24576), 3 plane waves",
-                       "sample": "128 spheres, extrapolated"},
+            "config": {"workload": f"precision cluster: {args.spheres} spheres lmax 4 (n={48 * args.spheres}), "
+                                   "3 plane waves", "precision": "fp64 (CPU restatement + LAPACK)",
+                       "parallelism": "rank 0 only", "sample": f"{args.cpu_sample_spheres} spheres, extrapolated"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": "128 spheres (n=6144), C++ restatement assembly + LAPACK zgesv, "
-                                       "extrapolated to n=24576"},
+                             "sample": f"{args.cpu_sample_spheres} spheres (n={48 * args.cpu_sample_spheres}), C++ "
+                                       f"restatement assembly + LAPACK zgesv, extrapolated to n={48 * args.spheres}"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -175,6 +178,8 @@ def main() -> None:
                     help="skip the plain FP64 comparison arm of the mixed headline")
     ap.add_argument("--compare-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
+    ap.add_argument("--cpu-sample-spheres", type=int, default=128,
+                    help="spheres of the bounded CPU sample (timed, then extrapolated to --spheres)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -238,7 +243,7 @@ def main() -> None:
                             "gpu_launches": o["gpu_launches"]}
             line["speedup_vs_fp64"] = line["value"] / o["value"]
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_reference(1, os.cpu_count() or 1)
+            line["cpu_baseline"] = cpu_reference(1, os.cpu_count() or 1, args.cpu_sample_spheres, args.spheres)
             line["cpu_baseline"].pop("seconds_per_solve_full_size", None)
         print(json.dumps(line), flush=True)
     ctx.close()
