@@ -42,8 +42,8 @@ typedef enum tcu_precision {
 
 typedef enum tcu_preconditioner {
     TCU_PRECOND_NONE = 0,          /* plain GMRES on I - T C */
-    TCU_PRECOND_BLOCK_JACOBI = 1,  /* neighbour-cluster block Jacobi */
-    TCU_PRECOND_LEARNED = 2        /* graph-network block-sparse approximate inverse */
+    TCU_PRECOND_BLOCK_JACOBI = 1,  /* block Jacobi over nearest-neighbour sphere groups (<= 96 modes) */
+    TCU_PRECOND_LEARNED = 2        /* learned polynomial in the block-sparse near-field couplings */
 } tcu_preconditioner;
 
 typedef struct tcu_context tcu_context;
@@ -152,6 +152,22 @@ tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0, size_t N, 
                                const double* eps, const double* positions, const double* B, int p,
                                const tcu_gmres_options* options, int preconditioner, double* X,
                                tcu_certificate* certificates);
+
+/* Settings of the GMRES preconditioners of this context (no counterpart in the reference):
+ * near-field reach in sphere diameters (<= 0: the compiled-in fit's reach) and, for TCU_PRECOND_LEARNED, the layer
+ * count and weights (alpha: layers + 1 complex; layers < 0 restores the compiled-in fit,
+ * alpha NULL with layers >= 0 uses weights 1, i.e. block-Jacobi relaxation sweeps). */
+tcu_status tcu_context_set_learned_preconditioner(tcu_context* ctx, double reach_diameters, int layers,
+                                                  const double* alpha);
+/* Training statistics of the learned preconditioner (no counterpart in the reference, whose
+ * iterative solver is unpreconditioned): for the cluster's layer basis u_k = A (D N)^k D v,
+ * k = 0..layers (D: block-Jacobi inverse, N: near-field couplings between blocks, A = I - T C),
+ * over nvec probe vectors V (n x nvec complex, column-major, host), returns
+ * gram[k * (layers+1) + l] = sum_v conj(u_k) . u_l and rhs[k] = sum_v conj(u_k) . v (complex),
+ * from which ||v - sum_k alpha_k u_k||^2 and its gradient in alpha follow for any alpha. */
+tcu_status tcu_learned_precond_gram(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                    const double* eps, const double* positions, int layers, int nvec,
+                                    const double* V, double* gram, double* rhs);
 
 /* ---- 2D lattice sums and periodic arrays --------------------------------------------- */
 /* Ewald lattice sums D_lm (lattice/mod.rs:11-15, 283; ewald.rs:39-270) of a 2D lattice

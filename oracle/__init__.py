@@ -66,6 +66,8 @@ def lib() -> ctypes.CDLL:
         L.orc_lsumsw2d.argtypes = [c_int, c_int, c_double, c_double, P, P, P, c_double, c_double, c_int, P]
         L.orc_lsumsw2d_table.restype = c_int
         L.orc_lsumsw2d_table.argtypes = [c_int, c_double, c_double, P, P, P, c_double, c_double, P]
+        L.orc_learned_gram.restype = c_int
+        L.orc_learned_gram.argtypes = [c_int, c_double, c_int, P, P, P, c_double, c_int, c_int, P, P, P]
         L.orc_array_solve.restype = c_int
         L.orc_array_solve.argtypes = [c_int, c_double, c_double, c_double, c_double, P, P, c_double, P]
     return _LIB
@@ -282,3 +284,20 @@ def array_solve(lmax: int, k0: float, radius: float, eps: complex, lattice, kpar
     if st:
         raise ValueError(f"oracle array solve failed with status {st}")
     return out.reshape(M, M, order="F")
+
+
+def learned_gram(lmax, k0, radii, eps, pos, layers: int, V, reach: float = 3.0):
+    """Gram matrix (layers+1)^2 and right-hand side of the learned preconditioner's layer basis."""
+    radii = np.ascontiguousarray(radii, np.float64)
+    eps = np.ascontiguousarray(eps, np.complex128)
+    pos = np.ascontiguousarray(pos, np.float64)
+    V = np.asfortranarray(V, np.complex128)
+    K1 = layers + 1
+    gram = np.zeros(K1 * K1, np.complex128)
+    rhs = np.zeros(K1, np.complex128)
+    st = lib().orc_learned_gram(lmax, k0, radii.size, _p(radii), _p(eps), _p(pos), float(reach), layers, V.shape[1],
+                                _p(V),
+                                _p(gram), _p(rhs))
+    if st:
+        raise ValueError(f"oracle Gram failed with status {st}")
+    return gram.reshape(K1, K1), rhs

@@ -152,3 +152,21 @@ def test_single_sphere_reduces_to_mie():
     Tb = np.concatenate([tb[0, l - 1] @ b[2 * q:2 * q + 2, 0] for l, q in
                          [(l, i) for i, l in enumerate([l for l in range(1, 4) for _ in range(2 * l + 1)])]])
     assert np.allclose(X[:, 0], Tb, rtol=0, atol=1e-15)
+
+
+def test_learned_preconditioner_statistics_are_a_gram_matrix():
+    # the oracle's Gram matrix of the layer basis is Hermitian positive semidefinite, and the
+    # least-squares layer weights fit the probe vectors at least as well as block Jacobi alone
+    w = workloads.learned_cluster(seed=91, count=12)
+    rng = np.random.default_rng(1)
+    V = rng.standard_normal((w.n, 2)) + 1j * rng.standard_normal((w.n, 2))
+    G, b = oracle.learned_gram(w.lmax, w.k0, w.radii, w.eps, w.positions, 3, V)
+    assert np.allclose(G, G.conj().T, rtol=0, atol=1e-12 * np.abs(G).max())
+    assert np.min(np.linalg.eigvalsh(G)) >= -1e-10 * np.abs(G).max()
+    vv = np.sum(np.abs(V) ** 2)
+    loss = lambda a: vv - 2 * np.real(np.vdot(a, b)) + np.real(np.vdot(a, G @ a))
+    a_opt = np.linalg.solve(G, b)
+    e0 = np.zeros(4, complex)
+    e0[0] = 1.0
+    assert loss(a_opt) <= loss(e0) + 1e-9 * vv
+    assert loss(a_opt) <= vv

@@ -95,6 +95,10 @@ struct tcu_context {
     cplx* d_csmall = nullptr;     // 64 complex
     int* d_status = nullptr;
     double* d_lfac = nullptr;     // sqrt((l-m)!/(l+m)!) table up to degree 16
+    // GMRES preconditioner settings (tcu_context_set_learned_preconditioner)
+    double precond_reach = -1.0;  // near-field reach in sphere diameters (< 0: the compiled-in fit's)
+    int learned_layers = -1;      // < 0: the compiled-in fit
+    std::vector<std::complex<double>> learned_alpha;
 };
 
 struct tcu_factor {
@@ -909,8 +913,11 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
     ++ctx->launches;
     std::unique_ptr<Preconditioner> pre;
     if (preconditioner != TCU_PRECOND_NONE) {
-        s = make_preconditioner(ctx->stream, preconditioner, *P, lmax, (int)N, k0, pos, T, &pre, &ctx->launches);
-        if (s) return s;
+        s = make_preconditioner(ctx->stream, preconditioner, *P, lmax, (int)N, k0, pos, positions, radii, T,
+                                ctx->precond_reach, ctx->learned_layers, ctx->learned_alpha, &pre, &ctx->launches);
+        if (s == TCU_OUT_OF_MEMORY) return fail(s, "preconditioner: out of device memory");
+        if (s == TCU_SINGULAR) return fail(s, "preconditioner: a diagonal block is numerically singular");
+        if (s) return fail(s, "preconditioner set-up failed");
     }
     tcu_status worst = TCU_OK;
     std::string msg;
@@ -1180,4 +1187,59 @@ extern "C" tcu_status tcu_array_solve_batch(tcu_context* ctx, int lmax, double k
     if (s) return s;
     CK(cudaMemcpyAsync(out, ar.at<void>(io.p, oX), nk * M * M * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
     return sync_status(ctx, "periodic array solve");
+}
+
+extern "C" tcu_status tcu_learned_precond_gram(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                               const double* eps, const double* positions, int layers, int nvec,
+                                               const double* V, double* gram, double* rhs) {
+    if (!ctx || !V || !gram || !rhs || layers < 0 || layers > 32 || nvec <= 0)
+        return fail(TCU_INVALID_INPUT, "require 0 <= layers <= 32, nvec >= 1 and non-null buffers");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    tcu_status s = validate_spheres(lmax, k0, N, radii, eps, positions);
+    if (s) return s;
+    const DevPlan* P;
+    if ((s = get_plan(ctx, lmax, &P))) return s;
+    const size_t n = N * 2 * (size_t)lmax * (lmax + 2);
+    if (!finite_all(V, 2 * n * (size_t)nvec)) return fail(TCU_INVALID_INPUT, "probe vectors must be finite");
+    Arena ar;
+    size_t oP = ar.add(N * 24), oR = ar.add(N * 8), oE = ar.add(N * 16), oT = ar.add(N * lmax * 64),
+           oV = ar.add(n * nvec * 16);
+    DevBuf buf(ctx);
+    CK(buf.alloc(ar.total), "Gram buffers");
+    double* pos = ar.at<double>(buf.p, oP);
+    double* r = ar.at<double>(buf.p, oR);
+    cplx* e = ar.at<cplx>(buf.p, oE);
+    cplx* T = ar.at<cplx>(buf.p, oT);
+    cplx* dV = ar.at<cplx>(buf.p, oV);
+    CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(dV, V, n * nvec * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
+    launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
+    ++ctx->launches;
+    if ((s = read_status(ctx, "Mie coefficients"))) return s;
+    s = learned_gram(ctx->stream, *P, lmax, (int)N, k0, pos, positions, radii, T, ctx->precond_reach, layers, nvec,
+                     dV, ctx->d_csmall,
+                     ctx->d_cpartial, (std::complex<double>*)gram, (std::complex<double>*)rhs, &ctx->launches);
+    if (s == TCU_OUT_OF_MEMORY) return fail(s, "learned preconditioner: out of device memory");
+    if (s == TCU_SINGULAR) return fail(s, "learned preconditioner: a diagonal block is numerically singular");
+    if (s) return fail(s, "learned preconditioner: device failure");
+    return sync_status(ctx, "learned preconditioner");
+}
+
+extern "C" tcu_status tcu_context_set_learned_preconditioner(tcu_context* ctx, double reach_diameters, int layers,
+                                                             const double* alpha) {
+    if (!ctx || !std::isfinite(reach_diameters) || reach_diameters > 20.0 || layers > 32 ||
+        (layers >= 0 && alpha && !finite_all(alpha, 2 * (size_t)(layers + 1))))
+        return fail(TCU_INVALID_INPUT, "require reach <= 20 diameters, layers <= 32 and finite weights");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ctx->precond_reach = reach_diameters > 0.0 ? reach_diameters : -1.0;
+    ctx->learned_layers = layers;
+    ctx->learned_alpha.clear();
+    if (layers >= 0 && alpha)
+        for (int k = 0; k <= layers; ++k) ctx->learned_alpha.emplace_back(alpha[2 * k], alpha[2 * k + 1]);
+    return TCU_OK;
 }

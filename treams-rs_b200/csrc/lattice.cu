@@ -33,6 +33,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "smem_lu.cuh"
 
 namespace tcu {
 
@@ -261,7 +262,6 @@ __global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const doubl
             double2 d = D[(size_t)kp * ldd + t];
             Z[t] = cscale(d, 1.0 / norm[t]);
         }
-        if (tid == 0) sing = 0;
         __syncthreads();
         // A = I - T S: item (s, d) writes rows 2d, 2d+1 of columns 2s, 2s+1
         for (int it = tid; it < P.nlm * P.nlm; it += nth) {
@@ -280,54 +280,7 @@ __global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const doubl
             A[(2 * s + 1) * M + 2 * d + 1] = mk(one - a11.x, -a11.y);
         }
         __syncthreads();
-        // LU with partial pivoting (largest modulus, first index on ties)
-        for (int kc = 0; kc < M; ++kc) {
-            if (tid < 32) {
-                double best = -1.0;
-                int bi = kc;
-                for (int i = kc + tid; i < M; i += 32) {
-                    double v = cabs2(A[kc * M + i]);
-                    if (v > best) {
-                        best = v;
-                        bi = i;
-                    }
-                }
-                for (int off = 16; off > 0; off >>= 1) {
-                    double ov = __shfl_down_sync(0xffffffffu, best, off);
-                    int oi = __shfl_down_sync(0xffffffffu, bi, off);
-                    if (ov > best || (ov == best && oi < bi)) {
-                        best = ov;
-                        bi = oi;
-                    }
-                }
-                if (tid == 0) {
-                    piv[kc] = bi;
-                    if (!(best > 0.0)) sing = 1;
-                }
-            }
-            __syncthreads();
-            const int pr = piv[kc];
-            if (pr != kc)
-                for (int j = tid; j < M; j += nth) {
-                    double2 t = A[j * M + kc];
-                    A[j * M + kc] = A[j * M + pr];
-                    A[j * M + pr] = t;
-                }
-            __syncthreads();
-            if (sing) break;
-            const cplx inv = cinv(A[kc * M + kc]);
-            for (int i = kc + 1 + tid; i < M; i += nth) A[kc * M + i] = cmul(A[kc * M + i], inv);
-            __syncthreads();
-            const int rem = M - kc - 1;
-            for (int it = tid; it < rem * rem; it += nth) {
-                int j = kc + 1 + it / rem, i = kc + 1 + it % rem;
-                cplx v = A[j * M + i];
-                cfma(v, cneg(A[kc * M + i]), A[j * M + kc]);
-                A[j * M + i] = v;
-            }
-            __syncthreads();
-        }
-        if (sing) {
+        if (!cta_lu(A, M, piv, &sing)) {
             if (tid == 0) atomicExch(status, 5);
             __syncthreads();
             continue;
@@ -348,38 +301,7 @@ __global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const doubl
                 B[jj * M + i] = v;
             }
             __syncthreads();
-            for (int kc = 0; kc < M; ++kc) {  // row interchanges in factorization order
-                const int pr = piv[kc];
-                if (pr != kc)
-                    for (int jj = tid; jj < nc; jj += nth) {
-                        double2 t = B[jj * M + kc];
-                        B[jj * M + kc] = B[jj * M + pr];
-                        B[jj * M + pr] = t;
-                    }
-                __syncthreads();
-            }
-            for (int kc = 0; kc < M - 1; ++kc) {  // unit lower
-                const int rem = M - kc - 1;
-                for (int it = tid; it < rem * nc; it += nth) {
-                    int jj = it / rem, i = kc + 1 + it % rem;
-                    cplx v = B[jj * M + i];
-                    cfma(v, cneg(A[kc * M + i]), B[jj * M + kc]);
-                    B[jj * M + i] = v;
-                }
-                __syncthreads();
-            }
-            for (int kc = M - 1; kc >= 0; --kc) {  // upper
-                const cplx inv = cinv(A[kc * M + kc]);
-                for (int jj = tid; jj < nc; jj += nth) B[jj * M + kc] = cmul(B[jj * M + kc], inv);
-                __syncthreads();
-                for (int it = tid; it < kc * nc; it += nth) {
-                    int jj = it / kc, i = it % kc;
-                    cplx v = B[jj * M + i];
-                    cfma(v, cneg(A[kc * M + i]), B[jj * M + kc]);
-                    B[jj * M + i] = v;
-                }
-                __syncthreads();
-            }
+            cta_lu_solve(A, M, piv, B, nc);
             for (int it = tid; it < M * nc; it += nth) {
                 int jj = it / M, i = it - jj * M;
                 Xk[(size_t)(c0 + jj) * M + i] = B[jj * M + i];

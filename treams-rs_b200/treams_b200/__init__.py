@@ -19,6 +19,7 @@ from ._lib import (  # noqa: F401
     cluster_operator,
     cross_sections,
     default_context,
+    learned_precond_gram,
     library_path,
     mie_blocks,
     plane_wave_expansion,

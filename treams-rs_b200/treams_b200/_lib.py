@@ -57,6 +57,8 @@ SIGNATURES = {
     "tcu_cluster_apply": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, P]),
     "tcu_cluster_apply_noalloc": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, P]),
     "tcu_iterative_solve": (c_int, [P, c_int, c_double, c_size, P, P, P, P, c_int, P, c_int, P, P]),
+    "tcu_context_set_learned_preconditioner": (c_int, [P, c_double, c_int, P]),
+    "tcu_learned_precond_gram": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, c_int, P, P, P]),
     "tcu_lsumsw2d_batch": (c_int, [P, c_int, c_double, P, c_size, P, c_double, P]),
     "tcu_array_solve_batch": (c_int, [P, c_int, c_double, c_double, P, P, c_size, P, c_double, P]),
 }
@@ -117,6 +119,16 @@ class Context:
         return lib().tcu_context_launches(self.handle)
 
     STAGES = ("assemble", "panel", "swap", "trsm", "gemm", "pack", "solve", "apply", "mie", "lattice", "small_lu")
+
+    def set_learned_preconditioner(self, reach: float = 3.0, alpha=None, layers: int | None = None) -> None:
+        """Near-field reach (sphere diameters) and layer weights of the GMRES preconditioners;
+        alpha None with layers None restores the compiled-in fit."""
+        if alpha is None:
+            nl = -1 if layers is None else int(layers)
+            _check(lib().tcu_context_set_learned_preconditioner(self.handle, float(reach), nl, None))
+        else:
+            a = np.ascontiguousarray(alpha, np.complex128)
+            _check(lib().tcu_context_set_learned_preconditioner(self.handle, float(reach), a.size - 1, _p(a)))
 
     def set_profiling(self, on: bool) -> None:
         _check(lib().tcu_context_set_profiling(self.handle, int(on)))
@@ -298,6 +310,22 @@ def sphere_cluster_factor(lmax: int, k0: float, radii, eps, positions, precision
 class IterativeSolution:
     value: np.ndarray
     convergence: list
+
+
+def learned_precond_gram(lmax: int, k0: float, radii, eps, positions, layers: int, V, ctx: Context | None = None):
+    """Training statistics of the learned preconditioner: (G, b) with G[k, l] = sum_v u_k^H u_l
+    and b[k] = sum_v u_k^H v for the layer basis u_k = A (D N)^k D v of the probe vectors V
+    (n x nvec). The loss sum_v ||v - sum_k alpha_k u_k||^2 is const - 2 Re(alpha^H b) +
+    alpha^H G alpha, with gradient 2 (G alpha - b)."""
+    ctx = ctx or default_context()
+    r, e, x = _geom(radii, eps, positions)
+    V = np.asfortranarray(V, np.complex128)
+    K1 = layers + 1
+    gram = np.zeros(K1 * K1, np.complex128)
+    rhs = np.zeros(K1, np.complex128)
+    _check(lib().tcu_learned_precond_gram(ctx.handle, lmax, float(k0), r.size, _p(r), _p(e), _p(x), layers,
+                                          V.shape[1], _p(V), _p(gram), _p(rhs)))
+    return gram.reshape(K1, K1), rhs
 
 
 class SphereCluster:

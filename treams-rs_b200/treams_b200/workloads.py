@@ -84,6 +84,14 @@ def learned_cluster(seed: int = 1004, count: int = 4096, fill: float = 0.2) -> C
                    np.array([1], np.int32))
 
 
+def training_cluster(i: int) -> Cluster:
+    """Training cluster i of the learned preconditioner: seed 2000 + i, N ~ U{64..1024}, otherwise
+    the 4096-sphere workload's distribution (r = 0.2 at 20% fill, eps 4+0.05i, k0 1.5, lmax 3)."""
+    rng = np.random.default_rng(2000 + i)
+    count = int(rng.integers(64, 1025))
+    return learned_cluster(seed=2000 + i, count=count)
+
+
 def batch_cluster(c: int, seed: int = 1003) -> Cluster:
     """Cluster c of the 256-cluster sweep: N ~ U{16..256}, lmax ~ U{3..6}, k0 ~ U[0.5, 3],
     r ~ U[0.1, 0.3], Re eps ~ U[2, 6], Im eps ~ U[0, 0.2], box for 15% fill."""
