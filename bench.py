@@ -141,6 +141,89 @@ def cpu_reference(samples: int, threads: int, count: int = 128, full: int = 512)
             "seconds_per_solve_full_size": best}
 
 
+def _timed(stream, fn):
+    """Device time (CUDA events on the library stream) and wall time of one call."""
+    import torch
+
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    out = fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return out, e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3
+
+
+def iterative_workload(ctx, stream) -> dict:
+    """The 4096-sphere lmax-3 matrix-free cluster (n = 122,880): GMRES(50) to 1e-8 without,
+    with block-Jacobi and with the learned preconditioner (set-up included)."""
+    import treams_b200 as t
+    from treams_b200 import workloads
+
+    w = workloads.learned_cluster()
+    c = t.SphereCluster(w.lmax, w.k0, w.radii, w.eps, w.positions, ctx=ctx)
+    B = t.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)[:, 0]
+    out = {"workload": "4096 spheres r 0.2, 20% fill, eps 4+0.05i, k0 1.5, lmax 3 (n=122880); GMRES(50) to 1e-8",
+           "unit": "solves/s"}
+    for kind in ("none", "block_jacobi", "learned"):
+        sol, ms, wall = _timed(stream, lambda: c.solve(B, rtol=1e-8, restart=50, max_iterations=600,
+                                                       preconditioner=kind))
+        cert = sol.convergence[0]
+        out[kind] = {"iterations": cert.iterations, "rel_residual": cert.residual_norm / cert.rhs_norm,
+                     "ms": ms, "value": 1e3 / ms}
+    out["iteration_ratio_block_jacobi_over_learned"] = out["block_jacobi"]["iterations"] / out["learned"]["iterations"]
+    return out
+
+
+def periodic_workload(ctx, stream) -> dict:
+    """The periodic array: square lattice (period 0.54), one sphere per cell (r 0.2, eps 9),
+    k0 4, lmax 6, 4096 Bloch vectors: lattice sums (degrees <= 12) and X = (I - T S)^-1 T."""
+    from treams_b200 import lattice as tl
+    from treams_b200 import workloads
+
+    w = workloads.periodic_array()
+    tl.array_solve_batch(w.lmax, w.k0, w.radius, w.eps, w.lattice, w.kpars[:8], ctx=ctx)  # warm-up
+    ctx.reset_stage_times()
+    ctx.set_profiling(True)
+    _, ms_sums, _ = _timed(stream, lambda: tl.lsumsw2d_batch(12, w.k0, w.lattice, w.kpars, ctx=ctx))
+    _, ms_all, _ = _timed(stream, lambda: tl.array_solve_batch(w.lmax, w.k0, w.radius, w.eps, w.lattice, w.kpars,
+                                                               ctx=ctx))
+    ctx.set_profiling(False)
+    st = ctx.stage_times()
+    nk = len(w.kpars)
+    lu_ms = st.get("small_lu", (0, 0.0))[1]
+    flops = nk * (8.0 / 3.0 * 96 ** 3 + 8.0 * 96 ** 3)
+    return {"workload": f"periodic array: period {w.period:.4f}, lmax 6, {nk} Bloch vectors", "unit": "kpar/s",
+            "lattice_sums_e2e_ms": ms_sums, "array_solve_e2e_ms": ms_all,
+            "array_solve_e2e_value": nk / (ms_all / 1e3),
+            "stages_ms": {k: v[1] for k, v in st.items()},
+            "array_kernel_fp64_tflops": flops / (lu_ms / 1e3) / 1e12 if lu_ms else None,
+            "note": "e2e includes the host copies of X (nk x 96 x 96 complex, 604 MB)"}
+
+
+def batch_workload(ctx, stream, count: int) -> dict:
+    """Clusters 0..count-1 of the 256-cluster heterogeneous sweep (N ~ U{16..256}, lmax ~
+    U{3..6}, k0 ~ U[0.5, 3]; one plane wave each) in one tcu_batch_solve call, precision auto."""
+    import treams_b200 as t
+    from treams_b200 import workloads
+
+    batch, modes = [], 0
+    for c in range(count):
+        w = workloads.batch_cluster(c)
+        B = t.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)
+        batch.append((w.lmax, w.k0, w.radii, w.eps, w.positions, B))
+        modes += w.n
+    t.batch_solve(batch[:2], "auto", ctx=ctx)  # warm-up
+    fb0 = ctx.fallbacks
+    (X, certs, order), ms, wall = _timed(stream, lambda: t.batch_solve(batch, "auto", ctx=ctx))
+    worst = max(c[0].residual_norm / c[0].rhs_norm for c in certs)
+    return {"workload": f"clusters 0..{count - 1} of the 256-cluster sweep ({modes} unknowns in total)",
+            "unit": "clusters/s", "value": count / (ms / 1e3), "ms": ms, "max_rel_residual": worst,
+            "fp64_fallbacks": ctx.fallbacks - fb0,
+            "precision": "auto (mixed from 2048 modes, else fp64)"}
+
+
 def run_reference(args, rank: int, world: int) -> None:
     if rank != 0:
         return
@@ -178,6 +261,10 @@ def main() -> None:
                     help="skip the plain FP64 comparison arm of the mixed headline")
     ap.add_argument("--compare-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
+    ap.add_argument("--no-extras", dest="extras", action="store_false",
+                    help="skip the 4096-sphere GMRES and the periodic-array workloads")
+    ap.add_argument("--batch-clusters", type=int, default=32,
+                    help="clusters of the 256-cluster heterogeneous sweep timed in the batch workload")
     ap.add_argument("--cpu-sample-spheres", type=int, default=128,
                     help="spheres of the bounded CPU sample (timed, then extrapolated to --spheres)")
     args = ap.parse_args()
@@ -230,6 +317,11 @@ def main() -> None:
                              dev=dev, world=world, local=local, dist=dist, barrier=barrier, reduce_max=reduce_max)
 
     head = measure(args.precision, args.steps, args.warmup, not args.no_e2e)
+    extras = {}
+    if args.extras:
+        extras["iterative"] = iterative_workload(ctx, stream)
+        extras["periodic"] = periodic_workload(ctx, stream)
+        extras["batch"] = batch_workload(ctx, stream, args.batch_clusters)
     other = None
     if args.compare and args.precision == "mixed":
         other = measure("fp64", min(args.steps, args.compare_steps), 1, False)
@@ -242,6 +334,7 @@ def main() -> None:
                             "roofline": o["roofline"], "stages_ms_per_step": o["stages_ms_per_step"],
                             "gpu_launches": o["gpu_launches"]}
             line["speedup_vs_fp64"] = line["value"] / o["value"]
+        line.update(extras)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference(1, os.cpu_count() or 1, args.cpu_sample_spheres, args.spheres)
             line["cpu_baseline"].pop("seconds_per_solve_full_size", None)

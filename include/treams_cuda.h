@@ -37,7 +37,8 @@ typedef enum tcu_status {
 
 typedef enum tcu_precision {
     TCU_FP64 = 0,   /* complex128 LU, FP64 DMMA trailing updates */
-    TCU_MIXED = 1   /* complex64 LU, 3-pass split-TF32 tcgen05 updates, FP64 refinement */
+    TCU_MIXED = 1,  /* complex64 LU, 3-pass split-TF32 tcgen05 updates, FP64 refinement */
+    TCU_AUTO = 2    /* batch solves only: per cluster, MIXED from n >= 2048 modes, else FP64 */
 } tcu_precision;
 
 typedef enum tcu_preconditioner {
@@ -74,6 +75,13 @@ void* tcu_context_stream(tcu_context* ctx);
 const char* tcu_last_error_message(void);
 /* Number of kernel launches the context has issued (a counter for benchmarks). */
 long long tcu_context_launches(tcu_context* ctx);
+/* Refinement tolerances of tcu_factor_solve on this context (no counterpart in the reference):
+ * sweeps stop at ||r|| <= target ||T b|| (default 1e-13); a mixed solve left above
+ * fallback_above ||T b|| (default 1e-12) is finished with an FP64 factor. */
+tcu_status tcu_context_set_refinement(tcu_context* ctx, double target, double fallback_above);
+/* Number of mixed-precision solves whose FP64 refinement stalled above 1e-12 and that were
+ * finished by an FP64 factor of the same cluster (made once per factor, then reused). */
+long long tcu_context_fallbacks(tcu_context* ctx);
 /* Per-stage device timing with CUDA events on the context stream (off by default).
  * Stages: 0 assembly, 1 LU panel, 2 row swaps, 3 triangular block (TRSM), 4 trailing
  * update GEMM, 5 operand packing, 6 triangular solves, 7 matrix-free operator, 8 Mie,
@@ -119,12 +127,39 @@ tcu_status tcu_sphere_cluster_factor_dev(tcu_context* ctx, int lmax, double k0, 
                                          tcu_factor** out);
 /* Solve (I - T C) X = T B for p incident columns B (n x p), X out (n x p); certificates
  * (p entries) may be NULL. Replaces InteractionFactor::solve (cluster/interaction.rs:214).
- * Mixed factors refine in FP64 until ||r|| <= 1e-13 ||T b|| (at most 10 sweeps). */
+ * The solve refines in FP64 until ||r|| <= 1e-13 ||T b|| (at most 10 sweeps on mixed factors, 2 on
+ * FP64 factors, stopping when a sweep does not halve the residual); if a mixed solve is left
+ * with ||r|| > 1e-12 ||T b||, it is
+ * finished with an FP64 factor (tcu_context_fallbacks counts these). */
 tcu_status tcu_factor_solve(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
 tcu_status tcu_factor_solve_dev(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
 /* Dimension n = N M of a factor. */
 size_t tcu_factor_dimension(const tcu_factor* f);
 tcu_status tcu_factor_destroy(tcu_factor* f);
+
+/* One cluster of a batch: geometry and materials (host arrays as for
+ * tcu_sphere_cluster_factor), p incident columns B (n x p) and the solution X (n x p). */
+typedef struct tcu_cluster_desc {
+    int lmax;
+    double k0;
+    size_t N;
+    const double* radii;
+    const double* eps;
+    const double* positions;
+    const double* B;
+    int p;
+    double* X;
+    tcu_certificate* certificates; /* p entries, or NULL */
+} tcu_cluster_desc;
+
+/* Solve a batch of independent clusters (no counterpart in the reference, which solves one
+ * cluster per call): largest first (n = N * 2 lmax (lmax + 2)), each assembled, factored,
+ * solved and released in turn on the context's stream, so device memory holds one cluster's
+ * operator at a time and the pooled allocator reuses it. precision: TCU_FP64, TCU_MIXED or
+ * TCU_AUTO. order (count entries, may be NULL) receives the processing order. Stops at the
+ * first failing cluster; the message names it. */
+tcu_status tcu_batch_solve(tcu_context* ctx, size_t count, const tcu_cluster_desc* clusters, int precision,
+                           int* order);
 
 /* The assembled operator I - T C (n x n complex128, column-major, host), for inspection. */
 tcu_status tcu_cluster_operator(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,

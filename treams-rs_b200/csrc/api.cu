@@ -98,6 +98,9 @@ struct tcu_context {
     // GMRES preconditioner settings (tcu_context_set_learned_preconditioner)
     double precond_reach = -1.0;  // near-field reach in sphere diameters (< 0: the compiled-in fit's)
     int learned_layers = -1;      // < 0: the compiled-in fit
+    long long fallbacks = 0;      // mixed solves finished by an FP64 factor
+    double refine_target = 1e-13; // refinement stops at ||r|| <= refine_target ||T b||
+    double fallback_above = 1e-12;  // mixed solves left above this finish in FP64
     std::vector<std::complex<double>> learned_alpha;
 };
 
@@ -114,6 +117,9 @@ struct tcu_factor {
     void* d_A = nullptr;
     double2* d_inv = nullptr;  // inverses of the diagonal blocks of L and U
     LuWork wk;
+    double* d_scale = nullptr;       // row scales (n) then column scales (n) when equilibrated
+    bool scaled = false;
+    tcu_factor* fallback = nullptr;  // FP64 factor of a mixed factor whose refinement stalled
 };
 
 namespace {
@@ -283,7 +289,7 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
     f->k0 = k0;
     auto cleanup = [&]() {
         for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
-                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack})
+                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack, (void*)f->d_scale})
             ctx->pool.free(q);
     };
     tcu_status e = TCU_OK;
@@ -318,6 +324,18 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
         if ((e = read_status(ctx, "Mie coefficients"))) break;
         launch_assemble(*P, (int)N, k0, f->d_pos, f->d_T, f->d_A, n, precision == TCU_MIXED, ctx->stream);
         ++ctx->launches;
+        {
+            // equilibrate when an entry exceeds 10 (then the unit diagonal no longer bounds the
+            // spread; linalg/mod.rs:137-228)
+            if ((e = dev_alloc(ctx, &f->d_scale, 2 * n, "scales"))) break;
+            DevBuf eq(ctx);
+            if ((e = cuda_check(eq.alloc(equilibrate_scratch_doubles((int)n) * sizeof(double)), "scales"))) break;
+            if ((e = equilibrate(f->d_A, precision == TCU_MIXED, (int)n, 10.0, f->d_scale, f->d_scale + n,
+                                 (double*)eq.p, &f->scaled, ctx->stream, &ctx->launches))) {
+                e = fail(e, "equilibration failed");
+                break;
+            }
+        }
         int rc;
         if (precision == TCU_FP64)
             rc = lu_factor_fp64((double2*)f->d_A, (int)n, f->wk, ctx->stream, &ctx->launches);
@@ -392,12 +410,17 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
     CK(cudaMemcpyAsync(bn.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "norms");
     int sweeps = 0;
     auto lu_apply = [&](cplx* v) {
+        if (f->scaled) scale_rows(v, f->d_scale, n, p, ctx->stream);  // R v
         if (f->precision == TCU_FP64)
             lu_solve_fp64((const double2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, p, ctx->stream,
                           &ctx->launches);
         else
             lu_solve_fp32((const float2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, p, ctx->stream,
                           &ctx->launches);
+        if (f->scaled) {
+            scale_rows(v, f->d_scale + n, n, p, ctx->stream);  // C (A')^-1 R v
+            ctx->launches += 2;
+        }
     };
     auto residual = [&]() -> tcu_status {
         // r = T b - (x - T C x)
@@ -411,10 +434,12 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
     lu_apply(x);
     sweeps = 1;
     if ((s = residual())) return s;
-    if (f->precision == TCU_MIXED) {
-        const double tol = 1e-13;
+    {
+        // iterative refinement in FP64: up to 10 sweeps on mixed factors, 2 on FP64 factors
+        const double tol = ctx->refine_target;
         double prev = INFINITY;
-        for (int it = 0; it < 10; ++it) {
+        const int max_sweeps = f->precision == TCU_MIXED ? 10 : 2;
+        for (int it = 0; it < max_sweeps; ++it) {
             double worst = 0.0;
             for (int c = 0; c < p; ++c) worst = std::max(worst, bn[c] > 0 ? rn[c] / bn[c] : rn[c]);
             if (worst <= tol || !(worst < 0.5 * prev)) break;
@@ -424,6 +449,26 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
             ++ctx->launches;
             ++sweeps;
             if ((s = residual())) return s;
+        }
+    }
+    if (f->precision == TCU_MIXED) {
+        // refinement stalled above the FP64 target (an ill-scaled operator beyond the reach of
+        // the TF32 factors): finish with an FP64 factor of the same cluster, kept for later solves
+        double worst = 0.0;
+        for (int c = 0; c < p; ++c) worst = std::max(worst, bn[c] > 0 ? rn[c] / bn[c] : rn[c]);
+        if (!(worst <= ctx->fallback_above)) {
+            if (!f->fallback) {
+                std::vector<double> hr(f->N), he(2 * (size_t)f->N), hp(3 * (size_t)f->N);
+                CK(cudaMemcpyAsync(hr.data(), f->d_radii, f->N * 8, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+                CK(cudaMemcpyAsync(he.data(), f->d_eps, f->N * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+                CK(cudaMemcpyAsync(hp.data(), f->d_pos, f->N * 24, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+                if ((s = sync_status(ctx, "fallback"))) return s;
+                if ((s = factor_impl(ctx, f->L, f->k0, f->N, hr.data(), he.data(), hp.data(), nullptr, nullptr,
+                                     nullptr, TCU_FP64, &f->fallback)))
+                    return s;
+            }
+            ++ctx->fallbacks;
+            return solve_impl(f->fallback, B, p, X, certs, device);
         }
     }
     for (int c = 0; c < p; ++c)
@@ -524,6 +569,7 @@ tcu_status tcu_context_reset_stage_times(tcu_context* ctx) {
     return TCU_OK;
 }
 long long tcu_context_launches(tcu_context* ctx) { return ctx ? ctx->launches : 0; }
+long long tcu_context_fallbacks(tcu_context* ctx) { return ctx ? ctx->fallbacks : 0; }
 
 tcu_status tcu_translation_block(tcu_context* ctx, int lmax, double k, const double* disp, int singular, int helicity,
                                  double* out) {
@@ -678,12 +724,13 @@ size_t tcu_factor_dimension(const tcu_factor* f) { return f ? f->n : 0; }
 
 tcu_status tcu_factor_destroy(tcu_factor* f) {
     if (!f) return TCU_OK;
+    if (f->fallback) tcu_factor_destroy(f->fallback);
     cudaSetDevice(f->ctx->device);
     cudaStreamSynchronize(f->ctx->stream);
     {
         std::lock_guard<std::recursive_mutex> lock(f->ctx->mu);
         for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
-                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack})
+                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack, (void*)f->d_scale})
             f->ctx->pool.free(q);
     }
     delete f;
@@ -1241,5 +1288,43 @@ extern "C" tcu_status tcu_context_set_learned_preconditioner(tcu_context* ctx, d
     ctx->learned_alpha.clear();
     if (layers >= 0 && alpha)
         for (int k = 0; k <= layers; ++k) ctx->learned_alpha.emplace_back(alpha[2 * k], alpha[2 * k + 1]);
+    return TCU_OK;
+}
+
+extern "C" tcu_status tcu_batch_solve(tcu_context* ctx, size_t count, const tcu_cluster_desc* clusters, int precision,
+                                      int* order) {
+    if (!ctx || (count > 0 && !clusters)) return fail(TCU_INVALID_INPUT, "null context or cluster list");
+    if (precision < TCU_FP64 || precision > TCU_AUTO) return fail(TCU_INVALID_INPUT, "unknown precision");
+    std::vector<size_t> idx(count);
+    for (size_t i = 0; i < count; ++i) {
+        const tcu_cluster_desc& c = clusters[i];
+        if (c.lmax < 1 || c.lmax > 7 || !c.B || !c.X || c.p <= 0)
+            return fail(TCU_INVALID_INPUT, "cluster " + std::to_string(i) + ": invalid lmax, incidence or output");
+        idx[i] = i;
+    }
+    auto modes = [&](size_t i) { return clusters[i].N * 2 * (size_t)clusters[i].lmax * (clusters[i].lmax + 2); };
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return modes(a) > modes(b); });
+    for (size_t q = 0; q < count; ++q) {
+        const size_t i = idx[q];
+        if (order) order[q] = (int)i;
+        const tcu_cluster_desc& c = clusters[i];
+        int prec = precision == TCU_AUTO ? (modes(i) >= 2048 ? TCU_MIXED : TCU_FP64) : precision;
+        tcu_factor* f = nullptr;
+        tcu_status s = tcu_sphere_cluster_factor(ctx, c.lmax, c.k0, c.N, c.radii, c.eps, c.positions, prec, &f);
+        if (s == TCU_OK) {
+            s = tcu_factor_solve(f, c.B, c.p, c.X, c.certificates);
+            tcu_factor_destroy(f);
+        }
+        if (s) return fail(s, "cluster " + std::to_string(i) + ": " + g_last_error);
+    }
+    return TCU_OK;
+}
+
+extern "C" tcu_status tcu_context_set_refinement(tcu_context* ctx, double target, double fallback_above) {
+    if (!ctx || !(target > 0.0) || !(fallback_above > 0.0) || !std::isfinite(target) || !std::isfinite(fallback_above))
+        return fail(TCU_INVALID_INPUT, "require positive finite refinement tolerances");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ctx->refine_target = target;
+    ctx->fallback_above = fallback_above;
     return TCU_OK;
 }

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include "../../include/treams_cuda.h"
 #include "plan.h"
 
 #include <vector>
@@ -87,6 +88,13 @@ void launch_plane_wave(int L, int N, const double* pos, int ncol, const cplx* kv
                        const double* lfac, cplx* out, cudaStream_t st);
 void launch_apply_t(int L, int N, const cplx* T, const cplx* x, int ncol, cplx* y, cudaStream_t st);
 void pairs_init_attributes();
+
+// equil.cu — power-of-two row/column equilibration of an n x n column-major matrix (FP64 or
+// FP32 storage) when its largest entry exceeds `threshold`; r, c: n scales each.
+size_t equilibrate_scratch_doubles(int n);
+tcu_status equilibrate(void* A, bool fp32, int n, double threshold, double* r, double* c, double* partial,
+                       bool* applied, cudaStream_t st, long long* launches);
+void scale_rows(cplx* v, const double* s, size_t n, int ncol, cudaStream_t st);
 
 // lattice.cu — 2D lattice sums at shift 0 and the batched periodic-array solve
 constexpr int LS_MAXL = 14;                // largest degree of a lattice sum

@@ -15,6 +15,7 @@ from ._lib import (  # noqa: F401
     InteractionFactor,
     SphereCluster,
     TreamsCudaError,
+    batch_solve,
     cluster_apply,
     cluster_operator,
     cross_sections,

@@ -40,6 +40,8 @@ SIGNATURES = {
     "tcu_context_stream": (P, [P]),
     "tcu_last_error_message": (ctypes.c_char_p, []),
     "tcu_context_launches": (ctypes.c_longlong, [P]),
+    "tcu_context_fallbacks": (ctypes.c_longlong, [P]),
+    "tcu_context_set_refinement": (c_int, [P, c_double, c_double]),
     "tcu_context_set_profiling": (c_int, [P, c_int]),
     "tcu_context_stage_time": (c_int, [P, c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(c_double)]),
     "tcu_context_reset_stage_times": (c_int, [P]),
@@ -57,6 +59,7 @@ SIGNATURES = {
     "tcu_cluster_apply": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, P]),
     "tcu_cluster_apply_noalloc": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, P]),
     "tcu_iterative_solve": (c_int, [P, c_int, c_double, c_size, P, P, P, P, c_int, P, c_int, P, P]),
+    "tcu_batch_solve": (c_int, [P, c_size, P, c_int, P]),
     "tcu_context_set_learned_preconditioner": (c_int, [P, c_double, c_int, P]),
     "tcu_learned_precond_gram": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, c_int, P, P, P]),
     "tcu_lsumsw2d_batch": (c_int, [P, c_int, c_double, P, c_size, P, c_double, P]),
@@ -119,6 +122,15 @@ class Context:
         return lib().tcu_context_launches(self.handle)
 
     STAGES = ("assemble", "panel", "swap", "trsm", "gemm", "pack", "solve", "apply", "mie", "lattice", "small_lu")
+
+    def set_refinement(self, target: float = 1e-13, fallback_above: float = 1e-12) -> None:
+        """Refinement stop tolerance and the residual above which mixed solves finish in FP64."""
+        _check(lib().tcu_context_set_refinement(self.handle, float(target), float(fallback_above)))
+
+    @property
+    def fallbacks(self) -> int:
+        """Mixed solves finished by an FP64 factor (refinement stalled)."""
+        return lib().tcu_context_fallbacks(self.handle)
 
     def set_learned_preconditioner(self, reach: float = 3.0, alpha=None, layers: int | None = None) -> None:
         """Near-field reach (sphere diameters) and layer weights of the GMRES preconditioners;
@@ -326,6 +338,38 @@ def learned_precond_gram(lmax: int, k0: float, radii, eps, positions, layers: in
     _check(lib().tcu_learned_precond_gram(ctx.handle, lmax, float(k0), r.size, _p(r), _p(e), _p(x), layers,
                                           V.shape[1], _p(V), _p(gram), _p(rhs)))
     return gram.reshape(K1, K1), rhs
+
+
+class ClusterDesc(ctypes.Structure):
+    _fields_ = [("lmax", c_int), ("k0", c_double), ("N", c_size), ("radii", P), ("eps", P), ("positions", P),
+                ("B", P), ("p", c_int), ("X", P), ("certificates", P)]
+
+
+PRECISION = {"fp64": 0, "mixed": 1, "auto": 2}
+
+
+def batch_solve(clusters, precision: str = "auto", ctx: Context | None = None):
+    """Solve independent clusters in one call (tcu_batch_solve): clusters is a list of
+    (lmax, k0, radii, eps, positions, B) with B (n, p); returns (list of X, list of certificate
+    lists, processing order). Largest clusters first; one operator resident at a time."""
+    ctx = ctx or default_context()
+    keep, descs, outs, certs = [], [], [], []
+    for lmax, k0, radii, eps, positions, B in clusters:
+        r, e, x = _geom(radii, eps, positions)
+        b = np.asfortranarray(B, np.complex128)
+        if b.ndim == 1:
+            b = b[:, None]
+        X = np.zeros_like(b, order="F")
+        cs = (Certificate * b.shape[1])()
+        keep += [r, e, x, b]
+        outs.append(X)
+        certs.append(cs)
+        descs.append(ClusterDesc(lmax, float(k0), r.size, _p(r), _p(e), _p(x), _p(b), b.shape[1], _p(X),
+                                 ctypes.addressof(cs)))
+    arr = (ClusterDesc * len(descs))(*descs)
+    order = (c_int * max(1, len(descs)))()
+    _check(lib().tcu_batch_solve(ctx.handle, len(descs), arr, PRECISION[precision], order))
+    return outs, [list(c) for c in certs], list(order)[:len(descs)]
 
 
 class SphereCluster:
