@@ -155,16 +155,16 @@ def _timed(stream, fn):
     return out, e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3
 
 
-def iterative_workload(ctx, stream) -> dict:
+def iterative_workload(ctx, stream, count: int = 4096) -> dict:
     """The 4096-sphere lmax-3 matrix-free cluster (n = 122,880): GMRES(50) to 1e-8 without,
     with block-Jacobi and with the learned preconditioner (set-up included)."""
     import treams_b200 as t
     from treams_b200 import workloads
 
-    w = workloads.learned_cluster()
+    w = workloads.learned_cluster(count=count)
     c = t.SphereCluster(w.lmax, w.k0, w.radii, w.eps, w.positions, ctx=ctx)
     B = t.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)[:, 0]
-    out = {"workload": "4096 spheres r 0.2, 20% fill, eps 4+0.05i, k0 1.5, lmax 3 (n=122880); GMRES(50) to 1e-8",
+    out = {"workload": f"{count} spheres r 0.2, 20% fill, eps 4+0.05i, k0 1.5, lmax 3 (n={w.n}); GMRES(50) to 1e-8",
            "unit": "solves/s"}
     for kind in ("none", "block_jacobi", "learned"):
         sol, ms, wall = _timed(stream, lambda: c.solve(B, rtol=1e-8, restart=50, max_iterations=600,
@@ -176,13 +176,13 @@ def iterative_workload(ctx, stream) -> dict:
     return out
 
 
-def periodic_workload(ctx, stream) -> dict:
+def periodic_workload(ctx, stream, nk: int = 4096) -> dict:
     """The periodic array: square lattice (period 0.54), one sphere per cell (r 0.2, eps 9),
     k0 4, lmax 6, 4096 Bloch vectors: lattice sums (degrees <= 12) and X = (I - T S)^-1 T."""
     from treams_b200 import lattice as tl
     from treams_b200 import workloads
 
-    w = workloads.periodic_array()
+    w = workloads.periodic_array(nk=nk)
     tl.array_solve_batch(w.lmax, w.k0, w.radius, w.eps, w.lattice, w.kpars[:8], ctx=ctx)  # warm-up
     ctx.reset_stage_times()
     ctx.set_profiling(True)
@@ -263,6 +263,8 @@ def main() -> None:
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
     ap.add_argument("--no-extras", dest="extras", action="store_false",
                     help="skip the 4096-sphere GMRES and the periodic-array workloads")
+    ap.add_argument("--iterative-spheres", type=int, default=4096)
+    ap.add_argument("--periodic-kpars", type=int, default=4096)
     ap.add_argument("--batch-clusters", type=int, default=32,
                     help="clusters of the 256-cluster heterogeneous sweep timed in the batch workload")
     ap.add_argument("--cpu-sample-spheres", type=int, default=128,
@@ -319,8 +321,8 @@ def main() -> None:
     head = measure(args.precision, args.steps, args.warmup, not args.no_e2e)
     extras = {}
     if args.extras:
-        extras["iterative"] = iterative_workload(ctx, stream)
-        extras["periodic"] = periodic_workload(ctx, stream)
+        extras["iterative"] = iterative_workload(ctx, stream, args.iterative_spheres)
+        extras["periodic"] = periodic_workload(ctx, stream, args.periodic_kpars)
         extras["batch"] = batch_workload(ctx, stream, args.batch_clusters)
     other = None
     if args.compare and args.precision == "mixed":

@@ -6,7 +6,9 @@
 
 namespace tcu {
 
-// A: M x M column-major (shared), piv: M (shared), sing: one shared int set to 1 when a
+constexpr int CTA_LU_MAXROWS = 3;  // rows per lane of the rank-1 update: M <= 96
+
+// A: M x M column-major (shared, M <= 96), piv: M (shared), sing: one shared int set to 1 when a
 // pivot is exactly zero. Returns false (on every thread) for a singular matrix.
 __device__ __forceinline__ bool cta_lu(double2* A, int M, int* piv, int* sing) {
     const int tid = threadIdx.x, nth = blockDim.x;
@@ -49,53 +51,71 @@ __device__ __forceinline__ bool cta_lu(double2* A, int M, int* piv, int* sing) {
         const cplx inv = cinv(A[kc * M + kc]);
         for (int i = kc + 1 + tid; i < M; i += nth) A[kc * M + i] = cmul(A[kc * M + i], inv);
         __syncthreads();
-        const int rem = M - kc - 1;
-        for (int it = tid; it < rem * rem; it += nth) {
-            int j = kc + 1 + it / rem, i = kc + 1 + it % rem;
-            cplx v = A[j * M + i];
-            cfma(v, cneg(A[kc * M + i]), A[j * M + kc]);
-            A[j * M + i] = v;
+        // rank-1 update: warps over columns, lanes over rows, the lane's multipliers in registers
+        const int lane = tid & 31, warp = tid >> 5, nwarps = nth >> 5;
+        cplx negl[CTA_LU_MAXROWS];
+#pragma unroll
+        for (int q = 0; q < CTA_LU_MAXROWS; ++q) {
+            const int i = kc + 1 + lane + 32 * q;
+            negl[q] = i < M ? cneg(A[kc * M + i]) : mk(0.0, 0.0);
+        }
+        for (int j = kc + 1 + warp; j < M; j += nwarps) {
+            const cplx xk = A[j * M + kc];
+#pragma unroll
+            for (int q = 0; q < CTA_LU_MAXROWS; ++q) {
+                const int i = kc + 1 + lane + 32 * q;
+                if (i < M) {
+                    cplx v = A[j * M + i];
+                    cfma(v, negl[q], xk);
+                    A[j * M + i] = v;
+                }
+            }
         }
         __syncthreads();
     }
     return true;
 }
 
-// B (M x nc column-major, shared) <- A^-1 B with the factors of cta_lu
+// B (M x nc column-major, shared) <- A^-1 B with the factors of cta_lu. One warp per
+// right-hand side: the row interchanges, then forward and backward substitution with lanes
+// over rows and only warp-level synchronisation between the steps. Every entry sees the same
+// operations in the same order as a row-parallel sweep would apply them.
 __device__ __forceinline__ void cta_lu_solve(const double2* A, int M, const int* piv, double2* B, int nc) {
-    const int tid = threadIdx.x, nth = blockDim.x;
-    for (int kc = 0; kc < M; ++kc) {  // row interchanges in factorization order
-        const int pr = piv[kc];
-        if (pr != kc)
-            for (int jj = tid; jj < nc; jj += nth) {
-                double2 t = B[jj * M + kc];
-                B[jj * M + kc] = B[jj * M + pr];
-                B[jj * M + pr] = t;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int jj = warp; jj < nc; jj += nwarps) {
+        double2* b = B + jj * M;
+        if (lane == 0)
+            for (int kc = 0; kc < M; ++kc) {
+                const int pr = piv[kc];
+                if (pr != kc) {
+                    double2 t = b[kc];
+                    b[kc] = b[pr];
+                    b[pr] = t;
+                }
             }
-        __syncthreads();
-    }
-    for (int kc = 0; kc < M - 1; ++kc) {  // unit lower
-        const int rem = M - kc - 1;
-        for (int it = tid; it < rem * nc; it += nth) {
-            int jj = it / rem, i = kc + 1 + it % rem;
-            cplx v = B[jj * M + i];
-            cfma(v, cneg(A[kc * M + i]), B[jj * M + kc]);
-            B[jj * M + i] = v;
+        __syncwarp();
+        for (int kc = 0; kc < M - 1; ++kc) {  // unit lower
+            const cplx xk = b[kc];
+            for (int i = kc + 1 + lane; i < M; i += 32) {
+                cplx v = b[i];
+                cfma(v, cneg(A[kc * M + i]), xk);
+                b[i] = v;
+            }
+            __syncwarp();
         }
-        __syncthreads();
-    }
-    for (int kc = M - 1; kc >= 0; --kc) {  // upper
-        const cplx inv = cinv(A[kc * M + kc]);
-        for (int jj = tid; jj < nc; jj += nth) B[jj * M + kc] = cmul(B[jj * M + kc], inv);
-        __syncthreads();
-        for (int it = tid; it < kc * nc; it += nth) {
-            int jj = it / kc, i = it % kc;
-            cplx v = B[jj * M + i];
-            cfma(v, cneg(A[kc * M + i]), B[jj * M + kc]);
-            B[jj * M + i] = v;
+        for (int kc = M - 1; kc >= 0; --kc) {  // upper
+            if (lane == 0) b[kc] = cmul(b[kc], cinv(A[kc * M + kc]));
+            __syncwarp();
+            const cplx xk = b[kc];
+            for (int i = lane; i < kc; i += 32) {
+                cplx v = b[i];
+                cfma(v, cneg(A[kc * M + i]), xk);
+                b[i] = v;
+            }
+            __syncwarp();
         }
-        __syncthreads();
     }
+    __syncthreads();
 }
 
 }  // namespace tcu

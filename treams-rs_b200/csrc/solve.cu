@@ -112,6 +112,10 @@ __global__ void __launch_bounds__(256) trsv_inv_step_kernel(const C* __restrict_
     __shared__ double2 part[4][NC][SB];
     __shared__ double2 xb[NC][SB];
     constexpr int KH = 16;  // preloaded first chunk of the block column
+    // Programmatic dependent launch: the next step may start its read-only preloads (its
+    // Dinv quarter and block column) while this one runs; it reads the right-hand side only
+    // after griddepcontrol.wait, i.e. after this grid has completed and its writes are visible.
+    asm volatile("griddepcontrol.launch_dependents;");
     const int tid = threadIdx.x;
     const int i = tid % SB, kq = tid / SB;  // Dinv row and K quarter
     double2 d[16];
@@ -130,6 +134,7 @@ __global__ void __launch_bounds__(256) trsv_inv_step_kernel(const C* __restrict_
             av[u].y = 0;
         }
     }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     for (int idx = tid; idx < SB * NC; idx += blockDim.x) {
         int ii = idx % SB, c = idx / SB;
         rb[c][ii] = ii < bw ? r[(size_t)c * n + b0 + ii] : make_double2(0.0, 0.0);
@@ -207,12 +212,28 @@ __global__ void __launch_bounds__(256) trsv_inv_step_kernel(const C* __restrict_
 
 static int g_sms = 0;
 
+template <typename C, bool LOWER, int NC>
+static void step_launch_nc(cudaStream_t st, const C* A, int n, int b0, int bw, const double2* dinv, double2* r,
+                           double2* sol) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(g_sms);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, trsv_inv_step_kernel<C, LOWER, NC>, A, (size_t)n, n, b0, bw, dinv, r, sol);
+}
+
 template <typename C, bool LOWER>
 static void step_launch(int nc, cudaStream_t st, const C* A, int n, int b0, int bw, const double2* dinv, double2* r,
                         double2* sol) {
     switch (nc) {
 #define TV_CASE(K) \
-    case K: trsv_inv_step_kernel<C, LOWER, K><<<g_sms, 256, 0, st>>>(A, n, n, b0, bw, dinv, r, sol); break;
+    case K: step_launch_nc<C, LOWER, K>(st, A, n, b0, bw, dinv, r, sol); break;
         TV_CASE(1) TV_CASE(2) TV_CASE(3) TV_CASE(4) TV_CASE(5) TV_CASE(6) TV_CASE(7) TV_CASE(8)
 #undef TV_CASE
     }
