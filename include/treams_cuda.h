@@ -37,7 +37,7 @@ typedef enum tcu_status {
 
 typedef enum tcu_precision {
     TCU_FP64 = 0,   /* complex128 LU, FP64 DMMA trailing updates */
-    TCU_MIXED = 1,  /* complex64 LU, 3-pass split-TF32 tcgen05 updates, FP64 refinement */
+    TCU_MIXED = 1,  /* complex64 LU, 3-pass split tcgen05 updates (FP16 or TF32 pieces), FP64 refinement */
     TCU_AUTO = 2    /* batch solves only: per cluster, MIXED from n >= 2048 modes, else FP64 */
 } tcu_precision;
 
@@ -68,6 +68,7 @@ typedef struct tcu_gmres_options {
 
 /* ---- context ------------------------------------------------------------------------ */
 tcu_status tcu_context_create(int device, tcu_context** out);
+/* Destroys the context and every factor still alive on it (their handles become invalid). */
 tcu_status tcu_context_destroy(tcu_context* ctx);
 /* The CUDA stream (cudaStream_t) the context runs on, for callers with device pointers. */
 void* tcu_context_stream(tcu_context* ctx);
@@ -79,8 +80,8 @@ long long tcu_context_launches(tcu_context* ctx);
  * sweeps stop at ||r|| <= target ||T b|| (default 1e-13); a mixed solve left above
  * fallback_above ||T b|| (default 1e-12) is finished with an FP64 factor. */
 tcu_status tcu_context_set_refinement(tcu_context* ctx, double target, double fallback_above);
-/* Number of mixed-precision solves whose FP64 refinement stalled above 1e-12 and that were
- * finished by an FP64 factor of the same cluster (made once per factor, then reused). */
+/* Number of mixed-precision solves whose FP64 refinement stalled above the fallback tolerance
+ * and that were finished by a second factor (TF32 pieces, then FP64) of the same cluster. */
 long long tcu_context_fallbacks(tcu_context* ctx);
 /* Per-stage device timing with CUDA events on the context stream (off by default).
  * Stages: 0 assembly, 1 LU panel, 2 row swaps, 3 triangular block (TRSM), 4 trailing
@@ -129,8 +130,9 @@ tcu_status tcu_sphere_cluster_factor_dev(tcu_context* ctx, int lmax, double k0, 
  * (p entries) may be NULL. Replaces InteractionFactor::solve (cluster/interaction.rs:214).
  * The solve refines in FP64 until ||r|| <= 1e-13 ||T b|| (at most 10 sweeps on mixed factors, 2 on
  * FP64 factors, stopping when a sweep does not halve the residual); if a mixed solve is left
- * with ||r|| > 1e-12 ||T b||, it is
- * finished with an FP64 factor (tcu_context_fallbacks counts these). */
+ * with ||r|| > 1e-12 ||T b||, it is finished with a second factor of the same cluster, made once
+ * and kept: a mixed one with TF32 pieces after FP16 pieces, an FP64 one after TF32 pieces
+ * (tcu_context_fallbacks counts these solves). */
 tcu_status tcu_factor_solve(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
 tcu_status tcu_factor_solve_dev(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
 /* Dimension n = N M of a factor. */

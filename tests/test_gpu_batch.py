@@ -50,26 +50,57 @@ def test_batch_reports_the_failing_cluster(ctx):
         t.batch_solve([(lmax, k0, r, e, x, B), (lmax, k0, r, e, bad, B)], "fp64", ctx=ctx)
 
 
-def test_mixed_solve_falls_back_to_fp64_when_refinement_stalls():
-    # With equilibration the sweep's clusters all refine to 1e-13 in a few sweeps, so the
-    # fallback is exercised by demanding a residual no refinement reaches (1e-300): the solve
-    # must then finish with an FP64 factor of the same cluster, kept for later solves.
+def test_stalled_mixed_refinement_falls_back_to_a_second_factor():
+    # Cluster 18 of the sweep (28 spheres, lmax 6, k0 d down to 0.21): the mixed factor refines
+    # to 1e-13 (with FP16 pieces, opt-in, after one step to TF32 pieces). Demanding a residual
+    # no refinement reaches (1e-300) then exercises the last level of the chain, FP64.
     ctx = t.Context(0)
-    w = workloads.batch_cluster(18)
-    B = t.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)
-    ref = t.sphere_cluster_factor(w.lmax, w.k0, w.radii, w.eps, w.positions, "fp64", ctx=ctx)
-    X0, _ = ref.solve(B)
-    f = t.sphere_cluster_factor(w.lmax, w.k0, w.radii, w.eps, w.positions, "mixed", ctx=ctx)
-    X1, c1 = f.solve(B)
-    assert ctx.fallbacks == 0 and c1[0].residual_norm <= 1e-13 * c1[0].rhs_norm
-    ctx.set_refinement(1e-13, 1e-300)
-    X, certs = f.solve(B)
-    assert ctx.fallbacks == 1
-    assert certs[0].residual_norm <= 1e-12 * certs[0].rhs_norm
-    assert np.linalg.norm(X - X0) <= 1e-10 * np.linalg.norm(X0)
-    X2, _ = f.solve(B)  # the FP64 factor is kept
-    assert ctx.fallbacks == 2 and np.array_equal(X2, X)
-    ctx.set_refinement()
-    f.close()
-    ref.close()
-    ctx.close()
+    try:
+        w = workloads.batch_cluster(18)
+        B = t.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)
+        ref = t.sphere_cluster_factor(w.lmax, w.k0, w.radii, w.eps, w.positions, "fp64", ctx=ctx)
+        X0, _ = ref.solve(B)
+        f = t.sphere_cluster_factor(w.lmax, w.k0, w.radii, w.eps, w.positions, "mixed", ctx=ctx)
+        X1, c1 = f.solve(B)
+        first = ctx.fallbacks
+        assert first <= 1  # at most the step to TF32 pieces
+        assert c1[0].residual_norm <= 1e-13 * c1[0].rhs_norm
+        assert np.linalg.norm(X1 - X0) <= 1e-10 * np.linalg.norm(X0)
+        ctx.set_refinement(1e-13, 1e-300)
+        X, certs = f.solve(B)
+        assert ctx.fallbacks > first
+        assert certs[0].residual_norm <= 1e-12 * certs[0].rhs_norm
+        assert np.linalg.norm(X - X0) <= 1e-10 * np.linalg.norm(X0)
+        n2 = ctx.fallbacks
+        X2, _ = f.solve(B)  # the second factors are kept
+        assert ctx.fallbacks > n2 and np.array_equal(X2, X)
+    finally:
+        ctx.close()
+
+
+def test_fp16_pieces_opt_in_reaches_the_fp64_target():
+    # TCU_SPLIT=f16 (read once per process, so in a child) switches the 3-pass split to
+    # row-scaled FP16 pieces; the solve must still reach the FP64 target, directly or through
+    # the fallback chain, and agree with the FP64 factor.
+    import os
+    import subprocess
+    import sys
+
+    from conftest import ROOT
+
+    code = """
+import numpy as np, treams_b200 as t
+from treams_b200 import workloads
+w = workloads.precision_cluster(count=64)
+ctx = t.Context(0)
+B = t.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)
+X0, _ = t.sphere_cluster_factor(w.lmax, w.k0, w.radii, w.eps, w.positions, 'fp64', ctx=ctx).solve(B)
+X, c = t.sphere_cluster_factor(w.lmax, w.k0, w.radii, w.eps, w.positions, 'mixed', ctx=ctx).solve(B)
+print(max(x.residual_norm / x.rhs_norm for x in c), np.linalg.norm(X - X0) / np.linalg.norm(X0), ctx.fallbacks)
+ctx.close()
+"""
+    env = dict(os.environ, TCU_SPLIT="f16", PYTHONPATH=f"{ROOT}:{ROOT / 'treams-rs_b200'}")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    res, err, fallbacks = out.stdout.split()
+    assert float(res) <= 1e-12 and float(err) <= 1e-10

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -98,7 +99,8 @@ struct tcu_context {
     // GMRES preconditioner settings (tcu_context_set_learned_preconditioner)
     double precond_reach = -1.0;  // near-field reach in sphere diameters (< 0: the compiled-in fit's)
     int learned_layers = -1;      // < 0: the compiled-in fit
-    long long fallbacks = 0;      // mixed solves finished by an FP64 factor
+    long long fallbacks = 0;      // mixed solves finished by a second factor
+    std::set<tcu_factor*> factors;  // live factors (destroyed with the context)
     double refine_target = 1e-13; // refinement stops at ||r|| <= refine_target ||T b||
     double fallback_above = 1e-12;  // mixed solves left above this finish in FP64
     std::vector<std::complex<double>> learned_alpha;
@@ -268,7 +270,7 @@ void apply_op(tcu_context* ctx, const DevPlan* P, int N, double k0, const double
 
 tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const double* radii_h, const double* eps_h,
                        const double* pos_h, const double* radii_d, const double* eps_d, const double* pos_d,
-                       int precision, tcu_factor** out) {
+                       int precision, tcu_factor** out, bool f16_pieces = true) {
     if (!out) return fail(TCU_INVALID_INPUT, "null output handle");
     *out = nullptr;
     if (precision != TCU_FP64 && precision != TCU_MIXED) return fail(TCU_INVALID_INPUT, "unknown precision");
@@ -287,6 +289,7 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
     f->n = n;
     f->precision = precision;
     f->k0 = k0;
+    f->wk.f16_pieces = f16_pieces && split_f16_default();
     auto cleanup = [&]() {
         for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
                         (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack, (void*)f->d_scale})
@@ -376,6 +379,7 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
         return e;
     }
     *out = f.release();
+    ctx->factors.insert(*out);
     return TCU_OK;
 }
 
@@ -457,14 +461,17 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
         double worst = 0.0;
         for (int c = 0; c < p; ++c) worst = std::max(worst, bn[c] > 0 ? rn[c] / bn[c] : rn[c]);
         if (!(worst <= ctx->fallback_above)) {
+            // FP16 pieces first fall back to a mixed factor with TF32 pieces (which keep 22
+            // bits relative to every element), that one in turn to FP64
             if (!f->fallback) {
                 std::vector<double> hr(f->N), he(2 * (size_t)f->N), hp(3 * (size_t)f->N);
                 CK(cudaMemcpyAsync(hr.data(), f->d_radii, f->N * 8, cudaMemcpyDeviceToHost, ctx->stream), "copy");
                 CK(cudaMemcpyAsync(he.data(), f->d_eps, f->N * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
                 CK(cudaMemcpyAsync(hp.data(), f->d_pos, f->N * 24, cudaMemcpyDeviceToHost, ctx->stream), "copy");
                 if ((s = sync_status(ctx, "fallback"))) return s;
+                const bool to_tf32 = f->wk.f16_pieces;
                 if ((s = factor_impl(ctx, f->L, f->k0, f->N, hr.data(), he.data(), hp.data(), nullptr, nullptr,
-                                     nullptr, TCU_FP64, &f->fallback)))
+                                     nullptr, to_tf32 ? TCU_MIXED : TCU_FP64, &f->fallback, false)))
                     return s;
             }
             ++ctx->fallbacks;
@@ -527,6 +534,7 @@ tcu_status tcu_context_destroy(tcu_context* ctx) {
     if (!ctx) return TCU_OK;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    while (!ctx->factors.empty()) tcu_factor_destroy(*ctx->factors.begin());  // factors left alive
     for (auto& kv : ctx->plans) cudaFree(kv.second->mem);
     ctx->pool.release();
     cudaFree(ctx->d_partial);
@@ -729,6 +737,7 @@ tcu_status tcu_factor_destroy(tcu_factor* f) {
     cudaStreamSynchronize(f->ctx->stream);
     {
         std::lock_guard<std::recursive_mutex> lock(f->ctx->mu);
+        f->ctx->factors.erase(f);
         for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
                         (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack, (void*)f->d_scale})
             f->ctx->pool.free(q);

@@ -6,24 +6,36 @@
 // so that D[2mu+c][nu] is part c of (L21 U12)[mu][nu] and the 2m x n' result maps onto
 // the interleaved storage of A22 (real leading dimension 2n).
 //
-// Precision: every operand is split x = hi + lo with hi = tf32(x), lo = tf32(x - hi), and
-// three tcgen05.mma kind::tf32 passes hi*hi + hi*lo + lo*hi accumulate in FP32 in TMEM
-// (the lo*lo term is below FP32 rounding).
+// Precision: every operand is split x = hi + lo into two 11-bit-significand pieces and three
+// passes hi*hi + hi*lo + lo*hi accumulate in FP32 in TMEM (the lo*lo term is below FP32
+// rounding). Two piece formats:
+//   FP16 (TCU_SPLIT=f16): each row of each operand (a complex row of L21, a column of U12) is
+//     first scaled by its own power of two 2^(14 - ceil log2 max|row|) (computed in the
+//     packing kernels; no host round trip), hi = f16(x s), lo = f16(x s - hi);
+//     tcgen05.mma kind::f16 runs at twice the TF32 rate and the epilogue multiplies each
+//     accumulator entry by the exact power of two 1/(s_row s_col). Pieces below the FP16
+//     normal range only lose absolute accuracy under 2^-38 of their row's maximum.
+//   TF32 (default): hi = tf32(x), lo = tf32(x - hi), tcgen05.mma kind::tf32.
+// Both give a product accurate to about 2^-22 of max|A| max|B| per term.
 //
 // Kernel layout (persistent, one CTA per SM, 192 threads):
-//   warp 0     TMA producer: 128-byte-swizzled boxes of the four packed operands into a
-//              2-stage shared-memory ring (96 KB per stage), mbarrier complete_tx;
-//   warp 1     TMEM allocator and MMA issuer (one thread): 4 K-steps x 3 passes per stage
+//   warp 0     TMA producer: 64-byte-swizzled boxes (64-byte K rows) of the four packed
+//              operands into a 3-stage shared-memory ring (48 KB per stage), mbarrier complete_tx;
+//   warp 1     TMEM allocator and MMA issuer (one thread): 2 K-steps x 3 passes per stage
 //              into a 128 x 256 FP32 accumulator, double-buffered in TMEM (512 columns);
-//   warps 2-5  epilogue: tcgen05.ld 32 columns at a time, A22 -= D with coalesced stores.
+//   warps 2-5  epilogue: tcgen05.ld 32 columns at a time into a shared-memory staging buffer,
+//              TMA reduce-add of -D into A22.
 // Every mbarrier wait is bounded; on timeout the kernel records status 8, drains its TMA
 // loads, frees TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 
 #include "kernels.h"
 #include "precond.h"
@@ -32,7 +44,7 @@ namespace tcu {
 
 constexpr int TB_M = 128;       // real rows per tile (64 complex rows)
 constexpr int TB_N = 256;       // columns per tile
-constexpr int TB_K = 16;        // floats per K chunk (one 64-byte swizzle row)
+constexpr int TB_K = 16;        // floats per K chunk (one 64-byte swizzle row); 32 for FP16 pieces
 constexpr int TB_STAGES = 3;
 constexpr int A_BYTES = TB_M * TB_K * 4;   // 8 KB
 constexpr int B_BYTES = TB_N * TB_K * 4;   // 16 KB
@@ -127,6 +139,28 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b
         "l"(a), "l"(b), "r"(idesc), "r"(acc)
         : "memory");
 }
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+template <bool F16>
+__device__ __forceinline__ void mma_split(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    if (F16)
+        mma_f16(d_tmem, a, b, idesc, acc);
+    else
+        mma_tf32(d_tmem, a, b, idesc, acc);
+}
+// Power-of-two scale that maps max |x| to (2^13, 2^14]: exact, and far inside the FP16 range.
+__device__ __forceinline__ float f16_scale(float mx) {
+    if (!(mx > 0.0f) || !isfinite(mx)) return 1.0f;
+    int e;
+    frexpf(mx, &e);  // mx = f 2^e, 0.5 <= f < 1
+    return ldexpf(1.0f, 14 - e);
+}
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
@@ -159,8 +193,11 @@ struct Tf32Args {
     int kchunks;     // K / TB_K
     int tiles_m, tiles_n, tiles;
     int* status;
+    const float* sA;      // FP16 pieces: scale of each complex row of the A operand (m2 / 2), else null
+    const float* sB;      // FP16 pieces: scale of each row of the B operand (ncols)
 };
 
+template <bool F16>
 __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_constant__ CUtensorMap mAhi,
                                                              const __grid_constant__ CUtensorMap mAlo,
                                                              const __grid_constant__ CUtensorMap mBhi,
@@ -229,7 +266,9 @@ __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_consta
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TB_N >> 3) << 17) |
+            // D F32; A, B TF32 (2) or F16 (0); K-major; N >> 3 at bit 17, M >> 4 at bit 24
+            const uint32_t ab = F16 ? 0u : 2u;
+            const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(TB_N >> 3) << 17) |
                                    ((uint32_t)(TB_M >> 4) << 24);
             int step = 0, it = 0;
             for (int t = blockIdx.x; t < args.tiles && !*abort_flag; t += gridDim.x, ++it) {
@@ -249,14 +288,14 @@ __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_consta
                     fence_after();
                     uint32_t st = tiles_smem + s * STAGE_BYTES;
 #pragma unroll
-                    for (int ks = 0; ks < TB_K / 8; ++ks) {
+                    for (int ks = 0; ks < 2; ++ks) {  // two 32-byte K-steps per 64-byte row
                         uint64_t ahi = swz_desc(st + ks * 32), alo = swz_desc(st + A_BYTES + ks * 32);
                         uint64_t bhi = swz_desc(st + 2 * A_BYTES + ks * 32);
                         uint64_t blo = swz_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
                         uint32_t first = (kb == 0 && ks == 0) ? 0u : 1u;
-                        mma_tf32(d, ahi, bhi, idesc, first);
-                        mma_tf32(d, ahi, blo, idesc, 1u);
-                        mma_tf32(d, alo, bhi, idesc, 1u);
+                        mma_split<F16>(d, ahi, bhi, idesc, first);
+                        mma_split<F16>(d, ahi, blo, idesc, 1u);
+                        mma_split<F16>(d, alo, bhi, idesc, 1u);
                     }
                     mma_commit(bar(EMPTY + s));
                 }
@@ -271,6 +310,8 @@ __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_consta
         const int R = q * 32 + lane;
         const bool issuer = (warp == 2 && lane == 0);
         volatile int* s_go = abort_flag + 1;  // the issuer's wait result, shared by the 4 warps
+        // FP16 pieces: -1 / (row scale x column scale) undoes the operand scaling exactly
+        const int grow = R;  // row of the tile this thread stores
         int it = 0, e = 0;
         for (int t = blockIdx.x; t < args.tiles; t += gridDim.x, ++it) {
             int acc = it & 1;
@@ -283,6 +324,11 @@ __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_consta
             fence_after();
             int tm, tn;
             tile_coords(t, args.tiles_m, args.tiles_n, tm, tn);
+            float rowneg = -1.0f;
+            if (F16) {
+                const int mu = (tm * TB_M + grow) >> 1;
+                rowneg = mu < (args.m2 >> 1) ? -1.0f / __ldg(&args.sA[mu]) : -1.0f;
+            }
             for (int sub = 0; sub < TB_N / EPI_COLS; ++sub, ++e) {
                 const int buf = e & 1;
                 if (issuer) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
@@ -295,7 +341,14 @@ __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_consta
                                      (uint32_t)(acc * TB_N + sub * EPI_COLS + cb * 32);
                     tmem_ld32(taddr, v);
 #pragma unroll
-                    for (int jj = 0; jj < 32; ++jj) stage[(cb * 32 + jj) * TB_M + R] = -v[jj];
+                    for (int jj = 0; jj < 32; ++jj) {
+                        float f = rowneg;
+                        if (F16) {
+                            const int col = tn * TB_N + sub * EPI_COLS + cb * 32 + jj;
+                            f = col < args.ncols ? rowneg / __ldg(&args.sB[col]) : rowneg;
+                        }
+                        stage[(cb * 32 + jj) * TB_M + R] = f * v[jj];
+                    }
                 }
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 asm volatile("bar.sync 1, 128;" ::: "memory");
@@ -381,6 +434,92 @@ __global__ void negate_kernel(float* __restrict__ p, size_t count) {
     if (t < count) p[t] = -p[t];
 }
 
+// ---- FP16 pieces -----------------------------------------------------------------------
+// Every row of the A operand (complex row mu of L21, both its real rows) and every row of the
+// B operand (column nu of U12) gets its own power-of-two scale f16_scale(max over its K
+// entries), so each row's pieces keep 22 bits relative to that row's largest entry.
+
+__device__ __forceinline__ void split16(float x, float s, __half& hi, __half& lo) {
+    float xs = x * s;
+    hi = __float2half_rn(xs);
+    lo = __float2half_rn(xs - __half2float(hi));
+}
+
+// Lemb pieces (2m x kp halves, row-major) of 32 complex rows per CTA (K <= 256 real, i.e.
+// w <= 128); sign -1 negates. sA[mu] receives the row's scale.
+__global__ void __launch_bounds__(256) pack_l16_kernel(const float2* __restrict__ A, size_t lda, int r0, int k0, int m,
+                                                       int w, int kp, float sign, __half* __restrict__ hi,
+                                                       __half* __restrict__ lo, float* __restrict__ sA) {
+    __shared__ float2 tile[128][33];  // [kk][mu]
+    __shared__ float scale[32];
+    const int mu0 = blockIdx.x * 32, half = kp / 2;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+    for (int kk = ty; kk < half; kk += 8) {
+        int mu = mu0 + tx;
+        tile[kk][tx] = (kk < w && mu < m) ? A[(size_t)(k0 + kk) * lda + r0 + mu] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {  // warp ty: rows r; lanes over K
+        float mx = 0.0f;
+        for (int kk = tx; kk < half; kk += 32) mx = fmaxf(mx, fmaxf(fabsf(tile[kk][r].x), fabsf(tile[kk][r].y)));
+        for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (tx == 0) {
+            float sc = f16_scale(mx);
+            scale[r] = sign * sc;
+            if (mu0 + r < m) sA[mu0 + r] = sc;
+        }
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int mu = mu0 + r;
+        if (mu >= m) continue;
+        const float sc = scale[r];
+        for (int kk = tx; kk < half; kk += 32) {
+            float2 l = tile[kk][r];
+            __half rh, rl, ih, il;
+            split16(l.x, sc, rh, rl);
+            split16(l.y, sc, ih, il);
+            size_t o0 = (size_t)(2 * mu) * kp + 2 * kk, o1 = o0 + kp;
+            *(__half2*)(hi + o0) = __halves2half2(rh, __hneg(ih));
+            *(__half2*)(hi + o1) = __halves2half2(ih, rh);
+            *(__half2*)(lo + o0) = __halves2half2(rl, __hneg(il));
+            *(__half2*)(lo + o1) = __halves2half2(il, rl);
+        }
+    }
+}
+
+// U pieces (n' x kp halves, row-major): row nu = interleaved column nu of U12; one warp per
+// row, sB[nu] its scale.
+__global__ void __launch_bounds__(256) pack_u16_kernel(const float2* __restrict__ A, size_t lda, int r0, int k0,
+                                                       int ncols, int w, int kp, __half* __restrict__ hi,
+                                                       __half* __restrict__ lo, float* __restrict__ sB) {
+    const int nu = (int)(((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (nu >= ncols) return;
+    const int half = kp / 2;
+    float2 u[4];  // kp / 2 <= 128 values per row
+    float mx = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        int kk = lane + 32 * q;
+        u[q] = (kk < w && kk < half) ? A[(size_t)(r0 + nu) * lda + k0 + kk] : make_float2(0.f, 0.f);
+        mx = fmaxf(mx, fmaxf(fabsf(u[q].x), fabsf(u[q].y)));
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const float sc = f16_scale(mx);
+    if (lane == 0) sB[nu] = sc;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        int kk = lane + 32 * q;
+        if (kk >= half) continue;
+        __half rh, rl, ih, il;
+        split16(u[q].x, sc, rh, rl);
+        split16(u[q].y, sc, ih, il);
+        size_t o = (size_t)nu * kp + 2 * kk;
+        *(__half2*)(hi + o) = __halves2half2(rh, ih);
+        *(__half2*)(lo + o) = __halves2half2(rl, il);
+    }
+}
+
 // ---- host -------------------------------------------------------------------------------
 typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -398,16 +537,32 @@ static EncodeTiled encoder() {
     return fn;
 }
 
-static bool make_map(CUtensorMap* map, float* base, int rows, int kp, int box_rows) {
+// K-major operand of `rows` rows of kp elements (4-byte TF32 pieces or 2-byte FP16 pieces);
+// boxes are one 64-byte swizzle row deep (16 or 32 elements).
+static bool make_map(CUtensorMap* map, void* base, int rows, int kp, int box_rows, bool f16) {
     EncodeTiled enc = encoder();
     if (!enc) return false;
+    const int eb = f16 ? 2 : 4;
     cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)kp * 4};
-    cuuint32_t box[2] = {(cuuint32_t)TB_K, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kp * eb};
+    cuuint32_t box[2] = {(cuuint32_t)(64 / eb), (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
-    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-               CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    return enc(map, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box,
+               estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// TF32 pieces by default; FP16 pieces (twice the tensor rate) with TCU_SPLIT=f16. On the
+// cluster operators measured here the entries of one row of L21 or one column of U12 span
+// more than 2^20 even after equilibration, and FP16 pieces (8 exponent bits fewer) then leave
+// the FP64 refinement stalled, so every solve fell back to TF32 pieces.
+bool split_f16_default() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = getenv("TCU_SPLIT");
+        on = (e && std::strcmp(e, "f16") == 0) ? 1 : 0;
+    }
+    return on == 1;
 }
 
 bool tf32_enabled() {
@@ -416,7 +571,8 @@ bool tf32_enabled() {
         const char* e = getenv("TCU_DISABLE_TCGEN05");
         on = (e && e[0] == '1') ? 0 : 1;
         if (on) {
-            cudaFuncSetAttribute(tf32_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
+            cudaFuncSetAttribute(tf32_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
+            cudaFuncSetAttribute(tf32_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
             if (!encoder()) on = 0;
         }
     }
@@ -531,12 +687,14 @@ static bool ensure_pack(LuWork& wk, size_t need, int n, cudaStream_t st) {
     return true;
 }
 
-// C[row0 .. row0+m2) x [col0 .. col0+ncols) -= Apack (m2 x kp) * Bpack (ncols x kp)^T
-static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, int kp, float* ahi, float* alo,
-                     float* bhi, float* blo, LuWork& wk, cudaStream_t st, long long* launches) {
+// C[row0 .. row0+m2) x [col0 .. col0+ncols) -= Apack (m2 x kp) * Bpack (ncols x kp)^T;
+// sA != null selects FP16 pieces (row scales sA of the A operand, sB of the B operand).
+static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, int kp, void* ahi, void* alo, void* bhi,
+                     void* blo, const float* sA, const float* sB, LuWork& wk, cudaStream_t st, long long* launches) {
+    const bool f16 = sA != nullptr;
     CUtensorMap mAhi, mAlo, mBhi, mBlo;
-    bool ok = make_map(&mAhi, ahi, m2, kp, TB_M) && make_map(&mAlo, alo, m2, kp, TB_M) &&
-              make_map(&mBhi, bhi, ncols, kp, TB_N) && make_map(&mBlo, blo, ncols, kp, TB_N);
+    bool ok = make_map(&mAhi, ahi, m2, kp, TB_M, f16) && make_map(&mAlo, alo, m2, kp, TB_M, f16) &&
+              make_map(&mBhi, bhi, ncols, kp, TB_N, f16) && make_map(&mBlo, blo, ncols, kp, TB_N, f16);
     // A viewed as a 2n x n float matrix (column-major): box of 128 real rows x 64 columns
     CUtensorMap mC;
     {
@@ -560,13 +718,18 @@ static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, in
     a.col0 = col0;
     a.m2 = m2;
     a.ncols = ncols;
-    a.kchunks = kp / TB_K;
+    a.kchunks = kp / (f16 ? 32 : TB_K);
     a.tiles_m = (m2 + TB_M - 1) / TB_M;
     a.tiles_n = (ncols + TB_N - 1) / TB_N;
     a.tiles = a.tiles_m * a.tiles_n;
     a.status = wk.status;
+    a.sA = sA;
+    a.sB = sB;
     int grid = std::min(num_sms(), a.tiles);
-    tf32_update_kernel<<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
+    if (f16)
+        tf32_update_kernel<true><<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
+    else
+        tf32_update_kernel<false><<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
     *launches += 1;
 }
 
@@ -574,7 +737,7 @@ static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, in
 // operands packed (A12 is read from its packed copy, so the in-place update is race free).
 void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches) {
     int r0 = k0 + w, ncols = n - r0;
-    int kp = ((2 * w + TB_K - 1) / TB_K) * TB_K;
+    int kp = ((2 * w + 31) / 32) * 32;  // whole 64-byte K rows of FP16 pieces (and of TF32)
     size_t need = ((size_t)2 * w * kp + (size_t)ncols * kp) * 2 * 4 + (size_t)w * w * 8 + 8192;
     if (!ensure_pack(wk, need, n, st)) return;
     float* ahi = (float*)wk.pack;
@@ -590,36 +753,62 @@ void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t 
     {
         StageScope sc(ST_TRSM, st);
         tri_inverse_l_kernel<<<1, 256, TI_SMEM, st>>>(A, (size_t)n, k0, w, Nm);
-        // A operand: -N embedded, so that the update C -= (-N) A12 adds N A12
         dim3 g1((w + 31) / 32, (kp / 2 + 31) / 32);
-        pack_l_kernel<<<g1, 256, 0, st>>>(Nm, (size_t)w, 0, 0, w, w, kp, ahi, alo);
         size_t tot = (size_t)ncols * (kp / 2);
-        pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
-        negate_kernel<<<(unsigned)(((size_t)4 * w * kp + 255) / 256), 256, 0, st>>>(ahi, (size_t)4 * w * kp);
-        run_gemm(A, n, 2 * k0, r0, 2 * w, ncols, kp, ahi, alo, bhi, blo, wk, st, launches);
-        *launches += 4;
+        if (wk.f16_pieces) {
+            // A operand: -N embedded, so that the update C -= (-N) A12 adds N A12
+            __half *h_ahi = (__half*)ahi, *h_alo = h_ahi + (size_t)2 * w * kp;
+            __half *h_bhi = h_alo + (size_t)2 * w * kp, *h_blo = h_bhi + (size_t)ncols * kp;
+            float* sA = (float*)(((uintptr_t)(h_blo + (size_t)ncols * kp) + 255) & ~(uintptr_t)255);
+            float* sB = (float*)(((uintptr_t)(sA + w) + 255) & ~(uintptr_t)255);
+            pack_l16_kernel<<<(w + 31) / 32, 256, 0, st>>>(Nm, (size_t)w, 0, 0, w, w, kp, -1.0f, h_ahi, h_alo, sA);
+            pack_u16_kernel<<<(unsigned)(((size_t)ncols * 32 + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w,
+                                                                                         kp, h_bhi, h_blo, sB);
+            run_gemm(A, n, 2 * k0, r0, 2 * w, ncols, kp, h_ahi, h_alo, h_bhi, h_blo, sA, sB, wk, st, launches);
+            *launches += 3;
+        } else {
+            pack_l_kernel<<<g1, 256, 0, st>>>(Nm, (size_t)w, 0, 0, w, w, kp, ahi, alo);
+            pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
+            negate_kernel<<<(unsigned)(((size_t)4 * w * kp + 255) / 256), 256, 0, st>>>(ahi, (size_t)4 * w * kp);
+            run_gemm(A, n, 2 * k0, r0, 2 * w, ncols, kp, ahi, alo, bhi, blo, nullptr, nullptr, wk, st, launches);
+            *launches += 4;
+        }
     }
 }
 
 void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches) {
     int r0 = k0 + w, m = n - r0, ncols = n - r0;
-    int kp = ((2 * w + TB_K - 1) / TB_K) * TB_K;
+    int kp = ((2 * w + 31) / 32) * 32;  // whole 64-byte K rows of FP16 pieces (and of TF32)
     size_t need = ((size_t)2 * m * kp + (size_t)ncols * kp) * 2 * 4 + 4096;
     if (!ensure_pack(wk, need, n, st)) return;
     float* ahi = (float*)wk.pack;
     float* alo = ahi + (size_t)2 * m * kp;
     float* bhi = alo + (size_t)2 * m * kp;
     float* blo = bhi + (size_t)ncols * kp;
+    const bool f16 = wk.f16_pieces;
+    __half *h_ahi = (__half*)ahi, *h_alo = h_ahi + (size_t)2 * m * kp;
+    __half *h_bhi = h_alo + (size_t)2 * m * kp, *h_blo = h_bhi + (size_t)ncols * kp;
+    float* sA = (float*)(((uintptr_t)(h_blo + (size_t)ncols * kp) + 255) & ~(uintptr_t)255);
+    float* sB = (float*)(((uintptr_t)(sA + m) + 255) & ~(uintptr_t)255);
     {
         StageScope sc(ST_PACK, st);
-        dim3 g1((m + 31) / 32, (kp / 2 + 31) / 32);
-        pack_l_kernel<<<g1, 256, 0, st>>>(A, (size_t)n, r0, k0, m, w, kp, ahi, alo);
-        size_t tot = (size_t)ncols * (kp / 2);
-        pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
+        if (f16) {
+            pack_l16_kernel<<<(m + 31) / 32, 256, 0, st>>>(A, (size_t)n, r0, k0, m, w, kp, 1.0f, h_ahi, h_alo, sA);
+            pack_u16_kernel<<<(unsigned)(((size_t)ncols * 32 + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w,
+                                                                                         kp, h_bhi, h_blo, sB);
+        } else {
+            dim3 g1((m + 31) / 32, (kp / 2 + 31) / 32);
+            size_t tot = (size_t)ncols * (kp / 2);
+            pack_l_kernel<<<g1, 256, 0, st>>>(A, (size_t)n, r0, k0, m, w, kp, ahi, alo);
+            pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
+        }
         *launches += 2;
     }
     StageScope sc(ST_GEMM, st);
-    run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, ahi, alo, bhi, blo, wk, st, launches);
+    if (f16)
+        run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, h_ahi, h_alo, h_bhi, h_blo, sA, sB, wk, st, launches);
+    else
+        run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, ahi, alo, bhi, blo, nullptr, nullptr, wk, st, launches);
 }
 
 }  // namespace tcu

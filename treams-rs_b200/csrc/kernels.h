@@ -134,7 +134,10 @@ struct LuWork {
     void* cand = nullptr;      // candidate values/rows, double-buffered
     void* pack = nullptr;      // packed GEMM operands (mixed path)
     size_t pack_bytes = 0;
+    bool f16_pieces = false;   // mixed path: FP16 (true) or TF32 (false) pieces of the 3-pass split
 };
+// FP16 pieces when the environment asks for them (TCU_SPLIT=f16), else TF32 pieces
+bool split_f16_default();
 int lu_factor_fp64(double2* A, int n, LuWork& w, cudaStream_t st, long long* launches);
 int lu_factor_fp32(float2* A, int n, LuWork& w, cudaStream_t st, long long* launches, bool tensor_cores);
 // solve.cu — inverses of the 64 x 64 diagonal blocks of L and U (FP64, lu_inverse_bytes),

@@ -4,6 +4,7 @@ from __future__ import annotations
 import ctypes
 import pathlib
 import threading
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -112,6 +113,7 @@ class Context:
         h = P()
         _check(lib().tcu_context_create(device, ctypes.byref(h)))
         self.handle = h
+        self._factors = weakref.WeakSet()  # closed before the context
 
     @property
     def stream(self) -> int:
@@ -161,6 +163,8 @@ class Context:
 
     def close(self) -> None:
         if self.handle:
+            for f in list(self._factors):
+                f.close()
             lib().tcu_context_destroy(self.handle)
             self.handle = None
 
@@ -276,6 +280,7 @@ class InteractionFactor:
         self.handle = handle
         self.ctx = ctx
         self.precision = precision
+        ctx._factors.add(self)
         self.dimension = int(lib().tcu_factor_dimension(handle))
 
     def solve(self, incident) -> tuple[np.ndarray, list[Certificate]]:
@@ -293,7 +298,8 @@ class InteractionFactor:
 
     def close(self) -> None:
         if self.handle:
-            lib().tcu_factor_destroy(self.handle)
+            if self.ctx.handle:
+                lib().tcu_factor_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
