@@ -20,7 +20,7 @@
 //
 // Kernel layout (persistent, one CTA per SM, 192 threads):
 //   warp 0     TMA producer: 64-byte-swizzled boxes (64-byte K rows) of the four packed
-//              operands into a 3-stage shared-memory ring (48 KB per stage), mbarrier complete_tx;
+//              operands into a 4-stage shared-memory ring (48 KB per stage), mbarrier complete_tx;
 //   warp 1     TMEM allocator and MMA issuer (one thread): 2 K-steps x 3 passes per stage
 //              into a 128 x 256 FP32 accumulator, double-buffered in TMEM (512 columns);
 //   warps 2-5  epilogue: tcgen05.ld 32 columns at a time into a shared-memory staging buffer,
@@ -45,13 +45,13 @@ namespace tcu {
 constexpr int TB_M = 128;       // real rows per tile (64 complex rows)
 constexpr int TB_N = 256;       // columns per tile
 constexpr int TB_K = 16;        // floats per K chunk (one 64-byte swizzle row); 32 for FP16 pieces
-constexpr int TB_STAGES = 3;
+constexpr int TB_STAGES = 4;
 constexpr int A_BYTES = TB_M * TB_K * 4;   // 8 KB
 constexpr int B_BYTES = TB_N * TB_K * 4;   // 16 KB
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;  // 48 KB
 constexpr int TMEM_COLS = 2 * TB_N;        // two accumulators
-constexpr int EPI_COLS = 64;                         // columns per epilogue staging buffer
-constexpr int EPI_BYTES = TB_M * EPI_COLS * 4;         // 32 KB
+constexpr int EPI_COLS = 32;                         // columns per epilogue staging buffer
+constexpr int EPI_BYTES = TB_M * EPI_COLS * 4;         // 16 KB
 constexpr size_t TF32_SMEM = (size_t)TB_STAGES * STAGE_BYTES + 2 * EPI_BYTES + 1024 + 256;
 
 // ---- device helpers ---------------------------------------------------------------------

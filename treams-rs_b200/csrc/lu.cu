@@ -1,5 +1,5 @@
 // Dense right-looking blocked LU with partial pivoting of a complex n x n column-major
-// matrix, FP64 (double2) or FP32 (float2) storage, and the triangular solves.
+// matrix, FP64 (double2) or FP32 (float2) storage.
 //
 // Per panel of width w (64 complex columns in FP64, 128 in FP32):
 //  1. panel_kernel (cooperative, one CTA per SM): every CTA holds a slab of the panel rows
@@ -7,10 +7,12 @@
 //     (largest |a|, ties to the lower row) with its row and the current diagonal row, so
 //     every CTA picks the same pivot, swaps locally and applies the rank-1 update.
 //  2. laswp_kernel: the panel's row swaps on the columns outside it (skips identities).
-//  3. trsm_kernel: U12 = L11^-1 A12, one warp per column.
+//  3. U12 = L11^-1 A12: trsm_kernel (FP64, one warp per column), or in the mixed path the
+//     blocked inverse of L11 (tri_inverse_l_kernel) and a tensor-core GEMM (gemm_tf32.cu).
 //  4. trailing update A22 -= L21 U12: FP64 DMMA (mma.sync m8n8k4 f64) complex GEMM, or in
-//     the mixed path the 3-pass split-TF32 tcgen05 GEMM of gemm_tf32.cu.
-// The solves gather x = P b, then run blocked forward/backward substitutions.
+//     the mixed path the 3-pass split tcgen05 GEMM of gemm_tf32.cu.
+// The permutation is composed from the pivots afterwards; the triangular solves with the
+// factors are in solve.cu.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -60,42 +62,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// Grid barrier for co-resident CTAs (cooperative launch). Every wait is bounded: after
-// 4 s, or once another CTA has raised an error, it records TIMEOUT (8) in *status and
-// returns false so the kernel can leave.
-// The arrival counter only grows (reset per launch): barrier instance g completes when the
-// counter reaches (g + 1) * nblocks, so one release-add and acquire polls suffice.
-__device__ bool grid_sync(unsigned* bar, unsigned nblocks, int* status) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int ok = 1;
-        unsigned old;
-        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(bar) : "memory");
-        unsigned target = (old / nblocks + 1) * nblocks;
-        if (old + 1 != target) {
-            unsigned long long t0 = global_ns();
-            unsigned spins = 0;
-            while ((int)(ld_acquire_u32(bar) - target) < 0) {
-                if ((++spins & 255u) == 0) {
-                    if (*(volatile int*)status == 8) {
-                        ok = 0;
-                        break;
-                    }
-                    if (global_ns() - t0 > 4000000000ull) {
-                        atomicExch(status, 8);
-                        ok = 0;
-                        break;
-                    }
-                }
-            }
-        }
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
 template <typename R>
 __device__ __forceinline__ double cx_abs2(typename Cx<R>::T a) {
     return (double)a.x * (double)a.x + (double)a.y * (double)a.y;
@@ -105,14 +71,12 @@ __device__ __forceinline__ double cx_abs2(typename Cx<R>::T a) {
 // Per column every CTA publishes its best local candidate row, folds its candidate key
 //   [|a|^2 as FP32 bits : 32][0xFFFFFFFF - row : 32]
 // into one 64-bit atomicMax word (three words cycle over the columns), and arrives at a grid
-// barrier (fire-and-forget release add on a counter that only grows; relaxed polls with a
-// short back-off keep the counter's L2 line lightly loaded). After the barrier every CTA
+// barrier (fire-and-forget release add on a counter that only grows, acquire polls). After
+// the barrier every CTA
 // reads the winning key and the pivot row: the largest |a| with ties to the lower row.
-__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
+// Grid barrier of the cooperative panel: thread 0 of each CTA arrives with a release add and
+// spins on acquire loads (no sleep: the wait is one column's latency); bounded at 4 s, after
+// which it records status 8 (TCU_TIMEOUT) and every CTA returns.
 __device__ bool column_barrier(unsigned* bar, unsigned target, int* status) {
     __shared__ int s_ok;
     __syncthreads();
@@ -120,12 +84,11 @@ __device__ bool column_barrier(unsigned* bar, unsigned target, int* status) {
         int ok = 1;
         __threadfence();
         asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(bar) : "memory");
-        if (ld_relaxed_u32(bar) < target) {
+        if (ld_acquire_u32(bar) < target) {
             unsigned long long t0 = global_ns();
             unsigned spins = 0;
-            while (ld_relaxed_u32(bar) < target) {
-                __nanosleep(20);
-                if ((++spins & 255u) == 0) {
+            while (ld_acquire_u32(bar) < target) {
+                if ((++spins & 1023u) == 0) {
                     if (*(volatile int*)status == 8 || global_ns() - t0 > 4000000000ull) {
                         atomicExch(status, 8);
                         ok = 0;
@@ -134,7 +97,6 @@ __device__ bool column_barrier(unsigned* bar, unsigned target, int* status) {
                 }
             }
         }
-        asm volatile("fence.acq_rel.gpu;" ::: "memory");
         s_ok = ok;
     }
     __syncthreads();
