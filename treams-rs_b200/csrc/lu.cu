@@ -17,6 +17,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -62,6 +63,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+constexpr int PANEL_THREADS = 256;  // measured: 512 threads per CTA were slower
+
 template <typename R>
 __device__ __forceinline__ double cx_abs2(typename Cx<R>::T a) {
     return (double)a.x * (double)a.x + (double)a.y * (double)a.y;
@@ -104,7 +107,7 @@ __device__ bool column_barrier(unsigned* bar, unsigned target, int* status) {
 }
 
 template <typename R, int NB>
-__global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t lda, int k0, int n, int w,
+__global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(typename Cx<R>::T* A, size_t lda, int k0, int n, int w,
                                                     int chunk, int* piv, int* perm, unsigned long long* keys,
                                                     typename Cx<R>::T* crow, typename Cx<R>::T* drow, unsigned* bar,
                                                     int* status) {
@@ -112,8 +115,8 @@ __global__ void __launch_bounds__(256) panel_kernel(typename Cx<R>::T* A, size_t
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tile = (C*)smem_raw;                      // chunk x (NB + 1)
     C* prow = tile + (size_t)chunk * (NB + 1);   // NB
-    __shared__ float s_val[8];
-    __shared__ int s_row[8];
+    __shared__ float s_val[PANEL_THREADS / 32];
+    __shared__ int s_row[PANEL_THREADS / 32];
     const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int rows = n - k0;
@@ -539,11 +542,24 @@ size_t lu_workspace_bytes(int n, bool fp32) {
            2 * 128 * sizeof(double2) + 1024;
 }
 
+// Smallest slab of rows per panel CTA (TCU_PANEL_ROWS, default 32; the smem slab caps it).
+static int panel_rows_per_cta() {
+    static int v = 0;
+    if (!v) {
+        const char* e = getenv("TCU_PANEL_ROWS");
+        int x = e ? atoi(e) : 0;
+        v = (x >= 16 && x <= 200) ? x : 32;
+    }
+    return v;
+}
+
 template <typename R, int NB>
 static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cudaStream_t st) {
     typedef typename Cx<R>::T C;
     int rows = n - k0;
-    int P = std::min(g_num_sms, std::max(1, (rows + 31) / 32));
+    // at least panel_rows_per_cta() rows per CTA: fewer CTAs arrive at each column's barrier
+    const int per = panel_rows_per_cta();
+    int P = std::min(g_num_sms, std::max(1, (rows + per - 1) / per));
     int chunk = (rows + P - 1) / P;
     size_t smem = panel_smem<R, NB>(chunk);
     if (smem > 220 * 1024) return 1;
@@ -554,7 +570,7 @@ static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cud
     cudaMemsetAsync(wk.barrier, 0, 2 * sizeof(unsigned), st);
     size_t lda = (size_t)n;
     void* args[] = {&A, &lda, &k0, &n, &w, &chunk, &wk.piv, &wk.perm, &keys, &crow, &drow, &wk.barrier, &wk.status};
-    cudaError_t e = cudaLaunchCooperativeKernel((void*)panel_kernel<R, NB>, dim3(P), dim3(256), args, smem, st);
+    cudaError_t e = cudaLaunchCooperativeKernel((void*)panel_kernel<R, NB>, dim3(P), dim3(PANEL_THREADS), args, smem, st);
     return e == cudaSuccess ? 0 : 2;
 }
 

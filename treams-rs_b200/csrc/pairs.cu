@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 #include "pairtable.cuh"
@@ -152,6 +154,113 @@ __global__ void __launch_bounds__(256) apply_kernel(DevPlan P, int N, double k, 
             const cplx* t4 = T + ((size_t)i * P.L + lam - 1) * 4;
             cplx tc0 = cadd(cmul(t4[0], sp), cmul(t4[1], sn));
             cplx tc1 = cadd(cmul(t4[2], sp), cmul(t4[3], sn));
+            y0 = cadd(cscale(x0, alpha), cscale(tc0, beta));
+            y1 = cadd(cscale(x1, alpha), cscale(tc1, beta));
+            if (zadd) {
+                y0 = cadd(y0, zadd[c * ldx + row]);
+                y1 = cadd(y1, zadd[c * ldx + row + 1]);
+            }
+        } else {
+            y0 = cadd(x0, sp);
+            y1 = cadd(x1, sn);
+        }
+        y[c * ldx + row] = y0;
+        y[c * ldx + row + 1] = y1;
+    }
+}
+
+// ---- matrix-free operator, slot-major mapping ----------------------------------------------
+// Same result as apply_kernel with Q = 16 source slots per batch, but thread t owns the slot
+// q = t % 16 and the destination modes d = t / 16 + 16 k: the 16 lanes of a half-warp read the
+// same plan term (one broadcast load) against 16 different harmonic tables (table stride
+// tsize = (2L+1)^2 entries, 4 banks apart mod 32: conflict-free), and the batch's source
+// coefficients are staged in shared memory with an odd row stride. Each thread sums its slots
+// over all batches; the slots are reduced in a fixed order at the end.
+constexpr int AP_Q = 16;
+template <int PASSES>  // ceil(nlm / 16) destination passes; at most 8 / PASSES columns
+__global__ void __launch_bounds__(256) apply2_kernel(DevPlan P, int N, double k, const double* __restrict__ pos,
+                                                     const cplx* __restrict__ T, const cplx* __restrict__ x,
+                                                     size_t ldx, int ncol, const cplx* __restrict__ zadd, double alpha,
+                                                     double beta, bool singular, cplx* __restrict__ y) {
+    extern __shared__ cplx ap_smem[];
+    const int nlm = P.nlm, M = 2 * nlm, XS = M + 1;  // odd row stride of the staged coefficients
+    cplx* Zs = ap_smem;                              // AP_Q * tsize
+    cplx* xs = Zs + (size_t)AP_Q * P.tsize;          // AP_Q * ncol * XS
+    cplx* red = ap_smem;                             // at the end: AP_Q * nlm * 2 * ncol (aliases the above)
+    const int i = blockIdx.x, tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const int q = tid % AP_Q, d0 = tid / AP_Q;       // d = d0 + 16 pass
+    constexpr int COLS = APPLY_MAXCOL / PASSES;
+    cplx accp[PASSES][COLS], accn[PASSES][COLS];
+#pragma unroll
+    for (int a = 0; a < PASSES; ++a)
+#pragma unroll
+        for (int c = 0; c < COLS; ++c) accp[a][c] = accn[a][c] = mk(0.0, 0.0);
+    const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
+    for (int j0 = 0; j0 < N; j0 += AP_Q) {
+        for (int w = warp; w < AP_Q; w += blockDim.x >> 5) {
+            const int j = j0 + w;
+            if (j < N && j != i)
+                pair_table(P, k, xi - pos[3 * j], yi - pos[3 * j + 1], zi - pos[3 * j + 2], singular, Zs + w * P.tsize,
+                           lane);
+        }
+        for (int t = tid; t < AP_Q * ncol * M; t += blockDim.x) {
+            const int qq = t / (ncol * M), r = t - qq * ncol * M, c = r / M, e = r - c * M;
+            const int j = j0 + qq;
+            xs[((size_t)qq * ncol + c) * XS + e] = (j < N && j != i) ? x[c * ldx + (size_t)j * M + e] : mk(0.0, 0.0);
+        }
+        __syncthreads();
+        const int j = j0 + q;
+        if (j < N && j != i) {
+            const cplx* Z = Zs + q * P.tsize;
+            const cplx* xq = xs + (size_t)q * ncol * XS;
+#pragma unroll
+            for (int a = 0; a < PASSES; ++a) {
+                const int d = d0 + 16 * a;
+                if (d >= nlm) continue;
+                for (int s = 0; s < nlm; ++s) {
+                    cplx A, B;
+                    combo_sums(P, s * nlm + d, Z, A, B);
+                    const cplx cp = cadd(A, B), cn = csub(A, B);
+#pragma unroll
+                    for (int c = 0; c < COLS; ++c) {
+                        if (c >= ncol) break;
+                        cfma(accp[a][c], cp, xq[c * XS + 2 * s]);
+                        cfma(accn[a][c], cn, xq[c * XS + 2 * s + 1]);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // fixed-order reduction over the slots
+#pragma unroll
+    for (int a = 0; a < PASSES; ++a) {
+        const int d = d0 + 16 * a;
+        if (d >= nlm) continue;
+#pragma unroll
+        for (int c = 0; c < COLS; ++c) {
+            if (c >= ncol) break;
+            red[((size_t)q * nlm + d) * 2 * ncol + 2 * c] = accp[a][c];
+            red[((size_t)q * nlm + d) * 2 * ncol + 2 * c + 1] = accn[a][c];
+        }
+    }
+    __syncthreads();
+    for (int t = tid; t < nlm * ncol; t += blockDim.x) {
+        const int dd = t % nlm, c = t / nlm;
+        cplx sp = mk(0.0, 0.0), sn = mk(0.0, 0.0);
+        for (int qq = 0; qq < AP_Q; ++qq) {
+            sp = cadd(sp, red[((size_t)qq * nlm + dd) * 2 * ncol + 2 * c]);
+            sn = cadd(sn, red[((size_t)qq * nlm + dd) * 2 * ncol + 2 * c + 1]);
+        }
+        const size_t row = (size_t)i * M + 2 * dd;
+        const cplx x0 = x[c * ldx + row], x1 = x[c * ldx + row + 1];
+        cplx y0, y1;
+        if (singular) {
+            const int lam = degree_of(dd);
+            const cplx* t4 = T + ((size_t)i * P.L + lam - 1) * 4;
+            const cplx tc0 = cadd(cmul(t4[0], sp), cmul(t4[1], sn));
+            const cplx tc1 = cadd(cmul(t4[2], sp), cmul(t4[3], sn));
             y0 = cadd(cscale(x0, alpha), cscale(tc0, beta));
             y1 = cadd(cscale(x1, alpha), cscale(tc1, beta));
             if (zadd) {
@@ -436,13 +545,33 @@ void launch_assemble(const DevPlan& P, int N, double k, const double* pos, const
         assemble_kernel<double2><<<grid, 256, smem, st>>>(P, N, k, pos, T, (double2*)out, ld, pairs);
 }
 
+static size_t apply2_smem(const DevPlan& P, int ncol) {
+    const size_t main = ((size_t)AP_Q * P.tsize + (size_t)AP_Q * ncol * (2 * P.nlm + 1)) * sizeof(cplx);
+    const size_t red = (size_t)AP_Q * P.nlm * 2 * ncol * sizeof(cplx);
+    return std::max(main, red);
+}
+
+// Columns per launch of the slot-major kernel: its per-thread accumulators hold
+// ceil(nlm / 16) destination passes x columns.
+static int apply2_cols(const DevPlan& P) { return std::max(1, APPLY_MAXCOL / ((P.nlm + 15) / 16)); }
+
 void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                   int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st) {
     StageScope sc(ST_APPLY, st);
-    int Q = 256 / P.nlm;
-    if (Q > 16) Q = 16;
-    size_t smem = (size_t)Q * P.tsize * sizeof(cplx) + (size_t)Q * P.nlm * 2 * ncol * sizeof(cplx);
-    apply_kernel<<<N, 256, smem, st>>>(P, N, k, pos, T, x, ldx, ncol, zadd, alpha, beta, singular, y, Q);
+    const int per = apply2_cols(P);
+    for (int c0 = 0; c0 < ncol; c0 += per) {
+        const int nc = std::min(per, ncol - c0);
+        const cplx* xc = x + (size_t)c0 * ldx;
+        const cplx* zc = zadd ? zadd + (size_t)c0 * ldx : nullptr;
+        cplx* yc = y + (size_t)c0 * ldx;
+        const size_t smem = apply2_smem(P, nc);
+        switch ((P.nlm + 15) / 16) {
+            case 1: apply2_kernel<1><<<N, 256, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
+            case 2: apply2_kernel<2><<<N, 256, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
+            case 3: apply2_kernel<3><<<N, 256, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
+            default: apply2_kernel<4><<<N, 256, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
+        }
+    }
 }
 
 void launch_block(const DevPlan& P, double k, const double* d, bool singular, bool helicity, cplx* out,
@@ -469,14 +598,14 @@ void launch_apply_t(int L, int N, const cplx* T, const cplx* x, int ncol, cplx* 
 
 void pairs_init_attributes() {
     cudaFuncSetAttribute(apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply2_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply2_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply2_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply2_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(assemble_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
     cudaFuncSetAttribute(assemble_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
 }
 
-size_t apply_smem_bytes(const DevPlan& P, int ncol) {
-    int Q = 256 / P.nlm;
-    if (Q > 16) Q = 16;
-    return (size_t)Q * P.tsize * sizeof(cplx) + (size_t)Q * P.nlm * 2 * ncol * sizeof(cplx);
-}
+size_t apply_smem_bytes(const DevPlan& P, int ncol) { return apply2_smem(P, std::min(ncol, apply2_cols(P))); }
 
 }  // namespace tcu
