@@ -170,15 +170,16 @@ __global__ void __launch_bounds__(256) apply_kernel(DevPlan P, int N, double k, 
 }
 
 // ---- matrix-free operator, slot-major mapping ----------------------------------------------
-// Same result as apply_kernel with Q = 16 source slots per batch, but thread t owns the slot
-// q = t % 16 and the destination modes d = t / 16 + 16 k: the 16 lanes of a half-warp read the
-// same plan term (one broadcast load) against 16 different harmonic tables (table stride
-// tsize = (2L+1)^2 entries, 4 banks apart mod 32: conflict-free), and the batch's source
-// coefficients are staged in shared memory with an odd row stride. Each thread sums its slots
-// over all batches; the slots are reduced in a fixed order at the end.
-constexpr int AP_Q = 16;
+// Same sums as apply_kernel, with Q = 32 source slots per batch and thread t owning the slot
+// q = t % 32 (its lane) and the destination modes d = t / 32 + 16 k: all lanes of a warp read
+// the same plan term (one broadcast load, no divergence) against 32 different harmonic tables
+// (table stride tsize = (2L+1)^2 entries, 4 banks apart mod 32: the minimum of 4 wavefronts per
+// 16-byte load), and the batch's source coefficients are staged in shared memory with an odd
+// row stride. Each thread sums its slot over all batches; slots are reduced in a fixed order.
+constexpr int AP_Q = 32;
+constexpr int AP_THREADS = 512;
 template <int PASSES>  // ceil(nlm / 16) destination passes; at most 8 / PASSES columns
-__global__ void __launch_bounds__(256) apply2_kernel(DevPlan P, int N, double k, const double* __restrict__ pos,
+__global__ void __launch_bounds__(AP_THREADS) apply2_kernel(DevPlan P, int N, double k, const double* __restrict__ pos,
                                                      const cplx* __restrict__ T, const cplx* __restrict__ x,
                                                      size_t ldx, int ncol, const cplx* __restrict__ zadd, double alpha,
                                                      double beta, bool singular, cplx* __restrict__ y) {
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(256) apply2_kernel(DevPlan P, int N, double k,
     cplx* red = ap_smem;                             // at the end: AP_Q * nlm * 2 * ncol (aliases the above)
     const int i = blockIdx.x, tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int q = tid % AP_Q, d0 = tid / AP_Q;       // d = d0 + 16 pass
+    const int q = tid % AP_Q, d0 = tid / AP_Q;       // d = d0 + 16 pass (16 warps)
     constexpr int COLS = APPLY_MAXCOL / PASSES;
     cplx accp[PASSES][COLS], accn[PASSES][COLS];
 #pragma unroll
@@ -553,7 +554,11 @@ static size_t apply2_smem(const DevPlan& P, int ncol) {
 
 // Columns per launch of the slot-major kernel: its per-thread accumulators hold
 // ceil(nlm / 16) destination passes x columns.
-static int apply2_cols(const DevPlan& P) { return std::max(1, APPLY_MAXCOL / ((P.nlm + 15) / 16)); }
+static int apply2_cols(const DevPlan& P) {
+    int c = std::max(1, APPLY_MAXCOL / ((P.nlm + 15) / 16));
+    while (c > 1 && apply2_smem(P, c) > 200 * 1024) --c;  // the shared-memory attribute
+    return c;
+}
 
 void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                   int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st) {
@@ -566,10 +571,10 @@ void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cp
         cplx* yc = y + (size_t)c0 * ldx;
         const size_t smem = apply2_smem(P, nc);
         switch ((P.nlm + 15) / 16) {
-            case 1: apply2_kernel<1><<<N, 256, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
-            case 2: apply2_kernel<2><<<N, 256, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
-            case 3: apply2_kernel<3><<<N, 256, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
-            default: apply2_kernel<4><<<N, 256, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
+            case 1: apply2_kernel<1><<<N, AP_THREADS, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
+            case 2: apply2_kernel<2><<<N, AP_THREADS, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
+            case 3: apply2_kernel<3><<<N, AP_THREADS, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
+            default: apply2_kernel<4><<<N, AP_THREADS, smem, st>>>(P, N, k, pos, T, xc, ldx, nc, zc, alpha, beta, singular, yc); break;
         }
     }
 }
