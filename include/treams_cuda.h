@@ -83,6 +83,11 @@ tcu_status tcu_context_set_refinement(tcu_context* ctx, double target, double fa
 /* Number of mixed-precision solves whose FP64 refinement stalled above the fallback tolerance
  * and that were finished by a second factor (TF32 pieces, then FP64) of the same cluster. */
 long long tcu_context_fallbacks(tcu_context* ctx);
+/* Failure-detection self-test (no counterpart in the reference): runs the LU panel's grid
+ * barrier with one arrival missing, so that its bounded wait gives up after limit_seconds
+ * (clamped to [0, 4] s). Returns TCU_TIMEOUT, as a factorization whose CTAs never meet
+ * would, and leaves the context usable; any other status means the wait did not give up. */
+tcu_status tcu_context_wait_selftest(tcu_context* ctx, double limit_seconds);
 /* Per-stage device timing with CUDA events on the context stream (off by default).
  * Stages: 0 assembly, 1 LU panel, 2 row swaps, 3 triangular block (TRSM), 4 trailing
  * update GEMM, 5 operand packing, 6 triangular solves, 7 matrix-free operator, 8 Mie,

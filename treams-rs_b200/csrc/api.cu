@@ -1329,6 +1329,23 @@ extern "C" tcu_status tcu_batch_solve(tcu_context* ctx, size_t count, const tcu_
     return TCU_OK;
 }
 
+extern "C" tcu_status tcu_context_wait_selftest(tcu_context* ctx, double limit_seconds) {
+    if (!ctx || !std::isfinite(limit_seconds) || limit_seconds < 0.0)
+        return fail(TCU_INVALID_INPUT, "require a context and a finite limit >= 0");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    DevBuf bar(ctx);
+    CK(bar.alloc(sizeof(unsigned) * 4), "self-test barrier");
+    CK(cudaMemsetAsync(bar.p, 0, sizeof(unsigned) * 4, ctx->stream), "self-test barrier");
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream), "self-test status");
+    launch_barrier_selftest((unsigned*)bar.p, ctx->d_status, limit_seconds, ctx->stream);
+    ctx->launches += 1;
+    tcu_status s = read_status(ctx, "bounded-wait self-test");
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream), "self-test status");
+    tcu_status s2 = sync_status(ctx, "bounded-wait self-test");
+    if (s == TCU_OK) return fail(TCU_DEVICE_ERROR, "bounded-wait self-test: the barrier passed with an arrival missing");
+    return s2 ? s2 : s;
+}
+
 extern "C" tcu_status tcu_context_set_refinement(tcu_context* ctx, double target, double fallback_above) {
     if (!ctx || !(target > 0.0) || !(fallback_above > 0.0) || !std::isfinite(target) || !std::isfinite(fallback_above))
         return fail(TCU_INVALID_INPUT, "require positive finite refinement tolerances");

@@ -588,7 +588,7 @@ bool tf32_enabled() {
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__global__ void __launch_bounds__(256) tri_inverse_l_kernel(const float2* __restrict__ A, size_t lda, int k0, int w,
+__global__ void __launch_bounds__(1024) tri_inverse_l_kernel(const float2* __restrict__ A, size_t lda, int k0, int w,
                                                             float2* __restrict__ N) {
     extern __shared__ float2 ti_smem[];
     const int LD = 129;
@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(256) tri_inverse_l_kernel(const float2* __rest
     }
     __syncthreads();
     // 16 x 16 diagonal blocks: X[i][j] = -sum_{k=j+1..i} X[i][k] L[k][j], X[i][i] = 1
-    {
+    if (warp < 8) {  // one warp per 16 x 16 block; the other warps join at the next barrier
         __shared__ float2 colbuf[8][16];
         const int o = warp * 16;
         for (int j = 14; j >= 0; --j) {
@@ -752,7 +752,7 @@ void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t 
     }
     {
         StageScope sc(ST_TRSM, st);
-        tri_inverse_l_kernel<<<1, 256, TI_SMEM, st>>>(A, (size_t)n, k0, w, Nm);
+        tri_inverse_l_kernel<<<1, 1024, TI_SMEM, st>>>(A, (size_t)n, k0, w, Nm);
         dim3 g1((w + 31) / 32, (kp / 2 + 31) / 32);
         size_t tot = (size_t)ncols * (kp / 2);
         if (wk.f16_pieces) {

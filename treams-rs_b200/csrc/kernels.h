@@ -139,6 +139,9 @@ struct LuWork {
 // FP16 pieces when the environment asks for them (TCU_SPLIT=f16), else TF32 pieces
 bool split_f16_default();
 int lu_factor_fp64(double2* A, int n, LuWork& w, cudaStream_t st, long long* launches);
+// The panel's grid barrier with one arrival missing (bar: a zeroed counter); it gives up
+// after limit_s (clamped to [0, 4] s) and records status 8.
+void launch_barrier_selftest(unsigned* bar, int* status, double limit_s, cudaStream_t st);
 int lu_factor_fp32(float2* A, int n, LuWork& w, cudaStream_t st, long long* launches, bool tensor_cores);
 // solve.cu — inverses of the 64 x 64 diagonal blocks of L and U (FP64, lu_inverse_bytes),
 // then x (n x ncol, FP64) <- A^-1 x; tmp holds 2 n min(ncol, 8) complex.

@@ -80,7 +80,9 @@ __device__ __forceinline__ double cx_abs2(typename Cx<R>::T a) {
 // Grid barrier of the cooperative panel: thread 0 of each CTA arrives with a release add and
 // spins on acquire loads (no sleep: the wait is one column's latency); bounded at 4 s, after
 // which it records status 8 (TCU_TIMEOUT) and every CTA returns.
-__device__ bool column_barrier(unsigned* bar, unsigned target, int* status) {
+constexpr unsigned long long BARRIER_LIMIT_NS = 4000000000ull;
+__device__ bool column_barrier(unsigned* bar, unsigned target, int* status,
+                               unsigned long long limit_ns = BARRIER_LIMIT_NS) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -92,7 +94,7 @@ __device__ bool column_barrier(unsigned* bar, unsigned target, int* status) {
             unsigned spins = 0;
             while (ld_acquire_u32(bar) < target) {
                 if ((++spins & 1023u) == 0) {
-                    if (*(volatile int*)status == 8 || global_ns() - t0 > 4000000000ull) {
+                    if (*(volatile int*)status == 8 || global_ns() - t0 > limit_ns) {
                         atomicExch(status, 8);
                         ok = 0;
                         break;
@@ -521,6 +523,18 @@ template <typename R, int NB>
 static size_t panel_smem(int chunk) {
     typedef typename Cx<R>::T C;
     return (size_t)chunk * (NB + 1) * sizeof(C) + NB * sizeof(C);
+}
+
+// The panel's grid barrier with one arrival missing: CTA 0 of a one-CTA grid waits for a
+// second CTA that does not exist, gives up after limit_ns and records status 8, exactly as a
+// factorization whose CTAs never meet would.
+__global__ void barrier_selftest_kernel(unsigned* bar, int* status, unsigned long long limit_ns) {
+    column_barrier(bar, 2u, status, limit_ns);
+}
+
+void launch_barrier_selftest(unsigned* bar, int* status, double limit_s, cudaStream_t st) {
+    const double ns = std::min(std::max(limit_s, 0.0), 4.0) * 1e9;
+    barrier_selftest_kernel<<<1, 32, 0, st>>>(bar, status, (unsigned long long)ns);
 }
 
 void lu_init_attributes() {

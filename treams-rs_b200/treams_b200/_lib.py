@@ -43,6 +43,7 @@ SIGNATURES = {
     "tcu_context_launches": (ctypes.c_longlong, [P]),
     "tcu_context_fallbacks": (ctypes.c_longlong, [P]),
     "tcu_context_set_refinement": (c_int, [P, c_double, c_double]),
+    "tcu_context_wait_selftest": (c_int, [P, c_double]),
     "tcu_context_set_profiling": (c_int, [P, c_int]),
     "tcu_context_stage_time": (c_int, [P, c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(c_double)]),
     "tcu_context_reset_stage_times": (c_int, [P]),
@@ -128,6 +129,12 @@ class Context:
     def set_refinement(self, target: float = 1e-13, fallback_above: float = 1e-12) -> None:
         """Refinement stop tolerance and the residual above which mixed solves finish in FP64."""
         _check(lib().tcu_context_set_refinement(self.handle, float(target), float(fallback_above)))
+
+    def wait_selftest(self, limit: float = 0.05) -> None:
+        """Run the LU panel's grid barrier with one arrival missing; its bounded wait gives up
+        after `limit` seconds and this raises TreamsCudaError (status TCU_TIMEOUT), leaving the
+        context usable."""
+        _check(lib().tcu_context_wait_selftest(self.handle, float(limit)))
 
     @property
     def fallbacks(self) -> int:
