@@ -213,47 +213,59 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(typename Cx<R>::T*
         C pivot = prow[j];
         double den = (double)pivot.x * pivot.x + (double)pivot.y * pivot.y;
         double ir = den > 0.0 ? pivot.x / den : 0.0, ii = den > 0.0 ? -pivot.y / den : 0.0;
-        // Multipliers first (one thread per row), then the update as independent (row, 32-column
-        // chunk) items so every thread has a run of independent shared-memory updates; the item
-        // holding column j+1 tracks the next column's candidate.
         bv = -1.f;
         br = 0x7fffffff;
         const int first = max(0, gj + 1 - row0);  // first local row below the pivot
-        for (int r = first + tid; r < myrows; r += blockDim.x) {
-            C a = tile[(size_t)r * LD + j];
-            C l;
-            l.x = (R)(a.x * ir - a.y * ii);
-            l.y = (R)(a.x * ii + a.y * ir);
-            if (den > 0.0) tile[(size_t)r * LD + j] = l;
-        }
-        __syncthreads();
         const int act = myrows - first;
-        const int q0 = (j + 1) >> 5, nq = ((w + 31) >> 5) - q0;
-        if (act > 0 && j + 1 < w)
-            for (int item = tid; item < act * nq; item += blockDim.x) {
-                int r = first + item % act, q = q0 + item / act;
+        if (act > 0) {
+            // S threads per row (a power of two up to 8, adjacent lanes of one warp): each forms
+            // the row's multiplier, part 0 stores it, and part p updates the column batches
+            // p, p + S, ... of j+1..w-1. A batch's loads are issued before its stores, so its
+            // shared-memory round trips overlap (a per-element loop would serialise them on the
+            // possible aliasing of the row and the pivot row).
+            constexpr int BATCH = sizeof(R) == 4 ? 8 : 4;
+            int S = 1;
+            while (S < 8 && act * S * 2 <= (int)blockDim.x) S *= 2;
+            for (int base = 0; base < act * S; base += blockDim.x) {  // one pass when S > 1
+                const int it = base + tid;
+                const bool valid = it < act * S;
+                const int r = first + (valid ? it / S : 0), part = it % S;
                 C* trow = tile + (size_t)r * LD;
-                int c0 = max(j + 1, q * 32), c1 = min(w, q * 32 + 32);
-                if (den > 0.0) {
-                    C l = trow[j];
-#pragma unroll 8
-                    for (int c = c0; c < c1; ++c) {
-                        C u = prow[c];
-                        C t = trow[c];
-                        t.x = t.x - (l.x * u.x - l.y * u.y);
-                        t.y = t.y - (l.x * u.y + l.y * u.x);
-                        trow[c] = t;
+                C a = trow[j];
+                if (S > 1) __syncwarp();  // every part has read a before part 0 overwrites it
+                C l;
+                l.x = (R)(a.x * ir - a.y * ii);
+                l.y = (R)(a.x * ii + a.y * ir);
+                if (valid && part == 0 && den > 0.0) trow[j] = l;
+                if (!valid) continue;
+                for (int c = j + 1 + part * BATCH; c < w; c += BATCH * S) {
+                    C u[BATCH], t[BATCH];
+#pragma unroll
+                    for (int k = 0; k < BATCH; ++k)
+                        if (c + k < w) {
+                            u[k] = prow[c + k];
+                            t[k] = trow[c + k];
+                        }
+                    if (den > 0.0) {
+#pragma unroll
+                        for (int k = 0; k < BATCH; ++k)
+                            if (c + k < w) {
+                                t[k].x = t[k].x - (l.x * u[k].x - l.y * u[k].y);
+                                t[k].y = t[k].y - (l.x * u[k].y + l.y * u[k].x);
+                                trow[c + k] = t[k];
+                            }
                     }
-                }
-                if (q == q0) {
-                    float v = (float)cx_abs2<R>(trow[j + 1]);
-                    int g = row0 + r;
-                    if (v > bv || (v == bv && g < br)) {
-                        bv = v;
-                        br = g;
+                    if (c == j + 1) {
+                        float v = (float)cx_abs2<R>(t[0]);
+                        int g = row0 + r;
+                        if (v > bv || (v == bv && g < br)) {
+                            bv = v;
+                            br = g;
+                        }
                     }
                 }
             }
+        }
         __syncthreads();
     }
     for (int idx = tid; idx < myrows * w; idx += blockDim.x) {
