@@ -63,7 +63,8 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-constexpr int PANEL_THREADS = 256;  // measured: 512 threads per CTA were slower
+constexpr int PANEL_THREADS = 256;
+constexpr int PANEL_SUB = 16;  // columns per sub-block of the blocked panel update  // measured: 512 threads per CTA were slower
 
 template <typename R>
 __device__ __forceinline__ double cx_abs2(typename Cx<R>::T a) {
@@ -108,7 +109,21 @@ __device__ bool column_barrier(unsigned* bar, unsigned target, int* status,
     return s_ok != 0;
 }
 
-template <typename R, int NB>
+// Candidate keys inside a CTA: [FP32 bits of |a|^2, + 1 : 32] (0 = no candidate) and the
+// global row; the maximum key wins, ties to the lower row (redux.sync on both words).
+__device__ __forceinline__ void warp_argmax(unsigned& key, unsigned& row) {
+    const unsigned m = __reduce_max_sync(0xffffffffu, key);
+    row = __reduce_min_sync(0xffffffffu, key == m ? row : 0xFFFFFFFFu);
+    key = m;
+}
+
+// SUB = 0: every column's rank-1 update spans the rest of the panel. SUB = 16: the rank-1
+// updates stay inside 16-column sub-blocks; after the last column of a sub-block every CTA
+// forms the sub-block's 16 rows of U over the remaining columns from the 16 broadcast pivot
+// rows it kept (forward substitution with their multipliers) and applies one rank-16 update
+// to its rows below, so the trailing part of the slab is read and written once per 16
+// columns instead of once per column.
+template <typename R, int NB, int SUB>
 __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(typename Cx<R>::T* A, size_t lda, int k0, int n, int w,
                                                     int chunk, int* piv, int* perm, unsigned long long* keys,
                                                     typename Cx<R>::T* crow, typename Cx<R>::T* drow, unsigned* bar,
@@ -116,9 +131,10 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(typename Cx<R>::T*
     typedef typename Cx<R>::T C;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* tile = (C*)smem_raw;                      // chunk x (NB + 1)
-    C* prow = tile + (size_t)chunk * (NB + 1);   // NB
-    __shared__ float s_val[PANEL_THREADS / 32];
-    __shared__ int s_row[PANEL_THREADS / 32];
+    C* pbuf = tile + (size_t)chunk * (NB + 1);   // max(SUB, 1) pivot rows of NB
+    __shared__ unsigned s_key[PANEL_THREADS / 32];
+    __shared__ unsigned s_row[PANEL_THREADS / 32];
+    __shared__ double s_inv[2];
     const int P = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int rows = n - k0;
@@ -131,41 +147,33 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(typename Cx<R>::T*
     }
     __syncthreads();
     // candidate of this thread's rows for column 0
-    float bv = -1.f;
-    int br = 0x7fffffff;
-    for (int r = tid; r < myrows; r += blockDim.x) {
-        float v = (float)cx_abs2<R>(tile[(size_t)r * LD]);
-        if (v > bv) {
-            bv = v;
-            br = row0 + r;
+    unsigned bk = 0u, br = 0xFFFFFFFFu;
+    auto offer = [&](C v, int g) {
+        const unsigned k = __float_as_uint((float)cx_abs2<R>(v)) + 1u;
+        if (k > bk || (k == bk && (unsigned)g < br)) {
+            bk = k;
+            br = (unsigned)g;
         }
-    }
+    };
+    for (int r = tid; r < myrows; r += blockDim.x) offer(tile[(size_t)r * LD], row0 + r);
     for (int j = 0; j < w; ++j) {
         const int gj = k0 + j;
         const int buf = j & 1;
-        for (int o = 16; o > 0; o >>= 1) {
-            float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            int orr = __shfl_xor_sync(0xffffffffu, br, o);
-            if (ov > bv || (ov == bv && orr < br)) {
-                bv = ov;
-                br = orr;
-            }
-        }
+        const int jb = SUB ? j - j % SUB : 0;
+        const int cend = SUB ? min(w, jb + SUB) : w;  // rank-1 updates stop here
+        C* prow = pbuf + (size_t)(SUB ? j - jb : 0) * NB;
+        warp_argmax(bk, br);
         if (lane == 0) {
-            s_val[warp] = bv;
+            s_key[warp] = bk;
             s_row[warp] = br;
         }
         __syncthreads();
-        float cv = s_val[0];
-        int crr = s_row[0];
-        for (int q = 1; q < (int)(blockDim.x >> 5); ++q)
-            if (s_val[q] > cv || (s_val[q] == cv && s_row[q] < crr)) {
-                cv = s_val[q];
-                crr = s_row[q];
-            }
-        const bool has = cv >= 0.f;
+        unsigned ck = lane < PANEL_THREADS / 32 ? s_key[lane] : 0u;
+        unsigned crr = lane < PANEL_THREADS / 32 ? s_row[lane] : 0xFFFFFFFFu;
+        warp_argmax(ck, crr);
+        const bool has = ck != 0u;
         if (has) {
-            int lr = crr - row0;
+            int lr = (int)crr - row0;
             for (int c = tid; c < w; c += blockDim.x) __stcg(&crow[((size_t)buf * P + b) * NB + c], tile[(size_t)lr * LD + c]);
         }
         if (gj >= row0 && gj < row0 + myrows) {
@@ -173,8 +181,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(typename Cx<R>::T*
             for (int c = tid; c < w; c += blockDim.x) __stcg(&drow[(size_t)buf * NB + c], tile[(size_t)lr * LD + c]);
         }
         if (tid == 0 && has) {
-            unsigned long long kv = ((unsigned long long)__float_as_uint(cv) << 32) |
-                                    (unsigned long long)(0xFFFFFFFFu - (unsigned)crr);
+            unsigned long long kv = ((unsigned long long)(ck - 1u) << 32) | (unsigned long long)(0xFFFFFFFFu - crr);
             asm volatile("red.relaxed.gpu.global.max.u64 [%0], %1;" ::"l"(&keys[j % 3]), "l"(kv) : "memory");
         }
         if (!column_barrier(bar, (unsigned)(j + 1) * (unsigned)P, status)) return;
@@ -203,29 +210,35 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(typename Cx<R>::T*
                 for (int c = tid; c < w; c += blockDim.x) tile[(size_t)lr * LD + c] = prow[c];
             }
         }
-        if (b == 0 && tid == 0) {
-            piv[gj] = pr;  // the row permutation is composed from piv after the factorization
-            C pvt = prow[j];
-            if (!((double)pvt.x * pvt.x + (double)pvt.y * pvt.y > 0.0)) atomicCAS(status, 0, 5);
+        if (tid == 0) {
+            // 1 / pivot once per CTA, in FP64
+            C pivot = prow[j];
+            double den = (double)pivot.x * pivot.x + (double)pivot.y * pivot.y;
+            s_inv[0] = den > 0.0 ? pivot.x / den : 0.0;
+            s_inv[1] = den > 0.0 ? -pivot.y / den : 0.0;
+            if (b == 0) {
+                piv[gj] = pr;  // the row permutation is composed from piv after the factorization
+                if (!(den > 0.0)) atomicCAS(status, 0, 5);
+            }
         }
         __syncthreads();
         // rank-1 update of the rows below the pivot; each thread keeps its next candidate
-        C pivot = prow[j];
-        double den = (double)pivot.x * pivot.x + (double)pivot.y * pivot.y;
-        double ir = den > 0.0 ? pivot.x / den : 0.0, ii = den > 0.0 ? -pivot.y / den : 0.0;
-        bv = -1.f;
-        br = 0x7fffffff;
+        const double ir = s_inv[0], ii = s_inv[1];
+        const bool nonzero = ir != 0.0 || ii != 0.0;
+        bk = 0u;
+        br = 0xFFFFFFFFu;
         const int first = max(0, gj + 1 - row0);  // first local row below the pivot
         const int act = myrows - first;
         if (act > 0) {
             // S threads per row (a power of two up to 8, adjacent lanes of one warp): each forms
             // the row's multiplier, part 0 stores it, and part p updates the column batches
-            // p, p + S, ... of j+1..w-1. A batch's loads are issued before its stores, so its
+            // p, p + S, ... of j+1..cend-1. A batch's loads are issued before its stores, so its
             // shared-memory round trips overlap (a per-element loop would serialise them on the
             // possible aliasing of the row and the pivot row).
             constexpr int BATCH = sizeof(R) == 4 ? 8 : 4;
+            const int ncols = cend - j - 1;
             int S = 1;
-            while (S < 8 && act * S * 2 <= (int)blockDim.x) S *= 2;
+            while (S < 8 && act * S * 2 <= (int)blockDim.x && BATCH * S < ncols) S *= 2;
             for (int base = 0; base < act * S; base += blockDim.x) {  // one pass when S > 1
                 const int it = base + tid;
                 const bool valid = it < act * S;
@@ -236,34 +249,80 @@ __global__ void __launch_bounds__(PANEL_THREADS) panel_kernel(typename Cx<R>::T*
                 C l;
                 l.x = (R)(a.x * ir - a.y * ii);
                 l.y = (R)(a.x * ii + a.y * ir);
-                if (valid && part == 0 && den > 0.0) trow[j] = l;
+                if (valid && part == 0 && nonzero) trow[j] = l;
                 if (!valid) continue;
-                for (int c = j + 1 + part * BATCH; c < w; c += BATCH * S) {
+                for (int c = j + 1 + part * BATCH; c < cend; c += BATCH * S) {
                     C u[BATCH], t[BATCH];
 #pragma unroll
                     for (int k = 0; k < BATCH; ++k)
-                        if (c + k < w) {
+                        if (c + k < cend) {
                             u[k] = prow[c + k];
                             t[k] = trow[c + k];
                         }
-                    if (den > 0.0) {
+                    if (nonzero) {
 #pragma unroll
                         for (int k = 0; k < BATCH; ++k)
-                            if (c + k < w) {
+                            if (c + k < cend) {
                                 t[k].x = t[k].x - (l.x * u[k].x - l.y * u[k].y);
                                 t[k].y = t[k].y - (l.x * u[k].y + l.y * u[k].x);
                                 trow[c + k] = t[k];
                             }
                     }
-                    if (c == j + 1) {
-                        float v = (float)cx_abs2<R>(t[0]);
-                        int g = row0 + r;
-                        if (v > bv || (v == bv && g < br)) {
-                            bv = v;
-                            br = g;
-                        }
-                    }
+                    if (c == j + 1) offer(t[0], row0 + r);
                 }
+            }
+        }
+        if (SUB && j + 1 == cend && cend < w) {
+            // end of a full sub-block: U rows of its pivots over columns cend..w-1 (forward
+            // substitution on the kept pivot rows, in place), then the rank-SUB update of the
+            // rows below, which also yields the candidates of column cend.
+            constexpr int SB = SUB ? SUB : 1;
+            __syncthreads();
+            for (int c = cend + tid; c < w; c += blockDim.x) {
+                C u[SB];
+#pragma unroll
+                for (int k = 0; k < SB; ++k) {
+                    C acc = pbuf[(size_t)k * NB + c];
+#pragma unroll
+                    for (int i = 0; i < k; ++i) {
+                        const C lki = pbuf[(size_t)k * NB + jb + i];
+                        acc.x = acc.x - (lki.x * u[i].x - lki.y * u[i].y);
+                        acc.y = acc.y - (lki.x * u[i].y + lki.y * u[i].x);
+                    }
+                    u[k] = acc;
+                    pbuf[(size_t)k * NB + c] = acc;
+                }
+            }
+            __syncthreads();
+            const int nt = w - cend;
+            for (int idx = tid; idx < SB * nt; idx += blockDim.x) {
+                const int k = idx / nt, c = cend + idx % nt, pos = k0 + jb + k;
+                if (pos >= row0 && pos < row0 + myrows) tile[(size_t)(pos - row0) * LD + c] = pbuf[(size_t)k * NB + c];
+            }
+            constexpr int G = sizeof(R) == 4 ? 8 : 4;  // columns per item
+            const int fc = max(0, k0 + cend - row0), ac = myrows - fc, ng = (nt + G - 1) / G;
+            for (int item = tid; item < ac * ng; item += blockDim.x) {
+                const int r = fc + item % ac, c0 = cend + (item / ac) * G;
+                C* trow = tile + (size_t)r * LD;
+                C acc[G];
+#pragma unroll
+                for (int k = 0; k < G; ++k)
+                    if (c0 + k < w) acc[k] = trow[c0 + k];
+#pragma unroll 4
+                for (int i = 0; i < SB; ++i) {
+                    const C li = trow[jb + i];
+#pragma unroll
+                    for (int k = 0; k < G; ++k)
+                        if (c0 + k < w) {
+                            const C u = pbuf[(size_t)i * NB + c0 + k];
+                            acc[k].x = acc[k].x - (li.x * u.x - li.y * u.y);
+                            acc[k].y = acc[k].y - (li.x * u.y + li.y * u.x);
+                        }
+                }
+#pragma unroll
+                for (int k = 0; k < G; ++k)
+                    if (c0 + k < w) trow[c0 + k] = acc[k];
+                if (c0 == cend) offer(acc[0], row0 + r);
             }
         }
         __syncthreads();
@@ -532,9 +591,9 @@ __global__ void __launch_bounds__(256) cgemm_simt_kernel(float2* A, size_t lda, 
 static int g_num_sms = 0;
 
 template <typename R, int NB>
-static size_t panel_smem(int chunk) {
+static size_t panel_smem(int chunk, int sub) {
     typedef typename Cx<R>::T C;
-    return (size_t)chunk * (NB + 1) * sizeof(C) + NB * sizeof(C);
+    return (size_t)chunk * (NB + 1) * sizeof(C) + (size_t)std::max(sub, 1) * NB * sizeof(C);
 }
 
 // The panel's grid barrier with one arrival missing: CTA 0 of a one-CTA grid waits for a
@@ -554,8 +613,10 @@ void lu_init_attributes() {
     int dev;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(panel_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    cudaFuncSetAttribute(panel_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(panel_kernel<double, 64, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(panel_kernel<float, 128, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(panel_kernel<double, 64, PANEL_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    cudaFuncSetAttribute(panel_kernel<float, 128, PANEL_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(trsm_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(trsm_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZG_SMEM);
@@ -579,6 +640,15 @@ static int panel_rows_per_cta() {
     return v;
 }
 
+static bool panel_sub_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("TCU_PANEL_SUB");
+        v = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    return v == 1;
+}
+
 template <typename R, int NB>
 static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cudaStream_t st) {
     typedef typename Cx<R>::T C;
@@ -587,7 +657,11 @@ static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cud
     const int per = panel_rows_per_cta();
     int P = std::min(g_num_sms, std::max(1, (rows + per - 1) / per));
     int chunk = (rows + P - 1) / P;
-    size_t smem = panel_smem<R, NB>(chunk);
+    // 16-column sub-blocks when their pivot rows fit next to the slab (TCU_PANEL_SUB=0 turns
+    // them off), else one rank-1 update per column over the whole panel
+    int sub = panel_sub_enabled() ? PANEL_SUB : 0;
+    if (sub && panel_smem<R, NB>(chunk, sub) > 220 * 1024) sub = 0;
+    size_t smem = panel_smem<R, NB>(chunk, sub);
     if (smem > 220 * 1024) return 1;
     unsigned long long* keys = (unsigned long long*)wk.cand;  // 3 pivot words
     C* crow = (C*)(keys + 2 * 160);
@@ -596,7 +670,8 @@ static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cud
     cudaMemsetAsync(wk.barrier, 0, 2 * sizeof(unsigned), st);
     size_t lda = (size_t)n;
     void* args[] = {&A, &lda, &k0, &n, &w, &chunk, &wk.piv, &wk.perm, &keys, &crow, &drow, &wk.barrier, &wk.status};
-    cudaError_t e = cudaLaunchCooperativeKernel((void*)panel_kernel<R, NB>, dim3(P), dim3(PANEL_THREADS), args, smem, st);
+    void* fn = sub ? (void*)panel_kernel<R, NB, PANEL_SUB> : (void*)panel_kernel<R, NB, 0>;
+    cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(P), dim3(PANEL_THREADS), args, smem, st);
     return e == cudaSuccess ? 0 : 2;
 }
 
