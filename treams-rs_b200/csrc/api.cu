@@ -122,6 +122,7 @@ struct tcu_factor {
     double* d_scale = nullptr;       // row scales (n) then column scales (n) when equilibrated
     bool scaled = false;
     tcu_factor* fallback = nullptr;  // FP64 factor of a mixed factor whose refinement stalled
+    unsigned sweep_epoch = 0;        // epochs of the persistent triangular sweeps
 };
 
 namespace {
@@ -417,22 +418,27 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
         if (f->scaled) scale_rows(v, f->d_scale, n, p, ctx->stream);  // R v
         if (f->precision == TCU_FP64)
             lu_solve_fp64((const double2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, p, ctx->stream,
-                          &ctx->launches);
+                          &ctx->launches, &f->sweep_epoch, f->wk.status);
         else
             lu_solve_fp32((const float2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, p, ctx->stream,
-                          &ctx->launches);
+                          &ctx->launches, &f->sweep_epoch, f->wk.status);
         if (f->scaled) {
             scale_rows(v, f->d_scale + n, n, p, ctx->stream);  // C (A')^-1 R v
             ctx->launches += 2;
         }
     };
+    int sweep_status = 0;
     auto residual = [&]() -> tcu_status {
         // r = T b - (x - T C x)
         apply_op(ctx, P, f->N, f->k0, f->d_pos, f->d_T, x, n, p, tb, -1.0, 1.0, true, r);
         vec_norms(r, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
         ctx->launches += 2;
         CK(cudaMemcpyAsync(rn.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "norms");
-        return sync_status(ctx, "residual");
+        CK(cudaMemcpyAsync(&sweep_status, f->wk.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "status");
+        tcu_status s2 = sync_status(ctx, "residual");
+        if (s2) return s2;
+        if (sweep_status == 8) return fail(TCU_TIMEOUT, "triangular sweep: a device-side wait gave up");
+        return TCU_OK;
     };
     CK(cudaMemcpyAsync(x, tb, per * 16, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
     lu_apply(x);

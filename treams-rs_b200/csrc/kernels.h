@@ -148,10 +148,12 @@ int lu_factor_fp32(float2* A, int n, LuWork& w, cudaStream_t st, long long* laun
 size_t lu_inverse_bytes(int n);
 void lu_block_inverses_fp64(const double2* A, int n, double2* inv, cudaStream_t st, long long* launches);
 void lu_block_inverses_fp32(const float2* A, int n, double2* inv, cudaStream_t st, long long* launches);
+// epoch: the factor's sweep counter (host), status: its device status word (8 when a sweep's
+// bounded wait gave up); both null select one launch per block step.
 void lu_solve_fp64(const double2* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp, int ncol,
-                   cudaStream_t st, long long* launches);
+                   cudaStream_t st, long long* launches, unsigned* epoch = nullptr, int* status = nullptr);
 void lu_solve_fp32(const float2* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp, int ncol,
-                   cudaStream_t st, long long* launches);
+                   cudaStream_t st, long long* launches, unsigned* epoch = nullptr, int* status = nullptr);
 size_t lu_workspace_bytes(int n, bool fp32);
 size_t tf32_pack_bytes(int n);  // packed tensor-core operands of the mixed LU
 void lu_init_attributes();
