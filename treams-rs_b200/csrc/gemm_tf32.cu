@@ -735,24 +735,46 @@ static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, in
 
 // U12 = L11^-1 A12 on the tensor cores: invert L11, then A12 -= (-(L11^-1 - I)) A12 with the
 // operands packed (A12 is read from its packed copy, so the in-place update is race free).
-void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches) {
+// Operand buffer of one TRSM step (sized on the host; a reallocation synchronises the device)
+// and the place of N = L11^-1 - I in it; null when it could not be sized.
+static float2* trsm_buffers(int n, int k0, int w, LuWork& wk, cudaStream_t st, int* kp_out) {
     int r0 = k0 + w, ncols = n - r0;
     int kp = ((2 * w + 31) / 32) * 32;  // whole 64-byte K rows of FP16 pieces (and of TF32)
     size_t need = ((size_t)2 * w * kp + (size_t)ncols * kp) * 2 * 4 + (size_t)w * w * 8 + 8192;
-    if (!ensure_pack(wk, need, n, st)) return;
-    float* ahi = (float*)wk.pack;
-    float* alo = ahi + (size_t)2 * w * kp;
-    float* bhi = alo + (size_t)2 * w * kp;
-    float* blo = bhi + (size_t)ncols * kp;
-    float2* Nm = (float2*)(((uintptr_t)(blo + (size_t)ncols * kp) + 255) & ~(uintptr_t)255);
+    if (!ensure_pack(wk, need, n, st)) return nullptr;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(tri_inverse_l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TI_SMEM);
         attr = true;
     }
+    *kp_out = kp;
+    float* blo = (float*)wk.pack + (size_t)4 * w * kp + (size_t)ncols * kp;
+    return (float2*)(((uintptr_t)(blo + (size_t)ncols * kp) + 255) & ~(uintptr_t)255);
+}
+
+bool launch_tf32_trsm_inverse(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, cudaStream_t side,
+                              long long* launches) {
+    int kp;
+    float2* Nm = trsm_buffers(n, k0, w, wk, st, &kp);
+    if (!Nm) return false;
+    tri_inverse_l_kernel<<<1, 1024, TI_SMEM, side>>>(A, (size_t)n, k0, w, Nm);
+    ++*launches;
+    return true;
+}
+
+void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches,
+                      bool inverse_done) {
+    int r0 = k0 + w, ncols = n - r0;
+    int kp;
+    float2* Nm = trsm_buffers(n, k0, w, wk, st, &kp);
+    if (!Nm) return;
+    float* ahi = (float*)wk.pack;
+    float* alo = ahi + (size_t)2 * w * kp;
+    float* bhi = alo + (size_t)2 * w * kp;
+    float* blo = bhi + (size_t)ncols * kp;
     {
         StageScope sc(ST_TRSM, st);
-        tri_inverse_l_kernel<<<1, 1024, TI_SMEM, st>>>(A, (size_t)n, k0, w, Nm);
+        if (!inverse_done) tri_inverse_l_kernel<<<1, 1024, TI_SMEM, st>>>(A, (size_t)n, k0, w, Nm);
         dim3 g1((w + 31) / 32, (kp / 2 + 31) / 32);
         size_t tot = (size_t)ncols * (kp / 2);
         if (wk.f16_pieces) {

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -695,7 +696,34 @@ __global__ void perm_from_piv_kernel(const int* __restrict__ piv, int* __restric
 }
 
 void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches);
-void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches);
+void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches,
+                      bool inverse_done);
+bool launch_tf32_trsm_inverse(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, cudaStream_t side,
+                              long long* launches);
+
+// A second stream of this thread and device (created once, kept for the process) on which the
+// inverse of each step's L11 runs while the main stream applies the row interchanges: the
+// inverse reads only the panel's diagonal block, the interchanges touch only the columns
+// outside the panel.
+struct SideStream {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t panel_done = nullptr, inverse_done = nullptr;
+    bool ok = false;
+};
+static SideStream* side_stream() {
+    thread_local std::map<int, SideStream> by_device;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    auto it = by_device.find(dev);
+    if (it == by_device.end()) {
+        SideStream s;
+        s.ok = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) == cudaSuccess &&
+               cudaEventCreateWithFlags(&s.panel_done, cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&s.inverse_done, cudaEventDisableTiming) == cudaSuccess;
+        it = by_device.emplace(dev, s).first;
+    }
+    return it->second.ok ? &it->second : nullptr;
+}
 
 template <typename R, int NB>
 static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t st, long long* launches,
@@ -712,18 +740,28 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
         }
         ++*launches;
         if (rc) return rc;
+        // the TRSM's inverse of L11 overlaps the row interchanges (mixed path)
+        SideStream* side = (sizeof(R) == 4 && tensor_cores && k0 + w < n) ? side_stream() : nullptr;
+        bool inverse_done = false;
+        if (side && cudaEventRecord(side->panel_done, st) == cudaSuccess &&
+            cudaStreamWaitEvent(side->stream, side->panel_done, 0) == cudaSuccess)
+            inverse_done = launch_tf32_trsm_inverse((float2*)A, n, k0, w, wk, st, side->stream, launches) &&
+                           cudaEventRecord(side->inverse_done, side->stream) == cudaSuccess;
         {
             StageScope sc(ST_SWAP, st);
             laswp_kernel<C><<<(n + 255) / 256, 256, 0, st>>>(A, lda, n, k0, w, wk.piv);
         }
         ++*launches;
+        if (inverse_done && cudaStreamWaitEvent(st, side->inverse_done, 0) != cudaSuccess) {
+            cudaStreamSynchronize(side->stream);  // ordering by the host instead
+        }
         int r0 = k0 + w;
         if (r0 >= n) break;
         int cols = n - r0;
         int cpc = 64;
         size_t smem = (size_t)NB * NB * sizeof(C);
         if (sizeof(R) == 4 && tensor_cores) {
-            launch_tf32_trsm((float2*)A, n, k0, w, wk, st, launches);
+            launch_tf32_trsm((float2*)A, n, k0, w, wk, st, launches, inverse_done);
         } else {
             StageScope sc(ST_TRSM, st);
             trsm_kernel<R, NB><<<(cols + cpc - 1) / cpc, 256, smem, st>>>(A, lda, k0, w, n, cpc);
