@@ -104,6 +104,18 @@ tcu_status tcu_context_reset_stage_times(tcu_context* ctx);
 tcu_status tcu_translation_block(tcu_context* ctx, int lmax, double k, const double* disp, int singular,
                                  int helicity, double* out);
 
+/* Translation coefficients of single mode pairs at complex polar arguments, the elementwise
+ * sw.translate (python/treams_rs/sw.py:70; treams-core sw/polar.rs:251 polar_translation_array).
+ * labels: count x 6 ints (lambda, mu, pol of the destination mode, l, m, qol of the source
+ * mode; degrees 1..7); args: count x 3 complex (kr, theta, phi of k (r_destination -
+ * r_source)); out: count complex. helicity != 0: A + (2 pol - 1) B for pol == qol, else 0;
+ * parity: A for pol == qol, else B. singular != 0 expands an outgoing wave (0 at kr = 0). */
+tcu_status tcu_translate(tcu_context* ctx, size_t count, const int* labels, const double* args, int helicity,
+                         int singular, double* out);
+/* Wigner 3j symbol (j1 j2 j3; m1 m2 m3) (special/wigner.rs:263 wigner3j), degrees <= 60,
+ * by Racah's closed formula in binary128 on the host (no device work, no context). */
+double tcu_wigner3j(int j1, int j2, int j3, int m1, int m2, int m3);
+
 /* ---- Mie T and incident fields -------------------------------------------------------- */
 /* 2 x 2 Mie blocks in mode order, lmax per sphere, N spheres: out N * lmax * 4 complex,
  * row-major per block (tmatrix/sphere.rs:43-80, coeffs/mie.rs:209). */
@@ -182,9 +194,10 @@ tcu_status tcu_cluster_apply(tcu_context* ctx, int lmax, double k0, size_t N, co
  * complex); the call runs on `stream` (a cudaStream_t, may be NULL) and needs no context.
  * Scratch (plan tables, Mie blocks, a status word) lives in one 8 MiB static device array
  * per GPU: the plan plus N * lmax * 64 bytes must fit, larger clusters are rejected with
- * TCU_INVALID_INPUT. The first call on a device looks up that array's address; make it
- * before any stream capture. Calls that overlap on the GPU race on the shared array. The
- * call synchronises `stream` (geometry check and status read). Errors: tcu_last_error_message(). */
+ * TCU_INVALID_INPUT. The first call on a device looks up that array's address. Calls that
+ * overlap on the GPU race on the shared array. The call copies from pageable host memory and
+ * synchronises `stream` (geometry check and status read), so it cannot be used under stream
+ * capture. Errors: tcu_last_error_message(). */
 tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k0, size_t N, const double* radii,
                                      const double* eps, const double* positions, int p, const double* x, double* y);
 /* Restarted GMRES on (I - T C) X = T B (cluster/iterative.rs:264-284, linalg/gmres.rs:119).

@@ -301,3 +301,30 @@ def learned_gram(lmax, k0, radii, eps, pos, layers: int, V, reach: float = 3.0):
     if st:
         raise ValueError(f"oracle Gram failed with status {st}")
     return gram.reshape(K1, K1), rhs
+
+
+def apply_t(lmax, tb, B):
+    """T B for the per-sphere 2x2 Mie blocks tb (N, lmax, 2, 2) in mode order."""
+    N = tb.shape[0]
+    M = 2 * lmax * (lmax + 2)
+    B = np.asarray(B, np.complex128)
+    squeeze = B.ndim == 1
+    if squeeze:
+        B = B[:, None]
+    degrees = np.array([l for l in range(1, lmax + 1) for _ in range(2 * l + 1)])
+    Tq = tb[:, degrees - 1]                                  # (N, M/2, 2, 2)
+    Bq = B.reshape(N, M // 2, 2, B.shape[1])
+    out = np.einsum("nqab,nqbp->nqap", Tq, Bq).reshape(N * M, B.shape[1])
+    return out[:, 0] if squeeze else np.asfortranarray(out)
+
+
+def lapack_cluster_solve(lmax, k0, radii, eps, pos, B):
+    """X = (I - T C)^-1 T B with the oracle's FP64 assembly and LAPACK zgetrf/zgetrs
+    (scipy, all host threads), factoring in place so the host holds one n x n copy."""
+    import scipy.linalg
+
+    A, tb = cluster_operator(lmax, k0, radii, eps, pos)
+    TB = apply_t(lmax, tb, B)
+    lu, piv = scipy.linalg.lu_factor(A, overwrite_a=True, check_finite=False)
+    del A
+    return scipy.linalg.lu_solve((lu, piv), TB, check_finite=False)

@@ -1,8 +1,9 @@
 """Batched heterogeneous cluster solves against the oracle's dense FP64 solves.
 
 Each cluster of the batch is checked on its own (relative error <= 1e-10, the tolerance of the
-single-cluster tests); the batch orders clusters by size and releases each operator before
-the next, so the results must equal those of separate calls.
+single-cluster tests), at lmax 3 to 6 (the degrees of the 256-cluster sweep); the batch orders
+clusters by size and releases each operator before the next, so the results must equal those
+of separate calls.
 """
 import numpy as np
 import pytest
@@ -20,6 +21,12 @@ def _small_batch():
         w = workloads.batch_cluster(c)
         # keep the test small: the first `count` spheres of the cluster, lmax capped at 4
         lmax = min(w.lmax, 4)
+        out.append((lmax, w.k0, w.radii[:count], w.eps[:count], w.positions[:count]))
+    # the sweep's highest degrees: first clusters of the sweep drawn with lmax 5 and 6, at
+    # their own lmax (n = 700 and 768 for 10 and 8 spheres)
+    for lmax, count in ((5, 10), (6, 8)):
+        c = next(c for c in range(256) if workloads.batch_cluster(c).lmax == lmax)
+        w = workloads.batch_cluster(c)
         out.append((lmax, w.k0, w.radii[:count], w.eps[:count], w.positions[:count]))
     return out
 

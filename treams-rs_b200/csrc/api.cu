@@ -607,6 +607,48 @@ tcu_status tcu_translation_block(tcu_context* ctx, int lmax, double k, const dou
     return sync_status(ctx, "translation block");
 }
 
+double tcu_wigner3j(int j1, int j2, int j3, int m1, int m2, int m3) {
+    if (j1 < 0 || j2 < 0 || j3 < 0 || j1 > 60 || j2 > 60 || j3 > 60) return 0.0;
+    return wigner3j_racah(j1, j2, j3, m1, m2, m3);
+}
+
+tcu_status tcu_translate(tcu_context* ctx, size_t count, const int* labels, const double* args, int helicity,
+                         int singular, double* out) {
+    if (!ctx || (count > 0 && (!labels || !args || !out))) return fail(TCU_INVALID_INPUT, "null argument");
+    int L = 1;
+    for (size_t e = 0; e < count; ++e) {
+        const int* lb = labels + 6 * e;
+        for (int side = 0; side < 2; ++side) {
+            const int l = lb[3 * side], m = lb[3 * side + 1], pol = lb[3 * side + 2];
+            if (l < 1 || l > 7 || m < -l || m > l || (pol != 0 && pol != 1))
+                return fail(TCU_INVALID_INPUT,
+                            "mode labels need 1 <= degree <= 7, |order| <= degree and polarization 0 or 1");
+            L = std::max(L, l);
+        }
+    }
+    if (!finite_all(args, 6 * count)) return fail(TCU_INVALID_INPUT, "translation arguments must be finite");
+    if (count == 0) return TCU_OK;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    const DevPlan* P;
+    tcu_status s = get_plan(ctx, L, &P);
+    if (s) return s;
+    DevBuf buf(ctx);
+    Arena ar;
+    size_t o_l = ar.add(count * 6 * sizeof(int)), o_a = ar.add(count * 48), o_o = ar.add(count * 16);
+    CK(buf.alloc(ar.total), "translation buffers");
+    CK(cudaMemcpyAsync(ar.at<void>(buf.p, o_l), labels, count * 6 * sizeof(int), cudaMemcpyHostToDevice, ctx->stream),
+       "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(buf.p, o_a), args, count * 48, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    launch_translate(*P, count, ar.at<int>(buf.p, o_l), ar.at<cplx>(buf.p, o_a), helicity != 0, singular != 0,
+                     ar.at<cplx>(buf.p, o_o), ctx->stream);
+    ++ctx->launches;
+    CK(cudaGetLastError(), "translation coefficients");
+    CK(cudaMemcpyAsync(out, ar.at<void>(buf.p, o_o), count * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    return sync_status(ctx, "translation coefficients");
+}
+
 tcu_status tcu_mie_blocks(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii, const double* eps,
                           double* out) {
     if (!ctx || !radii || !eps || !out || N == 0) return fail(TCU_INVALID_INPUT, "null argument");

@@ -34,6 +34,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 
@@ -552,6 +553,9 @@ static bool make_map(CUtensorMap* map, void* base, int rows, int kp, int box_row
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+__global__ void tri_inverse_l_kernel(const float2* __restrict__ A, size_t lda, int k0, int w, float2* __restrict__ N);
+constexpr size_t TI_SMEM = (size_t)(128 * 129 + 64 * 64) * sizeof(float2);
+
 // TF32 pieces by default; FP16 pieces (twice the tensor rate) with TCU_SPLIT=f16. On the
 // cluster operators measured here the entries of one row of L21 or one column of U12 span
 // more than 2^20 even after equilibration, and FP16 pieces (8 exponent bits fewer) then leave
@@ -570,10 +574,14 @@ bool tf32_enabled() {
     if (on < 0) {
         const char* e = getenv("TCU_DISABLE_TCGEN05");
         on = (e && e[0] == '1') ? 0 : 1;
-        if (on) {
+        if (on && !encoder()) on = 0;
+    }
+    if (on == 1) {
+        static std::atomic<unsigned long long> attr{0};
+        if (first_use_on_device(attr)) {
             cudaFuncSetAttribute(tf32_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
             cudaFuncSetAttribute(tf32_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
-            if (!encoder()) on = 0;
+            cudaFuncSetAttribute(tri_inverse_l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TI_SMEM);
         }
     }
     return on == 1;
@@ -656,8 +664,6 @@ __global__ void __launch_bounds__(1024) tri_inverse_l_kernel(const float2* __res
         N[(size_t)k * w + ii] = M[ii * LD + k];
     }
 }
-constexpr size_t TI_SMEM = (size_t)(128 * 129 + 64 * 64) * sizeof(float2);
-
 size_t tf32_pack_bytes(int n) {
     size_t kp = 256;
     return ((size_t)2 * n * kp + (size_t)n * kp) * 2 * 4 + (size_t)128 * 128 * 8 + 8192;
@@ -673,18 +679,13 @@ static int num_sms() {
     return sms;
 }
 
-static bool ensure_pack(LuWork& wk, size_t need, int n, cudaStream_t st) {
+// The packed operands live in the buffer the factor allocated from its context's pool
+// (tf32_pack_bytes(n), enough for every step of an n x n factorization); a step that would
+// need more records status 6 (out of memory) instead of reallocating outside the pool.
+static bool ensure_pack(LuWork& wk, size_t need, cudaStream_t st) {
     if (wk.pack && wk.pack_bytes >= need) return true;
-    if (wk.pack) cudaFree(wk.pack);
-    size_t want = std::max(need, tf32_pack_bytes(n));
-    if (cudaMalloc(&wk.pack, want) != cudaSuccess) {
-        wk.pack = nullptr;
-        wk.pack_bytes = 0;
-        cudaMemsetAsync(wk.status, 6, 1, st);
-        return false;
-    }
-    wk.pack_bytes = want;
-    return true;
+    cudaMemsetAsync(wk.status, 6, 1, st);
+    return false;
 }
 
 // C[row0 .. row0+m2) x [col0 .. col0+ncols) -= Apack (m2 x kp) * Bpack (ncols x kp)^T;
@@ -741,12 +742,7 @@ static float2* trsm_buffers(int n, int k0, int w, LuWork& wk, cudaStream_t st, i
     int r0 = k0 + w, ncols = n - r0;
     int kp = ((2 * w + 31) / 32) * 32;  // whole 64-byte K rows of FP16 pieces (and of TF32)
     size_t need = ((size_t)2 * w * kp + (size_t)ncols * kp) * 2 * 4 + (size_t)w * w * 8 + 8192;
-    if (!ensure_pack(wk, need, n, st)) return nullptr;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(tri_inverse_l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TI_SMEM);
-        attr = true;
-    }
+    if (!ensure_pack(wk, need, st)) return nullptr;
     *kp_out = kp;
     float* blo = (float*)wk.pack + (size_t)4 * w * kp + (size_t)ncols * kp;
     return (float2*)(((uintptr_t)(blo + (size_t)ncols * kp) + 255) & ~(uintptr_t)255);
@@ -759,7 +755,8 @@ bool launch_tf32_trsm_inverse(float2* A, int n, int k0, int w, LuWork& wk, cudaS
     if (!Nm) return false;
     tri_inverse_l_kernel<<<1, 1024, TI_SMEM, side>>>(A, (size_t)n, k0, w, Nm);
     ++*launches;
-    return true;
+    // a refused launch leaves the inverse to the main stream (launch_tf32_trsm, inverse_done false)
+    return cudaGetLastError() == cudaSuccess;
 }
 
 void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches,
@@ -774,7 +771,13 @@ void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t 
     float* blo = bhi + (size_t)ncols * kp;
     {
         StageScope sc(ST_TRSM, st);
-        if (!inverse_done) tri_inverse_l_kernel<<<1, 1024, TI_SMEM, st>>>(A, (size_t)n, k0, w, Nm);
+        if (!inverse_done) {
+            tri_inverse_l_kernel<<<1, 1024, TI_SMEM, st>>>(A, (size_t)n, k0, w, Nm);
+            if (cudaGetLastError() != cudaSuccess) {  // U12 would use a stale inverse: stop the factorization
+                cudaMemsetAsync(wk.status, 7, 1, st);
+                return;
+            }
+        }
         dim3 g1((w + 31) / 32, (kp / 2 + 31) / 32);
         size_t tot = (size_t)ncols * (kp / 2);
         if (wk.f16_pieces) {
@@ -802,7 +805,7 @@ void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_
     int r0 = k0 + w, m = n - r0, ncols = n - r0;
     int kp = ((2 * w + 31) / 32) * 32;  // whole 64-byte K rows of FP16 pieces (and of TF32)
     size_t need = ((size_t)2 * m * kp + (size_t)ncols * kp) * 2 * 4 + 4096;
-    if (!ensure_pack(wk, need, n, st)) return;
+    if (!ensure_pack(wk, need, st)) return;
     float* ahi = (float*)wk.pack;
     float* alo = ahi + (size_t)2 * m * kp;
     float* bhi = alo + (size_t)2 * m * kp;

@@ -6,11 +6,21 @@
 #include "../../include/treams_cuda.h"
 #include "plan.h"
 
+#include <atomic>
 #include <vector>
 
 namespace tcu {
 
 typedef double2 cplx;
+
+// Kernel attributes (large dynamic shared memory) are per device: each site keeps one bit per
+// device in `mask`, and this returns true the first time it runs with that device current.
+inline bool first_use_on_device(std::atomic<unsigned long long>& mask) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    const unsigned long long bit = 1ull << dev;
+    return (mask.fetch_or(bit) & bit) == 0;
+}
 
 // Per-stage CUDA-event timing (tcu_context_set_profiling). The API layer installs the
 // context's profiler as the calling thread's current one for the duration of a call; the
@@ -88,6 +98,10 @@ void launch_plane_wave(int L, int N, const double* pos, int ncol, const cplx* kv
                        const double* lfac, cplx* out, cudaStream_t st);
 void launch_apply_t(int L, int N, const cplx* T, const cplx* x, int ncol, cplx* y, cudaStream_t st);
 void pairs_init_attributes();
+// translate.cu — per-entry translation coefficients: labels 6 ints per element (lambda, mu,
+// pol, l, m, qol), args 3 complex per element (kr, theta, phi)
+void launch_translate(const DevPlan& P, size_t count, const int* labels, const cplx* args, bool helicity,
+                      bool singular, cplx* out, cudaStream_t st);
 
 // equil.cu — power-of-two row/column equilibration of an n x n column-major matrix (FP64 or
 // FP32 storage) when its largest entry exceeds `threshold`; r, c: n scales each.

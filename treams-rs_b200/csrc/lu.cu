@@ -609,11 +609,16 @@ void launch_barrier_selftest(unsigned* bar, int* status, double limit_s, cudaStr
     barrier_selftest_kernel<<<1, 32, 0, st>>>(bar, status, (unsigned long long)ns);
 }
 
+__global__ void perm_from_piv_kernel(const int* __restrict__ piv, int* __restrict__ perm, int n);
+
 void lu_init_attributes() {
-    if (g_num_sms) return;
+    static std::atomic<unsigned long long> done{0};
+    if (!first_use_on_device(done)) return;
     int dev;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g_num_sms = sms;
     cudaFuncSetAttribute(panel_kernel<double, 64, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(panel_kernel<float, 128, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
     cudaFuncSetAttribute(panel_kernel<double, 64, PANEL_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
@@ -621,6 +626,7 @@ void lu_init_attributes() {
     cudaFuncSetAttribute(trsm_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(trsm_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZG_SMEM);
+    cudaFuncSetAttribute(perm_from_piv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 size_t lu_workspace_bytes(int n, bool fp32) {
@@ -783,11 +789,6 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
         }
     }
     {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(perm_from_piv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            attr = true;
-        }
         StageScope sc(ST_SWAP, st);
         perm_from_piv_kernel<<<1, 1024, (size_t)n * sizeof(int), st>>>(wk.piv, wk.perm, n);
         ++*launches;

@@ -8,9 +8,11 @@
 // NOALLOC_BYTES. The array exists on every GPU that loads this library, for the life of
 // the process. Host code only ever sees a host-side stand-in for its name, so its device
 // address is looked up once per device (cudaGetSymbolAddress, with that device current)
-// on the first call on that device; make that first call before any stream capture.
-// Every call overwrites the whole used part of the array (the status word is cleared at
-// the start), and calls that overlap on the GPU, on any streams, race on it.
+// on the first call on that device. Every call copies the plan from pageable host memory
+// and synchronises its stream to read the geometry check and the status word, so it cannot
+// run inside a stream capture. Every call overwrites the whole used part of the array (the
+// status word is cleared at the start), and calls that overlap on the GPU, on any streams,
+// race on it.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -83,6 +85,7 @@ extern "C" tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k
         return noalloc_fail(TCU_INVALID_INPUT,
                             "require 1 <= lmax <= 7, positive finite k0, N >= 1, p >= 1 and device pointers");
     cudaStream_t st = (cudaStream_t)stream;
+    cudaGetLastError();  // an earlier failure of the caller's own work is not this call's
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
         return noalloc_fail(TCU_DEVICE_ERROR, "no current CUDA device");
@@ -125,13 +128,15 @@ extern "C" tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k
     validate_kernel<<<(unsigned)((pairs + 255) / 256), 256, 0, st>>>((int)N, radii, (const double2*)eps, positions,
                                                                      status);
     int hst = 0;
-    if (!ck(cudaMemcpyAsync(&hst, status, sizeof(int), cudaMemcpyDeviceToHost, st)) || !ck(cudaStreamSynchronize(st)))
+    if (!ck(cudaGetLastError()) || !ck(cudaMemcpyAsync(&hst, status, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        !ck(cudaStreamSynchronize(st)))
         return noalloc_fail(TCU_DEVICE_ERROR, "geometry check failed to run");
     if (hst)
         return noalloc_fail(TCU_INVALID_INPUT,
                             "require positive finite radii, finite permittivities and positions, and spheres that "
                             "neither touch nor overlap");
     launch_mie(lmax, k0, (int)N, radii, (const double2*)eps, T, status, st);
+    if (!ck(cudaGetLastError())) return noalloc_fail(TCU_DEVICE_ERROR, "Mie coefficients failed to launch");
     DevPlan P;
     P.L = lmax;
     P.nlm = h.nlm;
@@ -146,9 +151,12 @@ extern "C" tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k
         launch_apply(P, (int)N, k0, positions, T, (const double2*)x + (size_t)c0 * n, n, nc, nullptr, 1.0, -1.0, true,
                      (double2*)y + (size_t)c0 * n, st);
     }
-    if (!ck(cudaMemcpyAsync(&hst, status, sizeof(int), cudaMemcpyDeviceToHost, st)) || !ck(cudaStreamSynchronize(st)) ||
-        !ck(cudaGetLastError()))
+    if (!ck(cudaGetLastError()) || !ck(cudaMemcpyAsync(&hst, status, sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+        !ck(cudaStreamSynchronize(st)) || !ck(cudaGetLastError()))
         return noalloc_fail(TCU_DEVICE_ERROR, "matrix-free operator failed to run");
+    // the status words of the context path: 5 singular, 8 a bounded wait gave up, else a device fault
     if (hst == 5) return noalloc_fail(TCU_SINGULAR, "Mie coefficients: numerically singular");
+    if (hst == 8) return noalloc_fail(TCU_TIMEOUT, "matrix-free operator: a device-side wait gave up");
+    if (hst != 0) return noalloc_fail(TCU_DEVICE_ERROR, "matrix-free operator: nonzero device status");
     return TCU_OK;
 }

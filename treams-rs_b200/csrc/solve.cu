@@ -445,13 +445,12 @@ static void inverses_impl(const C* A, int n, double2* inv, cudaStream_t st, long
     int nb = (n + SB - 1) / SB;
     StageScope sc(ST_SOLVE, st);
     const size_t smem = (size_t)(SB * (SB + 1) + SB) * sizeof(double2);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_use_on_device(attr)) {
         cudaFuncSetAttribute(tri_block_inverse_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(tri_block_inverse_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(tri_block_inverse_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(tri_block_inverse_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
     }
     cudaMemsetAsync(chain_flags(inv, n), 0, (size_t)(nb + 64) * sizeof(unsigned), st);
     tri_block_inverse_kernel<C, true><<<nb, 256, smem, st>>>(A, n, n, inv);
@@ -478,14 +477,11 @@ static bool chain_enabled() {
 template <typename C, bool LOWER, int NC>
 static bool chain_launch_nc(cudaStream_t st, const C* A, int n, const double2* dinv, const double2* rhs,
                             double2* sol, unsigned* flags, unsigned epoch, int* status) {
-    static bool attr = false;
+    static std::atomic<unsigned long long> attr{0};
     const size_t smem = chain_smem_bytes<C>(NC);
-    if (!attr) {
-        if (cudaFuncSetAttribute(trsv_chain_kernel<C, LOWER, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return false;
-        attr = true;
-    }
+    // a refused attribute makes the cooperative launch below fail, and the caller takes the step path
+    if (first_use_on_device(attr))
+        cudaFuncSetAttribute(trsv_chain_kernel<C, LOWER, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int nb = (n + SB - 1) / SB;
     const int grid = std::min(nb, g_sms);
     size_t lda = (size_t)n;

@@ -48,6 +48,8 @@ SIGNATURES = {
     "tcu_context_stage_time": (c_int, [P, c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(c_double)]),
     "tcu_context_reset_stage_times": (c_int, [P]),
     "tcu_translation_block": (c_int, [P, c_int, c_double, P, c_int, c_int, P]),
+    "tcu_translate": (c_int, [P, c_size, P, P, c_int, c_int, P]),
+    "tcu_wigner3j": (c_double, [c_int] * 6),
     "tcu_mie_blocks": (c_int, [P, c_int, c_double, c_size, P, P, P]),
     "tcu_plane_wave_expansion": (c_int, [P, c_int, c_size, P, c_int, P, P, P]),
     "tcu_cross_sections": (c_int, [P, c_int, c_double, c_size, P, c_int, P, P, P, P]),
