@@ -44,7 +44,8 @@ typedef enum tcu_precision {
 typedef enum tcu_preconditioner {
     TCU_PRECOND_NONE = 0,          /* plain GMRES on I - T C */
     TCU_PRECOND_BLOCK_JACOBI = 1,  /* block Jacobi over nearest-neighbour sphere groups (<= 96 modes) */
-    TCU_PRECOND_LEARNED = 2        /* learned polynomial in the block-sparse near-field couplings */
+    TCU_PRECOND_LEARNED = 2,       /* coarse dipole solve + near field weighted by the trained graph network */
+    TCU_PRECOND_TWO_LEVEL = 3      /* coarse dipole solve + unweighted near field (the method without the network) */
 } tcu_preconditioner;
 
 typedef struct tcu_context tcu_context;
@@ -208,21 +209,37 @@ tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0, size_t N, 
                                const tcu_gmres_options* options, int preconditioner, double* X,
                                tcu_certificate* certificates);
 
-/* Settings of the GMRES preconditioners of this context (no counterpart in the reference):
- * near-field reach in sphere diameters (<= 0: the compiled-in fit's reach) and, for TCU_PRECOND_LEARNED, the layer
- * count and weights (alpha: layers + 1 complex; layers < 0 restores the compiled-in fit,
- * alpha NULL with layers >= 0 uses weights 1, i.e. block-Jacobi relaxation sweeps). */
-tcu_status tcu_context_set_learned_preconditioner(tcu_context* ctx, double reach_diameters, int layers,
-                                                  const double* alpha);
-/* Training statistics of the learned preconditioner (no counterpart in the reference, whose
- * iterative solver is unpreconditioned): for the cluster's layer basis u_k = A (D N)^k D v,
- * k = 0..layers (D: block-Jacobi inverse, N: near-field couplings between blocks, A = I - T C),
- * over nvec probe vectors V (n x nvec complex, column-major, host), returns
- * gram[k * (layers+1) + l] = sum_v conj(u_k) . u_l and rhs[k] = sum_v conj(u_k) . v (complex),
- * from which ||v - sum_k alpha_k u_k||^2 and its gradient in alpha follow for any alpha. */
-tcu_status tcu_learned_precond_gram(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
-                                    const double* eps, const double* positions, int layers, int nvec,
-                                    const double* V, double* gram, double* rhs);
+/* Preconditioners TCU_PRECOND_LEARNED and TCU_PRECOND_TWO_LEVEL (no counterpart in the
+ * reference, whose iterative solver is unpreconditioned): right preconditioner
+ *   z = P A_cc^-1 v_c + (I + T C_near^Theta)(v - A P A_cc^-1 v_c)
+ * with A_cc = I - T_1 C_11 the cluster's dipole (l = 1) system, factored once by this
+ * library's dense LU, P its injection into the full mode space, and C_near^Theta the
+ * translation blocks of the sphere pairs closer than the reach, every (degree, degree)
+ * sub-block of pair (i, j) scaled by Theta_ij. TWO_LEVEL uses Theta = 1; LEARNED predicts Theta
+ * with a graph network over the pairs (node features of each sphere, edge features of each
+ * pair; 2 lmax^2 real outputs per edge). */
+/* Near-field reach in sphere diameters (<= 0: the compiled-in 3) and network weights
+ * (count 0: the compiled-in weights of the lmax solved; a count that does not match
+ * tcu_learned_weight_count of that lmax uses Theta = 1). */
+tcu_status tcu_context_set_learned_weights(tcu_context* ctx, double reach_diameters, size_t count,
+                                           const double* weights);
+/* Number of network weights for lmax (0 outside 1..7). */
+size_t tcu_learned_weight_count(int lmax);
+
+/* Training of the network on the GPU (no counterpart in the reference). A training problem
+ * holds one cluster (host arrays as for tcu_sphere_cluster_factor) and nprobe probe vectors V
+ * (n x nprobe complex, column-major, host; 1 <= nprobe <= 64), turned into coarse-corrected
+ * unit-norm probes r1 = (v - A P A_cc^-1 v_c) / ||.||. loss_grad evaluates, on the device,
+ * loss = sum_p ||r1_p - A M_Theta r1_p||^2 (M_Theta r = r + T C_near^Theta r, A = I - T C in FP64)
+ * and its gradient in every weight (forward and backward kernels of the network; the gradient
+ * through Theta uses the adjoint operator A^H). probes copies the r1 to the host. */
+typedef struct tcu_learned_problem tcu_learned_problem;
+tcu_status tcu_learned_problem_create(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                      const double* eps, const double* positions, int nprobe, const double* V,
+                                      tcu_learned_problem** out);
+tcu_status tcu_learned_problem_loss_grad(tcu_learned_problem* p, const double* weights, double* loss, double* grad);
+tcu_status tcu_learned_problem_probes(tcu_learned_problem* p, double* out);
+tcu_status tcu_learned_problem_destroy(tcu_learned_problem* p);
 
 /* ---- 2D lattice sums and periodic arrays --------------------------------------------- */
 /* Ewald lattice sums D_lm (lattice/mod.rs:11-15, 283; ewald.rs:39-270) of a 2D lattice

@@ -66,8 +66,6 @@ def lib() -> ctypes.CDLL:
         L.orc_lsumsw2d.argtypes = [c_int, c_int, c_double, c_double, P, P, P, c_double, c_double, c_int, P]
         L.orc_lsumsw2d_table.restype = c_int
         L.orc_lsumsw2d_table.argtypes = [c_int, c_double, c_double, P, P, P, c_double, c_double, P]
-        L.orc_learned_gram.restype = c_int
-        L.orc_learned_gram.argtypes = [c_int, c_double, c_int, P, P, P, c_double, c_int, c_int, P, P, P]
         L.orc_array_solve.restype = c_int
         L.orc_array_solve.argtypes = [c_int, c_double, c_double, c_double, c_double, P, P, c_double, P]
     return _LIB
@@ -286,22 +284,6 @@ def array_solve(lmax: int, k0: float, radius: float, eps: complex, lattice, kpar
     return out.reshape(M, M, order="F")
 
 
-def learned_gram(lmax, k0, radii, eps, pos, layers: int, V, reach: float = 3.0):
-    """Gram matrix (layers+1)^2 and right-hand side of the learned preconditioner's layer basis."""
-    radii = np.ascontiguousarray(radii, np.float64)
-    eps = np.ascontiguousarray(eps, np.complex128)
-    pos = np.ascontiguousarray(pos, np.float64)
-    V = np.asfortranarray(V, np.complex128)
-    K1 = layers + 1
-    gram = np.zeros(K1 * K1, np.complex128)
-    rhs = np.zeros(K1, np.complex128)
-    st = lib().orc_learned_gram(lmax, k0, radii.size, _p(radii), _p(eps), _p(pos), float(reach), layers, V.shape[1],
-                                _p(V),
-                                _p(gram), _p(rhs))
-    if st:
-        raise ValueError(f"oracle Gram failed with status {st}")
-    return gram.reshape(K1, K1), rhs
-
 
 def apply_t(lmax, tb, B):
     """T B for the per-sphere 2x2 Mie blocks tb (N, lmax, 2, 2) in mode order."""
@@ -328,3 +310,96 @@ def lapack_cluster_solve(lmax, k0, radii, eps, pos, B):
     lu, piv = scipy.linalg.lu_factor(A, overwrite_a=True, check_finite=False)
     del A
     return scipy.linalg.lu_solve((lu, piv), TB, check_finite=False)
+
+
+# ---- learned preconditioner: restatement of the graph network and its training loss ----------
+GNN_H, GNN_NF, GNN_EF = 16, 6, 5
+
+
+def gnn_layout(lmax):
+    """Offsets of the weight vector: W1 (16x6), b1, W2 (16x37), b2, W3 (16x37), b3, W4 (2L^2 x 16), b4."""
+    H, nin, no = GNN_H, 2 * GNN_H + GNN_EF, 2 * lmax * lmax
+    sizes = [("W1", (H, GNN_NF)), ("b1", (H,)), ("W2", (H, nin)), ("b2", (H,)), ("W3", (H, nin)), ("b3", (H,)),
+             ("W4", (no, H)), ("b4", (no,))]
+    out, o = {}, 0
+    for name, shape in sizes:
+        size = int(np.prod(shape))
+        out[name] = (o, shape)
+        o += size
+    return out, o
+
+
+def gnn_graph(k0, radii, eps, pos, reach_diameters=3.0):
+    """Neighbours closer than reach_diameters * 2 max(radius) (rows sorted), node features
+    [deg/12, sum 1/(kd)/8, sum 1/(kd)^3/4, |r - centroid|/max|r - centroid|, k r, Re eps/8] and
+    edge features [1/(kd), 1/(kd)^2, 1/(kd)^3, kd/4, d/cutoff]."""
+    pos = np.asarray(pos, float)
+    N = len(pos)
+    cutoff = 2.0 * reach_diameters * float(np.max(radii))
+    D = np.linalg.norm(pos[:, None] - pos[None], axis=2)
+    rows, nbrs = [], []
+    for i in range(N):
+        for j in range(N):
+            if j != i and D[i, j] <= cutoff:
+                rows.append(i)
+                nbrs.append(j)
+    rows, nbrs = np.array(rows, int), np.array(nbrs, int)
+    d = D[rows, nbrs]
+    kd = k0 * d
+    E = np.stack([1 / kd, 1 / kd**2, 1 / kd**3, kd / 4, d / cutoff], axis=1) if len(d) else np.zeros((0, 5))
+    c = pos.mean(axis=0)
+    rc = np.linalg.norm(pos - c, axis=1)
+    R = rc.max() if rc.max() > 0 else 1.0
+    X = np.zeros((N, GNN_NF))
+    for i in range(N):
+        sel = rows == i
+        X[i] = [sel.sum() / 12, np.sum(1 / kd[sel]) / 8, np.sum(1 / kd[sel] ** 3) / 4, rc[i] / R, k0 * radii[i],
+                np.real(eps[i]) / 8]
+    return rows, nbrs, X, E
+
+
+def gnn_theta(lmax, weights, rows, nbrs, X, E):
+    """Raw network outputs per edge (nnz, 2 lmax^2): Theta = 1 + out[2q] + i out[2q+1]."""
+    lay, total = gnn_layout(lmax)
+    w = np.asarray(weights, float)
+    assert w.size == total
+    get = lambda name: w[lay[name][0]:lay[name][0] + int(np.prod(lay[name][1]))].reshape(lay[name][1])  # noqa: E731
+    h = np.tanh(X @ get("W1").T + get("b1"))
+    N = X.shape[0]
+    g = h.copy()
+    for i in range(N):
+        sel = np.where(rows == i)[0]
+        if len(sel):
+            z = np.concatenate([np.repeat(h[i:i + 1], len(sel), 0), h[nbrs[sel]], E[sel]], axis=1)
+            g[i] = h[i] + np.tanh(z @ get("W2").T + get("b2")).mean(axis=0)
+    z = np.concatenate([g[rows], g[nbrs], E], axis=1)
+    a = np.tanh(z @ get("W3").T + get("b3"))
+    return a @ get("W4").T + get("b4")
+
+
+def gnn_near_apply(lmax, k0, pos, tb, rows, nbrs, theta, R):
+    """M R = R + T sum_j (Theta_ij o C_ij) R_j over the near-field edges."""
+    M = 2 * lmax * (lmax + 2)
+    nlm = M // 2
+    deg = np.array([l for l in range(1, lmax + 1) for _ in range(2 * l + 1)])
+    Y = np.array(R, complex, copy=True)
+    CR = np.zeros_like(Y)
+    for e, (i, j) in enumerate(zip(rows, nbrs)):
+        blk = translation_block(lmax, k0, np.asarray(pos[i]) - np.asarray(pos[j]), singular=True, helicity=True)
+        th = 1.0 + theta[e, 0::2] + 1j * theta[e, 1::2]          # (lmax^2,), index (lam-1) L + (l-1)
+        scale = th[(deg[:, None] - 1) * lmax + (deg[None, :] - 1)]  # (nlm dest, nlm src)
+        S = np.repeat(np.repeat(scale, 2, axis=0), 2, axis=1)
+        CR[i * M:(i + 1) * M] += (blk * S) @ R[j * M:(j + 1) * M]
+    Y += apply_t(lmax, tb, CR)
+    return Y
+
+
+def gnn_loss(lmax, k0, radii, eps, pos, R, weights, reach_diameters=3.0, A=None, tb=None):
+    """sum_p ||r_p - A M_Theta r_p||^2 with the dense oracle operator A = I - T C."""
+    if A is None:
+        A, tb = cluster_operator(lmax, k0, radii, eps, pos)
+    rows, nbrs, X, E = gnn_graph(k0, np.asarray(radii), np.asarray(eps), pos, reach_diameters)
+    theta = gnn_theta(lmax, weights, rows, nbrs, X, E)
+    Y = gnn_near_apply(lmax, k0, np.asarray(pos), tb, rows, nbrs, theta, np.asarray(R).reshape(A.shape[0], -1))
+    Rr = np.asarray(R).reshape(A.shape[0], -1)
+    return float(np.sum(np.abs(Rr - A @ Y) ** 2))

@@ -1002,139 +1002,6 @@ int orc_array_solve(int lmax, double k0, double radius, double eps_re, double ep
     return 0;
 }
 
-// Learned-preconditioner statistics (no reference counterpart; restates the device
-// preconditioner of this repository with dense algebra): neighbours within `reach_diameters`
-// sphere diameters of the largest sphere, blocks of
-// at most 96 / M spheres (each free sphere in Morton order of the reach-sized cells takes its
-// nearest free neighbours), D = blockdiag((I - T C)_bb)^-1, N = near-field couplings T_i C_ij
-// between different blocks, u_k = A (D N)^k D v; gram[k][l] = sum_v u_k^H u_l, rhs[k] = u_k^H v.
-static uint64_t spread3_bits(uint64_t v) {
-    v &= 0x1fffff;
-    v = (v | v << 32) & 0x1f00000000ffffULL;
-    v = (v | v << 16) & 0x1f0000ff0000ffULL;
-    v = (v | v << 8) & 0x100f00f00f00f00fULL;
-    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
-    v = (v | v << 2) & 0x1249249249249249ULL;
-    return v;
-}
-int orc_learned_gram(int lmax, double k0, int N, const double* radii, const double* eps, const double* pos,
-                     double reach_diameters, int layers, int nvec, const double* V_, double* gram_, double* rhs_) {
-    Plan plan = plan_between(lmax, true);
-    const int M = plan.M;
-    const size_t n = (size_t)N * M;
-    std::vector<cd> A(n * n);
-    std::vector<double> tb((size_t)N * lmax * 8);
-    orc_cluster_operator(lmax, k0, N, radii, eps, pos, (double*)A.data(), tb.data());
-    const cd* T = (const cd*)tb.data();
-    double rmax = 0;
-    for (int i = 0; i < N; ++i) rmax = std::max(rmax, radii[i]);
-    const double reach = 2.0 * reach_diameters * rmax;
-    double lo[3] = {1e300, 1e300, 1e300};
-    for (int i = 0; i < N; ++i)
-        for (int a = 0; a < 3; ++a) lo[a] = std::min(lo[a], pos[3 * i + a]);
-    auto cell = [&](int i, int a) { return (long)std::floor((pos[3 * i + a] - lo[a]) / reach); };
-    auto dist = [&](int i, int j) {
-        return std::hypot(std::hypot(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1]), pos[3 * i + 2] - pos[3 * j + 2]);
-    };
-    std::vector<std::pair<uint64_t, int>> order(N);
-    for (int i = 0; i < N; ++i)
-        order[i] = {spread3_bits(cell(i, 0)) | spread3_bits(cell(i, 1)) << 1 | spread3_bits(cell(i, 2)) << 2, i};
-    std::sort(order.begin(), order.end());
-    std::vector<std::vector<int>> nb(N);
-    for (int i = 0; i < N; ++i)
-        for (int j = 0; j < N; ++j)
-            if (j != i && dist(i, j) <= reach) nb[i].push_back(j);
-    const int per_block = std::max(1, 96 / M);
-    std::vector<int> block_of(N, -1);
-    std::vector<std::vector<int>> blocks;
-    for (auto& o : order) {
-        int i = o.second;
-        if (block_of[i] >= 0) continue;
-        int b = (int)blocks.size();
-        blocks.push_back({i});
-        block_of[i] = b;
-        std::vector<std::pair<double, int>> cand;
-        for (int j : nb[i])
-            if (block_of[j] < 0) cand.push_back({dist(i, j), j});
-        std::sort(cand.begin(), cand.end());
-        for (size_t c = 0; c < cand.size() && (int)blocks[b].size() < per_block; ++c) {
-            block_of[cand[c].second] = b;
-            blocks[b].push_back(cand[c].second);
-        }
-    }
-    // block inverses from the assembled operator's entries
-    std::vector<LuFactor> fac(blocks.size());
-    for (size_t b = 0; b < blocks.size(); ++b) {
-        int nbm = (int)blocks[b].size() * M;
-        fac[b].n = nbm;
-        fac[b].a.assign((size_t)nbm * nbm, cd(0, 0));
-        for (size_t a = 0; a < blocks[b].size(); ++a)
-            for (size_t c = 0; c < blocks[b].size(); ++c)
-                for (int cc = 0; cc < M; ++cc)
-                    for (int rr = 0; rr < M; ++rr)
-                        fac[b].a[(size_t)(c * M + cc) * nbm + a * M + rr] =
-                            A[((size_t)blocks[b][c] * M + cc) * n + (size_t)blocks[b][a] * M + rr];
-        int st = lu_factor(fac[b]);
-        if (st) return st;
-    }
-    auto applyD = [&](const std::vector<cd>& x, std::vector<cd>& y) {
-        y.assign(n, cd(0, 0));
-        for (size_t b = 0; b < blocks.size(); ++b) {
-            int nbm = (int)blocks[b].size() * M;
-            std::vector<cd> t(nbm);
-            for (size_t a = 0; a < blocks[b].size(); ++a)
-                for (int rr = 0; rr < M; ++rr) t[a * M + rr] = x[(size_t)blocks[b][a] * M + rr];
-            lu_solve(fac[b], t.data(), 1);
-            for (size_t a = 0; a < blocks[b].size(); ++a)
-                for (int rr = 0; rr < M; ++rr) y[(size_t)blocks[b][a] * M + rr] = t[a * M + rr];
-        }
-    };
-    auto applyN = [&](const std::vector<cd>& x, std::vector<cd>& y) {  // near-field T_i C_ij, other blocks
-        y.assign(n, cd(0, 0));
-        for (int i = 0; i < N; ++i)
-            for (int j : nb[i]) {
-                if (block_of[i] == block_of[j]) continue;
-                for (int cc = 0; cc < M; ++cc)
-                    for (int rr = 0; rr < M; ++rr)
-                        y[(size_t)i * M + rr] -= A[((size_t)j * M + cc) * n + (size_t)i * M + rr] * x[(size_t)j * M + cc];
-            }
-    };
-    const int K1 = layers + 1;
-    cd* gram = (cd*)gram_;
-    cd* rhs = (cd*)rhs_;
-    for (int i = 0; i < K1 * K1; ++i) gram[i] = 0.0;
-    for (int i = 0; i < K1; ++i) rhs[i] = 0.0;
-    const cd* V = (const cd*)V_;
-    for (int v = 0; v < nvec; ++v) {
-        std::vector<cd> vin(V + (size_t)v * n, V + (size_t)(v + 1) * n), s, t;
-        std::vector<std::vector<cd>> U(K1, std::vector<cd>(n));
-        applyD(vin, s);
-        for (int k = 0; k < K1; ++k) {
-            if (k > 0) {
-                applyN(s, t);
-                applyD(t, s);
-            }
-            for (size_t r = 0; r < n; ++r) {
-                cd acc(0, 0);
-                for (size_t c = 0; c < n; ++c) acc += A[c * n + r] * s[c];
-                U[k][r] = acc;
-            }
-        }
-        for (int k = 0; k < K1; ++k) {
-            for (int l = 0; l < K1; ++l) {
-                cd acc(0, 0);
-                for (size_t r = 0; r < n; ++r) acc += std::conj(U[k][r]) * U[l][r];
-                gram[k * K1 + l] += acc;
-            }
-            cd acc(0, 0);
-            for (size_t r = 0; r < n; ++r) acc += std::conj(U[k][r]) * vin[r];
-            rhs[k] += acc;
-        }
-    }
-    return 0;
-}
-
-// General LU solve of a dense n x n column-major system (used to check the LU alone)
 int orc_lu_solve(int n, const double* A, double* B, int p) {
     LuFactor f;
     f.n = n;

@@ -154,19 +154,20 @@ def test_single_sphere_reduces_to_mie():
     assert np.allclose(X[:, 0], Tb, rtol=0, atol=1e-15)
 
 
-def test_learned_preconditioner_statistics_are_a_gram_matrix():
-    # the oracle's Gram matrix of the layer basis is Hermitian positive semidefinite, and the
-    # least-squares layer weights fit the probe vectors at least as well as block Jacobi alone
+def test_network_restatement_with_theta_one_is_the_near_field_neumann_term():
+    # all output weights zero: Theta = 1 and M r = r + T C_near r, with C_near the coupling
+    # blocks of the pairs within 3 sphere diameters (the dense oracle operator, masked)
     w = workloads.learned_cluster(seed=91, count=12)
+    A, tb = oracle.cluster_operator(w.lmax, w.k0, w.radii, w.eps, w.positions)
+    lay, total = oracle.gnn_layout(w.lmax)
     rng = np.random.default_rng(1)
-    V = rng.standard_normal((w.n, 2)) + 1j * rng.standard_normal((w.n, 2))
-    G, b = oracle.learned_gram(w.lmax, w.k0, w.radii, w.eps, w.positions, 3, V)
-    assert np.allclose(G, G.conj().T, rtol=0, atol=1e-12 * np.abs(G).max())
-    assert np.min(np.linalg.eigvalsh(G)) >= -1e-10 * np.abs(G).max()
-    vv = np.sum(np.abs(V) ** 2)
-    loss = lambda a: vv - 2 * np.real(np.vdot(a, b)) + np.real(np.vdot(a, G @ a))
-    a_opt = np.linalg.solve(G, b)
-    e0 = np.zeros(4, complex)
-    e0[0] = 1.0
-    assert loss(a_opt) <= loss(e0) + 1e-9 * vv
-    assert loss(a_opt) <= vv
+    W = rng.standard_normal(total) * 0.3
+    W[lay["W4"][0]:] = 0.0
+    R = rng.standard_normal((w.n, 2)) + 1j * rng.standard_normal((w.n, 2))
+    D = np.linalg.norm(w.positions[:, None] - w.positions[None], axis=2)
+    M = 2 * w.lmax * (w.lmax + 2)
+    near = np.kron((D <= 1.2) & (D > 0), np.ones((M, M), bool))
+    TC_near = np.where(near, np.eye(w.n) - A, 0.0)
+    expected = np.sum(np.abs(R - A @ (R + TC_near @ R)) ** 2)
+    got = oracle.gnn_loss(w.lmax, w.k0, w.radii, w.eps, w.positions, R, W, A=A, tb=tb)
+    assert got == pytest.approx(expected, rel=1e-12)

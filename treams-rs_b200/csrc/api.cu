@@ -96,14 +96,13 @@ struct tcu_context {
     cplx* d_csmall = nullptr;     // 64 complex
     int* d_status = nullptr;
     double* d_lfac = nullptr;     // sqrt((l-m)!/(l+m)!) table up to degree 16
-    // GMRES preconditioner settings (tcu_context_set_learned_preconditioner)
-    double precond_reach = -1.0;  // near-field reach in sphere diameters (< 0: the compiled-in fit's)
-    int learned_layers = -1;      // < 0: the compiled-in fit
+    // GMRES preconditioner settings (tcu_context_set_learned_weights)
+    double precond_reach = -1.0;  // near-field reach in sphere diameters (< 0: the compiled-in one)
+    std::vector<double> learned_weights;  // empty: the compiled-in weights
     long long fallbacks = 0;      // mixed solves finished by a second factor
     std::set<tcu_factor*> factors;  // live factors (destroyed with the context)
     double refine_target = 1e-13; // refinement stops at ||r|| <= refine_target ||T b||
     double fallback_above = 1e-12;  // mixed solves left above this finish in FP64
-    std::vector<std::complex<double>> learned_alpha;
 };
 
 struct tcu_factor {
@@ -495,6 +494,42 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
             certs[c].residual_norm = rn[c];
             certs[c].rhs_norm = bn[c];
         }
+    return TCU_OK;
+}
+
+// A factor applied once (no refinement): v <- A^-1 v with the row/column scales; the coarse
+// solve of the two-level preconditioners. Owns the factor.
+struct FactorCoarse : CoarseSolve {
+    tcu_factor* f = nullptr;
+    cplx* tmp = nullptr;
+    ~FactorCoarse() override {
+        if (tmp) f->ctx->pool.free(tmp);
+        if (f) tcu_factor_destroy(f);
+    }
+    tcu_status solve(double2* v, cudaStream_t st) override {
+        tcu_context* ctx = f->ctx;
+        const size_t n = f->n;
+        if (f->scaled) scale_rows(v, f->d_scale, n, 1, st);
+        if (f->precision == TCU_FP64)
+            lu_solve_fp64((const double2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, 1, st, &ctx->launches,
+                          &f->sweep_epoch, f->wk.status);
+        else
+            lu_solve_fp32((const float2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, 1, st, &ctx->launches,
+                          &f->sweep_epoch, f->wk.status);
+        if (f->scaled) scale_rows(v, f->d_scale + n, n, 1, st);
+        return TCU_OK;
+    }
+};
+
+// The dipole (lmax 1) system of a cluster, factored in complex64 from 2048 modes on, else in FP64.
+tcu_status make_coarse(tcu_context* ctx, double k0, size_t N, const double* radii, const double* eps,
+                       const double* pos, std::unique_ptr<CoarseSolve>* out) {
+    auto c = std::make_unique<FactorCoarse>();
+    const int prec = 6 * N >= 2048 ? TCU_MIXED : TCU_FP64;
+    tcu_status s = factor_impl(ctx, 1, k0, N, radii, eps, pos, nullptr, nullptr, nullptr, prec, &c->f);
+    if (s) return s;
+    if ((s = dev_alloc(ctx, &c->tmp, 2 * 6 * N, "coarse solve buffers"))) return s;
+    *out = std::move(c);
     return TCU_OK;
 }
 
@@ -980,7 +1015,7 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
         opt.rtol + opt.atol == 0.0 || opt.restart <= 0 || opt.max_iterations <= 0)
         return fail(TCU_INVALID_INPUT,
                     "GMRES needs finite nonnegative tolerances, a positive tolerance, restart and iteration limit");
-    if (preconditioner < 0 || preconditioner > 2) return fail(TCU_INVALID_INPUT, "unknown preconditioner");
+    if (preconditioner < 0 || preconditioner > 3) return fail(TCU_INVALID_INPUT, "unknown preconditioner");
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
     CK(cudaSetDevice(ctx->device), "device");
@@ -1016,12 +1051,20 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
     launch_apply_t(lmax, (int)N, T, b, p, tb, ctx->stream);
     ++ctx->launches;
     std::unique_ptr<Preconditioner> pre;
-    if (preconditioner != TCU_PRECOND_NONE) {
-        s = make_preconditioner(ctx->stream, preconditioner, *P, lmax, (int)N, k0, pos, positions, radii, T,
-                                ctx->precond_reach, ctx->learned_layers, ctx->learned_alpha, &pre, &ctx->launches);
+    if (preconditioner == TCU_PRECOND_BLOCK_JACOBI) {
+        s = make_block_jacobi(ctx->stream, *P, (int)N, k0, pos, positions, radii, T, &pre, &ctx->launches);
         if (s == TCU_OUT_OF_MEMORY) return fail(s, "preconditioner: out of device memory");
         if (s == TCU_SINGULAR) return fail(s, "preconditioner: a diagonal block is numerically singular");
         if (s) return fail(s, "preconditioner set-up failed");
+    } else if (preconditioner == TCU_PRECOND_LEARNED || preconditioner == TCU_PRECOND_TWO_LEVEL) {
+        std::unique_ptr<CoarseSolve> coarse;
+        if ((s = make_coarse(ctx, k0, N, radii, eps, positions, &coarse)))
+            return fail(s, std::string("coarse dipole system: ") + g_last_error);
+        s = make_two_level(ctx->stream, preconditioner == TCU_PRECOND_LEARNED, *P, lmax, (int)N, k0, pos, positions,
+                           radii, eps, T, ctx->precond_reach, ctx->learned_weights, std::move(coarse), &pre,
+                           &ctx->launches);
+        if (s == TCU_OUT_OF_MEMORY) return fail(s, "two-level preconditioner: out of device memory");
+        if (s) return fail(s, "two-level preconditioner set-up failed");
     }
     tcu_status worst = TCU_OK;
     std::string msg;
@@ -1293,11 +1336,42 @@ extern "C" tcu_status tcu_array_solve_batch(tcu_context* ctx, int lmax, double k
     return sync_status(ctx, "periodic array solve");
 }
 
-extern "C" tcu_status tcu_learned_precond_gram(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
-                                               const double* eps, const double* positions, int layers, int nvec,
-                                               const double* V, double* gram, double* rhs) {
-    if (!ctx || !V || !gram || !rhs || layers < 0 || layers > 32 || nvec <= 0)
-        return fail(TCU_INVALID_INPUT, "require 0 <= layers <= 32, nvec >= 1 and non-null buffers");
+extern "C" tcu_status tcu_context_set_learned_weights(tcu_context* ctx, double reach_diameters, size_t count,
+                                                      const double* weights) {
+    if (!ctx || !std::isfinite(reach_diameters) || reach_diameters > 20.0 || (count > 0 && !weights) ||
+        (count > 0 && !finite_all(weights, count)))
+        return fail(TCU_INVALID_INPUT, "require reach <= 20 diameters and finite weights");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ctx->precond_reach = reach_diameters > 0.0 ? reach_diameters : -1.0;
+    ctx->learned_weights.assign(weights, weights + count);
+    return TCU_OK;
+}
+
+extern "C" size_t tcu_learned_weight_count(int lmax) {
+    return lmax >= 1 && lmax <= 7 ? (size_t)learned_weight_count(lmax) : 0;
+}
+
+struct tcu_learned_problem {
+    tcu_context* ctx = nullptr;
+    int L = 0;
+    size_t N = 0, n = 0;
+    int nprobe = 0;
+    double* d_pos = nullptr;
+    cplx* d_T = nullptr;
+    cplx* d_V = nullptr;
+    LearnedProblem lp;
+    ~tcu_learned_problem() {
+        for (void* q : {(void*)d_pos, (void*)d_T, (void*)d_V})
+            if (q) ctx->pool.free(q);
+    }
+};
+
+extern "C" tcu_status tcu_learned_problem_create(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                                 const double* eps, const double* positions, int nprobe,
+                                                 const double* V, tcu_learned_problem** out) {
+    if (!ctx || !out || !V || nprobe <= 0 || nprobe > 64)
+        return fail(TCU_INVALID_INPUT, "require a context, an output handle and 1 <= nprobe <= 64 probe vectors");
+    *out = nullptr;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
     CK(cudaSetDevice(ctx->device), "device");
@@ -1306,45 +1380,70 @@ extern "C" tcu_status tcu_learned_precond_gram(tcu_context* ctx, int lmax, doubl
     const DevPlan* P;
     if ((s = get_plan(ctx, lmax, &P))) return s;
     const size_t n = N * 2 * (size_t)lmax * (lmax + 2);
-    if (!finite_all(V, 2 * n * (size_t)nvec)) return fail(TCU_INVALID_INPUT, "probe vectors must be finite");
-    Arena ar;
-    size_t oP = ar.add(N * 24), oR = ar.add(N * 8), oE = ar.add(N * 16), oT = ar.add(N * lmax * 64),
-           oV = ar.add(n * nvec * 16);
-    DevBuf buf(ctx);
-    CK(buf.alloc(ar.total), "Gram buffers");
-    double* pos = ar.at<double>(buf.p, oP);
-    double* r = ar.at<double>(buf.p, oR);
-    cplx* e = ar.at<cplx>(buf.p, oE);
-    cplx* T = ar.at<cplx>(buf.p, oT);
-    cplx* dV = ar.at<cplx>(buf.p, oV);
-    CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
-    CK(cudaMemcpyAsync(r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
-    CK(cudaMemcpyAsync(e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
-    CK(cudaMemcpyAsync(dV, V, n * nvec * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    if (!finite_all(V, 2 * n * (size_t)nprobe)) return fail(TCU_INVALID_INPUT, "probe vectors must be finite");
+    auto p = std::make_unique<tcu_learned_problem>();
+    p->ctx = ctx;
+    p->L = lmax;
+    p->N = N;
+    p->n = n;
+    p->nprobe = nprobe;
+    if ((s = dev_alloc(ctx, &p->d_pos, 3 * N, "positions")) || (s = dev_alloc(ctx, &p->d_T, N * lmax * 4, "T blocks")) ||
+        (s = dev_alloc(ctx, &p->d_V, n * nprobe, "probes")))
+        return s;
+    double* d_r = nullptr;
+    cplx* d_e = nullptr;
+    DevBuf tmp(ctx);
+    CK(tmp.alloc(N * 8 + N * 16), "geometry");
+    d_r = (double*)tmp.p;
+    d_e = (cplx*)(d_r + N);
+    CK(cudaMemcpyAsync(p->d_pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(d_r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(d_e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(p->d_V, V, n * nprobe * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
-    launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
+    launch_mie(lmax, k0, (int)N, d_r, d_e, p->d_T, ctx->d_status, ctx->stream);
     ++ctx->launches;
     if ((s = read_status(ctx, "Mie coefficients"))) return s;
-    s = learned_gram(ctx->stream, *P, lmax, (int)N, k0, pos, positions, radii, T, ctx->precond_reach, layers, nvec,
-                     dV, ctx->d_csmall,
-                     ctx->d_cpartial, (std::complex<double>*)gram, (std::complex<double>*)rhs, &ctx->launches);
-    if (s == TCU_OUT_OF_MEMORY) return fail(s, "learned preconditioner: out of device memory");
-    if (s == TCU_SINGULAR) return fail(s, "learned preconditioner: a diagonal block is numerically singular");
-    if (s) return fail(s, "learned preconditioner: device failure");
-    return sync_status(ctx, "learned preconditioner");
+    std::unique_ptr<CoarseSolve> coarse;
+    if ((s = make_coarse(ctx, k0, N, radii, eps, positions, &coarse)))
+        return fail(s, std::string("coarse dipole system: ") + g_last_error);
+    s = p->lp.build(ctx->stream, *P, lmax, (int)N, k0, p->d_pos, positions, radii, eps, p->d_T, ctx->precond_reach,
+                    nprobe, p->d_V, std::move(coarse), &ctx->launches);
+    if (s == TCU_OUT_OF_MEMORY) return fail(s, "training problem: out of device memory");
+    if (s) return fail(s, "training problem: device failure");
+    *out = p.release();
+    return TCU_OK;
 }
 
-extern "C" tcu_status tcu_context_set_learned_preconditioner(tcu_context* ctx, double reach_diameters, int layers,
-                                                             const double* alpha) {
-    if (!ctx || !std::isfinite(reach_diameters) || reach_diameters > 20.0 || layers > 32 ||
-        (layers >= 0 && alpha && !finite_all(alpha, 2 * (size_t)(layers + 1))))
-        return fail(TCU_INVALID_INPUT, "require reach <= 20 diameters, layers <= 32 and finite weights");
+extern "C" tcu_status tcu_learned_problem_loss_grad(tcu_learned_problem* p, const double* weights, double* loss,
+                                                    double* grad) {
+    if (!p || !weights || !loss || !grad) return fail(TCU_INVALID_INPUT, "null argument");
+    const size_t nw = (size_t)learned_weight_count(p->L);
+    if (!finite_all(weights, nw)) return fail(TCU_INVALID_INPUT, "weights must be finite");
+    std::lock_guard<std::recursive_mutex> lock(p->ctx->mu);
+    ProfGuard pg(p->ctx);
+    CK(cudaSetDevice(p->ctx->device), "device");
+    tcu_status s = p->lp.loss_grad(weights, loss, grad, p->ctx->stream);
+    if (s) return fail(s, "training problem: device failure");
+    return TCU_OK;
+}
+
+extern "C" tcu_status tcu_learned_problem_probes(tcu_learned_problem* p, double* out) {
+    if (!p || !out) return fail(TCU_INVALID_INPUT, "null argument");
+    std::lock_guard<std::recursive_mutex> lock(p->ctx->mu);
+    CK(cudaSetDevice(p->ctx->device), "device");
+    tcu_status s = p->lp.probes((double2*)out, p->ctx->stream);
+    if (s) return fail(s, "training problem: device failure");
+    return TCU_OK;
+}
+
+extern "C" tcu_status tcu_learned_problem_destroy(tcu_learned_problem* p) {
+    if (!p) return TCU_OK;
+    tcu_context* ctx = p->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
-    ctx->precond_reach = reach_diameters > 0.0 ? reach_diameters : -1.0;
-    ctx->learned_layers = layers;
-    ctx->learned_alpha.clear();
-    if (layers >= 0 && alpha)
-        for (int k = 0; k <= layers; ++k) ctx->learned_alpha.emplace_back(alpha[2 * k], alpha[2 * k + 1]);
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete p;
     return TCU_OK;
 }
 

@@ -1,0 +1,788 @@
+// Learned two-level preconditioner of the matrix-free GMRES on A = I - T C (new here: the
+// reference's iterative solver, cluster/iterative.rs:264-284 with linalg/gmres.rs:119, runs
+// unpreconditioned).
+//
+// Right preconditioner, applied to a vector v:
+//   1. coarse correction on the dipole modes (l = 1, the first 6 modes of every sphere):
+//      z_c = A_cc^-1 v_c with A_cc = I - T_1 C_11 factored once by the dense LU of this library,
+//      and the exact residual r1 = v - A[:, c] z_c through the stored dipole columns of A
+//      (complex64, n x 6N);
+//   2. near field: y = r1 + T sum_{j in nb(i)} (Theta_ij o C_ij) r1_j over the pairs closer
+//      than the reach, where Theta_ij scales every (destination degree, source degree)
+//      sub-block of the translation block C_ij by a complex number;
+//   3. out = z_c (scattered onto the dipole modes) + y.
+// With Theta = 1 this is the untrained two-level method (coarse dipole solve + first-order
+// near-field Neumann term). The learned method predicts Theta per edge with a small graph
+// network over the neighbour graph:
+//   h_i = tanh(W1 x_i + b1)                          node embedding (x_i: 6 node features)
+//   g_i = h_i + mean_j tanh(W2 [h_i, h_j, e_ij] + b2) one round of message passing
+//   Theta_ij = 1 + (W4 tanh(W3 [g_i, g_j, e_ij] + b3) + b4)   (2 L^2 outputs: re, im)
+// (e_ij: 5 edge features). Training minimises sum_p ||r1_p - A M_Theta r1_p||^2 over
+// coarse-corrected probe vectors r1_p of generated clusters; the loss and its gradient in
+// every weight come from the forward and backward kernels below (the Theta gradient needs
+// A^H, applied matrix-free through C^T = F C F with the order flip F x(l,m) = (-1)^m x(l,-m)).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "kernels.h"
+#include "nearfield.cuh"
+#include "pairtable.cuh"
+#include "precond.h"
+
+namespace tcu {
+
+// Trained weights of the network per lmax (generated by treams_b200/train_precond.py).
+#include "learned_weights.inc"
+
+namespace {
+
+using namespace nearfield;
+
+// ---- network shape -----------------------------------------------------------------------
+constexpr int GH = 16;            // hidden width
+constexpr int GNF = 6;            // node features
+constexpr int GEF = 5;            // edge features
+constexpr int GIN = 2 * GH + GEF; // input of the message and edge layers
+constexpr int GNO_MAX = 2 * 7 * 7;
+
+struct Layout {
+    int no, w1, b1, w2, b2, w3, b3, w4, b4, total;
+};
+__host__ __device__ inline Layout layout(int L) {
+    Layout o;
+    o.no = 2 * L * L;
+    o.w1 = 0;
+    o.b1 = o.w1 + GH * GNF;
+    o.w2 = o.b1 + GH;
+    o.b2 = o.w2 + GH * GIN;
+    o.w3 = o.b2 + GH;
+    o.b3 = o.w3 + GH * GIN;
+    o.w4 = o.b3 + GH;
+    o.b4 = o.w4 + o.no * GH;
+    o.total = o.b4 + o.no;
+    return o;
+}
+
+__device__ __forceinline__ int lm_degree(int lm) {  // lm = l*l - 1 + l + m
+    int l = (int)sqrt((double)(lm + 1));
+    while (l * l > lm + 1) --l;
+    while ((l + 1) * (l + 1) <= lm + 1) ++l;
+    return l;
+}
+
+// ---- forward ------------------------------------------------------------------------------
+__global__ void gnn_embed_kernel(int N, const double* __restrict__ X, const double* __restrict__ W, int L,
+                                 double* __restrict__ H) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const Layout o = layout(L);
+    for (int k = 0; k < GH; ++k) {
+        double a = W[o.b1 + k];
+        for (int c = 0; c < GNF; ++c) a = fma(W[o.w1 + k * GNF + c], X[i * GNF + c], a);
+        H[i * GH + k] = tanh(a);
+    }
+}
+
+__device__ __forceinline__ void layer_in(const double* hi, const double* hj, const double* e, double* z) {
+    for (int c = 0; c < GH; ++c) z[c] = hi[c];
+    for (int c = 0; c < GH; ++c) z[GH + c] = hj[c];
+    for (int c = 0; c < GEF; ++c) z[2 * GH + c] = e[c];
+}
+
+// g_i = h_i + mean over the neighbours of tanh(W2 [h_i, h_j, e_ij] + b2); U keeps every message
+__global__ void gnn_message_kernel(int N, const int* __restrict__ ptr, const int* __restrict__ nbr,
+                                   const double* __restrict__ E, const double* __restrict__ W, int L,
+                                   const double* __restrict__ H, double* __restrict__ U, double* __restrict__ G) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const Layout o = layout(L);
+    double acc[GH], z[GIN];
+    for (int k = 0; k < GH; ++k) acc[k] = 0.0;
+    const int e0 = ptr[i], e1 = ptr[i + 1];
+    for (int e = e0; e < e1; ++e) {
+        layer_in(H + i * GH, H + nbr[e] * GH, E + (size_t)e * GEF, z);
+        for (int k = 0; k < GH; ++k) {
+            double a = W[o.b2 + k];
+            for (int c = 0; c < GIN; ++c) a = fma(W[o.w2 + k * GIN + c], z[c], a);
+            const double u = tanh(a);
+            U[(size_t)e * GH + k] = u;
+            acc[k] += u;
+        }
+    }
+    const double inv = e1 > e0 ? 1.0 / double(e1 - e0) : 0.0;
+    for (int k = 0; k < GH; ++k) G[i * GH + k] = H[i * GH + k] + acc[k] * inv;
+}
+
+// per edge: a = tanh(W3 [g_i, g_j, e] + b3), raw outputs W4 a + b4 (Theta = 1 + re + i im)
+__global__ void gnn_edge_kernel(int nnz, const int* __restrict__ row, const int* __restrict__ nbr,
+                                const double* __restrict__ E, const double* __restrict__ W, int L,
+                                const double* __restrict__ G, double* __restrict__ Aact, double* __restrict__ TH) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const Layout o = layout(L);
+    double z[GIN], a[GH];
+    layer_in(G + row[e] * GH, G + nbr[e] * GH, E + (size_t)e * GEF, z);
+    for (int k = 0; k < GH; ++k) {
+        double s = W[o.b3 + k];
+        for (int c = 0; c < GIN; ++c) s = fma(W[o.w3 + k * GIN + c], z[c], s);
+        a[k] = tanh(s);
+        Aact[(size_t)e * GH + k] = a[k];
+    }
+    for (int q = 0; q < o.no; ++q) {
+        double s = W[o.b4 + q];
+        for (int k = 0; k < GH; ++k) s = fma(W[o.w4 + q * GH + k], a[k], s);
+        TH[(size_t)e * o.no + q] = s;
+    }
+}
+
+// B_e[s][d][h] = Theta_e[lambda(d)][l(s)] C_e[s][d][h] (TH null: Theta = 1, a copy)
+__global__ void scale_blocks_kernel(int nnz, int L, int nlm, const double* __restrict__ TH, const cplx* __restrict__ C,
+                                    cplx* __restrict__ B) {
+    const size_t per = (size_t)nlm * nlm * 2;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)nnz * per) return;
+    const size_t e = t / per, r = t - e * per;
+    const int sd = (int)(r >> 1), s = sd / nlm, d = sd - s * nlm;
+    cplx v = C[t];
+    if (TH) {
+        const int q = 2 * ((lm_degree(d) - 1) * L + (lm_degree(s) - 1));
+        const cplx th = mk(1.0 + TH[e * (size_t)(2 * L * L) + q], TH[e * (size_t)(2 * L * L) + q + 1]);
+        v = cmul(th, v);
+    }
+    B[t] = v;
+}
+
+// ---- loss gradient in Theta ---------------------------------------------------------------
+// dTH[e] from S_e[lambda][l] = sum_p sum_{d in lambda, s in l, h} conj(w_p[i,(d,h)]) C_e^h[s][d]
+// r_p[j,(s,h)] with w = T^H A^H (r - A M r): d loss = -2 Re sum dTheta S, so the derivative in
+// the real part of Theta is -2 Re S and in the imaginary part 2 Im S. One CTA per edge; the
+// (s, d) contributions are binned by (lambda, l) in a fixed order.
+__global__ void __launch_bounds__(256) theta_grad_kernel(int nnz, const int* __restrict__ row,
+                                                         const int* __restrict__ nbr, int L, int nlm,
+                                                         const cplx* __restrict__ C, const cplx* __restrict__ Wt,
+                                                         const cplx* __restrict__ R, size_t n, int p,
+                                                         double* __restrict__ dTH) {
+    extern __shared__ cplx tg_smem[];  // nlm * nlm
+    const int e = blockIdx.x;
+    const int i = row[e], j = nbr[e], M = 2 * nlm;
+    const cplx* Ce = C + (size_t)e * nlm * nlm * 2;
+    for (int sd = threadIdx.x; sd < nlm * nlm; sd += blockDim.x) {
+        const int s = sd / nlm, d = sd - s * nlm;
+        const cplx cp = Ce[2 * sd], cn = Ce[2 * sd + 1];
+        cplx acc = mk(0.0, 0.0);
+        for (int q = 0; q < p; ++q) {
+            const cplx* w = Wt + q * n + (size_t)i * M;
+            const cplx* r = R + q * n + (size_t)j * M;
+            cfma_conj(acc, w[2 * d], cmul(cp, r[2 * s]));
+            cfma_conj(acc, w[2 * d + 1], cmul(cn, r[2 * s + 1]));
+        }
+        tg_smem[sd] = acc;
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < L * L; b += blockDim.x) {
+        const int lam = b / L + 1, l = b % L + 1;
+        cplx S = mk(0.0, 0.0);
+        for (int s = l * l - 1; s < (l + 1) * (l + 1) - 1; ++s)
+            for (int d = lam * lam - 1; d < (lam + 1) * (lam + 1) - 1; ++d) S = cadd(S, tg_smem[s * nlm + d]);
+        dTH[(size_t)e * 2 * L * L + 2 * b] = -2.0 * S.x;
+        dTH[(size_t)e * 2 * L * L + 2 * b + 1] = 2.0 * S.y;
+    }
+}
+
+// ---- backward -----------------------------------------------------------------------------
+__global__ void gnn_edge_back_kernel(int nnz, const double* __restrict__ W, int L, const double* __restrict__ Aact,
+                                     const double* __restrict__ dTH, double* __restrict__ dP3, double* __restrict__ CGI,
+                                     double* __restrict__ CGJ) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nnz) return;
+    const Layout o = layout(L);
+    double dp[GH];
+    for (int k = 0; k < GH; ++k) {
+        double da = 0.0;
+        for (int q = 0; q < o.no; ++q) da = fma(W[o.w4 + q * GH + k], dTH[(size_t)e * o.no + q], da);
+        const double a = Aact[(size_t)e * GH + k];
+        dp[k] = da * (1.0 - a * a);
+        dP3[(size_t)e * GH + k] = dp[k];
+    }
+    for (int c = 0; c < GH; ++c) {
+        double gi = 0.0, gj = 0.0;
+        for (int k = 0; k < GH; ++k) {
+            gi = fma(W[o.w3 + k * GIN + c], dp[k], gi);
+            gj = fma(W[o.w3 + k * GIN + GH + c], dp[k], gj);
+        }
+        CGI[(size_t)e * GH + c] = gi;
+        CGJ[(size_t)e * GH + c] = gj;
+    }
+}
+
+// dg_i = sum over the edges of row i of their i-side part and the j-side part of the reverse edge
+__global__ void gnn_gather_kernel(int N, const int* __restrict__ ptr, const int* __restrict__ rev,
+                                  const double* __restrict__ CI, const double* __restrict__ CJ,
+                                  const double* __restrict__ base, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    for (int c = 0; c < GH; ++c) {
+        double s = base ? base[i * GH + c] : 0.0;
+        for (int e = ptr[i]; e < ptr[i + 1]; ++e) {
+            if (CI) s += CI[(size_t)e * GH + c];
+            s += CJ[(size_t)rev[e] * GH + c];
+        }
+        out[i * GH + c] = s;
+    }
+}
+
+// message layer: dP2[e] = (dg_i / deg_i) (1 - u_e^2); DHI_i = dg_i + sum_e W2_hi^T dP2[e];
+// CHJ[e] = W2_hj^T dP2[e] (the part that flows to the neighbour)
+__global__ void gnn_message_back_kernel(int N, const int* __restrict__ ptr, const double* __restrict__ W, int L,
+                                        const double* __restrict__ U, const double* __restrict__ DG,
+                                        double* __restrict__ dP2, double* __restrict__ DHI, double* __restrict__ CHJ) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const Layout o = layout(L);
+    const int e0 = ptr[i], e1 = ptr[i + 1];
+    const double inv = e1 > e0 ? 1.0 / double(e1 - e0) : 0.0;
+    double dhi[GH];
+    for (int c = 0; c < GH; ++c) dhi[c] = DG[i * GH + c];
+    for (int e = e0; e < e1; ++e) {
+        double dp[GH];
+        for (int k = 0; k < GH; ++k) {
+            const double u = U[(size_t)e * GH + k];
+            dp[k] = DG[i * GH + k] * inv * (1.0 - u * u);
+            dP2[(size_t)e * GH + k] = dp[k];
+        }
+        for (int c = 0; c < GH; ++c) {
+            double a = 0.0, b = 0.0;
+            for (int k = 0; k < GH; ++k) {
+                a = fma(W[o.w2 + k * GIN + c], dp[k], a);
+                b = fma(W[o.w2 + k * GIN + GH + c], dp[k], b);
+            }
+            dhi[c] += a;
+            CHJ[(size_t)e * GH + c] = b;
+        }
+    }
+    for (int c = 0; c < GH; ++c) DHI[i * GH + c] = dhi[c];
+}
+
+__global__ void gnn_embed_back_kernel(int N, const double* __restrict__ H, const double* __restrict__ DH,
+                                      double* __restrict__ dP1) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * GH) return;
+    const double h = H[t];
+    dP1[t] = DH[t] * (1.0 - h * h);
+}
+
+// Weight gradients as fixed-order sums over nodes and edges: one thread per parameter.
+__global__ void gnn_weight_grad_kernel(int N, int nnz, int L, const int* __restrict__ row, const int* __restrict__ nbr,
+                                       const double* __restrict__ X, const double* __restrict__ E,
+                                       const double* __restrict__ H, const double* __restrict__ G,
+                                       const double* __restrict__ Aact, const double* __restrict__ dP1,
+                                       const double* __restrict__ dP2, const double* __restrict__ dP3,
+                                       const double* __restrict__ dTH, double* __restrict__ grad) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const Layout o = layout(L);
+    if (t >= o.total) return;
+    double s = 0.0;
+    auto zin = [&](const double* V, int e, int c) -> double {  // [v_row, v_nbr, e] component c
+        if (c < GH) return V[row[e] * GH + c];
+        if (c < 2 * GH) return V[nbr[e] * GH + c - GH];
+        return E[(size_t)e * GEF + c - 2 * GH];
+    };
+    if (t < o.b1) {
+        const int k = t / GNF, c = t % GNF;
+        for (int i = 0; i < N; ++i) s = fma(dP1[i * GH + k], X[i * GNF + c], s);
+    } else if (t < o.w2) {
+        const int k = t - o.b1;
+        for (int i = 0; i < N; ++i) s += dP1[i * GH + k];
+    } else if (t < o.b2) {
+        const int k = (t - o.w2) / GIN, c = (t - o.w2) % GIN;
+        for (int e = 0; e < nnz; ++e) s = fma(dP2[(size_t)e * GH + k], zin(H, e, c), s);
+    } else if (t < o.w3) {
+        const int k = t - o.b2;
+        for (int e = 0; e < nnz; ++e) s += dP2[(size_t)e * GH + k];
+    } else if (t < o.b3) {
+        const int k = (t - o.w3) / GIN, c = (t - o.w3) % GIN;
+        for (int e = 0; e < nnz; ++e) s = fma(dP3[(size_t)e * GH + k], zin(G, e, c), s);
+    } else if (t < o.w4) {
+        const int k = t - o.b3;
+        for (int e = 0; e < nnz; ++e) s += dP3[(size_t)e * GH + k];
+    } else if (t < o.b4) {
+        const int q = (t - o.w4) / GH, k = (t - o.w4) % GH;
+        for (int e = 0; e < nnz; ++e) s = fma(dTH[(size_t)e * o.no + q], Aact[(size_t)e * GH + k], s);
+    } else {
+        const int q = t - o.b4;
+        for (int e = 0; e < nnz; ++e) s += dTH[(size_t)e * o.no + q];
+    }
+    grad[t] = s;
+}
+
+// ---- adjoint operator and coarse-space helpers --------------------------------------------
+// y = T^H x per sphere and degree (2 x 2 blocks in mode order, row-major)
+__global__ void th_apply_kernel(int N, int L, const cplx* __restrict__ T, const cplx* __restrict__ x, size_t n,
+                                int ncol, cplx* __restrict__ y) {
+    const int nlm = L * (L + 2);
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)N * nlm * ncol) return;
+    const int c = (int)(t / ((size_t)N * nlm));
+    const size_t r = t - (size_t)c * N * nlm;
+    const int i = (int)(r / nlm), lm = (int)(r % nlm);
+    const cplx* t4 = T + ((size_t)i * L + lm_degree(lm) - 1) * 4;
+    const size_t o = c * n + (size_t)i * 2 * nlm + 2 * lm;
+    const cplx a = x[o], b = x[o + 1];
+    cplx y0 = mk(0.0, 0.0), y1 = mk(0.0, 0.0);
+    cfma_conj(y0, t4[0], a);
+    cfma_conj(y0, t4[2], b);
+    cfma_conj(y1, t4[1], a);
+    cfma_conj(y1, t4[3], b);
+    y[o] = y0;
+    y[o + 1] = y1;
+}
+
+// y = base - conj(F x) (base null: y = conj(F x)); (F x)(l, m, pol) = (-1)^m x(l, -m, pol)
+__global__ void flip_conj_kernel(int N, int L, const cplx* __restrict__ x, const cplx* __restrict__ base, size_t n,
+                                 int ncol, cplx* __restrict__ y) {
+    const int M = 2 * L * (L + 2);
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)N * M * ncol) return;
+    const int c = (int)(t / ((size_t)N * M));
+    const size_t r = t - (size_t)c * N * M;
+    const int i = (int)(r / M), q = (int)(r % M);
+    const int lm = q >> 1, slot = q & 1, l = lm_degree(lm), m = lm + 1 - l * l - l;
+    const int src = 2 * (l * l - 1 + l - m) + slot;
+    cplx v = cconj(x[c * n + (size_t)i * M + src]);
+    if (m & 1) v = cneg(v);
+    const size_t o = c * n + r;
+    y[o] = base ? csub(base[o], v) : v;
+}
+
+__global__ void coarse_gather_kernel(int N, int M, const cplx* __restrict__ v, cplx* __restrict__ vc) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * 6) return;
+    vc[t] = v[(size_t)(t / 6) * M + t % 6];
+}
+__global__ void coarse_scatter_add_kernel(int N, int M, const cplx* __restrict__ vc, cplx* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= N * 6) return;
+    const size_t o = (size_t)(t / 6) * M + t % 6;
+    out[o] = cadd(out[o], vc[t]);
+}
+constexpr int CG_CHUNK = 512;  // columns per partial sum of the coarse-column product
+__global__ void __launch_bounds__(256) coarse_gemv_partial_kernel(size_t n, int nc, const float2* __restrict__ A,
+                                                                  const cplx* __restrict__ vc, cplx* __restrict__ part) {
+    __shared__ cplx xs[CG_CHUNK];
+    const int c0 = blockIdx.y * CG_CHUNK, cnt = min(CG_CHUNK, nc - c0);
+    for (int c = threadIdx.x; c < cnt; c += blockDim.x) xs[c] = vc[c0 + c];
+    __syncthreads();
+    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    cplx acc = mk(0.0, 0.0);
+    const float2* a = A + (size_t)c0 * n + r;
+#pragma unroll 8
+    for (int c = 0; c < cnt; ++c) {
+        const float2 v = __ldcs(a + (size_t)c * n);
+        cfma(acc, mk(v.x, v.y), xs[c]);
+    }
+    part[(size_t)blockIdx.y * n + r] = acc;
+}
+__global__ void coarse_gemv_final_kernel(size_t n, int nchunk, const cplx* __restrict__ part, const cplx* __restrict__ v,
+                                         cplx* __restrict__ r1) {
+    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    cplx s = mk(0.0, 0.0);
+    for (int k = 0; k < nchunk; ++k) s = cadd(s, part[(size_t)k * n + r]);
+    r1[r] = csub(v[r], s);
+}
+
+unsigned blocks_for(size_t count, int threads) { return (unsigned)((count + threads - 1) / threads); }
+
+// ---- shared set-up -------------------------------------------------------------------------
+// Node and edge features of the network (the tests restate them).
+//   node i: [deg/12, sum_j 1/(k d_ij)/8, sum_j 1/(k d_ij)^3/4, |r_i - c|/R, k r_i, Re eps_i/8]
+//           (c: centroid, R: largest distance to it, sums over the neighbours)
+//   edge:   [1/(k d), 1/(k d)^2, 1/(k d)^3, k d/4, d/cutoff]
+void features(int N, const double* pos, const double* radii, const double* eps, double k, double cutoff,
+              const Graph& g, std::vector<double>& X, std::vector<double>& E) {
+    double c[3] = {0, 0, 0};
+    for (int i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a) c[a] += pos[3 * i + a] / N;
+    double R = 0.0;
+    for (int i = 0; i < N; ++i)
+        R = std::max(R, std::hypot(std::hypot(pos[3 * i] - c[0], pos[3 * i + 1] - c[1]), pos[3 * i + 2] - c[2]));
+    if (!(R > 0.0)) R = 1.0;
+    X.assign((size_t)N * GNF, 0.0);
+    E.assign(g.nbr.size() * GEF, 0.0);
+    for (int i = 0; i < N; ++i) {
+        double s1 = 0.0, s3 = 0.0;
+        for (int e = g.ptr[i]; e < g.ptr[i + 1]; ++e) {
+            const int j = g.nbr[e];
+            const double d = std::hypot(std::hypot(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1]),
+                                        pos[3 * i + 2] - pos[3 * j + 2]);
+            const double kd = k * d;
+            s1 += 1.0 / kd;
+            s3 += 1.0 / (kd * kd * kd);
+            double* f = E.data() + (size_t)e * GEF;
+            f[0] = 1.0 / kd;
+            f[1] = 1.0 / (kd * kd);
+            f[2] = 1.0 / (kd * kd * kd);
+            f[3] = kd / 4.0;
+            f[4] = d / cutoff;
+        }
+        double* x = X.data() + (size_t)i * GNF;
+        x[0] = (g.ptr[i + 1] - g.ptr[i]) / 12.0;
+        x[1] = s1 / 8.0;
+        x[2] = s3 / 4.0;
+        x[3] = std::hypot(std::hypot(pos[3 * i] - c[0], pos[3 * i + 1] - c[1]), pos[3 * i + 2] - c[2]) / R;
+        x[4] = k * radii[i];
+        x[5] = eps[2 * i] / 8.0;
+    }
+}
+
+// reverse edge of every edge (the neighbour lists are symmetric and sorted)
+std::vector<int> reverse_edges(const Graph& g) {
+    std::vector<int> rev(g.nbr.size(), -1);
+    for (size_t e = 0; e < g.nbr.size(); ++e) {
+        const int i = g.row_of[e], j = g.nbr[e];
+        auto b = g.nbr.begin() + g.ptr[j], en = g.nbr.begin() + g.ptr[j + 1];
+        auto it = std::lower_bound(b, en, i);
+        rev[e] = (it != en && *it == i) ? (int)(it - g.nbr.begin()) : (int)e;
+    }
+    return rev;
+}
+
+struct DevArray {
+    void* p = nullptr;
+    ~DevArray() {
+        if (p) cudaFree(p);
+    }
+    template <typename T>
+    T* as() const {
+        return (T*)p;
+    }
+    bool alloc(size_t bytes) { return cudaMalloc(&p, std::max<size_t>(bytes, 16)) == cudaSuccess; }
+};
+
+// Everything the network and the near field need on the device for one cluster.
+struct GraphData {
+    int N = 0, L = 0, nlm = 0, M = 0;
+    size_t n = 0, nnz = 0;
+    DevArray ptr, nbr, row, rev, X, E, C, B, H, G, U, A, TH;
+    bool build(cudaStream_t st, const DevPlan& P, int L_, int N_, double k0, const double* d_pos, const double* h_pos,
+               const double* h_radii, const double* h_eps, double cutoff, long long* launches) {
+        L = L_;
+        N = N_;
+        nlm = P.nlm;
+        M = 2 * nlm;
+        n = (size_t)N * M;
+        Graph g = build_graph(N, h_pos, cutoff, 1);
+        nnz = g.nbr.size();
+        std::vector<int> rv = reverse_edges(g);
+        std::vector<double> X_, E_;
+        features(N, h_pos, h_radii, h_eps, k0, cutoff, g, X_, E_);
+        auto up = [&](DevArray& a, const void* h, size_t bytes) {
+            return a.alloc(bytes) && (bytes == 0 || cudaMemcpyAsync(a.p, h, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess);
+        };
+        const size_t nb = nnz * (size_t)nlm * nlm * 2 * sizeof(cplx);
+        if (!up(ptr, g.ptr.data(), g.ptr.size() * 4) || !up(nbr, g.nbr.data(), nnz * 4) ||
+            !up(row, g.row_of.data(), nnz * 4) || !up(rev, rv.data(), nnz * 4) ||
+            !up(X, X_.data(), X_.size() * 8) || !up(E, E_.data(), E_.size() * 8) || !C.alloc(nb) || !B.alloc(nb) ||
+            !H.alloc((size_t)N * GH * 8) || !G.alloc((size_t)N * GH * 8) || !U.alloc(nnz * GH * 8) ||
+            !A.alloc(nnz * GH * 8) || !TH.alloc(nnz * GNO_MAX * 8))
+            return false;
+        if (nnz > 0) {
+            int Q = std::min(16, 256 / nlm);
+            nf_block_kernel<<<blocks_for(nnz, Q), 256, (size_t)Q * P.tsize * sizeof(cplx), st>>>(
+                P, k0, d_pos, row.as<int>(), nbr.as<int>(), (int)nnz, Q, C.as<cplx>());
+            if (launches) ++*launches;
+        }
+        return true;
+    }
+    // Theta from the weights (null: Theta = 1) and the scaled blocks B
+    void forward(const double* d_w, cudaStream_t st, long long* launches) {
+        if (nnz == 0) return;
+        if (d_w) {
+            gnn_embed_kernel<<<blocks_for(N, 128), 128, 0, st>>>(N, X.as<double>(), d_w, L, H.as<double>());
+            gnn_message_kernel<<<blocks_for(N, 128), 128, 0, st>>>(N, ptr.as<int>(), nbr.as<int>(), E.as<double>(), d_w,
+                                                                  L, H.as<double>(), U.as<double>(), G.as<double>());
+            gnn_edge_kernel<<<blocks_for(nnz, 128), 128, 0, st>>>((int)nnz, row.as<int>(), nbr.as<int>(),
+                                                                 E.as<double>(), d_w, L, G.as<double>(),
+                                                                 A.as<double>(), TH.as<double>());
+            if (launches) *launches += 3;
+        }
+        const size_t tot = nnz * (size_t)nlm * nlm * 2;
+        scale_blocks_kernel<<<blocks_for(tot, 256), 256, 0, st>>>((int)nnz, L, nlm, d_w ? TH.as<double>() : nullptr,
+                                                                  C.as<cplx>(), B.as<cplx>());
+        if (launches) ++*launches;
+    }
+    // out = zadd + T sum_e B_e x (one column)
+    void near_apply(const cplx* T, const cplx* x, const cplx* zadd, cplx* out, cudaStream_t st, long long* launches,
+                    const uint8_t* noskip) {
+        const int Q = std::min(16, 256 / nlm);
+        nf_apply_kernel<<<N, 256, (size_t)Q * nlm * 2 * sizeof(cplx), st>>>(L, nlm, ptr.as<int>(), nbr.as<int>(),
+                                                                           noskip, B.as<cplx>(), T, x, zadd, out, Q);
+        if (launches) ++*launches;
+    }
+};
+
+// The coarse dipole system: A[:, c] (complex64, n x 6N) and the LU of A_cc.
+struct Coarse {
+    int N = 0, M = 0, nc = 0, nchunk = 0;
+    size_t n = 0;
+    DevArray Acols, vc, part;
+    std::unique_ptr<CoarseSolve> solver;
+    bool build(cudaStream_t st, const DevPlan& P, int N_, double k0, const double* d_pos, const cplx* d_T,
+               std::unique_ptr<CoarseSolve> s, long long* launches) {
+        N = N_;
+        M = 2 * P.nlm;
+        n = (size_t)N * M;
+        nc = 6 * N;
+        nchunk = (nc + CG_CHUNK - 1) / CG_CHUNK;
+        solver = std::move(s);
+        if (!Acols.alloc(n * (size_t)nc * sizeof(float2)) || !vc.alloc((size_t)nc * sizeof(cplx)) ||
+            !part.alloc(n * (size_t)nchunk * sizeof(cplx)))
+            return false;
+        launch_assemble_sources(P, N, k0, d_pos, d_T, Acols.as<float2>(), n, 3, st);
+        if (launches) ++*launches;
+        return true;
+    }
+    // z_c = A_cc^-1 v_c (into vc) and r1 = v - A[:, c] z_c
+    tcu_status correct(const cplx* v, cplx* r1, cudaStream_t st, long long* launches) {
+        coarse_gather_kernel<<<blocks_for(nc, 256), 256, 0, st>>>(N, M, v, vc.as<cplx>());
+        tcu_status s = solver->solve(vc.as<cplx>(), st);
+        if (s) return s;
+        dim3 grid(blocks_for(n, 256), nchunk);
+        coarse_gemv_partial_kernel<<<grid, 256, 0, st>>>(n, nc, Acols.as<float2>(), vc.as<cplx>(), part.as<cplx>());
+        coarse_gemv_final_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, nchunk, part.as<cplx>(), v, r1);
+        if (launches) *launches += 3;
+        return TCU_OK;
+    }
+    void add_coarse(cplx* out, cudaStream_t st, long long* launches) {
+        coarse_scatter_add_kernel<<<blocks_for(nc, 256), 256, 0, st>>>(N, M, vc.as<cplx>(), out);
+        if (launches) ++*launches;
+    }
+};
+
+class TwoLevelPre : public Preconditioner {
+   public:
+    GraphData graph;
+    Coarse coarse;
+    DevArray r1, weights, noskip;
+    const cplx* T = nullptr;
+    long long* launches = nullptr;
+    tcu_status status = TCU_OK;
+    void apply(const cplx* in, cplx* out, cudaStream_t st) override {
+        tcu_status s = coarse.correct(in, r1.as<cplx>(), st, launches);
+        if (s) {
+            status = s;
+            cudaMemcpyAsync(out, in, graph.n * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+            return;
+        }
+        graph.near_apply(T, r1.as<cplx>(), r1.as<cplx>(), out, st, launches, noskip.as<uint8_t>());
+        coarse.add_coarse(out, st, launches);
+    }
+};
+
+}  // namespace
+
+int learned_weight_count(int L) { return layout(L).total; }
+
+tcu_status make_two_level(cudaStream_t st, bool learned, const DevPlan& P, int L, int N, double k0,
+                          const double* d_pos, const double* h_pos, const double* h_radii, const double* h_eps,
+                          const double2* d_T, double reach, const std::vector<double>& weights_in,
+                          std::unique_ptr<CoarseSolve> coarse, std::unique_ptr<Preconditioner>* out,
+                          long long* launches) {
+    auto pre = std::make_unique<TwoLevelPre>();
+    pre->T = d_T;
+    pre->launches = launches;
+    double rmax = 0.0;
+    for (int i = 0; i < N; ++i) rmax = std::max(rmax, h_radii[i]);
+    const double cutoff = 2.0 * (reach > 0.0 ? reach : LEARNED_REACH) * rmax;
+    if (!pre->graph.build(st, P, L, N, k0, d_pos, h_pos, h_radii, h_eps, cutoff, launches)) return TCU_OUT_OF_MEMORY;
+    if (!pre->coarse.build(st, P, N, k0, d_pos, d_T, std::move(coarse), launches)) return TCU_OUT_OF_MEMORY;
+    if (!pre->r1.alloc(pre->graph.n * sizeof(cplx)) || !pre->noskip.alloc(std::max<size_t>(pre->graph.nnz, 1)))
+        return TCU_OUT_OF_MEMORY;
+    cudaMemsetAsync(pre->noskip.p, 0, std::max<size_t>(pre->graph.nnz, 1), st);
+    std::vector<double> w = weights_in;
+    if (learned && w.empty()) w = learned_weights(L);
+    const bool use = learned && (int)w.size() == learned_weight_count(L);
+    if (use) {
+        if (!pre->weights.alloc(w.size() * 8)) return TCU_OUT_OF_MEMORY;
+        cudaMemcpyAsync(pre->weights.p, w.data(), w.size() * 8, cudaMemcpyHostToDevice, st);
+    }
+    pre->graph.forward(use ? pre->weights.as<double>() : nullptr, st, launches);
+    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return TCU_DEVICE_ERROR;
+    *out = std::move(pre);
+    return TCU_OK;
+}
+
+// ---- training problems -------------------------------------------------------------------------
+struct LearnedProblem::Impl {
+    GraphData graph;
+    Coarse coarse;
+    int p = 0;
+    DevArray R1, Y, AY, Eb, U, Wt, tmp, tmp2, Tid, noskip, dTH, dP1, dP2, dP3, CGI, CGJ, DG, DHI, CHJ, DH, w, grad,
+        norms, partial;
+};
+
+LearnedProblem::LearnedProblem() : impl(new Impl) {}
+LearnedProblem::~LearnedProblem() = default;
+
+tcu_status LearnedProblem::build(cudaStream_t st, const DevPlan& P, int L_, int N_, double k0_, const double* d_pos_,
+                                 const double* h_pos, const double* h_radii, const double* h_eps, const double2* d_T_,
+                                 double reach, int nprobe, const double2* d_V, std::unique_ptr<CoarseSolve> cs,
+                                 long long* launches_) {
+    L = L_;
+    N = N_;
+    k0 = k0_;
+    plan = &P;
+    d_pos = d_pos_;
+    d_T = d_T_;
+    launches = launches_;
+    Impl& m = *impl;
+    double rmax = 0.0;
+    for (int i = 0; i < N; ++i) rmax = std::max(rmax, h_radii[i]);
+    const double cutoff = 2.0 * (reach > 0.0 ? reach : LEARNED_REACH) * rmax;
+    if (!m.graph.build(st, P, L, N, k0, d_pos, h_pos, h_radii, h_eps, cutoff, launches)) return TCU_OUT_OF_MEMORY;
+    if (!m.coarse.build(st, P, N, k0, d_pos, d_T, std::move(cs), launches)) return TCU_OUT_OF_MEMORY;
+    n = m.graph.n;
+    m.p = nprobe;
+    const size_t vb = n * (size_t)nprobe * sizeof(cplx), nnz = m.graph.nnz;
+    const Layout o = layout(L);
+    for (DevArray* a : {&m.R1, &m.Y, &m.AY, &m.Eb, &m.U, &m.Wt, &m.tmp, &m.tmp2})
+        if (!a->alloc(vb)) return TCU_OUT_OF_MEMORY;
+    if (!m.Tid.alloc((size_t)N * L * 4 * sizeof(cplx)) || !m.noskip.alloc(std::max<size_t>(nnz, 1)) ||
+        !m.dTH.alloc(nnz * o.no * 8) || !m.dP1.alloc((size_t)N * GH * 8) || !m.dP2.alloc(nnz * GH * 8) ||
+        !m.dP3.alloc(nnz * GH * 8) || !m.CGI.alloc(nnz * GH * 8) || !m.CGJ.alloc(nnz * GH * 8) ||
+        !m.DG.alloc((size_t)N * GH * 8) || !m.DHI.alloc((size_t)N * GH * 8) || !m.CHJ.alloc(nnz * GH * 8) ||
+        !m.DH.alloc((size_t)N * GH * 8) || !m.w.alloc(o.total * 8) || !m.grad.alloc(o.total * 8) ||
+        !m.norms.alloc((size_t)std::max(nprobe, 64) * 8) || !m.partial.alloc((size_t)std::max(nprobe, 8) * 256 * 8))
+        return TCU_OUT_OF_MEMORY;
+    cudaMemsetAsync(m.noskip.p, 0, std::max<size_t>(nnz, 1), st);
+    {
+        std::vector<cplx> id((size_t)N * L * 4);
+        for (size_t b = 0; b < (size_t)N * L; ++b) {
+            id[4 * b] = mk(1.0, 0.0);
+            id[4 * b + 1] = mk(0.0, 0.0);
+            id[4 * b + 2] = mk(0.0, 0.0);
+            id[4 * b + 3] = mk(1.0, 0.0);
+        }
+        cudaMemcpyAsync(m.Tid.p, id.data(), id.size() * sizeof(cplx), cudaMemcpyHostToDevice, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) return TCU_DEVICE_ERROR;
+    }
+    // coarse-corrected probes r1 = v - A[:, c] A_cc^-1 v_c, each scaled to unit norm
+    for (int q = 0; q < nprobe; ++q) {
+        tcu_status s = m.coarse.correct(d_V + (size_t)q * n, m.R1.as<cplx>() + (size_t)q * n, st, launches);
+        if (s) return s;
+    }
+    std::vector<double> nr(nprobe);
+    vec_norms(m.R1.as<cplx>(), n, nprobe, m.norms.as<double>(), m.partial.as<double>(), st);
+    cudaMemcpyAsync(nr.data(), m.norms.p, nprobe * 8, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return TCU_DEVICE_ERROR;
+    for (int q = 0; q < nprobe; ++q)
+        vec_scale_copy(m.R1.as<cplx>() + (size_t)q * n, m.R1.as<cplx>() + (size_t)q * n, n,
+                       nr[q] > 0.0 ? 1.0 / nr[q] : 0.0, st);
+    return cudaStreamSynchronize(st) == cudaSuccess && cudaGetLastError() == cudaSuccess ? TCU_OK : TCU_DEVICE_ERROR;
+}
+
+tcu_status LearnedProblem::probes(double2* h_out, cudaStream_t st) {
+    cudaMemcpyAsync(h_out, impl->R1.p, n * (size_t)impl->p * sizeof(cplx), cudaMemcpyDeviceToHost, st);
+    return cudaStreamSynchronize(st) == cudaSuccess ? TCU_OK : TCU_DEVICE_ERROR;
+}
+
+// y = (I - T C) x for ncol columns, and y = (I - T C)^H x = x - F conj(C conj(F T^H x)) (C^T = F C F)
+static void op_apply(const LearnedProblem& lp, const cplx* x, cplx* y, int ncol, cudaStream_t st) {
+    for (int c0 = 0; c0 < ncol; c0 += 8) {
+        const int nc = std::min(8, ncol - c0);
+        launch_apply(*lp.plan, lp.N, lp.k0, lp.d_pos, lp.d_T, x + (size_t)c0 * lp.n, lp.n, nc, nullptr, 1.0, -1.0, true,
+                     y + (size_t)c0 * lp.n, st);
+        if (lp.launches) ++*lp.launches;
+    }
+}
+static void op_apply_adjoint(const LearnedProblem& lp, const cplx* x, cplx* y, cplx* t1, cplx* t2, const cplx* Tid,
+                             int ncol, cudaStream_t st) {
+    const int nlm = lp.L * (lp.L + 2);
+    th_apply_kernel<<<blocks_for((size_t)lp.N * nlm * ncol, 256), 256, 0, st>>>(lp.N, lp.L, lp.d_T, x, lp.n, ncol, t1);
+    flip_conj_kernel<<<blocks_for(lp.n * ncol, 256), 256, 0, st>>>(lp.N, lp.L, t1, nullptr, lp.n, ncol, t2);
+    for (int c0 = 0; c0 < ncol; c0 += 8) {
+        const int nc = std::min(8, ncol - c0);
+        launch_apply(*lp.plan, lp.N, lp.k0, lp.d_pos, Tid, t2 + (size_t)c0 * lp.n, lp.n, nc, nullptr, 0.0, 1.0, true,
+                     t1 + (size_t)c0 * lp.n, st);
+    }
+    flip_conj_kernel<<<blocks_for(lp.n * ncol, 256), 256, 0, st>>>(lp.N, lp.L, t1, x, lp.n, ncol, y);
+    if (lp.launches) *lp.launches += 3 + (ncol + 7) / 8;
+}
+
+tcu_status LearnedProblem::adjoint_apply(const double2* d_x, double2* d_y, int ncol, cudaStream_t st) {
+    Impl& m = *impl;
+    if (ncol > m.p) return TCU_INVALID_INPUT;
+    op_apply_adjoint(*this, d_x, d_y, m.tmp.as<cplx>(), m.tmp2.as<cplx>(), m.Tid.as<cplx>(), ncol, st);
+    return cudaStreamSynchronize(st) == cudaSuccess && cudaGetLastError() == cudaSuccess ? TCU_OK : TCU_DEVICE_ERROR;
+}
+
+tcu_status LearnedProblem::loss_grad(const double* h_weights, double* loss, double* h_grad, cudaStream_t st) {
+    Impl& m = *impl;
+    GraphData& g = m.graph;
+    const Layout o = layout(L);
+    const int p = m.p, N_ = N;
+    const size_t nnz = g.nnz;
+    cudaMemcpyAsync(m.w.p, h_weights, o.total * 8, cudaMemcpyHostToDevice, st);
+    g.forward(m.w.as<double>(), st, launches);
+    // Y = M r1 = r1 + T sum B r1, AY = A Y, E = r1 - A Y
+    for (int q = 0; q < p; ++q) {
+        const cplx* r = m.R1.as<cplx>() + (size_t)q * n;
+        g.near_apply(d_T, r, r, m.Y.as<cplx>() + (size_t)q * n, st, launches, m.noskip.as<uint8_t>());
+    }
+    op_apply(*this, m.Y.as<cplx>(), m.AY.as<cplx>(), p, st);
+    vec_sub(m.Eb.as<cplx>(), m.R1.as<cplx>(), m.AY.as<cplx>(), n, p, st);
+    std::vector<double> en(p);
+    vec_norms(m.Eb.as<cplx>(), n, p, m.norms.as<double>(), m.partial.as<double>(), st);
+    cudaMemcpyAsync(en.data(), m.norms.p, p * 8, cudaMemcpyDeviceToHost, st);
+    // U = A^H E, Wt = T^H U
+    op_apply_adjoint(*this, m.Eb.as<cplx>(), m.U.as<cplx>(), m.tmp.as<cplx>(), m.tmp2.as<cplx>(), m.Tid.as<cplx>(), p,
+                     st);
+    const int nlm = L * (L + 2);
+    th_apply_kernel<<<blocks_for((size_t)N_ * nlm * p, 256), 256, 0, st>>>(N_, L, d_T, m.U.as<cplx>(), n, p,
+                                                                          m.Wt.as<cplx>());
+    if (nnz > 0) {
+        const size_t smem = (size_t)nlm * nlm * sizeof(cplx);
+        static std::atomic<unsigned long long> attr{0};
+        if (first_use_on_device(attr))
+            cudaFuncSetAttribute(theta_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        theta_grad_kernel<<<(unsigned)nnz, 256, smem, st>>>((int)nnz, g.row.as<int>(), g.nbr.as<int>(), L, nlm,
+                                                            g.C.as<cplx>(), m.Wt.as<cplx>(), m.R1.as<cplx>(), n, p,
+                                                            m.dTH.as<double>());
+        gnn_edge_back_kernel<<<blocks_for(nnz, 128), 128, 0, st>>>((int)nnz, m.w.as<double>(), L, g.A.as<double>(),
+                                                                  m.dTH.as<double>(), m.dP3.as<double>(),
+                                                                  m.CGI.as<double>(), m.CGJ.as<double>());
+        gnn_gather_kernel<<<blocks_for(N_, 128), 128, 0, st>>>(N_, g.ptr.as<int>(), g.rev.as<int>(), m.CGI.as<double>(),
+                                                               m.CGJ.as<double>(), nullptr, m.DG.as<double>());
+        gnn_message_back_kernel<<<blocks_for(N_, 128), 128, 0, st>>>(N_, g.ptr.as<int>(), m.w.as<double>(), L,
+                                                                    g.U.as<double>(), m.DG.as<double>(),
+                                                                    m.dP2.as<double>(), m.DHI.as<double>(),
+                                                                    m.CHJ.as<double>());
+        gnn_gather_kernel<<<blocks_for(N_, 128), 128, 0, st>>>(N_, g.ptr.as<int>(), g.rev.as<int>(), nullptr,
+                                                               m.CHJ.as<double>(), m.DHI.as<double>(), m.DH.as<double>());
+        gnn_embed_back_kernel<<<blocks_for((size_t)N_ * GH, 256), 256, 0, st>>>(N_, g.H.as<double>(), m.DH.as<double>(),
+                                                                                m.dP1.as<double>());
+        gnn_weight_grad_kernel<<<blocks_for(o.total, 128), 128, 0, st>>>(
+            N_, (int)nnz, L, g.row.as<int>(), g.nbr.as<int>(), g.X.as<double>(), g.E.as<double>(), g.H.as<double>(),
+            g.G.as<double>(), g.A.as<double>(), m.dP1.as<double>(), m.dP2.as<double>(), m.dP3.as<double>(),
+            m.dTH.as<double>(), m.grad.as<double>());
+        if (launches) *launches += 8;
+    } else {
+        cudaMemsetAsync(m.grad.p, 0, o.total * 8, st);
+    }
+    cudaMemcpyAsync(h_grad, m.grad.p, o.total * 8, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return TCU_DEVICE_ERROR;
+    double s = 0.0;
+    for (int q = 0; q < p; ++q) s += en[q] * en[q];
+    *loss = s;
+    return TCU_OK;
+}
+
+}  // namespace tcu

@@ -88,6 +88,10 @@ struct StageScope {
 // pairs.cu
 void launch_assemble(const DevPlan& P, int N, double k, const double* pos, const cplx* T, void* out, size_t ld,
                      bool fp32, cudaStream_t st);
+// columns of I - T C for the first nsrc source lm of every sphere only (2 nsrc columns per
+// sphere, complex64, rows of all modes; ld >= N M)
+void launch_assemble_sources(const DevPlan& P, int N, double k, const double* pos, const cplx* T, float2* out,
+                             size_t ld, int nsrc, cudaStream_t st);
 void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                   int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st);
 size_t apply_smem_bytes(const DevPlan& P, int ncol);

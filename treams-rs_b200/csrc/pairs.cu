@@ -37,10 +37,12 @@ __device__ __forceinline__ void store_c<float2>(float2* p, cplx v) {
 // four entries (2d..2d+1) x (2s..2s+1): coalesced 2-entry segments, contiguous over a warp.
 // Out is column-major n x n with leading dimension ld; column j*M + e is source mode e of
 // sphere j. T is N * L * 4 complex (mode-order 2x2 per degree, row-major).
+// nsrc < nlm keeps only the first nsrc source lm of every sphere (the dipoles for nsrc = 3):
+// the output then has 2 nsrc columns per source sphere.
 template <typename OutT>
 __global__ void __launch_bounds__(256) assemble_kernel(DevPlan P, int N, double k, const double* __restrict__ pos,
                                                        const cplx* __restrict__ T, OutT* __restrict__ out, size_t ld,
-                                                       int pairs) {
+                                                       int pairs, int nsrc) {
     extern __shared__ cplx Zs[];  // pairs * tsize
     int j = blockIdx.x;
     int i0 = blockIdx.y * pairs;
@@ -54,14 +56,15 @@ __global__ void __launch_bounds__(256) assemble_kernel(DevPlan P, int N, double 
     }
     __syncthreads();
     int items = pairs * P.nlm;
+    const int Mc = 2 * nsrc;
     for (int t = threadIdx.x; t < items; t += blockDim.x) {
         int il = t / P.nlm, d = t - il * P.nlm;
         int i = i0 + il;
         if (i >= N) continue;
         size_t row = (size_t)i * M + 2 * d;
         if (i == j) {
-            for (int s = 0; s < P.nlm; ++s) {
-                size_t col = (size_t)j * M + 2 * s;
+            for (int s = 0; s < nsrc; ++s) {
+                size_t col = (size_t)j * Mc + 2 * s;
                 cplx one = mk(s == d ? 1.0 : 0.0, 0.0), zero = mk(0.0, 0.0);
                 store_c(out + col * ld + row, one);
                 store_c(out + col * ld + row + 1, zero);
@@ -74,11 +77,11 @@ __global__ void __launch_bounds__(256) assemble_kernel(DevPlan P, int N, double 
         const cplx* t4 = T + ((size_t)i * P.L + lam - 1) * 4;
         cplx t00 = t4[0], t01 = t4[1], t10 = t4[2], t11 = t4[3];
         const cplx* Z = Zs + il * P.tsize;
-        for (int s = 0; s < P.nlm; ++s) {
+        for (int s = 0; s < nsrc; ++s) {
             cplx A, B;
             combo_sums(P, s * P.nlm + d, Z, A, B);
             cplx cp = cadd(A, B), cn = csub(A, B);
-            size_t col = (size_t)j * M + 2 * s;
+            size_t col = (size_t)j * Mc + 2 * s;
             store_c(out + col * ld + row, cneg(cmul(t00, cp)));
             store_c(out + col * ld + row + 1, cneg(cmul(t10, cp)));
             store_c(out + (col + 1) * ld + row, cneg(cmul(t01, cn)));
@@ -541,9 +544,18 @@ void launch_assemble(const DevPlan& P, int N, double k, const double* pos, const
     dim3 grid(N, (N + pairs - 1) / pairs);
     size_t smem = (size_t)pairs * P.tsize * sizeof(cplx);
     if (fp32)
-        assemble_kernel<float2><<<grid, 256, smem, st>>>(P, N, k, pos, T, (float2*)out, ld, pairs);
+        assemble_kernel<float2><<<grid, 256, smem, st>>>(P, N, k, pos, T, (float2*)out, ld, pairs, P.nlm);
     else
-        assemble_kernel<double2><<<grid, 256, smem, st>>>(P, N, k, pos, T, (double2*)out, ld, pairs);
+        assemble_kernel<double2><<<grid, 256, smem, st>>>(P, N, k, pos, T, (double2*)out, ld, pairs, P.nlm);
+}
+
+void launch_assemble_sources(const DevPlan& P, int N, double k, const double* pos, const cplx* T, float2* out,
+                             size_t ld, int nsrc, cudaStream_t st) {
+    StageScope sc(ST_ASSEMBLE, st);
+    int pairs = assemble_pairs_per_cta(P.nlm);
+    dim3 grid(N, (N + pairs - 1) / pairs);
+    size_t smem = (size_t)pairs * P.tsize * sizeof(cplx);
+    assemble_kernel<float2><<<grid, 256, smem, st>>>(P, N, k, pos, T, out, ld, pairs, nsrc);
 }
 
 static size_t apply2_smem(const DevPlan& P, int ncol) {

@@ -20,7 +20,8 @@ from ._lib import (  # noqa: F401
     cluster_operator,
     cross_sections,
     default_context,
-    learned_precond_gram,
+    LearnedProblem,
+    learned_weight_count,
     library_path,
     mie_blocks,
     plane_wave_expansion,

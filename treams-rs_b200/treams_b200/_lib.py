@@ -14,7 +14,7 @@ _LIB_PATH = PKG_ROOT / "libtreams_b200.so"
 
 FP64 = 0
 MIXED = 1
-PRECOND = {"none": 0, "block_jacobi": 1, "learned": 2}
+PRECOND = {"none": 0, "block_jacobi": 1, "learned": 2, "two_level": 3}
 
 c_int, c_double, c_size, P = ctypes.c_int, ctypes.c_double, ctypes.c_size_t, ctypes.c_void_p
 
@@ -64,8 +64,12 @@ SIGNATURES = {
     "tcu_cluster_apply_noalloc": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, P]),
     "tcu_iterative_solve": (c_int, [P, c_int, c_double, c_size, P, P, P, P, c_int, P, c_int, P, P]),
     "tcu_batch_solve": (c_int, [P, c_size, P, c_int, P]),
-    "tcu_context_set_learned_preconditioner": (c_int, [P, c_double, c_int, P]),
-    "tcu_learned_precond_gram": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, c_int, P, P, P]),
+    "tcu_context_set_learned_weights": (c_int, [P, c_double, c_size, P]),
+    "tcu_learned_weight_count": (c_size, [c_int]),
+    "tcu_learned_problem_create": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, ctypes.POINTER(P)]),
+    "tcu_learned_problem_loss_grad": (c_int, [P, P, P, P]),
+    "tcu_learned_problem_probes": (c_int, [P, P]),
+    "tcu_learned_problem_destroy": (c_int, [P]),
     "tcu_lsumsw2d_batch": (c_int, [P, c_int, c_double, P, c_size, P, c_double, P]),
     "tcu_array_solve_batch": (c_int, [P, c_int, c_double, c_double, P, P, c_size, P, c_double, P]),
 }
@@ -143,15 +147,11 @@ class Context:
         """Mixed solves finished by an FP64 factor (refinement stalled)."""
         return lib().tcu_context_fallbacks(self.handle)
 
-    def set_learned_preconditioner(self, reach: float = 3.0, alpha=None, layers: int | None = None) -> None:
-        """Near-field reach (sphere diameters) and layer weights of the GMRES preconditioners;
-        alpha None with layers None restores the compiled-in fit."""
-        if alpha is None:
-            nl = -1 if layers is None else int(layers)
-            _check(lib().tcu_context_set_learned_preconditioner(self.handle, float(reach), nl, None))
-        else:
-            a = np.ascontiguousarray(alpha, np.complex128)
-            _check(lib().tcu_context_set_learned_preconditioner(self.handle, float(reach), a.size - 1, _p(a)))
+    def set_learned_weights(self, weights=None, reach: float = 0.0) -> None:
+        """Network weights (None: the compiled-in ones) and near-field reach in sphere diameters
+        (<= 0: the compiled-in 3) of the learned and two-level preconditioners."""
+        w = np.zeros(0) if weights is None else np.ascontiguousarray(weights, np.float64)
+        _check(lib().tcu_context_set_learned_weights(self.handle, float(reach), w.size, _p(w) if w.size else None))
 
     def set_profiling(self, on: bool) -> None:
         _check(lib().tcu_context_set_profiling(self.handle, int(on)))
@@ -339,20 +339,52 @@ class IterativeSolution:
     convergence: list
 
 
-def learned_precond_gram(lmax: int, k0: float, radii, eps, positions, layers: int, V, ctx: Context | None = None):
-    """Training statistics of the learned preconditioner: (G, b) with G[k, l] = sum_v u_k^H u_l
-    and b[k] = sum_v u_k^H v for the layer basis u_k = A (D N)^k D v of the probe vectors V
-    (n x nvec). The loss sum_v ||v - sum_k alpha_k u_k||^2 is const - 2 Re(alpha^H b) +
-    alpha^H G alpha, with gradient 2 (G alpha - b)."""
-    ctx = ctx or default_context()
-    r, e, x = _geom(radii, eps, positions)
-    V = np.asfortranarray(V, np.complex128)
-    K1 = layers + 1
-    gram = np.zeros(K1 * K1, np.complex128)
-    rhs = np.zeros(K1, np.complex128)
-    _check(lib().tcu_learned_precond_gram(ctx.handle, lmax, float(k0), r.size, _p(r), _p(e), _p(x), layers,
-                                          V.shape[1], _p(V), _p(gram), _p(rhs)))
-    return gram.reshape(K1, K1), rhs
+def learned_weight_count(lmax: int) -> int:
+    return int(lib().tcu_learned_weight_count(lmax))
+
+
+class LearnedProblem:
+    """One training cluster of the learned preconditioner's graph network on the GPU
+    (tcu_learned_problem): loss_grad(weights) -> (loss, gradient) from the device's forward and
+    backward kernels; probes() -> the coarse-corrected unit-norm probe vectors (n, nprobe)."""
+
+    def __init__(self, lmax, k0, radii, eps, positions, V, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        r, e, x = _geom(radii, eps, positions)
+        V = np.asfortranarray(V, np.complex128)
+        if V.ndim == 1:
+            V = V[:, None]
+        self.lmax, self.n, self.nprobe = lmax, V.shape[0], V.shape[1]
+        self.nweights = learned_weight_count(lmax)
+        h = P()
+        _check(lib().tcu_learned_problem_create(self.ctx.handle, lmax, float(k0), r.size, _p(r), _p(e), _p(x),
+                                                V.shape[1], _p(V), ctypes.byref(h)))
+        self.handle = h
+
+    def loss_grad(self, weights):
+        w = np.ascontiguousarray(weights, np.float64)
+        if w.size != self.nweights:
+            raise ValueError(f"expected {self.nweights} weights")
+        loss = c_double()
+        grad = np.zeros(self.nweights)
+        _check(lib().tcu_learned_problem_loss_grad(self.handle, _p(w), ctypes.byref(loss), _p(grad)))
+        return loss.value, grad
+
+    def probes(self) -> np.ndarray:
+        out = np.zeros((self.n, self.nprobe), np.complex128, order="F")
+        _check(lib().tcu_learned_problem_probes(self.handle, _p(out)))
+        return out
+
+    def close(self) -> None:
+        if self.handle:
+            lib().tcu_learned_problem_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class ClusterDesc(ctypes.Structure):

@@ -1,104 +1,139 @@
-"""Fit the layer weights of the learned GMRES preconditioner and write them into the library.
+"""Train the graph network of the learned GMRES preconditioner on the GPU and write its weights
+into the library.
 
-The preconditioner is M = sum_k alpha_k (D N)^k D (block-Jacobi inverse D, near-field couplings
-N between blocks; csrc/precond.cu). Its loss on a probe vector v is ||v - A M v||^2 with
-A = I - T C, which is quadratic in alpha: summed over probe vectors it equals
-const - 2 Re(alpha^H b) + alpha^H G alpha with the statistics (G, b) that the GPU returns
-(tcu_learned_precond_gram; its gradient 2 (G alpha - b) is checked against the CPU oracle in
-the GPU tests). Training minimises the loss over training clusters (seeds 2000 + i,
-N ~ U{64..1024}, the 4096-sphere workload's material and packing), each probe normalised to
-unit norm, with a small ridge term; the minimiser solves (G + lambda I) alpha = b.
+The preconditioner (csrc/gnn.cu) is two-level: a coarse solve of the cluster's dipole system,
+then the near field (pairs closer than 3 sphere diameters) with every (degree, degree) sub-block
+of each translation block scaled by Theta_ij, which a small graph network predicts from node and
+edge features. Training minimises the mean over coarse-corrected probe vectors r1 of
+||r1 - A M_Theta r1||^2 (A = I - T C in FP64) over generated clusters (seeds 2000 + i,
+N ~ U{64..1024}, the 4096-sphere workload's material and packing). The probes are the
+right-hand sides the solver sees, T b for plane waves of several directions and helicities, and
+random vectors. Loss and gradient come from the library's forward and backward kernels
+(tcu_learned_problem_loss_grad); the optimiser (Adam) runs on the host over the few thousand
+weights. Theta = 1 (all output weights zero) is the untrained two-level method, and training
+starts there.
 
-Run on a GPU:  python -m treams_b200.train_precond [--clusters 12] [--layers 6] [--reach 6] --write
-It rewrites treams-rs_b200/csrc/learned_coefficients.inc; rebuild the library afterwards.
+Run on a GPU:  python -m treams_b200.train_precond [--clusters 8] [--steps 300] --write
+It rewrites treams-rs_b200/csrc/learned_weights.inc; rebuild the library afterwards.
 """
 from __future__ import annotations
 
 import argparse
+import json
 import pathlib
+import time
 
 import numpy as np
 
 from . import _lib, workloads
 
-INC = pathlib.Path(__file__).resolve().parent.parent / "csrc" / "learned_coefficients.inc"
+INC = pathlib.Path(__file__).resolve().parent.parent / "csrc" / "learned_weights.inc"
+H, NF, EF = 16, 6, 5
 
 
-def statistics(i: int, layers: int, nrandom: int, ctx) -> tuple[np.ndarray, np.ndarray, float]:
-    w = workloads.training_cluster(i)
-    rng = np.random.default_rng(7000 + i)
-    probes = [rng.standard_normal(w.n) + 1j * rng.standard_normal(w.n) for _ in range(nrandom)]
-    # the incident field T b of a plane wave along +z, the right-hand side GMRES sees
-    B = _lib.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)[:, 0]
+def init_weights(lmax: int, seed: int = 0) -> np.ndarray:
+    """Random hidden layers (variance 1/fan-in), zero output layer: Theta = 1 at the start."""
+    rng = np.random.default_rng(seed)
+    nin, no = 2 * H + EF, 2 * lmax * lmax
+    parts = [rng.standard_normal(H * NF) / np.sqrt(NF), np.zeros(H), rng.standard_normal(H * nin) / np.sqrt(nin),
+             np.zeros(H), rng.standard_normal(H * nin) / np.sqrt(nin), np.zeros(H), np.zeros(no * H), np.zeros(no)]
+    w = np.concatenate(parts)
+    assert w.size == _lib.learned_weight_count(lmax)
+    return w
+
+
+def probes(w: workloads.Cluster, nrandom: int, seed: int, ctx) -> np.ndarray:
+    """T b for plane waves along +z, +x, -y and oblique (both helicities mixed), plus random vectors."""
+    k0 = w.k0
+    s, c = np.sin(np.pi / 6), np.cos(np.pi / 6)
+    kv = np.array([[0, 0, k0], [k0, 0, 0], [0, -k0, 0], [k0 * s, 0, k0 * c]], complex)
+    pols = np.array([1, 0, 1, 0], np.int32)
+    B = _lib.plane_wave_expansion(w.lmax, w.positions, kv, pols, ctx=ctx)
     T = _lib.mie_blocks(w.lmax, w.k0, w.radii, w.eps, ctx=ctx)
-    tb = np.empty_like(B)
     M = 2 * w.lmax * (w.lmax + 2)
-    for s in range(w.radii.size):
-        for lm in range(M // 2):
-            l = int(np.sqrt(lm + 1))
-            t4 = T[s, l - 1]
-            x = B[s * M + 2 * lm: s * M + 2 * lm + 2]
-            tb[s * M + 2 * lm: s * M + 2 * lm + 2] = t4 @ x
-    probes.append(tb)
-    V = np.stack([p / np.linalg.norm(p) for p in probes], axis=1)
-    G, b = _lib.learned_precond_gram(w.lmax, w.k0, w.radii, w.eps, w.positions, layers, V, ctx=ctx)
-    return G, b, float(V.shape[1])
+    deg = np.array([l for l in range(1, w.lmax + 1) for _ in range(2 * l + 1)])
+    Bq = B.reshape(w.radii.size, M // 2, 2, B.shape[1])
+    TB = np.einsum("nqab,nqbp->nqap", T[:, deg - 1], Bq).reshape(w.n, B.shape[1])
+    rng = np.random.default_rng(seed)
+    Rn = rng.standard_normal((w.n, nrandom)) + 1j * rng.standard_normal((w.n, nrandom))
+    return np.asfortranarray(np.concatenate([TB, Rn], axis=1))
 
 
-def fit(clusters: int, layers: int, nrandom: int = 3, ridge: float = 1e-8, ctx=None):
+def train(clusters: int = 8, steps: int = 300, lr: float = 3e-3, nrandom: int = 2, seed: int = 0, ctx=None,
+          log=print):
     ctx = ctx or _lib.default_context()
-    K1 = layers + 1
-    G = np.zeros((K1, K1), complex)
-    b = np.zeros(K1, complex)
-    total = 0.0
+    ctx.set_learned_weights(None, 0.0)
+    problems, names = [], []
     for i in range(clusters):
-        g, r, nv = statistics(i, layers, nrandom, ctx)
-        G += g
-        b += r
-        total += nv
-    scale = np.trace(G).real / K1
-    alpha = np.linalg.solve(G + ridge * scale * np.eye(K1), b)
-    loss = lambda a: (total - 2 * np.real(np.vdot(a, b)) + np.real(np.vdot(a, G @ a))) / total
-    e0 = np.zeros(K1, complex)
-    e0[0] = 1.0
-    return alpha, {"loss_fit": loss(alpha), "loss_block_jacobi": loss(e0), "loss_relaxation": loss(np.ones(K1)),
-                   "probes": total}
+        w = workloads.training_cluster(i)
+        problems.append(_lib.LearnedProblem(w.lmax, w.k0, w.radii, w.eps, w.positions,
+                                            probes(w, nrandom, 7000 + i, ctx), ctx=ctx))
+        names.append(f"{w.radii.size} spheres")
+    lmax = 3
+    wts = init_weights(lmax, seed)
+    nprobe = sum(p.nprobe for p in problems)
+
+    def total(wv):
+        loss, grad = 0.0, np.zeros_like(wv)
+        for p in problems:
+            l, g = p.loss_grad(wv)
+            loss += l
+            grad += g
+        return loss / nprobe, grad / nprobe
+
+    loss0, _ = total(wts)
+    m, v = np.zeros_like(wts), np.zeros_like(wts)
+    b1, b2, eps = 0.9, 0.999, 1e-8
+    best = (loss0, wts.copy())
+    t0 = time.time()
+    for it in range(1, steps + 1):
+        loss, g = total(wts)
+        if loss < best[0]:
+            best = (loss, wts.copy())
+        m = b1 * m + (1 - b1) * g
+        v = b2 * v + (1 - b2) * g * g
+        wts = wts - lr * (m / (1 - b1**it)) / (np.sqrt(v / (1 - b2**it)) + eps)
+        if it % 25 == 0 or it == 1:
+            log(f"step {it}: mean probe loss {loss:.5g} (untrained {loss0:.5g}), {time.time() - t0:.1f} s")
+    loss, _ = total(wts)
+    if loss < best[0]:
+        best = (loss, wts.copy())
+    for p in problems:
+        p.close()
+    return best[1], {"loss_untrained": loss0, "loss_trained": best[0], "clusters": names, "steps": steps,
+                     "probes": nprobe}
 
 
-def write_inc(alpha_by_lmax: dict[int, np.ndarray], layers: int, reach: float, note: str) -> None:
+def write_inc(weights_by_lmax: dict, note: str, reach: float = 3.0) -> None:
     lines = [
-        "// Layer weights alpha_k of the learned preconditioner per lmax (generated by",
-        "// treams-rs_b200/treams_b200/train_precond.py from least-squares fits on training clusters;",
-        "// lmax without a fit uses alpha_k = 1, i.e. plain block-Jacobi relaxation sweeps).",
+        "// Trained weights of the graph network of the learned preconditioner per lmax (generated by",
+        "// treams-rs_b200/treams_b200/train_precond.py; lmax without trained weights uses Theta = 1).",
         f"// {note}",
-        f"constexpr int LEARNED_LAYERS = {layers};",
-        f"constexpr double LEARNED_REACH = {float(reach)!r};",
-        "inline std::complex<double> learned_alpha(int lmax, int k) {",
+        f"constexpr double LEARNED_REACH = {float(reach)!r};  // near-field reach in sphere diameters",
+        "inline std::vector<double> learned_weights(int lmax) {",
     ]
-    for L, a in sorted(alpha_by_lmax.items()):
-        vals = ", ".join(f"{{{float(z.real)!r}, {float(z.imag)!r}}}" for z in a)
-        lines.append(f"    static const double a{L}[][2] = {{{vals}}};")
-        lines.append(f"    if (lmax == {L} && k >= 0 && k < {len(a)}) return {{a{L}[k][0], a{L}[k][1]}};")
-    lines += ["    (void)lmax;", "    (void)k;", "    return {1.0, 0.0};", "}", ""]
+    for L, w in sorted(weights_by_lmax.items()):
+        vals = ", ".join(repr(float(x)) for x in w)
+        lines.append(f"    if (lmax == {L}) return {{{vals}}};")
+    lines += ["    return {};", "}", ""]
     INC.write_text("\n".join(lines))
 
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--clusters", type=int, default=12)
-    ap.add_argument("--layers", type=int, default=6)
-    ap.add_argument("--reach", type=float, default=6.0, help="near-field reach in sphere diameters")
-    ap.add_argument("--write", action="store_true", help="rewrite csrc/learned_coefficients.inc")
+    ap.add_argument("--clusters", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--lr", type=float, default=3e-3)
+    ap.add_argument("--write", action="store_true", help="rewrite csrc/learned_weights.inc")
+    ap.add_argument("--out", default=None, help="also write the weights and the training record to this JSON file")
     args = ap.parse_args()
-    ctx = _lib.default_context()
-    ctx.set_learned_preconditioner(args.reach, layers=args.layers)
-    alpha, info = fit(args.clusters, args.layers, ctx=ctx)
-    print({"alpha": [complex(a) for a in alpha], **info})
+    w, info = train(args.clusters, args.steps, args.lr)
+    print(json.dumps(info))
+    if args.out:
+        pathlib.Path(args.out).write_text(json.dumps({"weights": list(map(float, w)), **info}))
     if args.write:
-        write_inc({3: alpha}, args.layers, args.reach,
-                  f"fit on {args.clusters} training clusters at reach {args.reach:g} diameters: mean probe loss "
-                  f"{info['loss_fit']:.4g} (relaxation {info['loss_relaxation']:.4g}, block Jacobi "
-                  f"{info['loss_block_jacobi']:.4g})")
+        write_inc({3: w}, f"trained on {args.clusters} clusters, {args.steps} Adam steps: mean probe loss "
+                          f"{info['loss_trained']:.4g} (untrained two-level {info['loss_untrained']:.4g})")
 
 
 if __name__ == "__main__":
