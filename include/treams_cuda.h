@@ -153,6 +153,14 @@ tcu_status tcu_sphere_cluster_factor_dev(tcu_context* ctx, int lmax, double k0, 
  * (tcu_context_fallbacks counts these solves). */
 tcu_status tcu_factor_solve(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
 tcu_status tcu_factor_solve_dev(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
+/* Adjoint solve Y = (I - T C)^-H G with the factor (linalg/mod.rs:436 solve_adjoint_in_place),
+ * refined in FP64 against the matrix-free adjoint operator like tcu_factor_solve; certificates
+ * report ||G - (I - T C)^H Y|| and ||G||. No counterpart as a public call in the reference. */
+tcu_status tcu_factor_solve_adjoint(tcu_factor* f, const double* G, int p, double* Y, tcu_certificate* certificates);
+/* Gradient of incident columns for the factor: out = T^H (I - T C)^-H G
+ * (InteractionFactor::pullback_incident, cluster/interaction.rs:221-227). */
+tcu_status tcu_factor_pullback_incident(tcu_factor* f, const double* G, int p, double* out,
+                                        tcu_certificate* certificates);
 /* Dimension n = N M of a factor. */
 size_t tcu_factor_dimension(const tcu_factor* f);
 tcu_status tcu_factor_destroy(tcu_factor* f);
@@ -208,6 +216,15 @@ tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0, size_t N, 
                                const double* eps, const double* positions, const double* B, int p,
                                const tcu_gmres_options* options, int preconditioner, double* X,
                                tcu_certificate* certificates);
+
+/* Incident-field gradient of the matrix-free cluster: out = T^H Y with Y = (I - T C)^-H G from
+ * one unpreconditioned adjoint GMRES solve per column (IterativeSphereCluster::pullback,
+ * cluster/iterative.rs:460-488, its `incident` part; the position, radius and permittivity
+ * gradients of that call are not built). Certificates report the adjoint GMRES residuals. */
+tcu_status tcu_iterative_pullback_incident(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
+                                           const double* eps, const double* positions, const double* G, int p,
+                                           const tcu_gmres_options* options, double* out,
+                                           tcu_certificate* certificates);
 
 /* Preconditioners TCU_PRECOND_LEARNED and TCU_PRECOND_TWO_LEVEL (no counterpart in the
  * reference, whose iterative solver is unpreconditioned): right preconditioner

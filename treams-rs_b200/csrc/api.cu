@@ -7,6 +7,7 @@
 #include <complex>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <set>
 #include <memory>
@@ -497,6 +498,107 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
     return TCU_OK;
 }
 
+// Adjoint solve Y = (I - T C)^-H G with a factor (cluster/interaction.rs:221-227 uses it for
+// pullback_incident; linalg/mod.rs:436 solve_adjoint_in_place): A^-H g = R P^T L^-H U^-H C g with
+// the scales R, C of the factor, refined in FP64 against the matrix-free adjoint operator like
+// the forward solve. th: return T^H Y instead (the incident-field gradient).
+tcu_status solve_adjoint_impl(tcu_factor* f, const double* G, int p, double* Y, tcu_certificate* certs, bool th) {
+    if (!f || !G || !Y || p <= 0) return fail(TCU_INVALID_INPUT, "require a factor and at least one column");
+    tcu_context* ctx = f->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    const DevPlan* P;
+    tcu_status s = get_plan(ctx, f->L, &P);
+    if (s) return s;
+    const size_t n = f->n, per = n * p;
+    if (!finite_all(G, 2 * per))
+        return fail(TCU_INVALID_INPUT, "require finite channel-by-illumination columns matching the factorization");
+    DevBuf bufs(ctx);
+    const size_t tmpc = adjoint_solve_tmp((int)n, p);
+    CK(bufs.alloc((5 * per + tmpc) * sizeof(cplx)), "adjoint solve buffers");
+    cplx* g = (cplx*)bufs.p;
+    cplx* y = g + per;
+    cplx* r = y + per;
+    cplx* t1 = r + per;
+    cplx* t2 = t1 + per;
+    cplx* tmp = t2 + per;
+    CK(cudaMemcpyAsync(g, G, per * 16, cudaMemcpyHostToDevice, ctx->stream), "copy rhs");
+    std::vector<double> rn(p), bn(p);
+    vec_norms(g, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
+    CK(cudaMemcpyAsync(bn.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "norms");
+    auto lu_adjoint = [&](cplx* v) {
+        if (f->scaled) scale_rows(v, f->d_scale + n, n, p, ctx->stream);  // C g
+        if (f->precision == TCU_FP64)
+            lu_solve_adjoint_fp64((const double2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, p, ctx->stream,
+                                  &ctx->launches);
+        else
+            lu_solve_adjoint_fp32((const float2*)f->d_A, (int)n, f->wk.perm, f->d_inv, v, tmp, p, ctx->stream,
+                                  &ctx->launches);
+        if (f->scaled) scale_rows(v, f->d_scale, n, p, ctx->stream);  // R
+    };
+    auto residual = [&]() -> tcu_status {  // r = g - A^H y
+        launch_apply_adjoint(*P, f->N, f->k0, f->d_pos, f->d_T, y, n, p, r, t1, t2, ctx->stream, &ctx->launches);
+        vec_sub(r, g, r, n, p, ctx->stream);
+        vec_norms(r, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
+        ctx->launches += 3;
+        CK(cudaMemcpyAsync(rn.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "norms");
+        return sync_status(ctx, "adjoint residual");
+    };
+    CK(cudaMemcpyAsync(y, g, per * 16, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
+    lu_adjoint(y);
+    int sweeps = 1;
+    if ((s = residual())) return s;
+    const double tol = ctx->refine_target;
+    double prev = INFINITY;
+    const int max_sweeps = f->precision == TCU_MIXED ? 10 : 2;
+    auto worst_of = [&]() {
+        double w = 0.0;
+        for (int c = 0; c < p; ++c) w = std::max(w, bn[c] > 0 ? rn[c] / bn[c] : rn[c]);
+        return w;
+    };
+    for (int it = 0; it < max_sweeps; ++it) {
+        const double worst = worst_of();
+        if (worst <= tol || !(worst < 0.5 * prev)) break;
+        prev = worst;
+        lu_adjoint(r);
+        vec_axpy(y, r, n, p, ctx->stream);
+        ++ctx->launches;
+        ++sweeps;
+        if ((s = residual())) return s;
+    }
+    if (f->precision == TCU_MIXED && !(worst_of() <= ctx->fallback_above)) {
+        if (!f->fallback) {
+            std::vector<double> hr(f->N), he(2 * (size_t)f->N), hp(3 * (size_t)f->N);
+            CK(cudaMemcpyAsync(hr.data(), f->d_radii, f->N * 8, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+            CK(cudaMemcpyAsync(he.data(), f->d_eps, f->N * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+            CK(cudaMemcpyAsync(hp.data(), f->d_pos, f->N * 24, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+            if ((s = sync_status(ctx, "fallback"))) return s;
+            const bool to_tf32 = f->wk.f16_pieces;
+            if ((s = factor_impl(ctx, f->L, f->k0, f->N, hr.data(), he.data(), hp.data(), nullptr, nullptr, nullptr,
+                                 to_tf32 ? TCU_MIXED : TCU_FP64, &f->fallback, false)))
+                return s;
+        }
+        ++ctx->fallbacks;
+        return solve_adjoint_impl(f->fallback, G, p, Y, certs, th);
+    }
+    for (int c = 0; c < p; ++c)
+        if (!std::isfinite(rn[c])) return fail(TCU_SINGULAR, "non-finite solution: numerically singular operator");
+    if (th) {
+        launch_apply_th(f->L, f->N, f->d_T, y, n, p, r, ctx->stream);
+        ++ctx->launches;
+    }
+    CK(cudaMemcpyAsync(Y, th ? r : y, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy solution");
+    if ((s = sync_status(ctx, "adjoint solve"))) return s;
+    if (certs)
+        for (int c = 0; c < p; ++c) {
+            certs[c].iterations = sweeps;
+            certs[c].residual_norm = rn[c];
+            certs[c].rhs_norm = bn[c];
+        }
+    return TCU_OK;
+}
+
 // A factor applied once (no refinement): v <- A^-1 v with the row/column scales; the coarse
 // solve of the two-level preconditioners. Owns the factor.
 struct FactorCoarse : CoarseSolve {
@@ -813,6 +915,14 @@ tcu_status tcu_factor_solve_dev(tcu_factor* f, const double* B, int p, double* X
 }
 size_t tcu_factor_dimension(const tcu_factor* f) { return f ? f->n : 0; }
 
+tcu_status tcu_factor_solve_adjoint(tcu_factor* f, const double* G, int p, double* Y, tcu_certificate* certificates) {
+    return solve_adjoint_impl(f, G, p, Y, certificates, false);
+}
+tcu_status tcu_factor_pullback_incident(tcu_factor* f, const double* G, int p, double* out,
+                                        tcu_certificate* certificates) {
+    return solve_adjoint_impl(f, G, p, out, certificates, true);
+}
+
 tcu_status tcu_factor_destroy(tcu_factor* f) {
     if (!f) return TCU_OK;
     if (f->fallback) tcu_factor_destroy(f->fallback);
@@ -900,9 +1010,9 @@ namespace tcu {
 // Gram-Schmidt passes (each a fixed-order batched dot product), Givens rotations and the
 // Hessenberg solve on the host, true residual b - A x at every restart. With a right
 // preconditioner M the Krylov space is built for A M and x = M y.
-tcu_status gmres_device(tcu_context* ctx, const DevPlan* P, int N, double k0, const double* d_pos, const cplx* d_T,
-                        const cplx* rhs, size_t n, const tcu_gmres_options& opt, Preconditioner* pre, cplx* x,
-                        cplx* work, tcu_certificate* cert) {
+// op(in, out): out = A in for one device column (the cluster operator or its adjoint).
+tcu_status gmres_device(tcu_context* ctx, const std::function<void(const cplx*, cplx*)>& op, const cplx* rhs, size_t n,
+                        const tcu_gmres_options& opt, Preconditioner* pre, cplx* x, cplx* work, tcu_certificate* cert) {
     int restart = (int)std::min<long long>(std::min<long long>(opt.restart, (long long)n), opt.max_iterations);
     cplx* V = work;                       // (restart + 1) * n
     cplx* w = V + (size_t)(restart + 1) * n;
@@ -946,8 +1056,7 @@ tcu_status gmres_device(tcu_context* ctx, const DevPlan* P, int N, double k0, co
                 pre->apply(vin, Z + (size_t)j * n, st);
                 vin = Z + (size_t)j * n;
             }
-            launch_apply(*P, N, k0, d_pos, d_T, vin, n, 1, nullptr, 1.0, -1.0, true, w, st);
-            ctx->launches += 2;
+            op(vin, w);
             for (int pass = 0; pass < 2; ++pass) {
                 vec_dots(V, n, j + 1, w, n, ctx->d_csmall, ctx->d_cpartial, st);
                 vec_gemv_sub(w, V, n, j + 1, ctx->d_csmall, n, st);
@@ -995,7 +1104,8 @@ tcu_status gmres_device(tcu_context* ctx, const DevPlan* P, int N, double k0, co
         CK(cudaMemcpyAsync(ctx->d_csmall, g.data(), used * 16, cudaMemcpyHostToDevice, st), "coefficients");
         vec_lincomb(x, pre ? Z : V, n, used, ctx->d_csmall, n, st);
         // true residual r = rhs - A x
-        launch_apply(*P, N, k0, d_pos, d_T, x, n, 1, rhs, -1.0, 1.0, true, r, st);
+        op(x, r);
+        vec_sub(r, rhs, r, n, 1, st);
         vec_norms(r, n, 1, ctx->d_small, ctx->d_partial, st);
         CK(cudaMemcpyAsync(&rnorm, ctx->d_small, 8, cudaMemcpyDeviceToHost, st), "norm");
         if ((s = sync_status(ctx, "gmres"))) return s;
@@ -1070,7 +1180,11 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
     std::string msg;
     for (int c = 0; c < p; ++c) {
         tcu_certificate cert{};
-        s = gmres_device(ctx, P, (int)N, k0, pos, T, tb + c * n, n, opt, pre.get(), x + c * n, wk, &cert);
+        auto op = [&](const cplx* in, cplx* out) {
+            launch_apply(*P, (int)N, k0, pos, T, in, n, 1, nullptr, 1.0, -1.0, true, out, ctx->stream);
+            ++ctx->launches;
+        };
+        s = gmres_device(ctx, op, tb + c * n, n, opt, pre.get(), x + c * n, wk, &cert);
         if (certificates) certificates[c] = cert;
         if (s && !worst) {
             worst = s;
@@ -1079,6 +1193,73 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
     }
     CK(cudaMemcpyAsync(X, x, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
     s = sync_status(ctx, "GMRES");
+    if (s) return s;
+    if (worst) return fail(worst, msg);
+    return TCU_OK;
+}
+
+extern "C" tcu_status tcu_iterative_pullback_incident(tcu_context* ctx, int lmax, double k0, size_t N,
+                                                      const double* radii, const double* eps, const double* positions,
+                                                      const double* G, int p, const tcu_gmres_options* options,
+                                                      double* out, tcu_certificate* certificates) {
+    if (!ctx || !G || !out || p <= 0) return fail(TCU_INVALID_INPUT, "null argument");
+    tcu_gmres_options opt = options ? *options : tcu_gmres_options{1e-10, 0.0, 30, 300};
+    if (!std::isfinite(opt.rtol) || !std::isfinite(opt.atol) || opt.rtol < 0 || opt.atol < 0 ||
+        opt.rtol + opt.atol == 0.0 || opt.restart <= 0 || opt.max_iterations <= 0)
+        return fail(TCU_INVALID_INPUT,
+                    "GMRES needs finite nonnegative tolerances, a positive tolerance, restart and iteration limit");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    tcu_status s = validate_spheres(lmax, k0, N, radii, eps, positions);
+    if (s) return s;
+    const DevPlan* P;
+    if ((s = get_plan(ctx, lmax, &P))) return s;
+    const size_t M = 2 * (size_t)lmax * (lmax + 2), n = N * M, per = n * p;
+    if (!finite_all(G, 2 * per)) return fail(TCU_INVALID_INPUT, "invalid illumination cotangent");
+    int restart = std::min(opt.restart, opt.max_iterations);
+    if ((size_t)restart > n) restart = (int)n;
+    DevBuf buf(ctx);
+    const size_t work = (size_t)(2 * restart + 4) * n;
+    Arena ar;
+    size_t oP = ar.add(N * 24), oR = ar.add(N * 8), oE = ar.add(N * 16), oT = ar.add(N * lmax * 64),
+           oG = ar.add(per * 16), oY = ar.add(per * 16), oW = ar.add(work * 16), o1 = ar.add(n * 16), o2 = ar.add(n * 16);
+    CK(buf.alloc(ar.total), "adjoint GMRES buffers");
+    double* pos = ar.at<double>(buf.p, oP);
+    double* r = ar.at<double>(buf.p, oR);
+    cplx* e = ar.at<cplx>(buf.p, oE);
+    cplx* T = ar.at<cplx>(buf.p, oT);
+    cplx* g = ar.at<cplx>(buf.p, oG);
+    cplx* y = ar.at<cplx>(buf.p, oY);
+    cplx* wk = ar.at<cplx>(buf.p, oW);
+    cplx* t1 = ar.at<cplx>(buf.p, o1);
+    cplx* t2 = ar.at<cplx>(buf.p, o2);
+    CK(cudaMemcpyAsync(pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(g, G, per * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
+    launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
+    ++ctx->launches;
+    if ((s = read_status(ctx, "Mie coefficients"))) return s;
+    auto op = [&](const cplx* in, cplx* o) {
+        launch_apply_adjoint(*P, (int)N, k0, pos, T, in, n, 1, o, t1, t2, ctx->stream, &ctx->launches);
+    };
+    tcu_status worst = TCU_OK;
+    std::string msg;
+    for (int c = 0; c < p; ++c) {
+        tcu_certificate cert{};
+        s = gmres_device(ctx, op, g + c * n, n, opt, nullptr, y + c * n, wk, &cert);
+        if (certificates) certificates[c] = cert;
+        if (s && !worst) {
+            worst = s;
+            msg = g_last_error;
+        }
+    }
+    launch_apply_th(lmax, (int)N, T, y, n, p, g, ctx->stream);  // the incident gradient T^H Y
+    ++ctx->launches;
+    CK(cudaMemcpyAsync(out, g, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    s = sync_status(ctx, "adjoint GMRES");
     if (s) return s;
     if (worst) return fail(worst, msg);
     return TCU_OK;

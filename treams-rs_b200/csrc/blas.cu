@@ -125,7 +125,7 @@ void vec_axpy(cplx* y, const cplx* x, size_t n, int ncol, cudaStream_t st) {
     size_t t = n * ncol;
     axpy_kernel<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(y, x, t);
 }
-__global__ void sub_kernel(cplx* __restrict__ o, const cplx* __restrict__ a, const cplx* __restrict__ b, size_t total) {
+__global__ void sub_kernel(cplx* o, const cplx* a, const cplx* b, size_t total) {  // o may alias a or b
     size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q < total) o[q] = csub(a[q], b[q]);
 }
@@ -133,7 +133,7 @@ void vec_sub(cplx* out, const cplx* a, const cplx* b, size_t n, int ncol, cudaSt
     size_t t = n * ncol;
     sub_kernel<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(out, a, b, t);
 }
-__global__ void scale_kernel(cplx* __restrict__ o, const cplx* __restrict__ x, size_t n, double s) {
+__global__ void scale_kernel(cplx* o, const cplx* x, size_t n, double s) {  // o may alias x
     size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q < n) o[q] = cscale(x[q], s);
 }

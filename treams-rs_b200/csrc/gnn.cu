@@ -20,7 +20,7 @@
 // (e_ij: 5 edge features). Training minimises sum_p ||r1_p - A M_Theta r1_p||^2 over
 // coarse-corrected probe vectors r1_p of generated clusters; the loss and its gradient in
 // every weight come from the forward and backward kernels below (the Theta gradient needs
-// A^H, applied matrix-free through C^T = F C F with the order flip F x(l,m) = (-1)^m x(l,-m)).
+// A^H, applied matrix-free by adjoint.cu).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -322,45 +322,7 @@ __global__ void gnn_weight_grad_kernel(int N, int nnz, int L, const int* __restr
     grad[t] = s;
 }
 
-// ---- adjoint operator and coarse-space helpers --------------------------------------------
-// y = T^H x per sphere and degree (2 x 2 blocks in mode order, row-major)
-__global__ void th_apply_kernel(int N, int L, const cplx* __restrict__ T, const cplx* __restrict__ x, size_t n,
-                                int ncol, cplx* __restrict__ y) {
-    const int nlm = L * (L + 2);
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (size_t)N * nlm * ncol) return;
-    const int c = (int)(t / ((size_t)N * nlm));
-    const size_t r = t - (size_t)c * N * nlm;
-    const int i = (int)(r / nlm), lm = (int)(r % nlm);
-    const cplx* t4 = T + ((size_t)i * L + lm_degree(lm) - 1) * 4;
-    const size_t o = c * n + (size_t)i * 2 * nlm + 2 * lm;
-    const cplx a = x[o], b = x[o + 1];
-    cplx y0 = mk(0.0, 0.0), y1 = mk(0.0, 0.0);
-    cfma_conj(y0, t4[0], a);
-    cfma_conj(y0, t4[2], b);
-    cfma_conj(y1, t4[1], a);
-    cfma_conj(y1, t4[3], b);
-    y[o] = y0;
-    y[o + 1] = y1;
-}
-
-// y = base - conj(F x) (base null: y = conj(F x)); (F x)(l, m, pol) = (-1)^m x(l, -m, pol)
-__global__ void flip_conj_kernel(int N, int L, const cplx* __restrict__ x, const cplx* __restrict__ base, size_t n,
-                                 int ncol, cplx* __restrict__ y) {
-    const int M = 2 * L * (L + 2);
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (size_t)N * M * ncol) return;
-    const int c = (int)(t / ((size_t)N * M));
-    const size_t r = t - (size_t)c * N * M;
-    const int i = (int)(r / M), q = (int)(r % M);
-    const int lm = q >> 1, slot = q & 1, l = lm_degree(lm), m = lm + 1 - l * l - l;
-    const int src = 2 * (l * l - 1 + l - m) + slot;
-    cplx v = cconj(x[c * n + (size_t)i * M + src]);
-    if (m & 1) v = cneg(v);
-    const size_t o = c * n + r;
-    y[o] = base ? csub(base[o], v) : v;
-}
-
+// ---- coarse-space helpers ------------------------------------------------------------------
 __global__ void coarse_gather_kernel(int N, int M, const cplx* __restrict__ v, cplx* __restrict__ vc) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= N * 6) return;
@@ -625,7 +587,7 @@ struct LearnedProblem::Impl {
     GraphData graph;
     Coarse coarse;
     int p = 0;
-    DevArray R1, Y, AY, Eb, U, Wt, tmp, tmp2, Tid, noskip, dTH, dP1, dP2, dP3, CGI, CGJ, DG, DHI, CHJ, DH, w, grad,
+    DevArray R1, Y, AY, Eb, U, Wt, tmp, tmp2, noskip, dTH, dP1, dP2, dP3, CGI, CGJ, DG, DHI, CHJ, DH, w, grad,
         norms, partial;
 };
 
@@ -655,7 +617,7 @@ tcu_status LearnedProblem::build(cudaStream_t st, const DevPlan& P, int L_, int 
     const Layout o = layout(L);
     for (DevArray* a : {&m.R1, &m.Y, &m.AY, &m.Eb, &m.U, &m.Wt, &m.tmp, &m.tmp2})
         if (!a->alloc(vb)) return TCU_OUT_OF_MEMORY;
-    if (!m.Tid.alloc((size_t)N * L * 4 * sizeof(cplx)) || !m.noskip.alloc(std::max<size_t>(nnz, 1)) ||
+    if (!m.noskip.alloc(std::max<size_t>(nnz, 1)) ||
         !m.dTH.alloc(nnz * o.no * 8) || !m.dP1.alloc((size_t)N * GH * 8) || !m.dP2.alloc(nnz * GH * 8) ||
         !m.dP3.alloc(nnz * GH * 8) || !m.CGI.alloc(nnz * GH * 8) || !m.CGJ.alloc(nnz * GH * 8) ||
         !m.DG.alloc((size_t)N * GH * 8) || !m.DHI.alloc((size_t)N * GH * 8) || !m.CHJ.alloc(nnz * GH * 8) ||
@@ -663,17 +625,7 @@ tcu_status LearnedProblem::build(cudaStream_t st, const DevPlan& P, int L_, int 
         !m.norms.alloc((size_t)std::max(nprobe, 64) * 8) || !m.partial.alloc((size_t)std::max(nprobe, 8) * 256 * 8))
         return TCU_OUT_OF_MEMORY;
     cudaMemsetAsync(m.noskip.p, 0, std::max<size_t>(nnz, 1), st);
-    {
-        std::vector<cplx> id((size_t)N * L * 4);
-        for (size_t b = 0; b < (size_t)N * L; ++b) {
-            id[4 * b] = mk(1.0, 0.0);
-            id[4 * b + 1] = mk(0.0, 0.0);
-            id[4 * b + 2] = mk(0.0, 0.0);
-            id[4 * b + 3] = mk(1.0, 0.0);
-        }
-        cudaMemcpyAsync(m.Tid.p, id.data(), id.size() * sizeof(cplx), cudaMemcpyHostToDevice, st);
-        if (cudaStreamSynchronize(st) != cudaSuccess) return TCU_DEVICE_ERROR;
-    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return TCU_DEVICE_ERROR;
     // coarse-corrected probes r1 = v - A[:, c] A_cc^-1 v_c, each scaled to unit norm
     for (int q = 0; q < nprobe; ++q) {
         tcu_status s = m.coarse.correct(d_V + (size_t)q * n, m.R1.as<cplx>() + (size_t)q * n, st, launches);
@@ -694,7 +646,7 @@ tcu_status LearnedProblem::probes(double2* h_out, cudaStream_t st) {
     return cudaStreamSynchronize(st) == cudaSuccess ? TCU_OK : TCU_DEVICE_ERROR;
 }
 
-// y = (I - T C) x for ncol columns, and y = (I - T C)^H x = x - F conj(C conj(F T^H x)) (C^T = F C F)
+// y = (I - T C) x for ncol columns, and y = (I - T C)^H x (adjoint.cu)
 static void op_apply(const LearnedProblem& lp, const cplx* x, cplx* y, int ncol, cudaStream_t st) {
     for (int c0 = 0; c0 < ncol; c0 += 8) {
         const int nc = std::min(8, ncol - c0);
@@ -703,24 +655,15 @@ static void op_apply(const LearnedProblem& lp, const cplx* x, cplx* y, int ncol,
         if (lp.launches) ++*lp.launches;
     }
 }
-static void op_apply_adjoint(const LearnedProblem& lp, const cplx* x, cplx* y, cplx* t1, cplx* t2, const cplx* Tid,
-                             int ncol, cudaStream_t st) {
-    const int nlm = lp.L * (lp.L + 2);
-    th_apply_kernel<<<blocks_for((size_t)lp.N * nlm * ncol, 256), 256, 0, st>>>(lp.N, lp.L, lp.d_T, x, lp.n, ncol, t1);
-    flip_conj_kernel<<<blocks_for(lp.n * ncol, 256), 256, 0, st>>>(lp.N, lp.L, t1, nullptr, lp.n, ncol, t2);
-    for (int c0 = 0; c0 < ncol; c0 += 8) {
-        const int nc = std::min(8, ncol - c0);
-        launch_apply(*lp.plan, lp.N, lp.k0, lp.d_pos, Tid, t2 + (size_t)c0 * lp.n, lp.n, nc, nullptr, 0.0, 1.0, true,
-                     t1 + (size_t)c0 * lp.n, st);
-    }
-    flip_conj_kernel<<<blocks_for(lp.n * ncol, 256), 256, 0, st>>>(lp.N, lp.L, t1, x, lp.n, ncol, y);
-    if (lp.launches) *lp.launches += 3 + (ncol + 7) / 8;
+static void op_apply_adjoint(const LearnedProblem& lp, const cplx* x, cplx* y, cplx* t1, cplx* t2, int ncol,
+                             cudaStream_t st) {
+    launch_apply_adjoint(*lp.plan, lp.N, lp.k0, lp.d_pos, lp.d_T, x, lp.n, ncol, y, t1, t2, st, lp.launches);
 }
 
 tcu_status LearnedProblem::adjoint_apply(const double2* d_x, double2* d_y, int ncol, cudaStream_t st) {
     Impl& m = *impl;
     if (ncol > m.p) return TCU_INVALID_INPUT;
-    op_apply_adjoint(*this, d_x, d_y, m.tmp.as<cplx>(), m.tmp2.as<cplx>(), m.Tid.as<cplx>(), ncol, st);
+    op_apply_adjoint(*this, d_x, d_y, m.tmp.as<cplx>(), m.tmp2.as<cplx>(), ncol, st);
     return cudaStreamSynchronize(st) == cudaSuccess && cudaGetLastError() == cudaSuccess ? TCU_OK : TCU_DEVICE_ERROR;
 }
 
@@ -743,11 +686,9 @@ tcu_status LearnedProblem::loss_grad(const double* h_weights, double* loss, doub
     vec_norms(m.Eb.as<cplx>(), n, p, m.norms.as<double>(), m.partial.as<double>(), st);
     cudaMemcpyAsync(en.data(), m.norms.p, p * 8, cudaMemcpyDeviceToHost, st);
     // U = A^H E, Wt = T^H U
-    op_apply_adjoint(*this, m.Eb.as<cplx>(), m.U.as<cplx>(), m.tmp.as<cplx>(), m.tmp2.as<cplx>(), m.Tid.as<cplx>(), p,
-                     st);
+    op_apply_adjoint(*this, m.Eb.as<cplx>(), m.U.as<cplx>(), m.tmp.as<cplx>(), m.tmp2.as<cplx>(), p, st);
     const int nlm = L * (L + 2);
-    th_apply_kernel<<<blocks_for((size_t)N_ * nlm * p, 256), 256, 0, st>>>(N_, L, d_T, m.U.as<cplx>(), n, p,
-                                                                          m.Wt.as<cplx>());
+    launch_apply_th(L, N_, d_T, m.U.as<cplx>(), n, p, m.Wt.as<cplx>(), st);
     if (nnz > 0) {
         const size_t smem = (size_t)nlm * nlm * sizeof(cplx);
         static std::atomic<unsigned long long> attr{0};

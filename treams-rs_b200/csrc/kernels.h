@@ -107,6 +107,17 @@ void pairs_init_attributes();
 void launch_translate(const DevPlan& P, size_t count, const int* labels, const cplx* args, bool helicity,
                       bool singular, cplx* out, cudaStream_t st);
 
+// adjoint.cu — y = (I - T C)^H x for ncol columns of leading dimension ldx (t1, t2: ldx x ncol
+// scratch), y = T^H x, and x <- A^-H x with the LU factors (tmp: adjoint_solve_tmp(n, ncol))
+void launch_apply_adjoint(const DevPlan& P, int N, double k0, const double* pos, const cplx* T, const cplx* x,
+                          size_t ldx, int ncol, cplx* y, cplx* t1, cplx* t2, cudaStream_t st, long long* launches);
+void launch_apply_th(int L, int N, const cplx* T, const cplx* x, size_t ldx, int ncol, cplx* y, cudaStream_t st);
+size_t adjoint_solve_tmp(int n, int ncol);
+void lu_solve_adjoint_fp64(const double2* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp,
+                           int ncol, cudaStream_t st, long long* launches);
+void lu_solve_adjoint_fp32(const float2* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp,
+                           int ncol, cudaStream_t st, long long* launches);
+
 // equil.cu — power-of-two row/column equilibration of an n x n column-major matrix (FP64 or
 // FP32 storage) when its largest entry exceeds `threshold`; r, c: n scales each.
 size_t equilibrate_scratch_doubles(int n);

@@ -91,8 +91,8 @@ __global__ void __launch_bounds__(256) assemble_kernel(DevPlan P, int N, double 
 }
 
 // ---- matrix-free operator ---------------------------------------------------------------
-// y = zadd + alpha x + beta T (C x) (singular, with T) or y = x + R x (regular overlap,
-// apply_t false, self block = identity). One CTA per destination sphere i; Q source
+// y = zadd + alpha x + beta T (C x) (singular; T null: y = zadd + alpha x + beta C x) or
+// y = x + R x (regular overlap, apply_t false, self block = identity). One CTA per destination sphere i; Q source
 // spheres in flight, thread item (slot q, destination lm d) accumulates
 // sum_s C[(d,pol),(s,pol)] x_j[(s,pol)] for p <= 8 columns; slots reduce in a fixed order.
 constexpr int APPLY_MAXCOL = 8;
@@ -153,10 +153,13 @@ __global__ void __launch_bounds__(256) apply_kernel(DevPlan P, int N, double k, 
         cplx x0 = x[c * ldx + row], x1 = x[c * ldx + row + 1];
         cplx y0, y1;
         if (singular) {
-            int lam = degree_of(dd);
-            const cplx* t4 = T + ((size_t)i * P.L + lam - 1) * 4;
-            cplx tc0 = cadd(cmul(t4[0], sp), cmul(t4[1], sn));
-            cplx tc1 = cadd(cmul(t4[2], sp), cmul(t4[3], sn));
+            cplx tc0 = sp, tc1 = sn;  // T null: the coupling alone
+            if (T) {
+                int lam = degree_of(dd);
+                const cplx* t4 = T + ((size_t)i * P.L + lam - 1) * 4;
+                tc0 = cadd(cmul(t4[0], sp), cmul(t4[1], sn));
+                tc1 = cadd(cmul(t4[2], sp), cmul(t4[3], sn));
+            }
             y0 = cadd(cscale(x0, alpha), cscale(tc0, beta));
             y1 = cadd(cscale(x1, alpha), cscale(tc1, beta));
             if (zadd) {
@@ -261,10 +264,13 @@ __global__ void __launch_bounds__(AP_THREADS) apply2_kernel(DevPlan P, int N, do
         const cplx x0 = x[c * ldx + row], x1 = x[c * ldx + row + 1];
         cplx y0, y1;
         if (singular) {
-            const int lam = degree_of(dd);
-            const cplx* t4 = T + ((size_t)i * P.L + lam - 1) * 4;
-            const cplx tc0 = cadd(cmul(t4[0], sp), cmul(t4[1], sn));
-            const cplx tc1 = cadd(cmul(t4[2], sp), cmul(t4[3], sn));
+            cplx tc0 = sp, tc1 = sn;  // T null: the coupling alone
+            if (T) {
+                const int lam = degree_of(dd);
+                const cplx* t4 = T + ((size_t)i * P.L + lam - 1) * 4;
+                tc0 = cadd(cmul(t4[0], sp), cmul(t4[1], sn));
+                tc1 = cadd(cmul(t4[2], sp), cmul(t4[3], sn));
+            }
             y0 = cadd(cscale(x0, alpha), cscale(tc0, beta));
             y1 = cadd(cscale(x1, alpha), cscale(tc1, beta));
             if (zadd) {

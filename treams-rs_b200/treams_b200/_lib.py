@@ -58,6 +58,9 @@ SIGNATURES = {
     "tcu_factor_solve": (c_int, [P, P, c_int, P, P]),
     "tcu_factor_solve_dev": (c_int, [P, P, c_int, P, P]),
     "tcu_factor_dimension": (c_size, [P]),
+    "tcu_factor_solve_adjoint": (c_int, [P, P, c_int, P, P]),
+    "tcu_factor_pullback_incident": (c_int, [P, P, c_int, P, P]),
+    "tcu_iterative_pullback_incident": (c_int, [P, c_int, c_double, c_size, P, P, P, P, c_int, P, P, P]),
     "tcu_factor_destroy": (c_int, [P]),
     "tcu_cluster_operator": (c_int, [P, c_int, c_double, c_size, P, P, P, P]),
     "tcu_cluster_apply": (c_int, [P, c_int, c_double, c_size, P, P, P, c_int, P, P]),
@@ -305,6 +308,27 @@ class InteractionFactor:
         _check(lib().tcu_factor_solve(self.handle, _p(b), b.shape[1], _p(x), certs))
         return (x[:, 0] if squeeze else x), list(certs)
 
+    def _adjoint(self, cotangent, fn):
+        g = np.asfortranarray(cotangent, np.complex128)
+        squeeze = g.ndim == 1
+        if squeeze:
+            g = g[:, None]
+        if g.shape[0] != self.dimension or g.shape[1] == 0:
+            raise ValueError("require finite channel-by-illumination columns matching the factorization")
+        out = np.zeros_like(g, order="F")
+        certs = (Certificate * g.shape[1])()
+        _check(fn(self.handle, _p(g), g.shape[1], _p(out), certs))
+        return (out[:, 0] if squeeze else out), list(certs)
+
+    def solve_adjoint(self, cotangent):
+        """Y = (I - T C)^-H G with the saved factor (Lu::solve_adjoint_in_place)."""
+        return self._adjoint(cotangent, lib().tcu_factor_solve_adjoint)
+
+    def pullback_incident(self, cotangent):
+        """Gradient of the incident columns: T^H (I - T C)^-H G
+        (InteractionFactor::pullback_incident, cluster/interaction.rs:221)."""
+        return self._adjoint(cotangent, lib().tcu_factor_pullback_incident)
+
     def close(self) -> None:
         if self.handle:
             if self.ctx.handle:
@@ -445,3 +469,19 @@ class SphereCluster:
                                          _p(self.eps), _p(self.positions), _p(b), b.shape[1], ctypes.byref(opt),
                                          PRECOND[preconditioner], _p(x), certs))
         return IterativeSolution(x[:, 0] if squeeze else x, list(certs))
+
+    def pullback_incident(self, cotangent, rtol: float = 1e-10, atol: float = 0.0, restart: int = 30,
+                          max_iterations: int = 300) -> IterativeSolution:
+        """Incident-field gradient T^H (I - T C)^-H G by adjoint GMRES (the `incident` part of
+        IterativeSphereCluster::pullback, cluster/iterative.rs:460)."""
+        g = np.asfortranarray(cotangent, np.complex128)
+        squeeze = g.ndim == 1
+        if squeeze:
+            g = g[:, None]
+        out = np.zeros_like(g, order="F")
+        certs = (Certificate * g.shape[1])()
+        opt = GmresOptions(rtol, atol, restart, max_iterations)
+        _check(lib().tcu_iterative_pullback_incident(self.ctx.handle, self.lmax, self.k0, self.radii.size,
+                                                     _p(self.radii), _p(self.eps), _p(self.positions), _p(g),
+                                                     g.shape[1], ctypes.byref(opt), _p(out), certs))
+        return IterativeSolution(out[:, 0] if squeeze else out, list(certs))
