@@ -108,7 +108,7 @@ tcu_status tcu_translation_block(tcu_context* ctx, int lmax, double k, const dou
 /* Translation coefficients of single mode pairs at complex polar arguments, the elementwise
  * sw.translate (python/treams_rs/sw.py:70; treams-core sw/polar.rs:251 polar_translation_array).
  * labels: count x 6 ints (lambda, mu, pol of the destination mode, l, m, qol of the source
- * mode; degrees 1..7); args: count x 3 complex (kr, theta, phi of k (r_destination -
+ * mode; degrees 1..10); args: count x 3 complex (kr, theta, phi of k (r_destination -
  * r_source)); out: count complex. helicity != 0: A + (2 pol - 1) B for pol == qol, else 0;
  * parity: A for pol == qol, else B. singular != 0 expands an outgoing wave (0 at kr = 0). */
 tcu_status tcu_translate(tcu_context* ctx, size_t count, const int* labels, const double* args, int helicity,
@@ -153,6 +153,16 @@ tcu_status tcu_sphere_cluster_factor_dev(tcu_context* ctx, int lmax, double k0, 
  * (tcu_context_fallbacks counts these solves). */
 tcu_status tcu_factor_solve(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
 tcu_status tcu_factor_solve_dev(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certificates);
+/* Interacting T-matrix X = (I - T C)^-1 T of the cluster (n x n, column-major, host), the
+ * solution for every column of the block-diagonal T (cluster::interaction,
+ * cluster/interaction.rs:292-315), refined in FP64 like tcu_factor_solve. */
+tcu_status tcu_factor_interacting_tmatrix(tcu_factor* f, double* X);
+/* T-matrix of the whole cluster in one spherical basis of degree lmax_global (<= 10) at origin:
+ * sum_ij R(origin <- r_i) X_ij R(r_j <- origin) with regular translations (the cluster's
+ * expand into a global basis, python/treams_rs/_operators.py:183 expand), Mg x Mg column-major
+ * (Mg = 2 lmax_global (lmax_global + 2)). Valid for scatterers outside a sphere around origin
+ * that holds all the spheres' centres. */
+tcu_status tcu_factor_global_tmatrix(tcu_factor* f, int lmax_global, const double* origin, double* out);
 /* Adjoint solve Y = (I - T C)^-H G with the factor (linalg/mod.rs:436 solve_adjoint_in_place),
  * refined in FP64 against the matrix-free adjoint operator like tcu_factor_solve; certificates
  * report ||G - (I - T C)^H Y|| and ||G||. No counterpart as a public call in the reference. */

@@ -84,3 +84,45 @@ def test_translate_rejects_bad_labels(ctx):
     with pytest.raises(ValueError, match="mode labels"):
         sw.translate(0, 0, 1, 1, 0, 1, 1.0, 0.3, 0.1, ctx=ctx)
     assert sw.translate(1, 0, 1, 1, 0, 1, 0.0, 0.3, 0.1, ctx=ctx) == 0  # singular self term
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_sic_chain_absorption_matches_the_known_answer(ctx, precision):
+    # tests/tmatrix/test_particle_cluster.py:539-562: lmax 10, entries of I - T C near 1e22
+    import treams_b200 as t
+    from test_known_answers import absorption, sic_chain
+    L, k0, radii, eps, pos = sic_chain()
+    value, rtol = [float(v) for v in next(v for k, v in read_table("known_answers.txt")
+                                          if k[0] == "sic_chain_absorption_1e12")]
+    f = t.sphere_cluster_factor(L, k0, radii, eps, pos, precision, ctx=ctx)
+    try:
+        Tg = f.global_tmatrix(10)
+    finally:
+        f.close()
+    assert absorption(Tg, k0) * 1e12 == pytest.approx(value, rel=rtol)
+    orders = np.array([m for (l, m, p) in oracle.modes(L)])
+    assert np.abs(Tg[orders[:, None] != orders[None, :]]).max() <= 2e-20
+
+
+def test_interacting_tmatrix_matches_dense_solve(ctx):
+    import treams_b200 as t
+    from treams_b200 import workloads
+    w = workloads.small_cluster()
+    A, tb = oracle.cluster_operator(w.lmax, w.k0, w.radii, w.eps, w.positions)
+    Xo = np.linalg.solve(A, oracle.apply_t(w.lmax, tb, np.eye(w.n)))
+    f = t.sphere_cluster_factor(w.lmax, w.k0, w.radii, w.eps, w.positions, "fp64", ctx=ctx)
+    try:
+        X = f.interacting_tmatrix()
+        Tg = f.global_tmatrix(3, origin=w.positions.mean(axis=0))
+    finally:
+        f.close()
+    assert np.linalg.norm(X - Xo) <= 1e-10 * np.linalg.norm(Xo)
+    # the global T-matrix: sum_ij R(o <- r_i) X_ij R(r_j <- o) with the oracle's blocks
+    M, o = 30, w.positions.mean(axis=0)
+    Tgo = np.zeros((M, M), complex)
+    for i in range(8):
+        Ri = oracle.translation_block(3, w.k0, o - w.positions[i], singular=False)
+        for j in range(8):
+            Tgo += Ri @ Xo[i * M:(i + 1) * M, j * M:(j + 1) * M] @ oracle.translation_block(
+                3, w.k0, w.positions[j] - o, singular=False)
+    assert np.linalg.norm(Tg - Tgo) <= 1e-10 * np.linalg.norm(Tgo)

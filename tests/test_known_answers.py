@@ -67,3 +67,42 @@ def test_library_wigner3j_agrees_with_the_oracle_recurrence():
             continue
         a, b = sw.wigner3j(j1, j2, j3, m1, m2, m3), oracle.wigner3j(j1, j2, j3, m1, m2, m3)
         assert abs(a - b) <= 1e-13 * max(1.0, abs(b)) and abs(a - b) <= 2e-14 + 1e-11 * abs(b)
+
+
+def sic_chain():
+    """Four 250 nm SiC spheres with 20 nm gaps on the z axis at 3 THz, lmax 10
+    (tests/tmatrix/test_particle_cluster.py:539-562)."""
+    k0 = 2 * np.pi * 3e12 / 299792458.0
+    pos = np.array([[0.0, 0.0, z * 520e-9] for z in (-1.5, -0.5, 0.5, 1.5)])
+    return 10, k0, np.full(4, 250e-9), np.full(4, 12.87707323 + 0.19225647000000007j), pos
+
+
+def absorption(Tg, k0):
+    return -2 * np.pi * (np.trace(Tg).real + np.vdot(Tg, Tg).real) / k0**2
+
+
+def test_oracle_sic_chain_absorption_matches_the_known_answer():
+    # I - T C has a unit diagonal but entries near 1e22 at degree 10: the solve equilibrates
+    # rows and columns by powers of two (as the library's factorization does), then the
+    # cluster T-matrix is expanded into the lmax-10 basis at the origin with regular
+    # translations: T_g = sum_ij R(0 <- r_i) X_ij R(r_j <- 0)
+    import scipy.linalg
+    L, k0, radii, eps, pos = sic_chain()
+    value, rtol = [float(v) for v in next(v for k, v in read_table("known_answers.txt")
+                                          if k[0] == "sic_chain_absorption_1e12")]
+    A, tb = oracle.cluster_operator(L, k0, radii, eps, pos)
+    M = 2 * L * (L + 2)
+    n = 4 * M
+    T = oracle.apply_t(L, tb, np.eye(n))
+    R = 2.0 ** -np.round(np.log2(np.abs(A).max(axis=1)))
+    A1 = A * R[:, None]
+    C = 2.0 ** -np.round(np.log2(np.abs(A1).max(axis=0)))
+    X = C[:, None] * scipy.linalg.solve(A1 * C[None, :], R[:, None] * T)
+    Tg = np.zeros((M, M), complex)
+    for i in range(4):
+        Ri = oracle.translation_block(L, k0, -pos[i], singular=False)
+        for j in range(4):
+            Tg += Ri @ X[i * M:(i + 1) * M, j * M:(j + 1) * M] @ oracle.translation_block(L, k0, pos[j], singular=False)
+    assert absorption(Tg, k0) * 1e12 == pytest.approx(value, rel=rtol)
+    orders = np.array([m for (l, m, p) in oracle.modes(L)])
+    assert np.abs(Tg[orders[:, None] != orders[None, :]]).max() <= 2e-20

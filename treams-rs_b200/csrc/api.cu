@@ -152,7 +152,7 @@ bool finite_all(const double* p, size_t n) {
 
 // cluster/spheres.rs:99-133
 tcu_status validate_spheres(int L, double k0, size_t N, const double* radii, const double* eps, const double* pos) {
-    if (L < 1 || L > 7) return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 7");
+    if (L < 1 || L > 10) return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 10");
     if (!std::isfinite(k0) || k0 <= 0.0 || N == 0 || !radii || !eps || !pos)
         return fail(TCU_INVALID_INPUT,
                     "require positive finite k0 and radii, and matching finite permittivities and positions");
@@ -186,14 +186,14 @@ tcu_status get_plan(tcu_context* ctx, int L, const DevPlan** out) {
         auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
         size_t off_combo = 0, off_w = up(ncombo * 8), off_refl = up(off_w + nterm * 16),
                off_idx = up(off_refl + h.reflection.size() * 8);
-        size_t total = off_idx + nterm + 16;
+        size_t total = off_idx + nterm * 2 + 16;
         CK(cudaMalloc(&store->mem, total), "plan allocation");
         char* base = (char*)store->mem;
         CK(cudaMemcpy(base + off_combo, h.combo.data(), ncombo * 8, cudaMemcpyHostToDevice), "plan upload");
         CK(cudaMemcpy(base + off_w, h.w.data(), nterm * 16, cudaMemcpyHostToDevice), "plan upload");
         CK(cudaMemcpy(base + off_refl, h.reflection.data(), h.reflection.size() * 8, cudaMemcpyHostToDevice),
            "plan upload");
-        CK(cudaMemcpy(base + off_idx, h.idx.data(), nterm, cudaMemcpyHostToDevice), "plan upload");
+        CK(cudaMemcpy(base + off_idx, h.idx.data(), nterm * 2, cudaMemcpyHostToDevice), "plan upload");
         DevPlan& d = store->dev;
         d.L = L;
         d.nlm = h.nlm;
@@ -202,7 +202,7 @@ tcu_status get_plan(tcu_context* ctx, int L, const DevPlan** out) {
         d.combo = (const int2*)(base + off_combo);
         d.w = (const double2*)(base + off_w);
         d.reflection = (const double*)(base + off_refl);
-        d.idx = (const uint8_t*)(base + off_idx);
+        d.idx = (const uint16_t*)(base + off_idx);
         it = ctx->plans.emplace(L, std::move(store)).first;
     }
     *out = &it->second->dev;
@@ -725,8 +725,8 @@ long long tcu_context_fallbacks(tcu_context* ctx) { return ctx ? ctx->fallbacks 
 tcu_status tcu_translation_block(tcu_context* ctx, int lmax, double k, const double* disp, int singular, int helicity,
                                  double* out) {
     if (!ctx || !disp || !out) return fail(TCU_INVALID_INPUT, "null argument");
-    if (lmax < 1 || lmax > 7 || !std::isfinite(k) || k <= 0 || !finite_all(disp, 3))
-        return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 7, positive finite k and a finite displacement");
+    if (lmax < 1 || lmax > 10 || !std::isfinite(k) || k <= 0 || !finite_all(disp, 3))
+        return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 10, positive finite k and a finite displacement");
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
     CK(cudaSetDevice(ctx->device), "device");
@@ -757,9 +757,9 @@ tcu_status tcu_translate(tcu_context* ctx, size_t count, const int* labels, cons
         const int* lb = labels + 6 * e;
         for (int side = 0; side < 2; ++side) {
             const int l = lb[3 * side], m = lb[3 * side + 1], pol = lb[3 * side + 2];
-            if (l < 1 || l > 7 || m < -l || m > l || (pol != 0 && pol != 1))
+            if (l < 1 || l > 10 || m < -l || m > l || (pol != 0 && pol != 1))
                 return fail(TCU_INVALID_INPUT,
-                            "mode labels need 1 <= degree <= 7, |order| <= degree and polarization 0 or 1");
+                            "mode labels need 1 <= degree <= 10, |order| <= degree and polarization 0 or 1");
             L = std::max(L, l);
         }
     }
@@ -789,7 +789,8 @@ tcu_status tcu_translate(tcu_context* ctx, size_t count, const int* labels, cons
 tcu_status tcu_mie_blocks(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii, const double* eps,
                           double* out) {
     if (!ctx || !radii || !eps || !out || N == 0) return fail(TCU_INVALID_INPUT, "null argument");
-    if (lmax < 1 || lmax > 7 || !std::isfinite(k0) || k0 <= 0) return fail(TCU_INVALID_INPUT, "k0 must be finite and positive");
+    if (lmax < 1 || lmax > 10 || !std::isfinite(k0) || k0 <= 0)
+        return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 10 and a finite positive k0");
     for (size_t i = 0; i < N; ++i)
         if (!std::isfinite(radii[i]) || radii[i] <= 0) return fail(TCU_INVALID_INPUT, "radii must be finite and positive");
     if (!finite_all(eps, 2 * N)) return fail(TCU_INVALID_INPUT, "permittivities must be finite");
@@ -817,7 +818,7 @@ tcu_status tcu_mie_blocks(tcu_context* ctx, int lmax, double k0, size_t N, const
 tcu_status tcu_plane_wave_expansion(tcu_context* ctx, int lmax, size_t N, const double* positions, int p,
                                     const double* kvecs, const int* pols, double* out) {
     if (!ctx || !positions || !kvecs || !pols || !out || N == 0 || p <= 0) return fail(TCU_INVALID_INPUT, "null argument");
-    if (lmax < 1 || lmax > 7) return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 7");
+    if (lmax < 1 || lmax > 10) return fail(TCU_INVALID_INPUT, "require 1 <= lmax <= 10");
     for (int c = 0; c < p; ++c)
         if (pols[c] != 0 && pols[c] != 1) return fail(TCU_INVALID_INPUT, "polarization must be 0 or 1");
     if (!finite_all(kvecs, 6 * p) || !finite_all(positions, 3 * N))
@@ -846,7 +847,7 @@ tcu_status tcu_plane_wave_expansion(tcu_context* ctx, int lmax, size_t N, const 
 tcu_status tcu_cross_sections(tcu_context* ctx, int lmax, double k0, size_t N, const double* positions, int p,
                               const double* x, const double* b, double* sca, double* ext) {
     if (!ctx || !positions || !x || !b || !sca || !ext || N == 0 || p <= 0) return fail(TCU_INVALID_INPUT, "null argument");
-    if (lmax < 1 || lmax > 7 || !std::isfinite(k0) || k0 <= 0) return fail(TCU_INVALID_INPUT, "invalid lmax or k0");
+    if (lmax < 1 || lmax > 10 || !std::isfinite(k0) || k0 <= 0) return fail(TCU_INVALID_INPUT, "invalid lmax or k0");
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
     CK(cudaSetDevice(ctx->device), "device");
@@ -914,6 +915,60 @@ tcu_status tcu_factor_solve_dev(tcu_factor* f, const double* B, int p, double* X
     return solve_impl(f, B, p, X, certificates, true);
 }
 size_t tcu_factor_dimension(const tcu_factor* f) { return f ? f->n : 0; }
+
+tcu_status tcu_factor_interacting_tmatrix(tcu_factor* f, double* X) {
+    if (!f || !X) return fail(TCU_INVALID_INPUT, "null argument");
+    const size_t n = f->n;
+    const int chunk = 256;  // columns per solve (keeps the solve buffers at 6 n chunk complex)
+    std::vector<double> eye;
+    for (size_t c0 = 0; c0 < n; c0 += chunk) {
+        const int w = (int)std::min<size_t>(chunk, n - c0);
+        eye.assign(2 * n * w, 0.0);
+        for (int c = 0; c < w; ++c) eye[2 * ((size_t)c * n + c0 + c)] = 1.0;
+        tcu_status s = solve_impl(f, eye.data(), w, X + 2 * n * c0, nullptr, false);
+        if (s) return s;
+    }
+    return TCU_OK;
+}
+
+tcu_status tcu_factor_global_tmatrix(tcu_factor* f, int lmax_global, const double* origin, double* out) {
+    if (!f || !origin || !out) return fail(TCU_INVALID_INPUT, "null argument");
+    if (lmax_global < 1 || lmax_global > 10 || !finite_all(origin, 3))
+        return fail(TCU_INVALID_INPUT, "require 1 <= lmax_global <= 10 and a finite origin");
+    tcu_context* ctx = f->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ProfGuard pg(ctx);
+    CK(cudaSetDevice(ctx->device), "device");
+    const int Lmax = std::max(f->L, lmax_global);
+    const DevPlan* P;
+    tcu_status s = get_plan(ctx, Lmax, &P);
+    if (s) return s;
+    const size_t n = f->n, Mg = 2 * (size_t)lmax_global * (lmax_global + 2);
+    DevBuf buf(ctx);
+    Arena ar;
+    size_t oO = ar.add(24), oI = ar.add(n * Mg * 16), oY = ar.add(n * Mg * 16), oE = ar.add(n * Mg * 16),
+           oT = ar.add(Mg * Mg * 16);
+    CK(buf.alloc(ar.total), "expansion buffers");
+    double* d_o = ar.at<double>(buf.p, oO);
+    cplx* Ein = ar.at<cplx>(buf.p, oI);
+    cplx* Y = ar.at<cplx>(buf.p, oY);
+    cplx* Eout = ar.at<cplx>(buf.p, oE);
+    cplx* Tg = ar.at<cplx>(buf.p, oT);
+    CK(cudaMemcpyAsync(d_o, origin, 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemsetAsync(Ein, 0, n * Mg * 16, ctx->stream), "clear");
+    CK(cudaMemsetAsync(Eout, 0, n * Mg * 16, ctx->stream), "clear");
+    launch_expand_blocks(*P, f->N, f->k0, f->d_pos, origin, f->L * (f->L + 2), lmax_global * (lmax_global + 2), Ein,
+                         Eout, ctx->stream);
+    ++ctx->launches;
+    if ((s = sync_status(ctx, "expansion blocks"))) return s;
+    // Y = (I - T C)^-1 T Ein (refined in FP64), T_global = Eout Y
+    if ((s = solve_impl(f, (const double*)Ein, (int)Mg, (double*)Y, nullptr, true))) return s;
+    launch_zgemm_small((int)Mg, (int)Mg, (int)n, Eout, Mg, Y, n, Tg, Mg, ctx->stream);
+    ++ctx->launches;
+    CK(cudaMemcpyAsync(out, Tg, Mg * Mg * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
+    (void)d_o;
+    return sync_status(ctx, "global T-matrix");
+}
 
 tcu_status tcu_factor_solve_adjoint(tcu_factor* f, const double* G, int p, double* Y, tcu_certificate* certificates) {
     return solve_adjoint_impl(f, G, p, Y, certificates, false);
@@ -1550,8 +1605,9 @@ struct tcu_learned_problem {
 extern "C" tcu_status tcu_learned_problem_create(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
                                                  const double* eps, const double* positions, int nprobe,
                                                  const double* V, tcu_learned_problem** out) {
-    if (!ctx || !out || !V || nprobe <= 0 || nprobe > 64)
-        return fail(TCU_INVALID_INPUT, "require a context, an output handle and 1 <= nprobe <= 64 probe vectors");
+    if (!ctx || !out || !V || nprobe <= 0 || nprobe > 64 || lmax < 1 || lmax > 7)
+        return fail(TCU_INVALID_INPUT,
+                    "require a context, an output handle, 1 <= lmax <= 7 and 1 <= nprobe <= 64 probe vectors");
     *out = nullptr;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
@@ -1635,7 +1691,7 @@ extern "C" tcu_status tcu_batch_solve(tcu_context* ctx, size_t count, const tcu_
     std::vector<size_t> idx(count);
     for (size_t i = 0; i < count; ++i) {
         const tcu_cluster_desc& c = clusters[i];
-        if (c.lmax < 1 || c.lmax > 7 || !c.B || !c.X || c.p <= 0)
+        if (c.lmax < 1 || c.lmax > 10 || !c.B || !c.X || c.p <= 0)
             return fail(TCU_INVALID_INPUT, "cluster " + std::to_string(i) + ": invalid lmax, incidence or output");
         idx[i] = i;
     }

@@ -571,7 +571,7 @@ tcu_status make_two_level(cudaStream_t st, bool learned, const DevPlan& P, int L
     cudaMemsetAsync(pre->noskip.p, 0, std::max<size_t>(pre->graph.nnz, 1), st);
     std::vector<double> w = weights_in;
     if (learned && w.empty()) w = learned_weights(L);
-    const bool use = learned && (int)w.size() == learned_weight_count(L);
+    const bool use = learned && L <= 7 && (int)w.size() == learned_weight_count(L);  // GNO_MAX outputs
     if (use) {
         if (!pre->weights.alloc(w.size() * 8)) return TCU_OUT_OF_MEMORY;
         cudaMemcpyAsync(pre->weights.p, w.data(), w.size() * 8, cudaMemcpyHostToDevice, st);

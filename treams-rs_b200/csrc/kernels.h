@@ -101,6 +101,13 @@ void launch_mie(int L, double k0, int N, const double* radii, const cplx* eps, c
 void launch_plane_wave(int L, int N, const double* pos, int ncol, const cplx* kvecs, const int* pols,
                        const double* lfac, cplx* out, cudaStream_t st);
 void launch_apply_t(int L, int N, const cplx* T, const cplx* x, int ncol, cplx* y, cudaStream_t st);
+// regular translation blocks between the N spheres (nlm_loc lm per sphere) and the origin
+// (nlm_glob lm), cut from blocks of the plan P (P.nlm >= both): Ein n x Mg, Eout Mg x n
+// (cleared by the caller); and a small complex FP64 GEMM C = A B (column-major)
+void launch_expand_blocks(const DevPlan& P, int N, double k, const double* pos, const double* origin, int nlm_loc,
+                          int nlm_glob, cplx* Ein, cplx* Eout, cudaStream_t st);
+void launch_zgemm_small(int m, int n, int k, const cplx* A, size_t lda, const cplx* B, size_t ldb, cplx* C,
+                        size_t ldc, cudaStream_t st);
 void pairs_init_attributes();
 // translate.cu — per-entry translation coefficients: labels 6 ints per element (lambda, mu,
 // pol, l, m, qol), args 3 complex per element (kr, theta, phi)

@@ -107,8 +107,8 @@ extern "C" tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k
     const size_t ncombo = (size_t)h.nlm * h.nlm, nterm = h.idx.size();
     // scratch layout: status | combo | weights | reflection | term indices | T blocks
     size_t o_status = 0, o_combo = 256, o_w = up256(o_combo + ncombo * 8), o_refl = up256(o_w + nterm * 16),
-           o_idx = up256(o_refl + h.reflection.size() * 8), o_t = up256(o_idx + nterm);
-    size_t need = o_t + N * (size_t)lmax * 4 * sizeof(double2);
+           o_idx = up256(o_refl + h.reflection.size() * 8), o_t = up256(o_idx + nterm * 2);
+    size_t need = o_t + N * (size_t)lmax * 4 * sizeof(double2);  // o_t follows the 2-byte term indices
     if (need > NOALLOC_BYTES)
         return noalloc_fail(TCU_INVALID_INPUT,
                             "cluster too large for the 8 MiB allocation-free scratch (N * lmax * 64 bytes plus the "
@@ -122,7 +122,7 @@ extern "C" tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k
         !ck(cudaMemcpyAsync(b + o_combo, h.combo.data(), ncombo * 8, cudaMemcpyHostToDevice, st)) ||
         !ck(cudaMemcpyAsync(b + o_w, h.w.data(), nterm * 16, cudaMemcpyHostToDevice, st)) ||
         !ck(cudaMemcpyAsync(b + o_refl, h.reflection.data(), h.reflection.size() * 8, cudaMemcpyHostToDevice, st)) ||
-        !ck(cudaMemcpyAsync(b + o_idx, h.idx.data(), nterm, cudaMemcpyHostToDevice, st)))
+        !ck(cudaMemcpyAsync(b + o_idx, h.idx.data(), nterm * 2, cudaMemcpyHostToDevice, st)))
         return noalloc_fail(TCU_DEVICE_ERROR, "copy of the translation plan into the scratch failed");
     long long pairs = (long long)N * N;
     validate_kernel<<<(unsigned)((pairs + 255) / 256), 256, 0, st>>>((int)N, radii, (const double2*)eps, positions,
@@ -145,7 +145,7 @@ extern "C" tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k
     P.combo = (const int2*)(b + o_combo);
     P.w = (const double2*)(b + o_w);
     P.reflection = (const double*)(b + o_refl);
-    P.idx = (const uint8_t*)(b + o_idx);
+    P.idx = (const uint16_t*)(b + o_idx);
     for (int c0 = 0; c0 < p; c0 += 8) {
         int nc = p - c0 < 8 ? p - c0 : 8;
         launch_apply(P, (int)N, k0, positions, T, (const double2*)x + (size_t)c0 * n, n, nc, nullptr, 1.0, -1.0, true,

@@ -286,6 +286,76 @@ __global__ void __launch_bounds__(AP_THREADS) apply2_kernel(DevPlan P, int N, do
     }
 }
 
+// ---- expansion of a cluster into one global basis ----------------------------------------
+// Regular translation blocks between every sphere and the origin o, cut from the blocks of
+// the plan's lmax (the modes of a smaller lmax are a prefix of the mode order):
+//   Ein  (n x Mg, ld n):   rows of sphere j = R(r_j <- o), local modes x global modes;
+//   Eout (Mg x n, ld Mg):  columns of sphere i = R(o <- r_i), global modes x local modes.
+// Entries between different helicities stay zero (the buffers are cleared first).
+// grid (N, 2): y = 0 builds Ein, y = 1 Eout.
+__global__ void __launch_bounds__(256) expand_kernel(DevPlan P, int N, double k, const double* __restrict__ pos,
+                                                     double ox, double oy, double oz, int nlm_loc, int nlm_glob,
+                                                     cplx* __restrict__ Ein, cplx* __restrict__ Eout) {
+    extern __shared__ cplx ex_Z[];
+    const int i = blockIdx.x, out_side = blockIdx.y;
+    const double dx = pos[3 * i] - ox, dy = pos[3 * i + 1] - oy, dz = pos[3 * i + 2] - oz;
+    if (threadIdx.x < 32) {
+        if (out_side)
+            pair_table(P, k, -dx, -dy, -dz, false, ex_Z, threadIdx.x);
+        else
+            pair_table(P, k, dx, dy, dz, false, ex_Z, threadIdx.x);
+    }
+    __syncthreads();
+    const int Ml = 2 * nlm_loc, Mg = 2 * nlm_glob;
+    const size_t n = (size_t)N * Ml;
+    const int nd = out_side ? nlm_glob : nlm_loc, ns = out_side ? nlm_loc : nlm_glob;
+    for (int t = threadIdx.x; t < nd * ns; t += blockDim.x) {
+        const int s = t / nd, d = t - s * nd;
+        cplx A, B;
+        combo_sums(P, s * P.nlm + d, ex_Z, A, B);
+        const cplx cp = cadd(A, B), cn = csub(A, B);
+        if (out_side) {  // row 2d (+1) of the global modes, column i Ml + 2s (+1)
+            cplx* c0 = Eout + ((size_t)i * Ml + 2 * s) * Mg;
+            c0[2 * d] = cp;
+            c0[Mg + 2 * d + 1] = cn;
+        } else {  // row j Ml + 2d (+1), column 2s (+1) of the global modes
+            cplx* c0 = Ein + (size_t)(2 * s) * n + (size_t)i * Ml;
+            c0[2 * d] = cp;
+            c0[n + 2 * d + 1] = cn;
+        }
+    }
+}
+
+// C (m x n) = A (m x k) B (k x n), complex FP64, column-major with leading dimensions; 16 x 16
+// tiles through shared memory, fixed summation order.
+__global__ void zgemm_small_kernel(int m, int n, int kk, const cplx* __restrict__ A, size_t lda,
+                                   const cplx* __restrict__ B, size_t ldb, cplx* __restrict__ C, size_t ldc) {
+    __shared__ cplx As[16][17], Bs[16][17];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int row = blockIdx.x * 16 + tx, col = blockIdx.y * 16 + ty;
+    cplx acc = mk(0.0, 0.0);
+    for (int k0 = 0; k0 < kk; k0 += 16) {
+        As[ty][tx] = (row < m && k0 + ty < kk) ? A[(size_t)(k0 + ty) * lda + row] : mk(0.0, 0.0);
+        Bs[ty][tx] = (col < n && k0 + tx < kk) ? B[(size_t)col * ldb + k0 + tx] : mk(0.0, 0.0);
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 16; ++q) cfma(acc, As[q][tx], Bs[ty][q]);
+        __syncthreads();
+    }
+    if (row < m && col < n) C[(size_t)col * ldc + row] = acc;
+}
+
+void launch_expand_blocks(const DevPlan& P, int N, double k, const double* pos, const double* origin, int nlm_loc,
+                          int nlm_glob, cplx* Ein, cplx* Eout, cudaStream_t st) {
+    expand_kernel<<<dim3(N, 2), 256, P.tsize * sizeof(cplx), st>>>(P, N, k, pos, origin[0], origin[1], origin[2],
+                                                                  nlm_loc, nlm_glob, Ein, Eout);
+}
+
+void launch_zgemm_small(int m, int n, int k, const cplx* A, size_t lda, const cplx* B, size_t ldb, cplx* C,
+                        size_t ldc, cudaStream_t st) {
+    zgemm_small_kernel<<<dim3((m + 15) / 16, (n + 15) / 16), dim3(16, 16), 0, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
+}
+
 // ---- single translation block (tests and the per-block API) -------------------------------
 __global__ void block_kernel(DevPlan P, double k, double dx, double dy, double dz, bool singular, bool helicity,
                              cplx* out) {
@@ -581,6 +651,19 @@ static int apply2_cols(const DevPlan& P) {
 void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                   int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st) {
     StageScope sc(ST_APPLY, st);
+    if (P.nlm > 64) {
+        // lmax 8..10: the slot-major kernel's tables no longer fit; Q = 256 / nlm source slots
+        // per CTA with one destination lm per thread
+        const int Q = std::max(1, 256 / P.nlm);
+        for (int c0 = 0; c0 < ncol; c0 += APPLY_MAXCOL) {
+            const int nc = std::min(APPLY_MAXCOL, ncol - c0);
+            const size_t smem = ((size_t)Q * P.tsize + (size_t)Q * P.nlm * 2 * nc) * sizeof(cplx);
+            apply_kernel<<<N, 256, smem, st>>>(P, N, k, pos, T, x + (size_t)c0 * ldx, ldx, nc,
+                                               zadd ? zadd + (size_t)c0 * ldx : nullptr, alpha, beta, singular,
+                                               y + (size_t)c0 * ldx, Q);
+        }
+        return;
+    }
     const int per = apply2_cols(P);
     for (int c0 = 0; c0 < ncol; c0 += per) {
         const int nc = std::min(per, ncol - c0);

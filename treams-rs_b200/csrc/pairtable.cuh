@@ -6,7 +6,7 @@
 
 namespace tcu {
 
-constexpr int MAXP = 16;  // radial orders p <= 2 lmax <= 14 (+1)
+constexpr int MAXP = 22;  // radial orders p <= 2 lmax <= 20 (+1)
 
 // ---- per-pair harmonic table ------------------------------------------------------------
 // One warp fills Z (tsize complex) for displacement d = r_dest - r_src. Lanes 0..order each

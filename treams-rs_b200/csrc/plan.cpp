@@ -11,7 +11,7 @@
 //      sqrt(...) (l lambda p; m -mu mu-m) (l lambda p-1; 0 0 0),  p = l+lambda-1, ...
 // down to max(|l-lambda| (+1 for B), |m-mu|) (coupling.rs:146-160). The Wigner 3j symbols
 // here come from Racah's closed formula evaluated in binary128, exact to far below double
-// rounding for the degrees a plan uses (<= 2 * 16), instead of the reference's recurrence.
+// rounding for the degrees a plan uses (<= 2 * 10), instead of the reference's recurrence.
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -102,7 +102,7 @@ HostPlan build_plan(int L) {
                     double re, im;
                     ipow(lam - l + p, re, im);
                     if (mag * mag * (re * re + im * im) > 0.0) {
-                        plan.idx.push_back((uint8_t)(p * p + p + m - mu));
+                        plan.idx.push_back((uint16_t)(p * p + p + m - mu));
                         plan.w.push_back(mag * re);
                         plan.w.push_back(mag * im);
                         counts[cross] += 1;

@@ -13,7 +13,7 @@ namespace tcu {
 struct HostPlan {
     int L = 0, nlm = 0, order = 0;
     std::vector<int> combo;
-    std::vector<uint8_t> idx;
+    std::vector<uint16_t> idx;
     std::vector<double> w;
     std::vector<double> reflection;  // (order+1)^2 negative-order factors, table order
 };
@@ -25,7 +25,7 @@ double wigner3j_racah(int j1, int j2, int j3, int m1, int m2, int m3);
 struct DevPlan {
     int L, nlm, order, tsize;  // tsize = (order + 1)^2
     const int2* combo;
-    const uint8_t* idx;
+    const uint16_t* idx;
     const double2* w;
     const double* reflection;
 };

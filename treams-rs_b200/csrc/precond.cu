@@ -124,11 +124,26 @@ class BlockJacobiPre : public Preconditioner {
     }
 };
 
+// One-sphere blocks (more than PB_MAXMODES modes per sphere): (I - T C)_ii = I, the identity.
+class IdentityPre : public Preconditioner {
+   public:
+    size_t n = 0;
+    void apply(const cplx* in, cplx* out, cudaStream_t st) override {
+        cudaMemcpyAsync(out, in, n * sizeof(cplx), cudaMemcpyDeviceToDevice, st);
+    }
+};
+
 }  // namespace
 
 tcu_status make_block_jacobi(cudaStream_t st, const DevPlan& P, int N, double k0, const double* d_pos,
                              const double* h_pos, const double* h_radii, const double2* d_T,
                              std::unique_ptr<Preconditioner>* out, long long* launches) {
+    if (2 * P.nlm > PB_MAXMODES) {
+        auto id = std::make_unique<IdentityPre>();
+        id->n = (size_t)N * 2 * P.nlm;
+        *out = std::move(id);
+        return TCU_OK;
+    }
     auto pre = std::make_unique<BlockJacobiPre>();
     BlockJacobiPre& p = *pre;
     p.M = 2 * P.nlm;

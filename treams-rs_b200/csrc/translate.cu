@@ -15,7 +15,7 @@ namespace tcu {
 
 namespace {
 
-constexpr int TR_MAXP = 15;  // term degrees p <= l + lambda <= 14
+constexpr int TR_MAXP = 21;  // term degrees p <= l + lambda <= 20
 
 // Outgoing h_0..h_last(z) at complex z != 0. |z| >= 0.5: upward recurrence of h itself from
 // h_-1 = e^{iz}/z, h_0 = -i e^{iz}/z (DLMF 10.49.6, 10.51.1; stable, h is the dominant

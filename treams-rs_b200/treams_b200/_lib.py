@@ -59,6 +59,8 @@ SIGNATURES = {
     "tcu_factor_solve_dev": (c_int, [P, P, c_int, P, P]),
     "tcu_factor_dimension": (c_size, [P]),
     "tcu_factor_solve_adjoint": (c_int, [P, P, c_int, P, P]),
+    "tcu_factor_interacting_tmatrix": (c_int, [P, P]),
+    "tcu_factor_global_tmatrix": (c_int, [P, c_int, P, P]),
     "tcu_factor_pullback_incident": (c_int, [P, P, c_int, P, P]),
     "tcu_iterative_pullback_incident": (c_int, [P, c_int, c_double, c_size, P, P, P, P, c_int, P, P, P]),
     "tcu_factor_destroy": (c_int, [P]),
@@ -319,6 +321,21 @@ class InteractionFactor:
         certs = (Certificate * g.shape[1])()
         _check(fn(self.handle, _p(g), g.shape[1], _p(out), certs))
         return (out[:, 0] if squeeze else out), list(certs)
+
+    def interacting_tmatrix(self) -> np.ndarray:
+        """X = (I - T C)^-1 T, (n, n) (cluster::interaction, cluster/interaction.rs:292)."""
+        X = np.zeros((self.dimension, self.dimension), np.complex128, order="F")
+        _check(lib().tcu_factor_interacting_tmatrix(self.handle, _p(X)))
+        return X
+
+    def global_tmatrix(self, lmax_global: int, origin=(0.0, 0.0, 0.0)) -> np.ndarray:
+        """The cluster's T-matrix in one spherical basis of degree lmax_global at origin
+        (the expand of a cluster T-matrix into SphericalBasis.default(lmax_global))."""
+        o = np.ascontiguousarray(origin, np.float64)
+        Mg = 2 * lmax_global * (lmax_global + 2)
+        out = np.zeros((Mg, Mg), np.complex128, order="F")
+        _check(lib().tcu_factor_global_tmatrix(self.handle, int(lmax_global), _p(o), _p(out)))
+        return out
 
     def solve_adjoint(self, cotangent):
         """Y = (I - T C)^-H G with the saved factor (Lu::solve_adjoint_in_place)."""
