@@ -275,6 +275,11 @@ tcu_status tcu_learned_problem_destroy(tcu_learned_problem* p);
  * per cell), eta (0 = automatic split, cell.rs:164-175). out nk x (lmax_sum+1)^2. */
 tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
                               const double* kpars, double eta, double* out);
+/* The same at a shift r (lattice::sum with shift, lattice/mod.rs:283): D_lm(k, kpar, r) =
+ * sum'_R h_l(k|r+R|) Y_lm(-r-R) e^{i kpar.R}, r in the lattice plane (r[2] = 0; off-plane
+ * shifts are rejected), reduced into the cell on the host (lattice/ewald.rs:610-665). */
+tcu_status tcu_lsumsw2d_shift_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
+                                    const double* kpars, const double* shift, double eta, double* out);
 /* Periodic array of one sphere per cell: X(kpar) = (I - T S(kpar))^-1 T for nk Bloch
  * vectors (cluster/interaction.rs:292 with sw::lattice_expansion, sw/expansion.rs:418).
  * out nk x M x M (column-major per kpar). */

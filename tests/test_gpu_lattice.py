@@ -100,3 +100,21 @@ def test_array_solve_small_lmax_lossy(ctx):
 def test_array_solve_rejects_touching_spheres(ctx):
     with pytest.raises(ValueError, match="overlap"):
         tl.array_solve_batch(2, 2.0, 0.6, 4.0, np.eye(2), np.array([[0.1, 0.2]]), ctx=ctx)
+
+
+@pytest.mark.parametrize("shift", [(0.3, 0.1, 0.0), (-0.45, 0.2, 0.0), (2.4, -1.3, 0.0)])
+def test_shifted_lattice_sums_match_oracle(ctx, shift):
+    # in-plane shifts (two sphere positions of a multi-sphere cell); the last one lies outside
+    # the cell and is reduced into it with the Bloch phase e^{-i kpar.R0} (lattice/ewald.rs:610-665)
+    lat = np.array([[1.0, 0.0], [0.5, math.sqrt(3) / 2]])
+    kps = np.array([[0.3, -0.2], [1.1, 0.4], [-2.0, 0.7]])
+    D = tl.lsumsw2d_batch(8, 2.7, lat, kps, shift=shift, ctx=ctx)
+    for i, kp in enumerate(kps):
+        ref = oracle.lsumsw2d_table(8, 2.7, lat, kp, r=shift)
+        assert np.max(np.abs(D[i] - ref)) <= 1e-11 * max(1.0, np.max(np.abs(ref))), (shift, i)
+
+
+def test_shifted_sums_reject_off_plane_shifts(ctx):
+    lat = np.eye(2)
+    with pytest.raises(ValueError, match="lattice plane"):
+        tl.lsumsw2d_batch(2, 2.0, lat, [[0.1, 0.2]], shift=(0.1, 0.0, 0.2), ctx=ctx)

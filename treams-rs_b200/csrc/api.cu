@@ -1330,6 +1330,9 @@ double log_fact(int n) { return std::lgamma((double)n + 1.0); }
 // cutoff, reciprocal vectors within the reciprocal cutoff, and the per-(l, m) constants.
 struct LatticeSetup {
     double eta = 0, area = 0;
+    double sx = 0, sy = 0;      // in-plane shift reduced into the cell, r' = r - R0
+    double R0x = 0, R0y = 0;    // the lattice vector taken off (Bloch phase e^{-i kpar.R0})
+    bool at_origin = true;      // r' = 0: the self term, and no R = 0 real-space term
     std::vector<double2> R, G;
     std::vector<double> norm, reflection, coef;
     std::vector<double2> pref;
@@ -1337,7 +1340,7 @@ struct LatticeSetup {
 };
 
 tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const double* kpars, double eta_in,
-                         LatticeSetup& S) {
+                         LatticeSetup& S, const double* shift = nullptr) {
     if (lsum < 0 || lsum > LS_MAXL) return fail(TCU_INVALID_INPUT, "require 0 <= lmax_sum <= 14");
     if (!std::isfinite(k) || k <= 0.0)
         return fail(TCU_INVALID_INPUT, "the device lattice sums take a positive real wavenumber");
@@ -1358,6 +1361,17 @@ tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const
         return fail(TCU_INVALID_INPUT,
                     "Ewald split too small for the device lattice sums (require 1/(2 eta^2) <= 8); eta = 0 selects one");
     S.eta = eta;
+    if (shift) {
+        // reduce the shift into the cell (lattice/ewald.rs:610-665): r' = r - R0 with R0 the lattice
+        // vector of the rounded fractional coordinates, and the phase e^{-i kpar.R0} on the result
+        const double f0 = (a2y * shift[0] - a2x * shift[1]) / det, f1 = (-a1y * shift[0] + a1x * shift[1]) / det;
+        const double c0 = std::round(f0), c1 = std::round(f1);
+        S.R0x = c0 * a1x + c1 * a2x;
+        S.R0y = c0 * a1y + c1 * a2y;
+        S.sx = shift[0] - S.R0x;
+        S.sy = shift[1] - S.R0y;
+        S.at_origin = S.sx == 0.0 && S.sy == 0.0;
+    }
     const double ke = k * eta;
     // real space: Gaussian factor e^{-(k eta)^2 R^2/2 + c} below e^-46 times the polynomial growth
     double Rc = std::sqrt(2.0 * (46.0 + c) / (ke * ke));
@@ -1367,14 +1381,15 @@ tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const
                        (ke * ke));
     const double len1 = std::hypot(a1x, a1y), len2 = std::hypot(a2x, a2y);
     const double hdir = S.area / std::max(len1, len2);
-    long Nd = (long)std::ceil(Rc / hdir) + 1;
+    const double rin = std::hypot(S.sx, S.sy);
+    long Nd = (long)std::ceil((Rc + rin) / hdir) + 1;
     if (Nd > 64) return fail(TCU_INVALID_INPUT, "lattice too elongated for the device lattice sums");
-    for (long s = 1; s <= Nd; ++s)  // cube shells, fixed order
+    for (long s = S.at_origin ? 1 : 0; s <= Nd; ++s)  // cube shells, fixed order; R = 0 when shifted
         for (long n1 = -s; n1 <= s; ++n1)
             for (long n2 = -s; n2 <= s; ++n2) {
                 if (std::max(std::labs(n1), std::labs(n2)) != s) continue;
                 double x = n1 * a1x + n2 * a2x, y = n1 * a1y + n2 * a2y;
-                if (std::hypot(x, y) <= Rc) S.R.push_back(make_double2(x, y));
+                if (std::hypot(x + S.sx, y + S.sy) <= Rc) S.R.push_back(make_double2(x, y));
             }
     // reciprocal: e^{-v} (q/k)^lsum (2 eta^2)^n below e^-46
     const double b1x = 2 * M_PI * a2y / det, b1y = -2 * M_PI * a2x / det;
@@ -1457,7 +1472,7 @@ tcu_status lattice_sums_device(tcu_context* ctx, int lsum, double k, const Latti
     CK(cudaMemcpyAsync(ar.at<void>(b, oP), S.pref.data(), T * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
     double2* tab = ar.at<double2>(b, oTab);
-    launch_real_table(lsum, k, S.eta, (int)S.R.size(), ar.at<double2>(b, oR), ar.at<double>(b, oN),
+    launch_real_table(lsum, k, S.eta, (int)S.R.size(), ar.at<double2>(b, oR), S.sx, S.sy, ar.at<double>(b, oN),
                       ar.at<double>(b, oRf), tab, ctx->stream);
     ++ctx->launches;
     LatticeSumArgs a;
@@ -1471,7 +1486,11 @@ tcu_status lattice_sums_device(tcu_context* ctx, int lsum, double k, const Latti
     a.G = ar.at<double2>(b, oG);
     a.coef = ar.at<double>(b, oC);
     a.pref = ar.at<double2>(b, oP);
-    a.self0 = S.self0;
+    a.self0 = S.at_origin ? S.self0 : make_double2(0.0, 0.0);
+    a.sx = S.sx;
+    a.sy = S.sy;
+    a.R0x = S.R0x;
+    a.R0y = S.R0y;
     a.nk = (int)nk;
     a.kpar = d_kpar;
     a.out = d_out;
@@ -1529,14 +1548,18 @@ tcu_status array_solve_device(tcu_context* ctx, int lmax, double k0, double radi
 
 }  // namespace
 
-extern "C" tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
-                                         const double* kpars, double eta, double* out) {
-    if (!ctx || !out) return fail(TCU_INVALID_INPUT, "null context or output");
+extern "C" tcu_status tcu_lsumsw2d_shift_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice,
+                                               size_t nk, const double* kpars, const double* shift, double eta,
+                                               double* out) {
+    if (!ctx || !out || !shift) return fail(TCU_INVALID_INPUT, "null context, shift or output");
+    if (!finite_all(shift, 3)) return fail(TCU_INVALID_INPUT, "the shift must be finite");
+    if (shift[2] != 0.0)
+        return fail(TCU_INVALID_INPUT, "the device lattice sums take shifts in the lattice plane (r_z = 0)");
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
     ProfGuard pg(ctx);
     LatticeSetup S;
-    tcu_status s = lattice_setup(lmax_sum, k, lattice, nk, kpars, eta, S);
+    tcu_status s = lattice_setup(lmax_sum, k, lattice, nk, kpars, eta, S, shift);
     if (s) return s;
     const int T = (lmax_sum + 1) * (lmax_sum + 1);
     Arena ar;
@@ -1549,6 +1572,12 @@ extern "C" tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double 
         return s;
     CK(cudaMemcpyAsync(out, ar.at<void>(io.p, oO), nk * T * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
     return sync_status(ctx, "lattice sums");
+}
+
+extern "C" tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
+                                         const double* kpars, double eta, double* out) {
+    const double zero[3] = {0.0, 0.0, 0.0};
+    return tcu_lsumsw2d_shift_batch(ctx, lmax_sum, k, lattice, nk, kpars, zero, eta, out);
 }
 
 extern "C" tcu_status tcu_array_solve_batch(tcu_context* ctx, int lmax, double k0, double radius, const double* eps,

@@ -132,7 +132,7 @@ tcu_status equilibrate(void* A, bool fp32, int n, double threshold, double* r, d
                        bool* applied, cudaStream_t st, long long* launches);
 void scale_rows(cplx* v, const double* s, size_t n, int ncol, cudaStream_t st);
 
-// lattice.cu — 2D lattice sums at shift 0 and the batched periodic-array solve
+// lattice.cu — 2D lattice sums (in-plane shift) and the batched periodic-array solve
 constexpr int LS_MAXL = 14;                // largest degree of a lattice sum
 constexpr int LS_NMAX = LS_MAXL / 2 + 1;   // reciprocal orders n per (l, m) in the plane
 struct LatticeSumArgs {
@@ -145,15 +145,17 @@ struct LatticeSumArgs {
     const double2* G = nullptr;
     const double* coef = nullptr;          // T x LS_NMAX in-plane polynomial coefficients
     const double2* pref = nullptr;         // T reciprocal prefactors
-    double2 self0{0, 0};                   // self term of l = 0
+    double2 self0{0, 0};                   // self term of l = 0 (zero for a nonzero shift)
+    double sx = 0, sy = 0;                 // in-plane shift r' (reciprocal phase e^{-i q.r'})
+    double R0x = 0, R0y = 0;               // lattice vector taken off the shift: e^{-i kpar.R0}
     int nk = 0;
     const double2* kpar = nullptr;
     double2* out = nullptr;                // out[kp * ldo + l*l+l+m]
     size_t ldo = 0;
     int* status = nullptr;                 // 9: a diffraction order on its threshold
 };
-void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, const double* norm,
-                       const double* reflection, double2* tab, cudaStream_t st);
+void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, double sx, double sy,
+                       const double* norm, const double* reflection, double2* tab, cudaStream_t st);
 size_t lattice_sum_smem(int lsum, int NR);
 void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st);
 size_t array_solve_smem(int L);

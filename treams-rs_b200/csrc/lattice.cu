@@ -1,14 +1,15 @@
-// 2D Ewald lattice sums of outgoing spherical waves for one sphere per cell (shift 0, real
-// wavenumber, real split) and the batched periodic-array solve X = (I - T S)^-1 T.
+// 2D Ewald lattice sums of outgoing spherical waves at an in-plane shift r (real wavenumber,
+// real split) and the batched periodic-array solve X = (I - T S)^-1 T (one sphere per cell).
 //
-// D_lm(k, kpar, 0) = sum'_R h_l(k|R|) Y_lm(-R) e^{i kpar.R} (lattice/mod.rs:11-15) is split
-// at eta (lattice/ewald.rs:39-270) into
-//   real space  sum_R e^{i kpar.R} Treal_lm(R),  Treal_lm(R) = -i sqrt(2/pi) k^l |R|^l
-//               Y_lm(-R/|R|) I_2l(k|R|, eta)                         (lattice/real.rs:149-187)
+// D_lm(k, kpar, r) = sum'_R h_l(k|r+R|) Y_lm(-r-R) e^{i kpar.R} (lattice/mod.rs:11-15), with r
+// first reduced into the cell (r' = r - R0, a factor e^{-i kpar.R0}; lattice/ewald.rs:610-665), is
+// split at eta (lattice/ewald.rs:39-270) into
+//   real space  sum_R e^{i kpar.R} Treal_lm(r'+R), Treal_lm(rho) = -i sqrt(2/pi) k^l |rho|^l
+//               Y_lm(-rho/|rho|) I_2l(k|rho|, eta), R = 0 included for r' != 0 (real.rs:149-187)
 //   reciprocal  sum_G pref_lm az^|m| sum_n (2 eta^2)^n/(sqrt2 eta) F_(1/2-n)(v, 0) S_lmn(beta^2)
 //               with q = kpar + G, beta^2 = q.q/k^2, v = (beta^2 - 1)/(2 eta^2),
-//               az = (q_x +- i q_y)/k                                (lattice/reciprocal.rs:288-334)
-//   self term   at l = 0                                             (lattice/reciprocal.rs:467-487)
+//               az = (q_x +- i q_y)/k, times e^{-i q.r'}             (lattice/reciprocal.rs:288-334)
+//   self term   at l = 0, for r' = 0 only                            (lattice/reciprocal.rs:467-487)
 // In the lattice plane only the n with s = 2n of S_lmn survive, so l - |m| odd sums vanish and
 // n runs to (l - |m|)/2 (reciprocal.rs:22-60).
 //
@@ -76,7 +77,7 @@ __device__ double scaled_gamma_low(double d, double a) {
 
 // One warp per lattice point: Treal_lm(R) for every l <= lsum, |m| <= l.
 __global__ void __launch_bounds__(128) real_table_kernel(int lsum, double k, double eta, int NR,
-                                                         const double2* __restrict__ R,
+                                                         const double2* __restrict__ R, double sx, double sy,
                                                          const double* __restrict__ norm,
                                                          const double* __restrict__ reflection,
                                                          double2* __restrict__ tab) {
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(128) real_table_kernel(int lsum, double k, dou
     const int T = (lsum + 1) * (lsum + 1);
     const double2 p = R[r];
     double dist, u[3];
-    unit_direction(-p.x, -p.y, 0.0, dist, u);
+    unit_direction(-p.x - sx, -p.y - sy, 0.0, dist, u);  // rho = -r' - R
     const double a = 0.5 * (k * dist * eta) * (k * dist * eta), c = 0.5 / (eta * eta);
     // ladder[i] = R(lsum + 1/2 - i)
     const int nlad = lsum + 1 + LS_JMAX;
@@ -168,7 +169,8 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
     double2* ph = ls_smem;                               // NR
     double2* gF = ph + A.NR;                             // LS_CHUNK * (nmax + 1)
     double2* gaz = gF + LS_CHUNK * (A.lsum / 2 + 1);     // LS_CHUNK
-    double* gb2 = (double*)(gaz + LS_CHUNK);             // LS_CHUNK
+    double2* gph = gaz + LS_CHUNK;                       // LS_CHUNK: e^{-i q.r'}
+    double* gb2 = (double*)(gph + LS_CHUNK);             // LS_CHUNK
     const int T = (A.lsum + 1) * (A.lsum + 1), nmax = A.lsum / 2;
     const int tid = threadIdx.x;
     for (int kp = blockIdx.x; kp < A.nk; kp += gridDim.x) {
@@ -208,6 +210,9 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
                 }
                 gb2[tid] = b2;
                 gaz[tid] = mk(qx / A.k, qy / A.k);
+                double ps, pc;
+                sincos(-(qx * A.sx + qy * A.sy), &ps, &pc);
+                gph[tid] = mk(pc, ps);
             }
             __syncthreads();
             if (active && even) {
@@ -226,14 +231,16 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
                     if (m < 0) az.y = -az.y;
                     cplx azm = mk(1.0, 0.0);
                     for (int q = 0; q < am; ++q) azm = cmul(azm, az);
-                    cfma(rec, s, azm);
+                    cfma(rec, s, cmul(azm, gph[t]));
                 }
             }
         }
         if (active) {
             cplx v = cadd(acc, cmul(A.pref[lm], rec));
             if (lm == 0) v = cadd(v, A.self0);
-            A.out[(size_t)kp * A.ldo + lm] = v;
+            double cs, cc;  // e^{-i kpar.R0} of the shift reduced into the cell
+            sincos(-(kpar.x * A.R0x + kpar.y * A.R0y), &cs, &cc);
+            A.out[(size_t)kp * A.ldo + lm] = cmul(v, mk(cc, cs));
         }
         __syncthreads();
     }
@@ -313,14 +320,14 @@ __global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const doubl
 
 }  // namespace
 
-void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, const double* norm,
-                       const double* reflection, double2* tab, cudaStream_t st) {
+void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, double sx, double sy,
+                       const double* norm, const double* reflection, double2* tab, cudaStream_t st) {
     StageScope sc(ST_LATTICE, st);
-    real_table_kernel<<<(NR + 3) / 4, 128, 0, st>>>(lsum, k, eta, NR, R, norm, reflection, tab);
+    real_table_kernel<<<(NR + 3) / 4, 128, 0, st>>>(lsum, k, eta, NR, R, sx, sy, norm, reflection, tab);
 }
 
 size_t lattice_sum_smem(int lsum, int NR) {
-    return (size_t)NR * 16 + (size_t)LS_CHUNK * (lsum / 2 + 1) * 16 + LS_CHUNK * 16 + LS_CHUNK * 8;
+    return (size_t)NR * 16 + (size_t)LS_CHUNK * (lsum / 2 + 1) * 16 + 2 * LS_CHUNK * 16 + LS_CHUNK * 8;
 }
 
 void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st) {

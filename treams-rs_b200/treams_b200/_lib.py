@@ -76,6 +76,7 @@ SIGNATURES = {
     "tcu_learned_problem_probes": (c_int, [P, P]),
     "tcu_learned_problem_destroy": (c_int, [P]),
     "tcu_lsumsw2d_batch": (c_int, [P, c_int, c_double, P, c_size, P, c_double, P]),
+    "tcu_lsumsw2d_shift_batch": (c_int, [P, c_int, c_double, P, c_size, P, P, c_double, P]),
     "tcu_array_solve_batch": (c_int, [P, c_int, c_double, c_double, P, P, c_size, P, c_double, P]),
 }
 

@@ -6,14 +6,20 @@ import numpy as np
 from ._lib import _check, _p, default_context, lib
 
 
-def lsumsw2d_batch(lmax_sum: int, k: float, lattice, kpars, eta: float = 0.0, ctx=None) -> np.ndarray:
-    """D_lm for every l <= lmax_sum (table index l*l+l+m) and every Bloch vector (nk, 2),
-    one sphere per cell (shift 0)."""
+def lsumsw2d_batch(lmax_sum: int, k: float, lattice, kpars, eta: float = 0.0, shift=None, ctx=None) -> np.ndarray:
+    """D_lm(k, kpar, r) for every l <= lmax_sum (table index l*l+l+m) and every Bloch vector
+    (nk, 2) (lattice.lsumsw2d, lattice::sum); shift r in the lattice plane (default 0)."""
     ctx = ctx or default_context()
     a = np.ascontiguousarray(lattice, np.float64).reshape(2, 2)
     kp = np.ascontiguousarray(kpars, np.float64).reshape(-1, 2)
     out = np.zeros((kp.shape[0], (lmax_sum + 1) ** 2), np.complex128)
-    _check(lib().tcu_lsumsw2d_batch(ctx.handle, lmax_sum, float(k), _p(a), kp.shape[0], _p(kp), float(eta), _p(out)))
+    if shift is None:
+        _check(lib().tcu_lsumsw2d_batch(ctx.handle, lmax_sum, float(k), _p(a), kp.shape[0], _p(kp), float(eta),
+                                        _p(out)))
+    else:
+        r = np.ascontiguousarray(shift, np.float64).reshape(3)
+        _check(lib().tcu_lsumsw2d_shift_batch(ctx.handle, lmax_sum, float(k), _p(a), kp.shape[0], _p(kp), _p(r),
+                                              float(eta), _p(out)))
     return out
 
 
