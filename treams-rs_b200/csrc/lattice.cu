@@ -246,10 +246,160 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
     }
 }
 
+// ---- blocked shared-memory LU of the periodic-array kernel -------------------------------
+// A (M x M column-major, shared, M <= 128) = P^T L U with partial pivoting (largest modulus,
+// lowest row on ties), in panels of BP = 16 columns: warp 0 factors the panel (pivot search by
+// shuffles, swaps, scaling and rank-1 updates inside the panel with warp-level synchronisation
+// only), then every thread applies the panel's interchanges to the other columns, forms
+// U12 = L11^-1 A12 (thread per column) and the rank-16 trailing update (thread per entry).
+// dinv receives 1 / U[i][i]. Returns false on every thread for an exactly zero pivot.
+constexpr int BP = 16;
+__device__ bool blocked_lu(double2* A, int M, int* piv, double2* dinv, int* sing) {
+    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) *sing = 0;
+    __syncthreads();
+    for (int k0 = 0; k0 < M; k0 += BP) {
+        const int w = min(BP, M - k0), k1 = k0 + w;
+        if (warp == 0) {
+            for (int c = k0; c < k1; ++c) {
+                double best = -1.0;
+                int bi = c;
+                for (int i = c + lane; i < M; i += 32) {
+                    const double v = cabs2(A[c * M + i]);
+                    if (v > best) {
+                        best = v;
+                        bi = i;
+                    }
+                }
+                for (int off = 16; off > 0; off >>= 1) {
+                    const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                    if (ov > best || (ov == best && oi < bi)) {
+                        best = ov;
+                        bi = oi;
+                    }
+                }
+                if (lane == 0) {
+                    piv[c] = bi;
+                    if (!(best > 0.0)) *sing = 1;
+                }
+                if (bi != c && lane < w) {  // swap rows c and bi inside the panel
+                    const int j = k0 + lane;
+                    const double2 t = A[j * M + c];
+                    A[j * M + c] = A[j * M + bi];
+                    A[j * M + bi] = t;
+                }
+                __syncwarp();
+                const cplx d = A[c * M + c];
+                if (cabs2(d) > 0.0) {
+                    const cplx inv = cinv(d);
+                    if (lane == 0) dinv[c] = inv;
+                    for (int i = c + 1 + lane; i < M; i += 32) A[c * M + i] = cmul(A[c * M + i], inv);
+                    __syncwarp();
+                    for (int j = c + 1; j < k1; ++j) {
+                        const cplx u = cneg(A[j * M + c]);
+                        for (int i = c + 1 + lane; i < M; i += 32) {
+                            cplx v = A[j * M + i];
+                            cfma(v, A[c * M + i], u);
+                            A[j * M + i] = v;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        if (*sing) return false;
+        // interchanges of the panel on the columns outside it, in pivot order
+        for (int j = tid; j < M; j += nth) {
+            if (j >= k0 && j < k1) continue;
+            for (int c = k0; c < k1; ++c) {
+                const int pr = piv[c];
+                if (pr != c) {
+                    const double2 t = A[j * M + c];
+                    A[j * M + c] = A[j * M + pr];
+                    A[j * M + pr] = t;
+                }
+            }
+        }
+        __syncthreads();
+        // U12 = L11^-1 A12, one thread per column
+        for (int j = k1 + tid; j < M; j += nth)
+            for (int r = k0 + 1; r < k1; ++r) {
+                cplx v = A[j * M + r];
+                for (int c = k0; c < r; ++c) cfma(v, cneg(A[c * M + r]), A[j * M + c]);
+                A[j * M + r] = v;
+            }
+        __syncthreads();
+        // A22 -= L21 U12
+        const int m2 = M - k1;
+        for (int t = tid; t < m2 * m2; t += nth) {
+            const int i = k1 + t % m2, j = k1 + t / m2;
+            cplx v = A[j * M + i];
+            for (int c = k0; c < k1; ++c) cfma(v, cneg(A[c * M + i]), A[j * M + c]);
+            A[j * M + i] = v;
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+// B (M x nc, shared) <- U^-1 L^-1 P B with the factors of blocked_lu: the interchanges (thread
+// per column), then blocks of BP rows: the block's triangle (thread per column) and the update
+// of the remaining rows (thread per entry), forward with L and backward with U.
+__device__ void blocked_lu_solve(const double2* A, int M, const int* piv, const double2* dinv, double2* B, int nc) {
+    const int tid = threadIdx.x, nth = blockDim.x;
+    for (int j = tid; j < nc; j += nth)
+        for (int c = 0; c < M; ++c) {
+            const int pr = piv[c];
+            if (pr != c) {
+                const double2 t = B[j * M + c];
+                B[j * M + c] = B[j * M + pr];
+                B[j * M + pr] = t;
+            }
+        }
+    __syncthreads();
+    for (int k0 = 0; k0 < M; k0 += BP) {  // L y = b
+        const int k1 = min(M, k0 + BP);
+        for (int j = tid; j < nc; j += nth)
+            for (int r = k0 + 1; r < k1; ++r) {
+                cplx v = B[j * M + r];
+                for (int c = k0; c < r; ++c) cfma(v, cneg(A[c * M + r]), B[j * M + c]);
+                B[j * M + r] = v;
+            }
+        __syncthreads();
+        const int rows = M - k1;
+        for (int t = tid; t < rows * nc; t += nth) {
+            const int i = k1 + t % rows, j = t / rows;
+            cplx v = B[j * M + i];
+            for (int c = k0; c < k1; ++c) cfma(v, cneg(A[c * M + i]), B[j * M + c]);
+            B[j * M + i] = v;
+        }
+        __syncthreads();
+    }
+    for (int k1 = M; k1 > 0; k1 -= BP) {  // U x = y
+        const int k0 = max(0, k1 - BP);
+        for (int j = tid; j < nc; j += nth)
+            for (int r = k1 - 1; r >= k0; --r) {
+                cplx v = B[j * M + r];
+                for (int c = r + 1; c < k1; ++c) cfma(v, cneg(A[c * M + r]), B[j * M + c]);
+                B[j * M + r] = cmul(v, dinv[r]);
+            }
+        __syncthreads();
+        for (int t = tid; t < k0 * nc; t += nth) {
+            const int i = t % k0, j = t / k0;
+            cplx v = B[j * M + i];
+            for (int c = k0; c < k1; ++c) cfma(v, cneg(A[c * M + i]), B[j * M + c]);
+            B[j * M + i] = v;
+        }
+        __syncthreads();
+    }
+}
+
 // ---- batched periodic-array solve ----------------------------------------------------------
 // One CTA per Bloch vector: Z = D/N (harmonic table), A = I - T S in shared memory (S from the
 // translation plan, cluster/interaction.rs:292-315 with sw/plan.rs:383-413 evaluate_periodic),
-// partial-pivot LU in shared memory, then X = A^-1 T in panels of 48 right-hand-side columns.
+// blocked partial-pivot LU in shared memory, then X = A^-1 T in panels of 48 right-hand sides.
 constexpr int AS_PANEL = 48;
 
 __global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const double2* __restrict__ D, size_t ldd,
@@ -261,6 +411,7 @@ __global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const doubl
     double2* A = as_smem;                  // M x M column-major
     double2* B = A + M * M;                // M x AS_PANEL column-major; the harmonic table aliases it
     __shared__ int piv[128];
+    __shared__ double2 dinv[128];
     __shared__ int sing;
     const int tid = threadIdx.x, nth = blockDim.x;
     for (int kp = blockIdx.x; kp < nk; kp += gridDim.x) {
@@ -287,7 +438,7 @@ __global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const doubl
             A[(2 * s + 1) * M + 2 * d + 1] = mk(one - a11.x, -a11.y);
         }
         __syncthreads();
-        if (!cta_lu(A, M, piv, &sing)) {
+        if (!blocked_lu(A, M, piv, dinv, &sing)) {
             if (tid == 0) atomicExch(status, 5);
             __syncthreads();
             continue;
@@ -308,7 +459,7 @@ __global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const doubl
                 B[jj * M + i] = v;
             }
             __syncthreads();
-            cta_lu_solve(A, M, piv, B, nc);
+            blocked_lu_solve(A, M, piv, dinv, B, nc);
             for (int it = tid; it < M * nc; it += nth) {
                 int jj = it / M, i = it - jj * M;
                 Xk[(size_t)(c0 + jj) * M + i] = B[jj * M + i];
