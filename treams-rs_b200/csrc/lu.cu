@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cstdlib>
 #include <map>
+#include <string>
 
 #include "common.cuh"
 #include "kernels.h"
@@ -534,6 +535,108 @@ __global__ void __launch_bounds__(256, 2) zgemm_dmma_kernel(double2* A, size_t l
     }
 }
 
+// ---- FP64 complex GEMM on DMMA, 128 x 64 complex tiles, 3-stage cp.async ring --------------
+// The same real-embedding product as zgemm_dmma_kernel with a larger tile per CTA (8 warps in
+// 4 x 2, warp tile 64 real rows x 32 columns: 32 m8n8k4 products per 4-deep real k step from
+// 8 A and 4 B fragments; 64 accumulators per lane, ~200 registers, one CTA per SM) and K
+// chunks of 8 complex in a 3-stage cp.async ring (24 KB per stage for 2 Mflop of products).
+// A fragments come from the complex tile: the 32 lanes of a load touch 8
+// distinct 16-byte entries (one shared-memory wavefront), and select Re, -Im or Im.
+constexpr int ZH_M = 128;  // complex rows per CTA
+constexpr int ZH_N = 64;   // columns per CTA
+constexpr int ZH_KC = 8;   // complex K per stage
+constexpr int ZH_STAGES = 3;
+constexpr size_t ZH_SMEM = (size_t)ZH_STAGES * ZH_KC * (ZH_M + ZH_N) * sizeof(double2);
+
+__global__ void __launch_bounds__(256, 1) zgemm_dmma_big_kernel(double2* A, size_t lda, int k0, int w, int r0, int n) {
+    extern __shared__ __align__(16) unsigned char zh_smem[];
+    double2 (*Ls)[ZH_KC][ZH_M] = (double2 (*)[ZH_KC][ZH_M])zh_smem;
+    double2 (*Us)[ZH_KC][ZH_N] = (double2 (*)[ZH_KC][ZH_N])(zh_smem + (size_t)ZH_STAGES * ZH_KC * ZH_M * 16);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tr = r0 + blockIdx.x * ZH_M, tc = r0 + blockIdx.y * ZH_N;
+    const int wr = (warp & 3) * 64, wc = (warp >> 2) * 32;  // real rows, columns of the warp tile
+    double acc[8][4][2];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    const int nchunks = (w + ZH_KC - 1) / ZH_KC;
+    auto load = [&](int stage, int ch) {
+        const int kc = ch * ZH_KC;
+        for (int idx = tid; idx < ZH_KC * ZH_M; idx += 256) {
+            const int r = idx % ZH_M, k = idx / ZH_M;
+            const int row = tr + r, kk = kc + k;
+            const bool ok = row < n && kk < w;
+            cp_async16(&Ls[stage][k][r], A + (size_t)(k0 + (ok ? kk : 0)) * lda + (ok ? row : 0), ok);
+        }
+        for (int idx = tid; idx < ZH_KC * ZH_N; idx += 256) {
+            const int k = idx % ZH_KC, c = idx / ZH_KC;
+            const int col = tc + c, kk = kc + k;
+            const bool ok = col < n && kk < w;
+            cp_async16(&Us[stage][k][c], A + (size_t)(ok ? col : 0) * lda + k0 + (ok ? kk : 0), ok);
+        }
+    };
+#pragma unroll
+    for (int s = 0; s < ZH_STAGES - 1; ++s) {
+        if (s < nchunks) load(s, s);
+        cp_async_commit();
+    }
+    for (int ch = 0; ch < nchunks; ++ch) {
+        const int st = ch % ZH_STAGES;
+        if (ch + ZH_STAGES - 1 < nchunks) load((ch + ZH_STAGES - 1) % ZH_STAGES, ch + ZH_STAGES - 1);
+        cp_async_commit();
+        cp_async_wait<ZH_STAGES - 1>();
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < 2 * ZH_KC / 4; ++ks) {  // real k steps of 4
+            const int kr = ks * 4 + (lane & 3);
+            const int kc = kr >> 1, kp = kr & 1;
+            double bfrag[4];
+#pragma unroll
+            for (int cb = 0; cb < 4; ++cb) {
+                const double2 u = Us[st][kc][wc + cb * 8 + (lane >> 2)];
+                bfrag[cb] = kp ? u.y : u.x;
+            }
+#pragma unroll
+            for (int rb = 0; rb < 8; ++rb) {
+                const int rr = wr + rb * 8 + (lane >> 2);
+                const double2 l = Ls[st][kc][rr >> 1];
+                const int rp = rr & 1;
+                const double a = (rp == kp) ? l.x : (rp == 0 ? -l.y : l.y);
+#pragma unroll
+                for (int cb = 0; cb < 4; ++cb)
+                    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                                 : "+d"(acc[rb][cb][0]), "+d"(acc[rb][cb][1])
+                                 : "d"(a), "d"(bfrag[cb]));
+            }
+        }
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+    // epilogue: lanes (l, l ^ 4) hold the re/im rows of one complex row
+    const bool even = ((lane >> 2) & 1) == 0;
+    const int csel = 2 * (lane & 3) + (even ? 0 : 1);
+#pragma unroll
+    for (int rb = 0; rb < 8; ++rb) {
+        double2 upd[4], old[4];
+        const int grow = tr + ((wr + rb * 8 + (lane >> 2)) >> 1);
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb) {
+            const double d0 = acc[rb][cb][0], d1 = acc[rb][cb][1];
+            const double p0 = __shfl_xor_sync(0xffffffffu, d0, 4), p1 = __shfl_xor_sync(0xffffffffu, d1, 4);
+            upd[cb] = make_double2(even ? d0 : p1, even ? p0 : d1);
+            const int gcol = tc + wc + cb * 8 + csel;
+            old[cb] = (grow < n && gcol < n) ? A[(size_t)gcol * lda + grow] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb) {
+            const int gcol = tc + wc + cb * 8 + csel;
+            if (grow < n && gcol < n)
+                A[(size_t)gcol * lda + grow] = make_double2(old[cb].x - upd[cb].x, old[cb].y - upd[cb].y);
+        }
+    }
+}
+
 // ---- FP32 complex GEMM on CUDA cores (fallback when tcgen05 is disabled) -----------------
 __global__ void __launch_bounds__(256) cgemm_simt_kernel(float2* A, size_t lda, int k0, int w, int r0, int n) {
     __shared__ float2 Ls[ZG_KC][ZG_T + 1];
@@ -626,6 +729,7 @@ void lu_init_attributes() {
     cudaFuncSetAttribute(trsm_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(trsm_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZG_SMEM);
+    cudaFuncSetAttribute(zgemm_dmma_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZH_SMEM);
     cudaFuncSetAttribute(perm_from_piv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
@@ -645,6 +749,16 @@ static int panel_rows_per_cta() {
         v = (x >= 16 && x <= 200) ? x : 32;
     }
     return v;
+}
+
+// FP64 trailing update: 128 x 64 complex tiles unless TCU_FP64_GEMM=small (64 x 64 tiles).
+static bool fp64_big_tiles() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("TCU_FP64_GEMM");
+        v = (e && std::string(e) == "small") ? 0 : 1;
+    }
+    return v == 1;
 }
 
 static bool panel_sub_enabled() {
@@ -776,7 +890,12 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
         dim3 grid((cols + ZG_T - 1) / ZG_T, (cols + ZG_T - 1) / ZG_T);
         if constexpr (sizeof(R) == 8) {
             StageScope sc(ST_GEMM, st);
-            zgemm_dmma_kernel<<<grid, 256, ZG_SMEM, st>>>((double2*)A, lda, k0, w, r0, n);
+            if (fp64_big_tiles()) {
+                dim3 g2((cols + ZH_M - 1) / ZH_M, (cols + ZH_N - 1) / ZH_N);
+                zgemm_dmma_big_kernel<<<g2, 256, ZH_SMEM, st>>>((double2*)A, lda, k0, w, r0, n);
+            } else {
+                zgemm_dmma_kernel<<<grid, 256, ZG_SMEM, st>>>((double2*)A, lda, k0, w, r0, n);
+            }
             ++*launches;
         } else {
             if (tensor_cores) {
