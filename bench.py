@@ -268,13 +268,15 @@ def batch_workload(ctx, stream, count: int, with_cpu: bool = True) -> dict:
         batch.append((w.lmax, w.k0, w.radii, w.eps, w.positions, B))
         modes += w.n
         flops += 8.0 / 3.0 * float(w.n) ** 3
+    tuned = ctx.autotune()  # the FP64/mixed crossover of "auto", measured on this GPU
     t.batch_solve(batch[:2], "auto", ctx=ctx)  # warm-up
     fb0 = ctx.fallbacks
     (X, certs, order), ms, wall = _timed(stream, lambda: t.batch_solve(batch, "auto", ctx=ctx))
     worst = max(c[0].residual_norm / c[0].rhs_norm for c in certs)
     out = {"workload": f"clusters 0..{count - 1} of the 256-cluster sweep ({modes} unknowns in total)",
            "unit": "clusters/s", "value": count / (ms / 1e3), "ms": ms, "max_rel_residual": worst,
-           "fp64_fallbacks": ctx.fallbacks - fb0, "precision": "auto (mixed from 2048 modes, else fp64)",
+           "fp64_fallbacks": ctx.fallbacks - fb0,
+           "precision": f"auto (mixed from {tuned['crossover']} unknowns, else fp64; autotuned)", "autotune": tuned,
            "useful_lu_tflops": flops / (ms / 1e3) / 1e12}
     if with_cpu:
         import oracle

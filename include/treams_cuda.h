@@ -38,7 +38,8 @@ typedef enum tcu_status {
 typedef enum tcu_precision {
     TCU_FP64 = 0,   /* complex128 LU, FP64 DMMA trailing updates */
     TCU_MIXED = 1,  /* complex64 LU, 3-pass split tcgen05 updates (FP16 or TF32 pieces), FP64 refinement */
-    TCU_AUTO = 2    /* batch solves only: per cluster, MIXED from n >= 2048 modes, else FP64 */
+    TCU_AUTO = 2    /* batch solves only: per cluster, MIXED from the context's crossover on (2048 modes
+                       until tcu_context_autotune measures it), else FP64 */
 } tcu_precision;
 
 typedef enum tcu_preconditioner {
@@ -84,6 +85,13 @@ tcu_status tcu_context_set_refinement(tcu_context* ctx, double target, double fa
 /* Number of mixed-precision solves whose FP64 refinement stalled above the fallback tolerance
  * and that were finished by a second factor (TF32 pieces, then FP64) of the same cluster. */
 long long tcu_context_fallbacks(tcu_context* ctx);
+/* Precision autotuner of batched solves (no counterpart in the reference): times assembly +
+ * factorization + one refined solve in FP64 and in mixed precision on synthetic lmax-4 clusters
+ * of 384 to 9216 unknowns and sets TCU_AUTO's crossover to the smallest size from which the
+ * mixed path stays faster. crossover (may be NULL) receives it; the first count sizes and times
+ * (ms) go to sizes, ms_fp64, ms_mixed (each may be NULL). Takes about a second. */
+tcu_status tcu_context_autotune(tcu_context* ctx, size_t* crossover, int count, size_t* sizes, double* ms_fp64,
+                                double* ms_mixed);
 /* Failure-detection self-test (no counterpart in the reference): runs the LU panel's grid
  * barrier with one arrival missing, so that its bounded wait gives up after limit_seconds
  * (clamped to [0, 4] s). Returns TCU_TIMEOUT, as a factorization whose CTAs never meet

@@ -111,3 +111,23 @@ ctx.close()
     assert out.returncode == 0, out.stderr[-2000:]
     res, err, fallbacks = out.stdout.split()
     assert float(res) <= 1e-12 and float(err) <= 1e-10
+
+
+def test_autotuned_crossover_drives_auto_precision():
+    ctx = t.Context(0)
+    try:
+        tuned = ctx.autotune()
+        assert tuned["crossover"] in tuned["sizes"] or tuned["crossover"] > max(tuned["sizes"])
+        assert all(v > 0 for v in tuned["ms_fp64"] + tuned["ms_mixed"])
+        batch, refs = [], []
+        for lmax, k0, r, e, x in _small_batch()[:3]:
+            kv = np.array([[0, 0, k0]], complex)
+            B = oracle.plane_wave_expansion(lmax, x, kv, np.array([1], np.int32))
+            A, tb = oracle.cluster_operator(lmax, k0, r, e, x)
+            refs.append(oracle.dense_solve(lmax, A, tb, B))
+            batch.append((lmax, k0, r, e, x, B))
+        X, certs, _ = t.batch_solve(batch, "auto", ctx=ctx)
+        for Xi, Ri in zip(X, refs):
+            assert np.linalg.norm(Xi - Ri) <= 1e-10 * np.linalg.norm(Ri)
+    finally:
+        ctx.close()

@@ -104,6 +104,7 @@ struct tcu_context {
     std::set<tcu_factor*> factors;  // live factors (destroyed with the context)
     double refine_target = 1e-13; // refinement stops at ||r|| <= refine_target ||T b||
     double fallback_above = 1e-12;  // mixed solves left above this finish in FP64
+    size_t auto_crossover = 2048;   // TCU_AUTO: mixed from this many unknowns on (tcu_context_autotune)
 };
 
 struct tcu_factor {
@@ -1730,7 +1731,7 @@ extern "C" tcu_status tcu_batch_solve(tcu_context* ctx, size_t count, const tcu_
         const size_t i = idx[q];
         if (order) order[q] = (int)i;
         const tcu_cluster_desc& c = clusters[i];
-        int prec = precision == TCU_AUTO ? (modes(i) >= 2048 ? TCU_MIXED : TCU_FP64) : precision;
+        int prec = precision == TCU_AUTO ? (modes(i) >= ctx->auto_crossover ? TCU_MIXED : TCU_FP64) : precision;
         tcu_factor* f = nullptr;
         tcu_status s = tcu_sphere_cluster_factor(ctx, c.lmax, c.k0, c.N, c.radii, c.eps, c.positions, prec, &f);
         if (s == TCU_OK) {
@@ -1738,6 +1739,77 @@ extern "C" tcu_status tcu_batch_solve(tcu_context* ctx, size_t count, const tcu_
             tcu_factor_destroy(f);
         }
         if (s) return fail(s, "cluster " + std::to_string(i) + ": " + g_last_error);
+    }
+    return TCU_OK;
+}
+
+// Precision autotuner of the batched solves: times assembly + factorization + one refined
+// solve in FP64 and in mixed precision on synthetic clusters (spheres of radius 0.2 on a
+// jittered cubic grid of spacing 0.55, eps 2.25 + 0.01i, k0 2, lmax 4) of growing size, and
+// sets the crossover of TCU_AUTO to the smallest size from which the mixed path is faster
+// (and stays faster on the larger sizes). sizes: 0..count-1 unknown counts written out with
+// their times (ms), may be NULL.
+extern "C" tcu_status tcu_context_autotune(tcu_context* ctx, size_t* crossover, int count, size_t* sizes,
+                                           double* ms_fp64, double* ms_mixed) {
+    if (!ctx) return fail(TCU_INVALID_INPUT, "null context");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    CK(cudaSetDevice(ctx->device), "device");
+    const int spheres[] = {8, 16, 32, 64, 128, 192};
+    const int ns = sizeof(spheres) / sizeof(spheres[0]);
+    std::vector<double> tf(ns), tm(ns);
+    std::vector<size_t> nn(ns);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0), "event");
+    CK(cudaEventCreate(&e1), "event");
+    tcu_status s = TCU_OK;
+    for (int q = 0; q < ns && !s; ++q) {
+        const int N = spheres[q];
+        const int side = (int)std::ceil(std::cbrt((double)N));
+        std::vector<double> r(N, 0.2), eps(2 * N), pos(3 * N);
+        uint64_t st = 0x9E3779B97F4A7C15ull * (q + 1);
+        for (int i = 0; i < N; ++i) {
+            eps[2 * i] = 2.25;
+            eps[2 * i + 1] = 0.01;
+            const int a = i % side, b = (i / side) % side, c = i / (side * side);
+            const int idx[3] = {a, b, c};
+            for (int d = 0; d < 3; ++d) {
+                st = st * 6364136223846793005ull + 1442695040888963407ull;
+                const double jitter = ((st >> 11) * (1.0 / 9007199254740992.0) - 0.5) * 0.1;
+                pos[3 * i + d] = 0.55 * idx[d] + jitter;
+            }
+        }
+        nn[q] = (size_t)N * 48;
+        std::vector<double> B(2 * nn[q], 0.0), X(2 * nn[q]);
+        for (size_t j = 0; j < nn[q]; ++j) B[2 * j] = 1.0 / (1.0 + j % 7);
+        for (int prec = 0; prec < 2 && !s; ++prec) {
+            float best = 1e30f;
+            for (int rep = 0; rep < 2 && !s; ++rep) {
+                tcu_factor* f = nullptr;
+                cudaEventRecord(e0, ctx->stream);
+                s = tcu_sphere_cluster_factor(ctx, 4, 2.0, N, r.data(), eps.data(), pos.data(),
+                                              prec ? TCU_MIXED : TCU_FP64, &f);
+                if (!s) s = tcu_factor_solve(f, B.data(), 1, X.data(), nullptr);
+                cudaEventRecord(e1, ctx->stream);
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                best = std::min(best, ms);
+                if (f) tcu_factor_destroy(f);
+            }
+            (prec ? tm : tf)[q] = best;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s) return s;
+    size_t cross = nn[ns - 1] + 1;
+    for (int q = ns - 1; q >= 0 && tm[q] < tf[q]; --q) cross = nn[q];
+    ctx->auto_crossover = cross;
+    if (crossover) *crossover = cross;
+    for (int q = 0; q < count && q < ns; ++q) {
+        if (sizes) sizes[q] = nn[q];
+        if (ms_fp64) ms_fp64[q] = tf[q];
+        if (ms_mixed) ms_mixed[q] = tm[q];
     }
     return TCU_OK;
 }

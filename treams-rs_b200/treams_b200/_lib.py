@@ -44,6 +44,7 @@ SIGNATURES = {
     "tcu_context_fallbacks": (ctypes.c_longlong, [P]),
     "tcu_context_set_refinement": (c_int, [P, c_double, c_double]),
     "tcu_context_wait_selftest": (c_int, [P, c_double]),
+    "tcu_context_autotune": (c_int, [P, ctypes.POINTER(c_size), c_int, P, P, P]),
     "tcu_context_set_profiling": (c_int, [P, c_int]),
     "tcu_context_stage_time": (c_int, [P, c_int, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(c_double)]),
     "tcu_context_reset_stage_times": (c_int, [P]),
@@ -147,6 +148,17 @@ class Context:
         after `limit` seconds and this raises TreamsCudaError (status TCU_TIMEOUT), leaving the
         context usable."""
         _check(lib().tcu_context_wait_selftest(self.handle, float(limit)))
+
+    def autotune(self) -> dict:
+        """Measure the FP64/mixed crossover of batched solves (tcu_context_autotune): returns
+        {"crossover": unknowns, "sizes": [...], "ms_fp64": [...], "ms_mixed": [...]}."""
+        cross = c_size()
+        sizes = np.zeros(6, np.uint64)
+        f64 = np.zeros(6)
+        mix = np.zeros(6)
+        _check(lib().tcu_context_autotune(self.handle, ctypes.byref(cross), 6, _p(sizes), _p(f64), _p(mix)))
+        return {"crossover": int(cross.value), "sizes": [int(v) for v in sizes], "ms_fp64": f64.tolist(),
+                "ms_mixed": mix.tolist()}
 
     @property
     def fallbacks(self) -> int:
