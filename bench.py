@@ -217,7 +217,7 @@ def iterative_workload(ctx, stream, count: int = 4096, with_cpu: bool = True) ->
     return out
 
 
-def periodic_workload(ctx, stream, nk: int = 4096, with_cpu: bool = True) -> dict:
+def periodic_workload(ctx, stream, nk: int = 4096, with_cpu: bool = True, fp64_peak=None) -> dict:
     """The periodic array: square lattice (period 0.54), one sphere per cell (r 0.2, eps 9),
     k0 4, lmax 6, 4096 Bloch vectors: lattice sums (degrees <= 12) and X = (I - T S)^-1 T."""
     from treams_b200 import lattice as tl
@@ -240,6 +240,12 @@ def periodic_workload(ctx, stream, nk: int = 4096, with_cpu: bool = True) -> dic
            "array_solve_e2e_value": nk / (ms_all / 1e3),
            "stages_ms": {k: v[1] for k, v in st.items()},
            "array_kernel_fp64_tflops": flops / (lu_ms / 1e3) / 1e12 if lu_ms else None,
+           "array_kernel_roofline": {"bound": "fp64", "peak": fp64_peak, "unit": "TFLOP/s",
+                                     "frac": (flops / (lu_ms / 1e3) / 1e12) / fp64_peak if lu_ms and fp64_peak
+                                     else None,
+                                     "note": "(8/3) M^3 + 8 M^3 real flops per Bloch vector (LU + M right-hand "
+                                             "sides, M = 96) over the small-LU stage; peak = measured cuBLAS "
+                                             "float64 GEMM rate (of measured)"},
            "note": "e2e includes the host copies of X (nk x 96 x 96 complex, 604 MB)"}
     if with_cpu:
         import oracle
@@ -439,14 +445,16 @@ def main() -> None:
 
     head = measure(args.precision, args.steps, args.warmup, not args.no_e2e)
     with_cpu = world == 1 and rank == 0 and not args.no_cpu_baseline
-    extras = {}
-    if args.extras:
-        extras["iterative"] = iterative_workload(ctx, stream, args.iterative_spheres, with_cpu)
-        extras["periodic"] = periodic_workload(ctx, stream, args.periodic_kpars, with_cpu)
-        extras["batch"] = batch_workload(ctx, stream, args.batch_clusters, with_cpu)
     other, yard = None, None
     if args.compare and args.precision == "mixed":
         yard = fp64_yardsticks(w, ctx, dev)
+    extras = {}
+    if args.extras:
+        fp64_peak = yard["cublas_fp64_gemm_tflops"] if yard else None
+        extras["iterative"] = iterative_workload(ctx, stream, args.iterative_spheres, with_cpu)
+        extras["periodic"] = periodic_workload(ctx, stream, args.periodic_kpars, with_cpu, fp64_peak)
+        extras["batch"] = batch_workload(ctx, stream, args.batch_clusters, with_cpu)
+    if yard is not None:
         other = measure("fp64", min(args.steps, args.compare_steps), 1, False,
                         fp64_peak=yard["cublas_c128_gemm_tflops"])
     if rank == 0:
