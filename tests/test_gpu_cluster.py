@@ -147,3 +147,16 @@ def test_invalid_inputs_raise(ctx):
         t.sphere_cluster_factor(3, -1.0, [0.5], [4], [[0, 0, 0]], ctx=ctx)
     with pytest.raises(ValueError, match="GMRES needs"):
         t.SphereCluster(3, 1.0, [0.5], [4], [[0, 0, 0]], ctx=ctx).solve(np.ones(30), rtol=0.0, atol=0.0)
+
+
+def test_touching_pair_is_found_among_many_spheres(ctx):
+    # the cell-grid validation must find an overlapping pair wherever it sits in the list
+    import treams_b200 as t
+    g = np.stack(np.meshgrid(np.arange(6), np.arange(6), np.arange(6), indexing="ij"), -1).reshape(-1, 3) * 0.7
+    radii = np.full(len(g), 0.3)
+    ok = t.cluster_apply(1, 1.0, radii, np.full(len(g), 2.0 + 0j), g, np.ones(len(g) * 6, complex), ctx=ctx)
+    assert np.all(np.isfinite(ok))
+    bad = g.copy()
+    bad[150] = bad[3] + np.array([0.55, 0.1, 0.0])  # 0.559 < 0.6: overlaps sphere 3
+    with pytest.raises(ValueError, match="touch or overlap"):
+        t.cluster_apply(1, 1.0, radii, np.full(len(g), 2.0 + 0j), bad, np.ones(len(g) * 6, complex), ctx=ctx)

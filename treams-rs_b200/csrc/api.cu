@@ -164,14 +164,54 @@ tcu_status validate_spheres(int L, double k0, size_t N, const double* radii, con
     if (!finite_all(eps, 2 * N) || !finite_all(pos, 3 * N))
         return fail(TCU_INVALID_INPUT,
                     "require positive finite k0 and radii, and matching finite permittivities and positions");
-    for (size_t i = 0; i < N; ++i)
-        for (size_t j = 0; j < i; ++j) {
-            double d = std::hypot(std::hypot(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1]),
-                                  pos[3 * i + 2] - pos[3 * j + 2]);
-            if (d <= radii[i] + radii[j] || !std::isfinite(d))
-                return fail(TCU_INVALID_INPUT,
-                            "spherical particles must have finite separation and must not touch or overlap");
+    // Touching or overlapping pairs are closer than 2 max(radius): bin the centres into cubic
+    // cells of that edge and test each sphere against the spheres of its own and the 13
+    // preceding neighbour cells (every pair once), which finds the same pairs as testing all
+    // N^2 / 2 of them.
+    double rmax = 0.0, lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = 0; i < N; ++i) {
+        rmax = std::max(rmax, radii[i]);
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::min(lo[a], pos[3 * i + a]);
+            hi[a] = std::max(hi[a], pos[3 * i + a]);
         }
+    }
+    const double edge = 2.0 * rmax;
+    long dims[3];
+    for (int a = 0; a < 3; ++a) {
+        const double span = (hi[a] - lo[a]) / edge;
+        if (!std::isfinite(span) || span > 4.0e6)
+            return fail(TCU_INVALID_INPUT,
+                        "spherical particles must have finite separation and must not touch or overlap");
+        dims[a] = (long)span + 1;
+    }
+    auto cell = [&](size_t i, int a) { return std::min(dims[a] - 1, (long)((pos[3 * i + a] - lo[a]) / edge)); };
+    std::vector<std::pair<long long, size_t>> order(N);
+    for (size_t i = 0; i < N; ++i)
+        order[i] = {((long long)cell(i, 0) * dims[1] + cell(i, 1)) * dims[2] + cell(i, 2), i};
+    std::sort(order.begin(), order.end());
+    auto touching = [&](size_t i, size_t j) {
+        const double d = std::hypot(std::hypot(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1]),
+                                    pos[3 * i + 2] - pos[3 * j + 2]);
+        return d <= radii[i] + radii[j] || !std::isfinite(d);
+    };
+    for (size_t q = 0; q < N; ++q) {
+        const size_t i = order[q].second;
+        const long cx = cell(i, 0), cy = cell(i, 1), cz = cell(i, 2);
+        for (long dx = -1; dx <= 1; ++dx)
+            for (long dy = -1; dy <= 1; ++dy)
+                for (long dz = -1; dz <= 1; ++dz) {
+                    const long x = cx + dx, y = cy + dy, z = cz + dz;
+                    if (x < 0 || y < 0 || z < 0 || x >= dims[0] || y >= dims[1] || z >= dims[2]) continue;
+                    const long long key = ((long long)x * dims[1] + y) * dims[2] + z;
+                    auto it = std::lower_bound(order.begin(), order.end(), std::make_pair(key, (size_t)0));
+                    for (; it != order.end() && it->first == key; ++it)
+                        if (it->second < i && touching(i, it->second))
+                            return fail(TCU_INVALID_INPUT,
+                                        "spherical particles must have finite separation and must not touch or "
+                                        "overlap");
+                }
+    }
     return TCU_OK;
 }
 
@@ -387,6 +427,14 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
 
 tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_certificate* certs, bool device) {
     if (!f || !B || !X || p <= 0) return fail(TCU_INVALID_INPUT, "require a factor and at least one column");
+    if (p > 8) {  // the norms of a context reduce at most 8 columns at once
+        for (int c0 = 0; c0 < p; c0 += 8) {
+            const size_t off = 2 * f->n * (size_t)c0;
+            tcu_status s = solve_impl(f, B + off, std::min(8, p - c0), X + off, certs ? certs + c0 : nullptr, device);
+            if (s) return s;
+        }
+        return TCU_OK;
+    }
     tcu_context* ctx = f->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
@@ -505,6 +553,15 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
 // the forward solve. th: return T^H Y instead (the incident-field gradient).
 tcu_status solve_adjoint_impl(tcu_factor* f, const double* G, int p, double* Y, tcu_certificate* certs, bool th) {
     if (!f || !G || !Y || p <= 0) return fail(TCU_INVALID_INPUT, "require a factor and at least one column");
+    if (p > 8) {  // the norms of a context reduce at most 8 columns at once
+        for (int c0 = 0; c0 < p; c0 += 8) {
+            const size_t off = 2 * f->n * (size_t)c0;
+            tcu_status s =
+                solve_adjoint_impl(f, G + off, std::min(8, p - c0), Y + off, certs ? certs + c0 : nullptr, th);
+            if (s) return s;
+        }
+        return TCU_OK;
+    }
     tcu_context* ctx = f->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
@@ -1657,12 +1714,12 @@ extern "C" tcu_status tcu_learned_problem_create(tcu_context* ctx, int lmax, dou
     if ((s = dev_alloc(ctx, &p->d_pos, 3 * N, "positions")) || (s = dev_alloc(ctx, &p->d_T, N * lmax * 4, "T blocks")) ||
         (s = dev_alloc(ctx, &p->d_V, n * nprobe, "probes")))
         return s;
-    double* d_r = nullptr;
-    cplx* d_e = nullptr;
     DevBuf tmp(ctx);
-    CK(tmp.alloc(N * 8 + N * 16), "geometry");
-    d_r = (double*)tmp.p;
-    d_e = (cplx*)(d_r + N);
+    Arena ga;
+    const size_t o_r = ga.add(N * 8), o_e = ga.add(N * 16);
+    CK(tmp.alloc(ga.total), "geometry");
+    double* d_r = ga.at<double>(tmp.p, o_r);
+    cplx* d_e = ga.at<cplx>(tmp.p, o_e);
     CK(cudaMemcpyAsync(p->d_pos, positions, N * 24, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemcpyAsync(d_r, radii, N * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemcpyAsync(d_e, eps, N * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
