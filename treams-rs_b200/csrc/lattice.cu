@@ -251,9 +251,42 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
 // lowest row on ties), in panels of BP = 16 columns: warp 0 factors the panel (pivot search by
 // shuffles, swaps, scaling and rank-1 updates inside the panel with warp-level synchronisation
 // only), then every thread applies the panel's interchanges to the other columns, forms
-// U12 = L11^-1 A12 (thread per column) and the rank-16 trailing update (thread per entry).
+// U12 = L11^-1 A12 (thread per column) and the rank-16 trailing update (4 x 2 register tiles).
 // dinv receives 1 / U[i][i]. Returns false on every thread for an exactly zero pivot.
 constexpr int BP = 16;
+
+// X[j][i] -= sum_{c in [k0, k1)} A[c][i] X[j][c] for rows i in [r0, r1) and columns j in
+// [j0, j1) (column-major, leading dimension M). Each thread owns a 4-row x 2-column register
+// tile, so a step over c loads 6 entries for 8 products (the shared-memory traffic, not the
+// arithmetic, bounds these updates).
+__device__ void tile_update(const double2* A, double2* X, int M, int r0, int r1, int j0, int j1, int k0, int k1) {
+    const int rows = r1 - r0, cols = j1 - j0;
+    if (rows <= 0 || cols <= 0) return;
+    const int tr = (rows + 3) / 4, tc = (cols + 1) / 2;
+    for (int t = threadIdx.x; t < tr * tc; t += blockDim.x) {
+        const int i0 = r0 + 4 * (t % tr), jj = j0 + 2 * (t / tr);
+        cplx acc[4][2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) acc[a][0] = acc[a][1] = mk(0.0, 0.0);
+        for (int c = k0; c < k1; ++c) {
+            cplx l[4], u[2];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) l[a] = i0 + a < r1 ? A[c * M + i0 + a] : mk(0.0, 0.0);
+#pragma unroll
+            for (int b = 0; b < 2; ++b) u[b] = jj + b < j1 ? X[(jj + b) * M + c] : mk(0.0, 0.0);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b) cfma(acc[a][b], l[a], u[b]);
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+                if (i0 + a < r1 && jj + b < j1) X[(jj + b) * M + i0 + a] = csub(X[(jj + b) * M + i0 + a], acc[a][b]);
+    }
+}
+
 __device__ bool blocked_lu(double2* A, int M, int* piv, double2* dinv, int* sing) {
     const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) *sing = 0;
@@ -332,13 +365,7 @@ __device__ bool blocked_lu(double2* A, int M, int* piv, double2* dinv, int* sing
             }
         __syncthreads();
         // A22 -= L21 U12
-        const int m2 = M - k1;
-        for (int t = tid; t < m2 * m2; t += nth) {
-            const int i = k1 + t % m2, j = k1 + t / m2;
-            cplx v = A[j * M + i];
-            for (int c = k0; c < k1; ++c) cfma(v, cneg(A[c * M + i]), A[j * M + c]);
-            A[j * M + i] = v;
-        }
+        tile_update(A, A, M, k1, M, k1, M, k0, k1);
         __syncthreads();
     }
     return true;
@@ -346,7 +373,7 @@ __device__ bool blocked_lu(double2* A, int M, int* piv, double2* dinv, int* sing
 
 // B (M x nc, shared) <- U^-1 L^-1 P B with the factors of blocked_lu: the interchanges (thread
 // per column), then blocks of BP rows: the block's triangle (thread per column) and the update
-// of the remaining rows (thread per entry), forward with L and backward with U.
+// of the remaining rows (4 x 2 register tiles), forward with L and backward with U.
 __device__ void blocked_lu_solve(const double2* A, int M, const int* piv, const double2* dinv, double2* B, int nc) {
     const int tid = threadIdx.x, nth = blockDim.x;
     for (int j = tid; j < nc; j += nth)
@@ -368,13 +395,7 @@ __device__ void blocked_lu_solve(const double2* A, int M, const int* piv, const 
                 B[j * M + r] = v;
             }
         __syncthreads();
-        const int rows = M - k1;
-        for (int t = tid; t < rows * nc; t += nth) {
-            const int i = k1 + t % rows, j = t / rows;
-            cplx v = B[j * M + i];
-            for (int c = k0; c < k1; ++c) cfma(v, cneg(A[c * M + i]), B[j * M + c]);
-            B[j * M + i] = v;
-        }
+        tile_update(A, B, M, k1, M, 0, nc, k0, k1);
         __syncthreads();
     }
     for (int k1 = M; k1 > 0; k1 -= BP) {  // U x = y
@@ -386,12 +407,7 @@ __device__ void blocked_lu_solve(const double2* A, int M, const int* piv, const 
                 B[j * M + r] = cmul(v, dinv[r]);
             }
         __syncthreads();
-        for (int t = tid; t < k0 * nc; t += nth) {
-            const int i = t % k0, j = t / k0;
-            cplx v = B[j * M + i];
-            for (int c = k0; c < k1; ++c) cfma(v, cneg(A[c * M + i]), B[j * M + c]);
-            B[j * M + i] = v;
-        }
+        tile_update(A, B, M, 0, k0, 0, nc, k0, k1);
         __syncthreads();
     }
 }
