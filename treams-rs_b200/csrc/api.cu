@@ -681,9 +681,13 @@ struct FactorCoarse : CoarseSolve {
     }
 };
 
-// The dipole (lmax 1) system of a cluster, factored in complex64 from 2048 modes on, else in FP64.
+// The dipole (lmax 1) system of a cluster: factored (complex64 from 2048 modes on, else FP64) up
+// to 6144 dipole modes; above, no factor is made (out stays empty) and the two-level
+// preconditioner solves the dipole system by an inner GMRES on its stored dipole columns.
+constexpr size_t COARSE_LU_MAX = 6144;
 tcu_status make_coarse(tcu_context* ctx, double k0, size_t N, const double* radii, const double* eps,
-                       const double* pos, std::unique_ptr<CoarseSolve>* out) {
+                       const double* pos, std::unique_ptr<CoarseSolve>* out, bool factor_always = false) {
+    if (6 * N > COARSE_LU_MAX && !factor_always) return TCU_OK;
     auto c = std::make_unique<FactorCoarse>();
     const int prec = 6 * N >= 2048 ? TCU_MIXED : TCU_FP64;
     tcu_status s = factor_impl(ctx, 1, k0, N, radii, eps, pos, nullptr, nullptr, nullptr, prec, &c->f);
@@ -1729,7 +1733,8 @@ extern "C" tcu_status tcu_learned_problem_create(tcu_context* ctx, int lmax, dou
     ++ctx->launches;
     if ((s = read_status(ctx, "Mie coefficients"))) return s;
     std::unique_ptr<CoarseSolve> coarse;
-    if ((s = make_coarse(ctx, k0, N, radii, eps, positions, &coarse)))
+    // the training loss differentiates through a fixed linear preconditioner: always a factor
+    if ((s = make_coarse(ctx, k0, N, radii, eps, positions, &coarse, true)))
         return fail(s, std::string("coarse dipole system: ") + g_last_error);
     s = p->lp.build(ctx->stream, *P, lmax, (int)N, k0, p->d_pos, positions, radii, eps, p->d_T, ctx->precond_reach,
                     nprobe, p->d_V, std::move(coarse), &ctx->launches);

@@ -1,0 +1,280 @@
+// Matrix-free operator x - T C x in product form, for lmax 2..5.
+//
+// The coupling of destination sphere i is, per destination mode d and helicity,
+//   (C x)_i[d, +] = sum_{j != i} sum_s (A_ij(s,d) + B_ij(s,d)) x_j[2s]
+//   (C x)_i[d, -] = sum_{j != i} sum_s (A_ij(s,d) - B_ij(s,d)) x_j[2s+1]
+// with A and B the plan's term sums over the pair's harmonic table Z_ij (sw/plan.rs:224-251,
+// sw/coupling.rs:127-140). Exchanging the sums over j and over the plan's terms gives
+//   G_i[idx, e] = sum_{j != i} Z_ij[idx] x_j[e]            (tsize x 2 nlm per destination)
+//   (C x)_i[d, +] = sum_s sum_{t in A(s,d) + B(s,d)} w_t G_i[idx_t, 2s]   (and - for B at 2s+1)
+// The first line is a complex product of the generated table matrix Z_i (tsize x N) with the
+// coefficients X (N x 2 nlm): a register-tiled FP64 product whose A operand is built in shared
+// memory chunk by chunk and never stored. The plan's term lists then run once per destination
+// instead of once per pair. Work per ordered pair: tsize * 2 nlm complex multiply-adds
+// (1,470 at lmax 3, 3,888 at lmax 4) plus one harmonic table.
+//
+// CTA = DI destination spheres x one right-hand side, RG x CG threads; thread (rg, cg) owns
+// G rows rg + RG u (u < TR) and columns cg + CG t (t < TC). Per chunk of KJ sources:
+//   A) thread per pair: direction and radial sequence z_p(k r), p <= 2 lmax, to shared memory;
+//   B) thread per (pair, order m >= 0): the order column of the solid harmonics times z_p,
+//      written into the chunk's table matrix (rows dest * tsize + idx, one column per source);
+//   C) the chunk's product update from shared memory.
+// Finally G goes to shared memory and thread per (destination, d) applies the term lists,
+// the Mie block and the alpha / beta / zadd epilogue of the operator.
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <cstring>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "pairtable.cuh"
+#include "plan.h"
+
+namespace tcu {
+
+namespace {
+
+struct GemmShape {
+    int DI, TR, TC, RG, CG, KJ;
+};
+
+// Tile shapes per lmax: G rows DI * tsize <= TR * RG, columns 2 nlm <= TC * CG
+GemmShape gemm_shape(int L) {
+    switch (L) {
+        case 2: return {4, 4, 2, 25, 8, 32};   // 100 x 16, 200 threads
+        case 3: return {2, 4, 3, 25, 10, 32};  // 98 x 30, 250 threads
+        case 4: return {1, 4, 4, 21, 12, 32};  // 81 x 48, 252 threads
+        default: return {1, 4, 5, 31, 14, 16}; // lmax 5: 121 x 70, 434 threads
+    }
+}
+
+size_t gemm_smem(const DevPlan& P, const GemmShape& s) {
+    const size_t rows = (size_t)s.TR * s.RG, cols = (size_t)s.TC * s.CG, npair = (size_t)s.DI * s.KJ;
+    const size_t chunk = ((size_t)s.KJ * rows + (size_t)s.KJ * cols + npair * (P.order + 1)) * sizeof(cplx) +
+                         npair * sizeof(double4);
+    const size_t g = (size_t)s.DI * P.tsize * 2 * P.nlm * sizeof(cplx);
+    return chunk > g ? chunk : g;
+}
+
+template <int TR, int TC>
+__global__ void __launch_bounds__(512, 1)
+    apply_gemm_kernel(DevPlan P, int N, double k, const double* __restrict__ pos, const cplx* __restrict__ T,
+                      const cplx* __restrict__ x, size_t ldx, const cplx* __restrict__ zadd, double alpha, double beta,
+                      bool singular, cplx* __restrict__ y, int DI, int RG, int CG, int KJ) {
+    extern __shared__ __align__(16) unsigned char ag_smem[];
+    const int nlm = P.nlm, M = 2 * nlm, ts = P.tsize, order = P.order, ord1 = order + 1;
+    const int ROWS = TR * RG, COLS = TC * CG, npair = DI * KJ;
+    cplx* Zs = reinterpret_cast<cplx*>(ag_smem);                     // KJ x ROWS (source-major)
+    cplx* Xs = Zs + (size_t)KJ * ROWS;                               // KJ x COLS
+    cplx* Rs = Xs + (size_t)KJ * COLS;                               // npair x (order + 1)
+    double4* Ds = reinterpret_cast<double4*>(Rs + (size_t)npair * ord1);  // direction, state
+    cplx* Gs = reinterpret_cast<cplx*>(ag_smem);                     // at the end: DI * ts x M
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int rg = tid / CG, cg = tid - (tid / CG) * CG;
+    const bool worker = rg < RG;
+    const int i0 = blockIdx.x * DI;
+    const size_t coff = (size_t)blockIdx.y * ldx;
+    const cplx* xc = x + coff;
+
+    cplx acc[TR][TC];
+#pragma unroll
+    for (int u = 0; u < TR; ++u)
+#pragma unroll
+        for (int t = 0; t < TC; ++t) acc[u][t] = mk(0.0, 0.0);
+    for (int t = tid; t < KJ * ROWS; t += nthr) Zs[t] = mk(0.0, 0.0);  // padding rows stay zero
+
+    for (int j0 = 0; j0 < N; j0 += KJ) {
+        __syncthreads();  // the previous chunk's product is done with Zs / Xs
+        // A) per pair: state 2 = a table, 1 = coincident centres of the regular kind (Z = e_0),
+        //    0 = no coupling (the pair i = j, sources or destinations past N, coincident outgoing)
+        for (int p = tid; p < npair; p += nthr) {
+            const int il = p / KJ, jj = p - il * KJ, i = i0 + il, j = j0 + jj;
+            double u[3] = {0.0, 0.0, 0.0}, state = 0.0;
+            if (i < N && j < N && j != i) {
+                double r;
+                if (unit_direction(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1],
+                                   pos[3 * i + 2] - pos[3 * j + 2], r, u)) {
+                    state = 2.0;
+                    cplx* rad = Rs + (size_t)p * ord1;
+                    if (singular) {
+                        cplx h[MAXP];
+                        hankel_sequence<MAXP>(order, k * r, h);
+                        for (int q = 0; q <= order; ++q) rad[q] = h[q];
+                    } else {
+                        double jv[MAXP];
+                        bessel_j_sequence<MAXP>(order, k * r, jv);
+                        for (int q = 0; q <= order; ++q) rad[q] = mk(jv[q], 0.0);
+                    }
+                } else if (!singular) {
+                    state = 1.0;
+                }
+            }
+            Ds[p] = make_double4(u[0], u[1], u[2], state);
+        }
+        for (int t = tid; t < KJ * COLS; t += nthr) {
+            const int jj = t / COLS, col = t - jj * COLS, j = j0 + jj;
+            Xs[t] = (col < M && j < N) ? xc[(size_t)j * M + col] : mk(0.0, 0.0);
+        }
+        __syncthreads();
+        // B) per (pair, order m >= 0): column m of the table, entries deg = m..order at
+        //    deg^2 + deg + m and deg^2 + deg - m
+        for (int it = tid; it < npair * ord1; it += nthr) {
+            const int p = it / ord1, m = it - p * ord1;
+            const int il = p / KJ, jj = p - il * KJ;
+            cplx* Zp = Zs + (size_t)jj * ROWS + (size_t)il * ts;
+            const double4 D = Ds[p];
+            if (D.w == 2.0) {
+                const cplx* rad = Rs + (size_t)p * ord1;
+                const cplx xy = mk(D.x, D.y);
+                const double z = D.z, r2 = D.x * D.x + D.y * D.y + D.z * D.z;
+                cplx diag = mk(1.0, 0.0);
+                for (int q = 1; q <= m; ++q) diag = cscale(cmul(diag, xy), -double(2 * q - 1));
+                cplx pc = diag, prev = mk(0.0, 0.0);
+                for (int deg = m; deg <= order; ++deg) {
+                    if (deg > m) {
+                        const double a = double(2 * deg - 1) / double(deg - m);
+                        const double b = double(deg + m - 1) / double(deg - m);
+                        const cplx next = mk(a * z * pc.x - b * r2 * prev.x, a * z * pc.y - b * r2 * prev.y);
+                        prev = pc;
+                        pc = next;
+                    }
+                    const cplx rd = rad[deg];
+                    Zp[deg * deg + deg + m] = cmul(rd, pc);
+                    if (m > 0) {
+                        const int idx = deg * deg + deg - m;
+                        Zp[idx] = cmul(rd, cscale(cconj(pc), P.reflection[idx]));
+                    }
+                }
+            } else {
+                for (int deg = m; deg <= order; ++deg) {
+                    Zp[deg * deg + deg + m] = mk((D.w == 1.0 && deg == 0) ? 1.0 : 0.0, 0.0);
+                    if (m > 0) Zp[deg * deg + deg - m] = mk(0.0, 0.0);
+                }
+            }
+        }
+        __syncthreads();
+        // C) G += Z_chunk X_chunk
+        if (worker) {
+            const cplx* zr = Zs + rg;
+            const cplx* xr = Xs + cg;
+            for (int kk = 0; kk < KJ; ++kk) {
+                cplx a[TR], b[TC];
+#pragma unroll
+                for (int u = 0; u < TR; ++u) a[u] = zr[(size_t)kk * ROWS + u * RG];
+#pragma unroll
+                for (int t = 0; t < TC; ++t) b[t] = xr[(size_t)kk * COLS + t * CG];
+#pragma unroll
+                for (int u = 0; u < TR; ++u)
+#pragma unroll
+                    for (int t = 0; t < TC; ++t) cfma(acc[u][t], a[u], b[t]);
+            }
+        }
+    }
+    __syncthreads();
+    if (worker) {
+#pragma unroll
+        for (int u = 0; u < TR; ++u) {
+            const int row = rg + u * RG;
+#pragma unroll
+            for (int t = 0; t < TC; ++t) {
+                const int col = cg + t * CG;
+                if (row < DI * ts && col < M) Gs[(size_t)row * M + col] = acc[u][t];
+            }
+        }
+    }
+    __syncthreads();
+    // term lists of the plan, Mie block and epilogue: thread per (destination, d)
+    for (int it = tid; it < DI * nlm; it += nthr) {
+        const int il = it / nlm, d = it - il * nlm, i = i0 + il;
+        if (i >= N) continue;
+        const cplx* G = Gs + (size_t)il * ts * M;
+        cplx sp = mk(0.0, 0.0), sn = mk(0.0, 0.0);
+        for (int s = 0; s < nlm; ++s) {
+            const int2 cb = __ldg(&P.combo[s * nlm + d]);
+            int t = cb.x;
+            const int na = cb.y & 0xffff, nb = cb.y >> 16;
+            const cplx* g = G + 2 * s;
+            for (int e = 0; e < na; ++e, ++t) {
+                const cplx w = __ldg(&P.w[t]);
+                const cplx* ge = g + (size_t)__ldg(&P.idx[t]) * M;
+                cfma(sp, w, ge[0]);
+                cfma(sn, w, ge[1]);
+            }
+            for (int e = 0; e < nb; ++e, ++t) {
+                const cplx w = __ldg(&P.w[t]);
+                const cplx* ge = g + (size_t)__ldg(&P.idx[t]) * M;
+                cfma(sp, w, ge[0]);
+                cfma(sn, cneg(w), ge[1]);
+            }
+        }
+        const size_t row = (size_t)i * M + 2 * d;
+        const cplx x0 = xc[row], x1 = xc[row + 1];
+        cplx y0, y1;
+        if (singular) {
+            cplx tc0 = sp, tc1 = sn;  // T null: the coupling alone
+            if (T) {
+                const int lam = degree_of(d);
+                const cplx* t4 = T + ((size_t)i * P.L + lam - 1) * 4;
+                tc0 = cadd(cmul(t4[0], sp), cmul(t4[1], sn));
+                tc1 = cadd(cmul(t4[2], sp), cmul(t4[3], sn));
+            }
+            y0 = cadd(cscale(x0, alpha), cscale(tc0, beta));
+            y1 = cadd(cscale(x1, alpha), cscale(tc1, beta));
+            if (zadd) {
+                y0 = cadd(y0, zadd[coff + row]);
+                y1 = cadd(y1, zadd[coff + row + 1]);
+            }
+        } else {
+            y0 = cadd(x0, sp);
+            y1 = cadd(x1, sn);
+        }
+        y[coff + row] = y0;
+        y[coff + row + 1] = y1;
+    }
+}
+
+}  // namespace
+
+bool apply_gemm_supported(const DevPlan& P) {
+    if (P.L < 2 || P.L > 5) return false;
+    const char* e = getenv("TCU_APPLY");  // "terms": the per-pair term-sum kernels instead
+    return !(e && strcmp(e, "terms") == 0);
+}
+
+void launch_apply_gemm(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
+                       int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y,
+                       cudaStream_t st) {
+    if (N <= 0 || ncol <= 0) return;
+    const GemmShape s = gemm_shape(P.L);
+    const size_t smem = gemm_smem(P, s);
+    const dim3 grid((unsigned)((N + s.DI - 1) / s.DI), (unsigned)ncol);
+    const int threads = s.RG * s.CG;
+    switch (P.L) {
+        case 2:
+            apply_gemm_kernel<4, 2><<<grid, threads, smem, st>>>(P, N, k, pos, T, x, ldx, zadd, alpha, beta, singular,
+                                                                 y, s.DI, s.RG, s.CG, s.KJ);
+            break;
+        case 3:
+            apply_gemm_kernel<4, 3><<<grid, threads, smem, st>>>(P, N, k, pos, T, x, ldx, zadd, alpha, beta, singular,
+                                                                 y, s.DI, s.RG, s.CG, s.KJ);
+            break;
+        case 4:
+            apply_gemm_kernel<4, 4><<<grid, threads, smem, st>>>(P, N, k, pos, T, x, ldx, zadd, alpha, beta, singular,
+                                                                 y, s.DI, s.RG, s.CG, s.KJ);
+            break;
+        default:
+            apply_gemm_kernel<4, 5><<<grid, threads, smem, st>>>(P, N, k, pos, T, x, ldx, zadd, alpha, beta, singular,
+                                                                 y, s.DI, s.RG, s.CG, s.KJ);
+            break;
+    }
+}
+
+void apply_gemm_init_attributes() {
+    cudaFuncSetAttribute(apply_gemm_kernel<4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply_gemm_kernel<4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply_gemm_kernel<4, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply_gemm_kernel<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+}  // namespace tcu

@@ -95,6 +95,11 @@ void launch_assemble_sources(const DevPlan& P, int N, double k, const double* po
 void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                   int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st);
 size_t apply_smem_bytes(const DevPlan& P, int ncol);
+// Product form of the same operator (lmax 2..5; TCU_APPLY=terms selects the term-sum kernels)
+bool apply_gemm_supported(const DevPlan& P);
+void launch_apply_gemm(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
+                       int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st);
+void apply_gemm_init_attributes();
 void launch_block(const DevPlan& P, double k, const double* d, bool singular, bool helicity, cplx* out,
                   cudaStream_t st);
 void launch_mie(int L, double k0, int N, const double* radii, const cplx* eps, cplx* T, int* status, cudaStream_t st);

@@ -651,6 +651,10 @@ static int apply2_cols(const DevPlan& P) {
 void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                   int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st) {
     StageScope sc(ST_APPLY, st);
+    if (apply_gemm_supported(P)) {  // lmax 2..5: product form
+        launch_apply_gemm(P, N, k, pos, T, x, ldx, ncol, zadd, alpha, beta, singular, y, st);
+        return;
+    }
     if (P.nlm > 64) {
         // lmax 8..10: the slot-major kernel's tables no longer fit; Q = 256 / nlm source slots
         // per CTA with one destination lm per thread
@@ -710,6 +714,7 @@ void pairs_init_attributes() {
     cudaFuncSetAttribute(apply2_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(assemble_kernel<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
     cudaFuncSetAttribute(assemble_kernel<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+    apply_gemm_init_attributes();
 }
 
 size_t apply_smem_bytes(const DevPlan& P, int ncol) { return apply2_smem(P, std::min(ncol, apply2_cols(P))); }

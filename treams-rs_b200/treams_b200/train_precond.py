@@ -13,6 +13,13 @@ random vectors. Loss and gradient come from the library's forward and backward k
 weights. Theta = 1 (all output weights zero) is the untrained two-level method, and training
 starts there.
 
+The probe loss is a one-step proxy: lowering it can still cost GMRES iterations (Theta can
+absorb far-field coupling into the near-field blocks on average while spreading the spectrum).
+So every `eval_every` steps the current weights run preconditioned GMRES(50) to 1e-8 on held-out
+validation clusters (seeds 3000 + v, 512 spheres), and the weights kept are the ones with the
+fewest total iterations (ties: the smaller summed relative residual), Theta = 1 included. When no
+trained weights beat Theta = 1 the library keeps Theta = 1.
+
 Run on a GPU:  python -m treams_b200.train_precond [--clusters 8] [--steps 300] --write
 It rewrites treams-rs_b200/csrc/learned_weights.inc; rebuild the library afterwards.
 """
@@ -59,8 +66,20 @@ def probes(w: workloads.Cluster, nrandom: int, seed: int, ctx) -> np.ndarray:
     return np.asfortranarray(np.concatenate([TB, Rn], axis=1))
 
 
+def validation_score(ctx, weights, clusters) -> tuple[int, float]:
+    """Total GMRES(50) iterations to 1e-8 and summed relative residual of the learned
+    preconditioner with these weights over the validation clusters."""
+    ctx.set_learned_weights(weights, 3.0)
+    its, res = 0, 0.0
+    for c, b in clusters:
+        cert = c.solve(b, rtol=1e-8, restart=50, max_iterations=400, preconditioner="learned").convergence[0]
+        its += cert.iterations
+        res += cert.residual_norm / cert.rhs_norm
+    return its, res
+
+
 def train(clusters: int = 8, steps: int = 300, lr: float = 3e-3, nrandom: int = 2, seed: int = 0, ctx=None,
-          log=print):
+          log=print, eval_every: int = 25, nvalid: int = 2):
     ctx = ctx or _lib.default_context()
     ctx.set_learned_weights(None, 0.0)
     problems, names = [], []
@@ -69,9 +88,17 @@ def train(clusters: int = 8, steps: int = 300, lr: float = 3e-3, nrandom: int = 
         problems.append(_lib.LearnedProblem(w.lmax, w.k0, w.radii, w.eps, w.positions,
                                             probes(w, nrandom, 7000 + i, ctx), ctx=ctx))
         names.append(f"{w.radii.size} spheres")
+    valid = []
+    for v in range(nvalid):
+        w = workloads.learned_cluster(seed=3000 + v, count=512)
+        c = _lib.SphereCluster(w.lmax, w.k0, w.radii, w.eps, w.positions, ctx=ctx)
+        valid.append((c, _lib.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)[:, 0]))
     lmax = 3
     wts = init_weights(lmax, seed)
     nprobe = sum(p.nprobe for p in problems)
+    score0 = validation_score(ctx, wts, valid)
+    chosen = (score0, 0, wts.copy())
+    log(f"step 0: validation iterations {score0[0]} (two-level)")
 
     def total(wv):
         loss, grad = 0.0, np.zeros_like(wv)
@@ -84,24 +111,30 @@ def train(clusters: int = 8, steps: int = 300, lr: float = 3e-3, nrandom: int = 
     loss0, _ = total(wts)
     m, v = np.zeros_like(wts), np.zeros_like(wts)
     b1, b2, eps = 0.9, 0.999, 1e-8
-    best = (loss0, wts.copy())
     t0 = time.time()
+    history = []
     for it in range(1, steps + 1):
         loss, g = total(wts)
-        if loss < best[0]:
-            best = (loss, wts.copy())
         m = b1 * m + (1 - b1) * g
         v = b2 * v + (1 - b2) * g * g
         wts = wts - lr * (m / (1 - b1**it)) / (np.sqrt(v / (1 - b2**it)) + eps)
-        if it % 25 == 0 or it == 1:
-            log(f"step {it}: mean probe loss {loss:.5g} (untrained {loss0:.5g}), {time.time() - t0:.1f} s")
-    loss, _ = total(wts)
-    if loss < best[0]:
-        best = (loss, wts.copy())
+        if it % eval_every == 0 or it == steps:
+            score = validation_score(ctx, wts, valid)
+            history.append({"step": it, "loss": loss, "iterations": score[0], "residual": score[1]})
+            if score < chosen[0]:
+                chosen = (score, it, wts.copy())
+            log(f"step {it}: mean probe loss {loss:.5g} (untrained {loss0:.5g}), validation iterations "
+                f"{score[0]} (two-level {score0[0]}), {time.time() - t0:.1f} s")
+    ctx.set_learned_weights(None, 0.0)
     for p in problems:
         p.close()
-    return best[1], {"loss_untrained": loss0, "loss_trained": best[0], "clusters": names, "steps": steps,
-                     "probes": nprobe}
+    improved = chosen[1] > 0 and chosen[0][0] < score0[0]
+    return (chosen[2] if improved else None), {
+        "loss_untrained": loss0, "clusters": names, "steps": steps, "probes": nprobe,
+        "validation": {"clusters": [f"512 spheres, seed {3000 + i}" for i in range(nvalid)],
+                       "two_level_iterations": score0[0], "chosen_step": chosen[1] if improved else 0,
+                       "chosen_iterations": chosen[0][0] if improved else score0[0]},
+        "history": history}
 
 
 def write_inc(weights_by_lmax: dict, note: str, reach: float = 3.0) -> None:
@@ -124,16 +157,23 @@ def main() -> None:
     ap.add_argument("--clusters", type=int, default=8)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--lr", type=float, default=3e-3)
+    ap.add_argument("--nrandom", type=int, default=2, help="random probe vectors per cluster")
     ap.add_argument("--write", action="store_true", help="rewrite csrc/learned_weights.inc")
     ap.add_argument("--out", default=None, help="also write the weights and the training record to this JSON file")
     args = ap.parse_args()
-    w, info = train(args.clusters, args.steps, args.lr)
+    w, info = train(args.clusters, args.steps, args.lr, nrandom=args.nrandom)
     print(json.dumps(info))
     if args.out:
-        pathlib.Path(args.out).write_text(json.dumps({"weights": list(map(float, w)), **info}))
+        pathlib.Path(args.out).write_text(json.dumps({"weights": None if w is None else list(map(float, w)), **info}))
     if args.write:
-        write_inc({3: w}, f"trained on {args.clusters} clusters, {args.steps} Adam steps: mean probe loss "
-                          f"{info['loss_trained']:.4g} (untrained two-level {info['loss_untrained']:.4g})")
+        val = info["validation"]
+        if w is None:
+            write_inc({}, f"{args.clusters} clusters, {args.steps} Adam steps: no step beat Theta = 1 on the "
+                          f"validation clusters ({val['two_level_iterations']} GMRES iterations)")
+        else:
+            write_inc({3: w}, f"trained on {args.clusters} clusters, step {val['chosen_step']} of {args.steps}: "
+                              f"{val['chosen_iterations']} validation GMRES iterations (two-level "
+                              f"{val['two_level_iterations']})")
 
 
 if __name__ == "__main__":
