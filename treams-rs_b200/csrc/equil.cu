@@ -8,6 +8,14 @@
 // Kernels: row maxima over column chunks (threads over rows, coalesced column reads, one
 // partial per (row, chunk)) reduced in a fixed order; column maxima of R A (CTA per column);
 // one in-place scaling pass. Three passes over the matrix: HBM-bound.
+//
+// Then the balancing sweeps of linalg/mod.rs:229-310 (Sinkhorn and Knopp: unit magnitude sums
+// determine the scaled operator, whatever the units): every column factor y_j, then every row
+// factor x_i, moves by the power of two that puts its scaled magnitude sum into
+// [ln 2, 2 ln 2); sweeps stop after one that moves no factor by more than 2 (at most 64). A sum
+// that is not normal leaves the max scales alone; so do factors beyond 2^+-256. Two passes over
+// the matrix per sweep: column sums (CTA per column) and row sums (threads over rows, partial
+// per column chunk, fixed-order reduction).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -93,6 +101,130 @@ __global__ void scale_rows_kernel(cplx* __restrict__ v, const double* __restrict
         v[t] = cscale(v[t], s[t % n]);
 }
 
+// ---- balancing sweeps ---------------------------------------------------------------------
+constexpr int BAL_SWEEPS = 64;
+enum : int { BAL_COARSE = 1, BAL_ABORT = 2, BAL_UNFIT = 4 };
+
+// factor *= 1 / (largest power of two <= sum * factor / ln 2); flags the step's size
+__device__ __forceinline__ void bal_advance(double& factor, double sum, int* flags) {
+    const double ratio = sum * factor / 0.69314718055994530942;
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(ratio);
+    const unsigned long long ex = bits & 0x7ff0000000000000ULL;
+    if (ex == 0 || ex == 0x7ff0000000000000ULL || ratio < 0.0) {  // zero, subnormal, inf, NaN
+        atomicOr(flags, BAL_ABORT);
+        return;
+    }
+    const double step = 1.0 / __longlong_as_double((long long)ex);
+    factor *= step;
+    if (step < 0.5 || step > 2.0) atomicOr(flags, BAL_COARSE);
+}
+
+template <typename C>
+__global__ void bal_col_kernel(const C* __restrict__ A, int n, const double* __restrict__ x, double* __restrict__ y,
+                               int* flags) {
+    __shared__ double sh[256];
+    const int j = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += x[i] * mag(A[(size_t)j * n + i]);
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bal_advance(y[j], sh[0], flags);
+}
+
+template <typename C>
+__global__ void bal_row_partial(const C* __restrict__ A, int n, const double* __restrict__ y,
+                                double* __restrict__ partial) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int per = (n + EQ_CHUNKS - 1) / EQ_CHUNKS;
+    const int j0 = blockIdx.y * per, j1 = min(n, j0 + per);
+    double s = 0.0;
+    for (int j = j0; j < j1; ++j) s += mag(A[(size_t)j * n + i]) * y[j];
+    partial[(size_t)blockIdx.y * n + i] = s;
+}
+
+__global__ void bal_row_update(const double* __restrict__ partial, int n, double* __restrict__ x, int* flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+    for (int c = 0; c < EQ_CHUNKS; ++c) s += partial[(size_t)c * n + i];
+    bal_advance(x[i], s, flags);
+}
+
+// factors within 2^+-256 and normal products with the max scales, else BAL_UNFIT
+__global__ void bal_fit_kernel(int n, const double* __restrict__ x, const double* __restrict__ y,
+                               const double* __restrict__ r, const double* __restrict__ c, int* flags) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double lo = 8.636168555094445e-78, hi = 1.157920892373162e77;  // 2^-256, 2^256
+    const double a = x[i], b = y[i], ra = r[i] * a, cb = c[i] * b;
+    const bool ok = a >= lo && a <= hi && b >= lo && b <= hi && isfinite(ra) && isfinite(cb) &&
+                    fabs(ra) >= 2.2250738585072014e-308 && fabs(cb) >= 2.2250738585072014e-308;
+    if (!ok) atomicOr(flags, BAL_UNFIT);
+}
+
+__global__ void bal_fold_kernel(int n, const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ r,
+                                double* __restrict__ c) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    r[i] *= x[i];
+    c[i] *= y[i];
+}
+
+__global__ void fill_kernel(double* __restrict__ v, size_t n, double value) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = value;
+}
+
+// Balancing sweeps over the max-equilibrated A (R A C, scales r and c); on success A, r and c
+// take the factors. scratch: x (n), y (n), partial (EQ_CHUNKS n), flags (one int).
+template <typename C>
+tcu_status balance_impl(C* A, int n, double* r, double* c, double* scratch, int* sweeps_out, cudaStream_t st,
+                        long long* launches) {
+    double* x = scratch;
+    double* y = x + n;
+    double* partial = y + n;
+    int* d_flags = reinterpret_cast<int*>(partial + (size_t)EQ_CHUNKS * n);
+    const int nb = (n + 255) / 256;
+    fill_kernel<<<(2 * n + 255) / 256, 256, 0, st>>>(x, 2 * (size_t)n, 1.0);
+    if (launches) ++*launches;
+    int flags = 0, sweep = 0;
+    for (; sweep < BAL_SWEEPS; ++sweep) {
+        if (cudaMemsetAsync(d_flags, 0, sizeof(int), st) != cudaSuccess) return TCU_DEVICE_ERROR;
+        bal_col_kernel<C><<<n, 256, 0, st>>>(A, n, x, y, d_flags);
+        bal_row_partial<C><<<dim3(nb, EQ_CHUNKS), 256, 0, st>>>(A, n, y, partial);
+        bal_row_update<<<nb, 256, 0, st>>>(partial, n, x, d_flags);
+        if (launches) *launches += 3;
+        if (cudaMemcpyAsync(&flags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess)
+            return TCU_DEVICE_ERROR;
+        if (flags & BAL_ABORT) {  // a sum that is not normal: keep the max scales
+            *sweeps_out = -(sweep + 1);
+            return TCU_OK;
+        }
+        if (!(flags & BAL_COARSE)) break;
+    }
+    if (cudaMemsetAsync(d_flags, 0, sizeof(int), st) != cudaSuccess) return TCU_DEVICE_ERROR;
+    bal_fit_kernel<<<nb, 256, 0, st>>>(n, x, y, r, c, d_flags);
+    if (launches) ++*launches;
+    if (cudaMemcpyAsync(&flags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return TCU_DEVICE_ERROR;
+    if (flags & BAL_UNFIT) {
+        *sweeps_out = -(sweep + 1);
+        return TCU_OK;
+    }
+    apply_scales<C><<<148 * 16, 256, 0, st>>>(A, n, x, y);
+    bal_fold_kernel<<<nb, 256, 0, st>>>(n, x, y, r, c);
+    if (launches) *launches += 2;
+    *sweeps_out = std::min(sweep + 1, BAL_SWEEPS);
+    return TCU_OK;
+}
+
 template <typename C>
 tcu_status equilibrate_impl(C* A, int n, double threshold, double* r, double* c, double* partial, bool* applied,
                             cudaStream_t st, long long* launches) {
@@ -113,12 +245,13 @@ tcu_status equilibrate_impl(C* A, int n, double threshold, double* r, double* c,
     apply_scales<C><<<148 * 16, 256, 0, st>>>(A, n, r, c);
     if (launches) *launches += 2;
     *applied = true;
-    return TCU_OK;
+    int sweeps = 0;
+    return balance_impl<C>(A, n, r, c, partial, &sweeps, st, launches);
 }
 
 }  // namespace
 
-size_t equilibrate_scratch_doubles(int n) { return (size_t)EQ_CHUNKS * n + (n + 255) / 256; }
+size_t equilibrate_scratch_doubles(int n) { return (size_t)(EQ_CHUNKS + 2) * n + (n + 255) / 256 + 1; }
 
 tcu_status equilibrate(void* A, bool fp32, int n, double threshold, double* r, double* c, double* partial,
                        bool* applied, cudaStream_t st, long long* launches) {

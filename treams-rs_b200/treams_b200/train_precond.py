@@ -158,10 +158,11 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--nrandom", type=int, default=2, help="random probe vectors per cluster")
+    ap.add_argument("--eval-every", type=int, default=25, help="Adam steps between validation solves")
     ap.add_argument("--write", action="store_true", help="rewrite csrc/learned_weights.inc")
     ap.add_argument("--out", default=None, help="also write the weights and the training record to this JSON file")
     args = ap.parse_args()
-    w, info = train(args.clusters, args.steps, args.lr, nrandom=args.nrandom)
+    w, info = train(args.clusters, args.steps, args.lr, nrandom=args.nrandom, eval_every=args.eval_every)
     print(json.dumps(info))
     if args.out:
         pathlib.Path(args.out).write_text(json.dumps({"weights": None if w is None else list(map(float, w)), **info}))
