@@ -163,7 +163,6 @@ void launch_real_table(int lsum, double k, double eta, int NR, const double2* R,
                        const double* norm, const double* reflection, double2* tab, cudaStream_t st);
 size_t lattice_sum_smem(int lsum, int NR);
 void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st);
-size_t array_solve_smem(int L);
 void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const double* norm, const double2* Tm, int nk,
                         double2* X, int* status, int grid, cudaStream_t st);
 

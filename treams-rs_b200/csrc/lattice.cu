@@ -246,242 +246,223 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
     }
 }
 
-// ---- blocked shared-memory LU of the periodic-array kernel -------------------------------
-// A (M x M column-major, shared, M <= 128) = P^T L U with partial pivoting (largest modulus,
-// lowest row on ties), in panels of BP = 16 columns: warp 0 factors the panel (pivot search by
-// shuffles, swaps, scaling and rank-1 updates inside the panel with warp-level synchronisation
-// only), then every thread applies the panel's interchanges to the other columns, forms
-// U12 = L11^-1 A12 (thread per column) and the rank-16 trailing update (4 x 2 register tiles).
-// dinv receives 1 / U[i][i]. Returns false on every thread for an exactly zero pivot.
-constexpr int BP = 16;
+// ---- batched periodic-array solve ----------------------------------------------------------
+// One CTA per Bloch vector, X = (I - T S)^-1 T (cluster/interaction.rs:292-315 with
+// sw/plan.rs:383-413 evaluate_periodic). The M x M operator (M = 2 lmax (lmax + 2), 96 at
+// lmax 6) lives in registers: thread (tr, tc) of a ceil(nlm/2) x ceil(nlm/2) grid owns the
+// 4 x 4 tile of rows 4 tr.., columns 4 tc.., i.e. the 2 x 2 mode blocks of destinations
+// d = 2 tr, 2 tr + 1 and sources s = 2 tc, 2 tc + 1, assembled there from the harmonic table
+// D / N and the plan's term lists. The inverse comes from in-place Gauss-Jordan elimination
+// with column pivoting: at step k the pivot is the largest |a_kj|^2, j >= k (ties to the lower
+// column), columns k and p are exchanged, row k is scaled by 1 / a_kk and eliminated from every
+// other row (a rank-1 update of the whole tile grid, 16 complex multiply-adds per thread).
+// Per step the owners of row k publish their candidates and row k, the owners of columns k and
+// p their columns, through shared memory; two barriers per step. The result R satisfies
+// A^-1 = the rows of R exchanged in the reverse order of the column exchanges, so
+// X = A^-1 T = that row exchange applied to R T; T is block diagonal per mode pair and a tile
+// holds both columns of each of its pairs, so R T is formed in registers and each row is stored
+// at its final position. (8/3 + 8 - 8/3 =) 8 M^3 real flops of elimination per Bloch vector.
+constexpr int GJ_MAXM = 96;
 
-// X[j][i] -= sum_{c in [k0, k1)} A[c][i] X[j][c] for rows i in [r0, r1) and columns j in
-// [j0, j1) (column-major, leading dimension M). Each thread owns a 4-row x 2-column register
-// tile, so a step over c loads 6 entries for 8 products (the shared-memory traffic, not the
-// arithmetic, bounds these updates).
-__device__ void tile_update(const double2* A, double2* X, int M, int r0, int r1, int j0, int j1, int k0, int k1) {
-    const int rows = r1 - r0, cols = j1 - j0;
-    if (rows <= 0 || cols <= 0) return;
-    const int tr = (rows + 3) / 4, tc = (cols + 1) / 2;
-    for (int t = threadIdx.x; t < tr * tc; t += blockDim.x) {
-        const int i0 = r0 + 4 * (t % tr), jj = j0 + 2 * (t / tr);
-        cplx acc[4][2];
+// (48 / 2)^2 = 576 threads at lmax 6: at most 112 registers each
+__global__ void __maxnreg__(112) array_solve_kernel(DevPlan P, const double2* __restrict__ D,
+                                                                    size_t ldd, const double* __restrict__ norm,
+                                                                    const double2* __restrict__ Tm, int nk,
+                                                                    double2* __restrict__ X, int* __restrict__ status) {
+    __shared__ double2 Z[(2 * 12 + 1) * (2 * 12 + 1)];  // harmonic table, order <= 2 lmax = 12
+    __shared__ double2 colk[GJ_MAXM], colp[GJ_MAXM], rowk[GJ_MAXM];
+    __shared__ double cval[GJ_MAXM / 4];
+    __shared__ int cidx[GJ_MAXM / 4];
+    __shared__ int piv[GJ_MAXM], dest[GJ_MAXM];
+    const int nlm = P.nlm, M = 2 * nlm, TG = (nlm + 1) / 2;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int tr = tid / TG, tc = tid - (tid / TG) * TG;
+    const bool own = tr < TG;
+    const int i0 = 4 * tr, j0 = 4 * tc;
+    for (int kp = blockIdx.x; kp < nk; kp += gridDim.x) {
+        for (int t = tid; t < P.tsize; t += blockDim.x) Z[t] = cscale(D[(size_t)kp * ldd + t], 1.0 / norm[t]);
+        __syncthreads();
+        // A = I - T S on the tile: combo (s, d) gives rows 2d, 2d+1 of columns 2s, 2s+1
+        cplx a[4][4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) acc[a][0] = acc[a][1] = mk(0.0, 0.0);
-        for (int c = k0; c < k1; ++c) {
-            cplx l[4], u[2];
+        for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int a = 0; a < 4; ++a) l[a] = i0 + a < r1 ? A[c * M + i0 + a] : mk(0.0, 0.0);
+            for (int c = 0; c < 4; ++c) a[r][c] = mk(0.0, 0.0);
+        if (own) {
 #pragma unroll
-            for (int b = 0; b < 2; ++b) u[b] = jj + b < j1 ? X[(jj + b) * M + c] : mk(0.0, 0.0);
+            for (int dd = 0; dd < 2; ++dd)
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 2; ++b) cfma(acc[a][b], l[a], u[b]);
+                for (int ss = 0; ss < 2; ++ss) {
+                    const int d = 2 * tr + dd, sidx = 2 * tc + ss;
+                    if (d >= nlm || sidx >= nlm) continue;
+                    int lam = 1;
+                    while ((lam + 1) * (lam + 1) - 1 <= d) ++lam;
+                    const double2* t4 = Tm + (lam - 1) * 4;
+                    cplx Aa, Bb;
+                    plan_combo_sums(P, sidx * nlm + d, Z, Aa, Bb);
+                    const cplx cp = cadd(Aa, Bb), cn = csub(Aa, Bb);
+                    const double one = sidx == d ? 1.0 : 0.0;
+                    const cplx a00 = cmul(t4[0], cp), a10 = cmul(t4[2], cp), a01 = cmul(t4[1], cn),
+                               a11 = cmul(t4[3], cn);
+                    a[2 * dd][2 * ss] = mk(one - a00.x, -a00.y);
+                    a[2 * dd + 1][2 * ss] = cneg(a10);
+                    a[2 * dd][2 * ss + 1] = cneg(a01);
+                    a[2 * dd + 1][2 * ss + 1] = mk(one - a11.x, -a11.y);
+                }
         }
+        // candidates of row 0 (tile row 0)
+        if (own && tr == 0) {
+            double best = -1.0;
+            int bj = 0x7fffffff;
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+            for (int c = 0; c < 4; ++c)
+                if (j0 + c < M && cabs2(a[0][c]) > best) {
+                    best = cabs2(a[0][c]);
+                    bj = j0 + c;
+                }
+            cval[tc] = best;
+            cidx[tc] = bj;
+        }
+        __syncthreads();
+        bool singular = false;
+        for (int k = 0; k < M; ++k) {
+            // pivot column: every warp reduces the TG candidates (largest, ties to the lower column)
+            double bv = lane < TG ? cval[lane] : -1.0;
+            int bj = lane < TG ? cidx[lane] : 0x7fffffff;
 #pragma unroll
-            for (int b = 0; b < 2; ++b)
-                if (i0 + a < r1 && jj + b < j1) X[(jj + b) * M + i0 + a] = csub(X[(jj + b) * M + i0 + a], acc[a][b]);
-    }
-}
-
-__device__ bool blocked_lu(double2* A, int M, int* piv, double2* dinv, int* sing) {
-    const int tid = threadIdx.x, nth = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) *sing = 0;
-    __syncthreads();
-    for (int k0 = 0; k0 < M; k0 += BP) {
-        const int w = min(BP, M - k0), k1 = k0 + w;
-        if (warp == 0) {
-            for (int c = k0; c < k1; ++c) {
-                double best = -1.0;
-                int bi = c;
-                for (int i = c + lane; i < M; i += 32) {
-                    const double v = cabs2(A[c * M + i]);
-                    if (v > best) {
-                        best = v;
-                        bi = i;
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+                const int oj = __shfl_xor_sync(0xffffffffu, bj, off);
+                if (ov > bv || (ov == bv && oj < bj)) {
+                    bv = ov;
+                    bj = oj;
+                }
+            }
+            const int p = bj;
+            if (!(bv > 0.0)) {  // an exactly zero row: singular (uniform over the CTA)
+                singular = true;
+                break;
+            }
+            if (tid == 0) piv[k] = p;
+            // publish row k and columns k and p (values before the exchange)
+            if (own) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    if (i0 + r == k) {
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            if (j0 + c < M) rowk[j0 + c] = a[r][c];
                     }
                 }
-                for (int off = 16; off > 0; off >>= 1) {
-                    const double ov = __shfl_xor_sync(0xffffffffu, best, off);
-                    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                    if (ov > best || (ov == best && oi < bi)) {
-                        best = ov;
-                        bi = oi;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    if (j0 + c == k) {
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            if (i0 + r < M) colk[i0 + r] = a[r][c];
+                    }
+                    if (j0 + c == p) {
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            if (i0 + r < M) colp[i0 + r] = a[r][c];
                     }
                 }
-                if (lane == 0) {
-                    piv[c] = bi;
-                    if (!(best > 0.0)) *sing = 1;
+            }
+            __syncthreads();
+            const cplx inv = cinv(rowk[p]);
+            if (own) {
+                // scaled pivot row after the exchange: u_j = a_kj / a_kp (j != k), u_k = 1 / a_kp
+                cplx u[4];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const int j = j0 + c;
+                    const int js = j == k ? p : (j == p ? k : j);
+                    u[c] = j == k ? inv : (j < M ? cmul(rowk[js], inv) : mk(0.0, 0.0));
                 }
-                if (bi != c && lane < w) {  // swap rows c and bi inside the panel
-                    const int j = k0 + lane;
-                    const double2 t = A[j * M + c];
-                    A[j * M + c] = A[j * M + bi];
-                    A[j * M + bi] = t;
-                }
-                __syncwarp();
-                const cplx d = A[c * M + c];
-                if (cabs2(d) > 0.0) {
-                    const cplx inv = cinv(d);
-                    if (lane == 0) dinv[c] = inv;
-                    for (int i = c + 1 + lane; i < M; i += 32) A[c * M + i] = cmul(A[c * M + i], inv);
-                    __syncwarp();
-                    for (int j = c + 1; j < k1; ++j) {
-                        const cplx u = cneg(A[j * M + c]);
-                        for (int i = c + 1 + lane; i < M; i += 32) {
-                            cplx v = A[j * M + i];
-                            cfma(v, A[c * M + i], u);
-                            A[j * M + i] = v;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int i = i0 + r;
+                    const cplx l = i < M ? colp[i] : mk(0.0, 0.0);
+                    const cplx nl = cneg(l);
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        const int j = j0 + c;
+                        if (i == k) {
+                            a[r][c] = u[c];
+                        } else if (j == k) {
+                            a[r][c] = cmul(nl, inv);
+                        } else {
+                            cplx cur = j == p ? colk[i < M ? i : 0] : a[r][c];
+                            cfma(cur, nl, u[c]);
+                            a[r][c] = cur;
                         }
                     }
                 }
-                __syncwarp();
-            }
-        }
-        __syncthreads();
-        if (*sing) return false;
-        // interchanges of the panel on the columns outside it, in pivot order
-        for (int j = tid; j < M; j += nth) {
-            if (j >= k0 && j < k1) continue;
-            for (int c = k0; c < k1; ++c) {
-                const int pr = piv[c];
-                if (pr != c) {
-                    const double2 t = A[j * M + c];
-                    A[j * M + c] = A[j * M + pr];
-                    A[j * M + pr] = t;
+                // candidates of row k + 1 over columns >= k + 1
+                const int kn = k + 1;
+                if (kn < M && kn >= i0 && kn < i0 + 4) {
+                    double best = -1.0;
+                    int bjn = 0x7fffffff;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        if (i0 + r != kn) continue;  // registers are indexed statically only
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) {
+                            const int j = j0 + c;
+                            const double v = cabs2(a[r][c]);
+                            if (j >= kn && j < M && v > best) {
+                                best = v;
+                                bjn = j;
+                            }
+                        }
+                    }
+                    cval[tc] = best;
+                    cidx[tc] = bjn;
                 }
             }
+            __syncthreads();
         }
-        __syncthreads();
-        // U12 = L11^-1 A12, one thread per column
-        for (int j = k1 + tid; j < M; j += nth)
-            for (int r = k0 + 1; r < k1; ++r) {
-                cplx v = A[j * M + r];
-                for (int c = k0; c < r; ++c) cfma(v, cneg(A[c * M + r]), A[j * M + c]);
-                A[j * M + r] = v;
-            }
-        __syncthreads();
-        // A22 -= L21 U12
-        tile_update(A, A, M, k1, M, k1, M, k0, k1);
-        __syncthreads();
-    }
-    return true;
-}
-
-// B (M x nc, shared) <- U^-1 L^-1 P B with the factors of blocked_lu: the interchanges (thread
-// per column), then blocks of BP rows: the block's triangle (thread per column) and the update
-// of the remaining rows (4 x 2 register tiles), forward with L and backward with U.
-__device__ void blocked_lu_solve(const double2* A, int M, const int* piv, const double2* dinv, double2* B, int nc) {
-    const int tid = threadIdx.x, nth = blockDim.x;
-    for (int j = tid; j < nc; j += nth)
-        for (int c = 0; c < M; ++c) {
-            const int pr = piv[c];
-            if (pr != c) {
-                const double2 t = B[j * M + c];
-                B[j * M + c] = B[j * M + pr];
-                B[j * M + pr] = t;
-            }
-        }
-    __syncthreads();
-    for (int k0 = 0; k0 < M; k0 += BP) {  // L y = b
-        const int k1 = min(M, k0 + BP);
-        for (int j = tid; j < nc; j += nth)
-            for (int r = k0 + 1; r < k1; ++r) {
-                cplx v = B[j * M + r];
-                for (int c = k0; c < r; ++c) cfma(v, cneg(A[c * M + r]), B[j * M + c]);
-                B[j * M + r] = v;
-            }
-        __syncthreads();
-        tile_update(A, B, M, k1, M, 0, nc, k0, k1);
-        __syncthreads();
-    }
-    for (int k1 = M; k1 > 0; k1 -= BP) {  // U x = y
-        const int k0 = max(0, k1 - BP);
-        for (int j = tid; j < nc; j += nth)
-            for (int r = k1 - 1; r >= k0; --r) {
-                cplx v = B[j * M + r];
-                for (int c = r + 1; c < k1; ++c) cfma(v, cneg(A[c * M + r]), B[j * M + c]);
-                B[j * M + r] = cmul(v, dinv[r]);
-            }
-        __syncthreads();
-        tile_update(A, B, M, 0, k0, 0, nc, k0, k1);
-        __syncthreads();
-    }
-}
-
-// ---- batched periodic-array solve ----------------------------------------------------------
-// One CTA per Bloch vector: Z = D/N (harmonic table), A = I - T S in shared memory (S from the
-// translation plan, cluster/interaction.rs:292-315 with sw/plan.rs:383-413 evaluate_periodic),
-// blocked partial-pivot LU in shared memory, then X = A^-1 T in panels of 48 right-hand sides.
-constexpr int AS_PANEL = 48;
-
-__global__ void __launch_bounds__(512) array_solve_kernel(DevPlan P, const double2* __restrict__ D, size_t ldd,
-                                                          const double* __restrict__ norm,
-                                                          const double2* __restrict__ Tm, int nk,
-                                                          double2* __restrict__ X, int* __restrict__ status) {
-    extern __shared__ double2 as_smem[];
-    const int M = 2 * P.nlm;
-    double2* A = as_smem;                  // M x M column-major
-    double2* B = A + M * M;                // M x AS_PANEL column-major; the harmonic table aliases it
-    __shared__ int piv[128];
-    __shared__ double2 dinv[128];
-    __shared__ int sing;
-    const int tid = threadIdx.x, nth = blockDim.x;
-    for (int kp = blockIdx.x; kp < nk; kp += gridDim.x) {
-        double2* Z = B;
-        for (int t = tid; t < P.tsize; t += nth) {
-            double2 d = D[(size_t)kp * ldd + t];
-            Z[t] = cscale(d, 1.0 / norm[t]);
-        }
-        __syncthreads();
-        // A = I - T S: item (s, d) writes rows 2d, 2d+1 of columns 2s, 2s+1
-        for (int it = tid; it < P.nlm * P.nlm; it += nth) {
-            int s = it / P.nlm, d = it - s * P.nlm;
-            int lam = 1;
-            while ((lam + 1) * (lam + 1) - 1 <= d) ++lam;
-            const double2* t4 = Tm + (lam - 1) * 4;
-            cplx Aa, Bb;
-            plan_combo_sums(P, s * P.nlm + d, Z, Aa, Bb);
-            cplx cp = cadd(Aa, Bb), cn = csub(Aa, Bb);
-            double one = s == d ? 1.0 : 0.0;
-            cplx a00 = cmul(t4[0], cp), a10 = cmul(t4[2], cp), a01 = cmul(t4[1], cn), a11 = cmul(t4[3], cn);
-            A[(2 * s) * M + 2 * d] = mk(one - a00.x, -a00.y);
-            A[(2 * s) * M + 2 * d + 1] = cneg(a10);
-            A[(2 * s + 1) * M + 2 * d] = cneg(a01);
-            A[(2 * s + 1) * M + 2 * d + 1] = mk(one - a11.x, -a11.y);
-        }
-        __syncthreads();
-        if (!blocked_lu(A, M, piv, dinv, &sing)) {
+        if (singular) {
             if (tid == 0) atomicExch(status, 5);
             __syncthreads();
             continue;
         }
-        // X = U^-1 L^-1 P T, panels of AS_PANEL columns
-        double2* Xk = X + (size_t)kp * M * M;
-        for (int c0 = 0; c0 < M; c0 += AS_PANEL) {
-            const int nc = min(AS_PANEL, M - c0);
-            // B = T (block diagonal: columns 2i, 2i+1 of mode pair i carry t[.][0], t[.][1])
-            for (int it = tid; it < M * nc; it += nth) {
-                int jj = it / M, i = it - jj * M, col = c0 + jj;
-                cplx v = mk(0.0, 0.0);
-                if ((i >> 1) == (col >> 1)) {
-                    int lm = col >> 1, lam = 1;
-                    while ((lam + 1) * (lam + 1) - 1 <= lm) ++lam;
-                    v = Tm[(lam - 1) * 4 + (i & 1) * 2 + (col & 1)];
+        // final row of each row of R: the column exchanges undone on the rows in reverse order
+        if (tid == 0) {
+            for (int i = 0; i < M; ++i) dest[i] = i;  // dest holds idx: position -> row of R
+            for (int k = M - 1; k >= 0; --k) {
+                const int p = piv[k];
+                if (p != k) {
+                    const int t = dest[k];
+                    dest[k] = dest[p];
+                    dest[p] = t;
                 }
-                B[jj * M + i] = v;
             }
-            __syncthreads();
-            blocked_lu_solve(A, M, piv, dinv, B, nc);
-            for (int it = tid; it < M * nc; it += nth) {
-                int jj = it / M, i = it - jj * M;
-                Xk[(size_t)(c0 + jj) * M + i] = B[jj * M + i];
-            }
-            __syncthreads();
+            for (int pos = 0; pos < M; ++pos) piv[dest[pos]] = pos;  // piv: row of R -> position
         }
+        __syncthreads();
+        if (own) {
+            double2* Xk = X + (size_t)kp * M * M;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int col = j0 + c;
+                if (col >= M) continue;
+                const int lm = col >> 1, q = col & 1;
+                int lam = 1;
+                while ((lam + 1) * (lam + 1) - 1 <= lm) ++lam;
+                const double2* t4 = Tm + (lam - 1) * 4;
+                const int cb = c & ~1;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int i = i0 + r;
+                    if (i >= M) continue;
+                    cplx v = cmul(a[r][cb], t4[q]);
+                    cfma(v, a[r][cb + 1], t4[2 + q]);
+                    Xk[(size_t)col * M + piv[i]] = v;
+                }
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -504,17 +485,12 @@ void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st) {
     lattice_sum_kernel<<<grid, 256, smem, st>>>(a);
 }
 
-size_t array_solve_smem(int L) {
-    int M = 2 * L * (L + 2);
-    return (size_t)M * M * 16 + (size_t)M * AS_PANEL * 16;
-}
-
 void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const double* norm, const double2* Tm, int nk,
                         double2* X, int* status, int grid, cudaStream_t st) {
     StageScope sc(ST_SMALL_LU, st);
-    size_t smem = array_solve_smem(P.L);
-    cudaFuncSetAttribute(array_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    array_solve_kernel<<<grid, 512, smem, st>>>(P, D, ldd, norm, Tm, nk, X, status);
+    const int tg = (P.nlm + 1) / 2;
+    const int threads = std::max(32, (tg * tg + 31) / 32 * 32);  // whole warps: the pivot reduction shuffles
+    array_solve_kernel<<<grid, threads, 0, st>>>(P, D, ldd, norm, Tm, nk, X, status);
 }
 
 }  // namespace tcu
