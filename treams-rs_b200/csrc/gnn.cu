@@ -27,6 +27,7 @@
 #include <atomic>
 #include <cmath>
 #include <complex>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -538,6 +539,7 @@ struct GraphData {
 class IterativeCoarse : public CoarseSolve {
    public:
     int nc = 0, m = 0, max_it = 0, nchunk = 0;
+    long long inner_iterations = 0;  // over all applications
     double rtol = 1e-3;
     DevArray Acc, V, w, part, h, small, dpart;
     long long* launches = nullptr;
@@ -613,6 +615,7 @@ class IterativeCoarse : public CoarseSolve {
             g[j + 1] = -std::conj(sn) * g[j];
             g[j] *= c;
             used = j + 1;
+            ++inner_iterations;
             if (std::abs(g[j + 1]) <= rtol * beta || next == 0.0) break;
             vec_scale_copy(Vb + (size_t)(j + 1) * nc, w.as<cplx>(), nc, 1.0 / next, st);
         }
@@ -650,7 +653,10 @@ struct Coarse {
         if (!solver) {  // no factor given: an inexact GMRES on the dipole rows of A[:, c]
             auto it = std::make_unique<IterativeCoarse>();
             it->launches = launches;
-            if (!it->build(N, M, n, Acols.as<float2>(), 30, 30, 1e-3, st)) return false;
+            // relative tolerance of the inner solve: 1e-3, or TCU_COARSE_RTOL
+            const char* e = getenv("TCU_COARSE_RTOL");
+            const double rtol = (e && atof(e) > 0.0 && atof(e) < 1.0) ? atof(e) : 1e-3;
+            if (!it->build(N, M, n, Acols.as<float2>(), 30, 30, rtol, st)) return false;
             solver = std::move(it);
         }
         return true;

@@ -249,13 +249,14 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
 // ---- batched periodic-array solve ----------------------------------------------------------
 // One CTA per Bloch vector, X = (I - T S)^-1 T (cluster/interaction.rs:292-315 with
 // sw/plan.rs:383-413 evaluate_periodic). The M x M operator (M = 2 lmax (lmax + 2), 96 at
-// lmax 6) lives in registers: thread (tr, tc) of a ceil(nlm/2) x ceil(nlm/2) grid owns the
-// 4 x 4 tile of rows 4 tr.., columns 4 tc.., i.e. the 2 x 2 mode blocks of destinations
-// d = 2 tr, 2 tr + 1 and sources s = 2 tc, 2 tc + 1, assembled there from the harmonic table
-// D / N and the plan's term lists. The inverse comes from in-place Gauss-Jordan elimination
+// lmax 6) lives in registers: thread (tr, tc) of a ceil(nlm/2) x ceil(nlm/3) grid owns the
+// 4 x 6 tile of rows 4 tr.., columns 6 tc.., i.e. the 2 x 2 mode blocks of destinations
+// d = 2 tr, 2 tr + 1 and sources s = 3 tc .. 3 tc + 2, assembled there from the harmonic table
+// D / N and the plan's term lists (384 threads at lmax 6: three warps per SM sub-partition
+// leave 168 registers a thread). The inverse comes from in-place Gauss-Jordan elimination
 // with column pivoting: at step k the pivot is the largest |a_kj|^2, j >= k (ties to the lower
 // column), columns k and p are exchanged, row k is scaled by 1 / a_kk and eliminated from every
-// other row (a rank-1 update of the whole tile grid, 16 complex multiply-adds per thread).
+// other row (a rank-1 update of the whole tile grid, 24 complex multiply-adds per thread).
 // Per step the owners of row k publish their candidates and row k, the owners of columns k and
 // p their columns, through shared memory; two barriers per step. The result R satisfies
 // A^-1 = the rows of R exchanged in the reverse order of the column exchanges, so
@@ -263,37 +264,37 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
 // holds both columns of each of its pairs, so R T is formed in registers and each row is stored
 // at its final position. (8/3 + 8 - 8/3 =) 8 M^3 real flops of elimination per Bloch vector.
 constexpr int GJ_MAXM = 96;
+constexpr int GJ_C = 6;  // tile columns (three mode pairs)
 
-// (48 / 2)^2 = 576 threads at lmax 6: at most 112 registers each
-__global__ void __maxnreg__(112) array_solve_kernel(DevPlan P, const double2* __restrict__ D,
+__global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const double2* __restrict__ D,
                                                                     size_t ldd, const double* __restrict__ norm,
                                                                     const double2* __restrict__ Tm, int nk,
                                                                     double2* __restrict__ X, int* __restrict__ status) {
     __shared__ double2 Z[(2 * 12 + 1) * (2 * 12 + 1)];  // harmonic table, order <= 2 lmax = 12
     __shared__ double2 colk[GJ_MAXM], colp[GJ_MAXM], rowk[GJ_MAXM];
-    __shared__ double cval[GJ_MAXM / 4];
-    __shared__ int cidx[GJ_MAXM / 4];
+    __shared__ double cval[GJ_MAXM / GJ_C];
+    __shared__ int cidx[GJ_MAXM / GJ_C];
     __shared__ int piv[GJ_MAXM], dest[GJ_MAXM];
-    const int nlm = P.nlm, M = 2 * nlm, TG = (nlm + 1) / 2;
+    const int nlm = P.nlm, M = 2 * nlm, TR = (nlm + 1) / 2, TC = (nlm + 2) / 3;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int tr = tid / TG, tc = tid - (tid / TG) * TG;
-    const bool own = tr < TG;
-    const int i0 = 4 * tr, j0 = 4 * tc;
+    const int tr = tid / TC, tc = tid - (tid / TC) * TC;
+    const bool own = tr < TR;
+    const int i0 = 4 * tr, j0 = GJ_C * tc;
     for (int kp = blockIdx.x; kp < nk; kp += gridDim.x) {
         for (int t = tid; t < P.tsize; t += blockDim.x) Z[t] = cscale(D[(size_t)kp * ldd + t], 1.0 / norm[t]);
         __syncthreads();
         // A = I - T S on the tile: combo (s, d) gives rows 2d, 2d+1 of columns 2s, 2s+1
-        cplx a[4][4];
+        cplx a[4][GJ_C];
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) a[r][c] = mk(0.0, 0.0);
+            for (int c = 0; c < GJ_C; ++c) a[r][c] = mk(0.0, 0.0);
         if (own) {
 #pragma unroll
             for (int dd = 0; dd < 2; ++dd)
 #pragma unroll
-                for (int ss = 0; ss < 2; ++ss) {
-                    const int d = 2 * tr + dd, sidx = 2 * tc + ss;
+                for (int ss = 0; ss < GJ_C / 2; ++ss) {
+                    const int d = 2 * tr + dd, sidx = (GJ_C / 2) * tc + ss;
                     if (d >= nlm || sidx >= nlm) continue;
                     int lam = 1;
                     while ((lam + 1) * (lam + 1) - 1 <= d) ++lam;
@@ -315,7 +316,7 @@ __global__ void __maxnreg__(112) array_solve_kernel(DevPlan P, const double2* __
             double best = -1.0;
             int bj = 0x7fffffff;
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int c = 0; c < GJ_C; ++c)
                 if (j0 + c < M && cabs2(a[0][c]) > best) {
                     best = cabs2(a[0][c]);
                     bj = j0 + c;
@@ -326,9 +327,9 @@ __global__ void __maxnreg__(112) array_solve_kernel(DevPlan P, const double2* __
         __syncthreads();
         bool singular = false;
         for (int k = 0; k < M; ++k) {
-            // pivot column: every warp reduces the TG candidates (largest, ties to the lower column)
-            double bv = lane < TG ? cval[lane] : -1.0;
-            int bj = lane < TG ? cidx[lane] : 0x7fffffff;
+            // pivot column: every warp reduces the TC candidates (largest, ties to the lower column)
+            double bv = lane < TC ? cval[lane] : -1.0;
+            int bj = lane < TC ? cidx[lane] : 0x7fffffff;
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) {
                 const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
@@ -350,12 +351,12 @@ __global__ void __maxnreg__(112) array_solve_kernel(DevPlan P, const double2* __
                 for (int r = 0; r < 4; ++r) {
                     if (i0 + r == k) {
 #pragma unroll
-                        for (int c = 0; c < 4; ++c)
+                        for (int c = 0; c < GJ_C; ++c)
                             if (j0 + c < M) rowk[j0 + c] = a[r][c];
                     }
                 }
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
+                for (int c = 0; c < GJ_C; ++c) {
                     if (j0 + c == k) {
 #pragma unroll
                         for (int r = 0; r < 4; ++r)
@@ -372,29 +373,29 @@ __global__ void __maxnreg__(112) array_solve_kernel(DevPlan P, const double2* __
             const cplx inv = cinv(rowk[p]);
             if (own) {
                 // scaled pivot row after the exchange: u_j = a_kj / a_kp (j != k), u_k = 1 / a_kp
-                cplx u[4];
+                cplx nl[4];  // minus the multipliers (column k after the exchange)
 #pragma unroll
-                for (int c = 0; c < 4; ++c) {
+                for (int r = 0; r < 4; ++r) nl[r] = i0 + r < M ? cneg(colp[i0 + r]) : mk(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < GJ_C; ++c) {
                     const int j = j0 + c;
-                    const int js = j == k ? p : (j == p ? k : j);
-                    u[c] = j == k ? inv : (j < M ? cmul(rowk[js], inv) : mk(0.0, 0.0));
-                }
+                    if (j >= M) continue;
+                    if (j == k) {
 #pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int i = i0 + r;
-                    const cplx l = i < M ? colp[i] : mk(0.0, 0.0);
-                    const cplx nl = cneg(l);
+                        for (int r = 0; r < 4; ++r) a[r][c] = i0 + r == k ? inv : cmul(nl[r], inv);
+                    } else {
+                        const cplx u = cmul(rowk[j == p ? k : j], inv);
+                        const bool swapped = j == p;
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) {
-                        const int j = j0 + c;
-                        if (i == k) {
-                            a[r][c] = u[c];
-                        } else if (j == k) {
-                            a[r][c] = cmul(nl, inv);
-                        } else {
-                            cplx cur = j == p ? colk[i < M ? i : 0] : a[r][c];
-                            cfma(cur, nl, u[c]);
-                            a[r][c] = cur;
+                        for (int r = 0; r < 4; ++r) {
+                            const int i = i0 + r;
+                            if (i == k) {
+                                a[r][c] = u;
+                            } else {
+                                cplx cur = swapped ? colk[i < M ? i : 0] : a[r][c];
+                                cfma(cur, nl[r], u);
+                                a[r][c] = cur;
+                            }
                         }
                     }
                 }
@@ -407,7 +408,7 @@ __global__ void __maxnreg__(112) array_solve_kernel(DevPlan P, const double2* __
                     for (int r = 0; r < 4; ++r) {
                         if (i0 + r != kn) continue;  // registers are indexed statically only
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) {
+                        for (int c = 0; c < GJ_C; ++c) {
                             const int j = j0 + c;
                             const double v = cabs2(a[r][c]);
                             if (j >= kn && j < M && v > best) {
@@ -444,7 +445,7 @@ __global__ void __maxnreg__(112) array_solve_kernel(DevPlan P, const double2* __
         if (own) {
             double2* Xk = X + (size_t)kp * M * M;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
+            for (int c = 0; c < GJ_C; ++c) {
                 const int col = j0 + c;
                 if (col >= M) continue;
                 const int lm = col >> 1, q = col & 1;
@@ -488,8 +489,8 @@ void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st) {
 void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const double* norm, const double2* Tm, int nk,
                         double2* X, int* status, int grid, cudaStream_t st) {
     StageScope sc(ST_SMALL_LU, st);
-    const int tg = (P.nlm + 1) / 2;
-    const int threads = std::max(32, (tg * tg + 31) / 32 * 32);  // whole warps: the pivot reduction shuffles
+    const int tr = (P.nlm + 1) / 2, tc = (P.nlm + 2) / 3;
+    const int threads = std::max(32, (tr * tc + 31) / 32 * 32);  // whole warps: the pivot reduction shuffles
     array_solve_kernel<<<grid, threads, 0, st>>>(P, D, ldd, norm, Tm, nk, X, status);
 }
 
