@@ -653,9 +653,10 @@ struct Coarse {
         if (!solver) {  // no factor given: an inexact GMRES on the dipole rows of A[:, c]
             auto it = std::make_unique<IterativeCoarse>();
             it->launches = launches;
-            // relative tolerance of the inner solve: 1e-3, or TCU_COARSE_RTOL
+            // relative tolerance of the inner solve: 3e-2 (the 4096-sphere workload measured 300,
+            // 291, 256 and 269 ms at 1e-3, 1e-2, 3e-2 and 1e-1), or TCU_COARSE_RTOL
             const char* e = getenv("TCU_COARSE_RTOL");
-            const double rtol = (e && atof(e) > 0.0 && atof(e) < 1.0) ? atof(e) : 1e-3;
+            const double rtol = (e && atof(e) > 0.0 && atof(e) < 1.0) ? atof(e) : 3e-2;
             if (!it->build(N, M, n, Acols.as<float2>(), 30, 30, rtol, st)) return false;
             solver = std::move(it);
         }

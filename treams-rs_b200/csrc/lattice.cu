@@ -253,28 +253,32 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
 // 4 x 6 tile of rows 4 tr.., columns 6 tc.., i.e. the 2 x 2 mode blocks of destinations
 // d = 2 tr, 2 tr + 1 and sources s = 3 tc .. 3 tc + 2, assembled there from the harmonic table
 // D / N and the plan's term lists (384 threads at lmax 6: three warps per SM sub-partition
-// leave 168 registers a thread). The inverse comes from in-place Gauss-Jordan elimination
-// with column pivoting: at step k the pivot is the largest |a_kj|^2, j >= k (ties to the lower
-// column), columns k and p are exchanged, row k is scaled by 1 / a_kk and eliminated from every
-// other row (a rank-1 update of the whole tile grid, 24 complex multiply-adds per thread).
-// Per step the owners of row k publish their candidates and row k, the owners of columns k and
-// p their columns, through shared memory; two barriers per step. The result R satisfies
-// A^-1 = the rows of R exchanged in the reverse order of the column exchanges, so
-// X = A^-1 T = that row exchange applied to R T; T is block diagonal per mode pair and a tile
-// holds both columns of each of its pairs, so R T is formed in registers and each row is stored
-// at its final position. (8/3 + 8 - 8/3 =) 8 M^3 real flops of elimination per Bloch vector.
+// leave 168 registers a thread).
+//
+// The inverse comes from in-place Gauss-Jordan exchange steps without any row or column
+// interchange: step k pivots on (k, p_k), p_k the not yet pivotal column with the largest
+// |a_kj|^2 (ties to the lower column). With inv = 1 / a_kp, u_j = a_kj inv (j != p) and
+// u_p = 1 + inv, every row i != k takes a_ij -= a_ip u_j, and row k becomes u_j (j != p) and
+// inv at p. The table B then expresses the unknowns through the right-hand sides:
+// (A^-1)[p_k][k'] = B[k][p_k'], so X[p_k][col] = sum_q' B[k][p_(2 lm + q')] t_lm[q'][q]
+// for col = 2 lm + q (T is block diagonal per mode pair). Per step the owners of row k and of
+// column p publish them through shared memory, two barriers per step, 24 complex multiply-adds
+// per thread; B goes through shared memory once for the final gather. 8 M^3 real flops of
+// elimination per Bloch vector.
 constexpr int GJ_MAXM = 96;
 constexpr int GJ_C = 6;  // tile columns (three mode pairs)
 
 __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const double2* __restrict__ D,
-                                                                    size_t ldd, const double* __restrict__ norm,
-                                                                    const double2* __restrict__ Tm, int nk,
-                                                                    double2* __restrict__ X, int* __restrict__ status) {
+                                                             size_t ldd, const double* __restrict__ norm,
+                                                             const double2* __restrict__ Tm, int nk,
+                                                             double2* __restrict__ X, int* __restrict__ status) {
+    extern __shared__ double2 gj_smem[];                 // B (M x M, column-major) for the final gather
     __shared__ double2 Z[(2 * 12 + 1) * (2 * 12 + 1)];  // harmonic table, order <= 2 lmax = 12
-    __shared__ double2 colk[GJ_MAXM], colp[GJ_MAXM], rowk[GJ_MAXM];
+    __shared__ double2 rowk[GJ_MAXM], colp[GJ_MAXM];
+    __shared__ double2 s_inv;
     __shared__ double cval[GJ_MAXM / GJ_C];
     __shared__ int cidx[GJ_MAXM / GJ_C];
-    __shared__ int piv[GJ_MAXM], dest[GJ_MAXM];
+    __shared__ int piv[GJ_MAXM];
     const int nlm = P.nlm, M = 2 * nlm, TR = (nlm + 1) / 2, TC = (nlm + 2) / 3;
     const int tid = threadIdx.x, lane = tid & 31;
     const int tr = tid / TC, tc = tid - (tid / TC) * TC;
@@ -311,8 +315,8 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
                     a[2 * dd + 1][2 * ss + 1] = mk(one - a11.x, -a11.y);
                 }
         }
-        // candidates of row 0 (tile row 0)
-        if (own && tr == 0) {
+        unsigned used = 0u;  // bit c: column j0 + c is already pivotal
+        if (own && tr == 0) {  // candidates of row 0
             double best = -1.0;
             int bj = 0x7fffffff;
 #pragma unroll
@@ -340,66 +344,55 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
                 }
             }
             const int p = bj;
-            if (!(bv > 0.0)) {  // an exactly zero row: singular (uniform over the CTA)
+            if (!(bv > 0.0)) {  // no nonzero entry left in row k: singular (uniform over the CTA)
                 singular = true;
                 break;
             }
             if (tid == 0) piv[k] = p;
-            // publish row k and columns k and p (values before the exchange)
+            // publish row k, column p and 1 / a_kp
             if (own) {
 #pragma unroll
                 for (int r = 0; r < 4; ++r) {
-                    if (i0 + r == k) {
+                    if (i0 + r != k) continue;
 #pragma unroll
-                        for (int c = 0; c < GJ_C; ++c)
-                            if (j0 + c < M) rowk[j0 + c] = a[r][c];
+                    for (int c = 0; c < GJ_C; ++c) {
+                        if (j0 + c >= M) continue;
+                        rowk[j0 + c] = a[r][c];
+                        if (j0 + c == p) s_inv = cinv(a[r][c]);
                     }
                 }
 #pragma unroll
                 for (int c = 0; c < GJ_C; ++c) {
-                    if (j0 + c == k) {
+                    if (j0 + c != p) continue;
 #pragma unroll
-                        for (int r = 0; r < 4; ++r)
-                            if (i0 + r < M) colk[i0 + r] = a[r][c];
-                    }
-                    if (j0 + c == p) {
-#pragma unroll
-                        for (int r = 0; r < 4; ++r)
-                            if (i0 + r < M) colp[i0 + r] = a[r][c];
-                    }
+                    for (int r = 0; r < 4; ++r)
+                        if (i0 + r < M) colp[i0 + r] = a[r][c];
                 }
             }
             __syncthreads();
-            const cplx inv = cinv(rowk[p]);
             if (own) {
-                // scaled pivot row after the exchange: u_j = a_kj / a_kp (j != k), u_k = 1 / a_kp
-                cplx nl[4];  // minus the multipliers (column k after the exchange)
+                const cplx inv = s_inv;
+                cplx nl[4];  // minus the multipliers a_ip
 #pragma unroll
                 for (int r = 0; r < 4; ++r) nl[r] = i0 + r < M ? cneg(colp[i0 + r]) : mk(0.0, 0.0);
 #pragma unroll
                 for (int c = 0; c < GJ_C; ++c) {
                     const int j = j0 + c;
                     if (j >= M) continue;
-                    if (j == k) {
+                    const bool jp = j == p;
+                    const cplx rk = cmul(rowk[j], inv);
+                    const cplx u = jp ? mk(1.0 + inv.x, inv.y) : rk;
 #pragma unroll
-                        for (int r = 0; r < 4; ++r) a[r][c] = i0 + r == k ? inv : cmul(nl[r], inv);
-                    } else {
-                        const cplx u = cmul(rowk[j == p ? k : j], inv);
-                        const bool swapped = j == p;
-#pragma unroll
-                        for (int r = 0; r < 4; ++r) {
-                            const int i = i0 + r;
-                            if (i == k) {
-                                a[r][c] = u;
-                            } else {
-                                cplx cur = swapped ? colk[i < M ? i : 0] : a[r][c];
-                                cfma(cur, nl[r], u);
-                                a[r][c] = cur;
-                            }
+                    for (int r = 0; r < 4; ++r) {
+                        if (i0 + r == k) {
+                            a[r][c] = jp ? inv : rk;
+                        } else {
+                            cfma(a[r][c], nl[r], u);
                         }
                     }
+                    if (jp) used |= 1u << c;
                 }
-                // candidates of row k + 1 over columns >= k + 1
+                // candidates of row k + 1 over the columns not yet pivotal
                 const int kn = k + 1;
                 if (kn < M && kn >= i0 && kn < i0 + 4) {
                     double best = -1.0;
@@ -411,7 +404,7 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
                         for (int c = 0; c < GJ_C; ++c) {
                             const int j = j0 + c;
                             const double v = cabs2(a[r][c]);
-                            if (j >= kn && j < M && v > best) {
+                            if (j < M && !((used >> c) & 1u) && v > best) {
                                 best = v;
                                 bjn = j;
                             }
@@ -428,40 +421,26 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
             __syncthreads();
             continue;
         }
-        // final row of each row of R: the column exchanges undone on the rows in reverse order
-        if (tid == 0) {
-            for (int i = 0; i < M; ++i) dest[i] = i;  // dest holds idx: position -> row of R
-            for (int k = M - 1; k >= 0; --k) {
-                const int p = piv[k];
-                if (p != k) {
-                    const int t = dest[k];
-                    dest[k] = dest[p];
-                    dest[p] = t;
-                }
-            }
-            for (int pos = 0; pos < M; ++pos) piv[dest[pos]] = pos;  // piv: row of R -> position
+        // X[p_k][col] = sum_q' B[k][p_(2 lm + q')] t_lm[q'][q], B through shared memory
+        double2* Bs = gj_smem;
+        if (own) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < GJ_C; ++c)
+                    if (i0 + r < M && j0 + c < M) Bs[(size_t)(j0 + c) * M + i0 + r] = a[r][c];
         }
         __syncthreads();
-        if (own) {
-            double2* Xk = X + (size_t)kp * M * M;
-#pragma unroll
-            for (int c = 0; c < GJ_C; ++c) {
-                const int col = j0 + c;
-                if (col >= M) continue;
-                const int lm = col >> 1, q = col & 1;
-                int lam = 1;
-                while ((lam + 1) * (lam + 1) - 1 <= lm) ++lam;
-                const double2* t4 = Tm + (lam - 1) * 4;
-                const int cb = c & ~1;
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int i = i0 + r;
-                    if (i >= M) continue;
-                    cplx v = cmul(a[r][cb], t4[q]);
-                    cfma(v, a[r][cb + 1], t4[2 + q]);
-                    Xk[(size_t)col * M + piv[i]] = v;
-                }
-            }
+        double2* Xk = X + (size_t)kp * M * M;
+        for (int t = tid; t < M * M; t += blockDim.x) {
+            const int col = t / M, k = t - col * M;  // consecutive threads: consecutive k
+            const int lm = col >> 1, q = col & 1;
+            int lam = 1;
+            while ((lam + 1) * (lam + 1) - 1 <= lm) ++lam;
+            const double2* t4 = Tm + (lam - 1) * 4;
+            cplx v = cmul(Bs[(size_t)piv[2 * lm] * M + k], t4[q]);
+            cfma(v, Bs[(size_t)piv[2 * lm + 1] * M + k], t4[2 + q]);
+            Xk[(size_t)col * M + piv[k]] = v;
         }
         __syncthreads();
     }
@@ -489,9 +468,11 @@ void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st) {
 void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const double* norm, const double2* Tm, int nk,
                         double2* X, int* status, int grid, cudaStream_t st) {
     StageScope sc(ST_SMALL_LU, st);
-    const int tr = (P.nlm + 1) / 2, tc = (P.nlm + 2) / 3;
+    const int tr = (P.nlm + 1) / 2, tc = (P.nlm + 2) / 3, M = 2 * P.nlm;
     const int threads = std::max(32, (tr * tc + 31) / 32 * 32);  // whole warps: the pivot reduction shuffles
-    array_solve_kernel<<<grid, threads, 0, st>>>(P, D, ldd, norm, Tm, nk, X, status);
+    const size_t smem = (size_t)M * M * sizeof(double2);
+    cudaFuncSetAttribute(array_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    array_solve_kernel<<<grid, threads, smem, st>>>(P, D, ldd, norm, Tm, nk, X, status);
 }
 
 }  // namespace tcu
