@@ -200,10 +200,11 @@ typedef struct tcu_cluster_desc {
 
 /* Solve a batch of independent clusters (no counterpart in the reference, which solves one
  * cluster per call): largest first (n = N * 2 lmax (lmax + 2)), each assembled, factored,
- * solved and released in turn on the context's stream, so device memory holds one cluster's
- * operator at a time and the pooled allocator reuses it. precision: TCU_FP64, TCU_MIXED or
- * TCU_AUTO. order (count entries, may be NULL) receives the processing order. Stops at the
- * first failing cluster; the message names it. */
+ * solved and released. TCU_BATCH_WORKERS (default 4) host threads with one stream each take
+ * the clusters from a shared queue, so the latency-bound stages of different clusters overlap
+ * and device memory holds at most that many operators at a time. precision: TCU_FP64,
+ * TCU_MIXED or TCU_AUTO. order (count entries, may be NULL) receives the dispatch order (size
+ * order). Stops at the first failing cluster; the message names it. */
 tcu_status tcu_batch_solve(tcu_context* ctx, size_t count, const tcu_cluster_desc* clusters, int precision,
                            int* order);
 

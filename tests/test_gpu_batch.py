@@ -131,3 +131,22 @@ def test_autotuned_crossover_drives_auto_precision():
             assert np.linalg.norm(Xi - Ri) <= 1e-10 * np.linalg.norm(Ri)
     finally:
         ctx.close()
+
+
+def test_worker_threads_give_the_sequential_results(ctx, monkeypatch):
+    # 12 clusters of the sweep (whole clusters: n up to ~20,000, mixed and FP64 by the crossover)
+    # solved by 4 host workers with a stream each and by one: the same factors and refinements,
+    # so the same solutions and certificates
+    batch = []
+    for c in range(12):
+        w = workloads.batch_cluster(c)
+        B = t.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)
+        batch.append((w.lmax, w.k0, w.radii, w.eps, w.positions, B))
+    monkeypatch.setenv("TCU_BATCH_WORKERS", "4")
+    X4, c4, o4 = t.batch_solve(batch, "auto", ctx=ctx)
+    monkeypatch.setenv("TCU_BATCH_WORKERS", "1")
+    X1, c1, o1 = t.batch_solve(batch, "auto", ctx=ctx)
+    assert o4 == o1
+    for a, b, ca, cb in zip(X4, X1, c4, c1):
+        assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(b)
+        assert ca[0].residual_norm <= 1e-12 * ca[0].rhs_norm

@@ -13,6 +13,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/treams_cuda.h"
@@ -105,6 +106,7 @@ struct tcu_context {
     double refine_target = 1e-13; // refinement stops at ||r|| <= refine_target ||T b||
     double fallback_above = 1e-12;  // mixed solves left above this finish in FP64
     size_t auto_crossover = 2048;   // TCU_AUTO: mixed from this many unknowns on (tcu_context_autotune)
+    std::vector<tcu_context*> workers;  // batched solves: a context (stream, scratch, pool) per host worker
 };
 
 struct tcu_factor {
@@ -681,6 +683,13 @@ struct FactorCoarse : CoarseSolve {
     }
 };
 
+// Host worker threads of tcu_batch_solve: TCU_BATCH_WORKERS (1..8), default 4.
+int batch_workers() {
+    const char* e = getenv("TCU_BATCH_WORKERS");
+    const int v = e ? atoi(e) : 4;
+    return std::max(1, std::min(8, v));
+}
+
 // The dipole (lmax 1) system of a cluster: factored (complex64 from 2048 modes on, else FP64) up
 // to 6144 dipole modes; above, no factor is made (out stays empty) and the two-level
 // preconditioner solves the dipole system by an inner GMRES on its stored dipole columns.
@@ -740,6 +749,7 @@ tcu_status tcu_context_destroy(tcu_context* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     while (!ctx->factors.empty()) tcu_factor_destroy(*ctx->factors.begin());  // factors left alive
+    for (tcu_context* w : ctx->workers) tcu_context_destroy(w);
     for (auto& kv : ctx->plans) cudaFree(kv.second->mem);
     ctx->pool.release();
     cudaFree(ctx->d_partial);
@@ -1789,19 +1799,75 @@ extern "C" tcu_status tcu_batch_solve(tcu_context* ctx, size_t count, const tcu_
     }
     auto modes = [&](size_t i) { return clusters[i].N * 2 * (size_t)clusters[i].lmax * (clusters[i].lmax + 2); };
     std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return modes(a) > modes(b); });
-    for (size_t q = 0; q < count; ++q) {
-        const size_t i = idx[q];
-        if (order) order[q] = (int)i;
+    for (size_t q = 0; q < count && order; ++q) order[q] = (int)idx[q];
+    auto solve_one = [&](tcu_context* c_ctx, size_t i) -> tcu_status {
         const tcu_cluster_desc& c = clusters[i];
         int prec = precision == TCU_AUTO ? (modes(i) >= ctx->auto_crossover ? TCU_MIXED : TCU_FP64) : precision;
         tcu_factor* f = nullptr;
-        tcu_status s = tcu_sphere_cluster_factor(ctx, c.lmax, c.k0, c.N, c.radii, c.eps, c.positions, prec, &f);
+        tcu_status s = tcu_sphere_cluster_factor(c_ctx, c.lmax, c.k0, c.N, c.radii, c.eps, c.positions, prec, &f);
         if (s == TCU_OK) {
             s = tcu_factor_solve(f, c.B, c.p, c.X, c.certificates);
             tcu_factor_destroy(f);
         }
-        if (s) return fail(s, "cluster " + std::to_string(i) + ": " + g_last_error);
+        return s;
+    };
+    const int K = (int)std::min<size_t>((size_t)batch_workers(), count);
+    if (K <= 1) {
+        for (size_t q = 0; q < count; ++q) {
+            tcu_status s = solve_one(ctx, idx[q]);
+            if (s) return fail(s, "cluster " + std::to_string(idx[q]) + ": " + g_last_error);
+        }
+        return TCU_OK;
     }
+    // K host threads, each with its own context (stream, scratch, pooled allocator), take the
+    // clusters largest first from a shared counter: the latency-bound panels and sweeps of
+    // different clusters overlap on the GPU.
+    {
+        std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+        while ((int)ctx->workers.size() < K) {
+            tcu_context* w = nullptr;
+            tcu_status s = tcu_context_create(ctx->device, &w);
+            if (s) return s;
+            ctx->workers.push_back(w);
+        }
+    }
+    std::vector<long long> fb0(K), ln0(K);
+    for (int w = 0; w < K; ++w) {
+        tcu_context* wc = ctx->workers[w];
+        wc->refine_target = ctx->refine_target;
+        wc->fallback_above = ctx->fallback_above;
+        fb0[w] = wc->fallbacks;
+        ln0[w] = wc->launches;
+    }
+    std::atomic<size_t> next{0};
+    std::atomic<bool> stop{false};
+    std::mutex emu;
+    tcu_status first = TCU_OK;
+    std::string msg;
+    std::vector<std::thread> threads;
+    for (int w = 0; w < K; ++w)
+        threads.emplace_back([&, w] {
+            cudaSetDevice(ctx->device);
+            while (!stop.load()) {
+                const size_t q = next.fetch_add(1);
+                if (q >= count) break;
+                const tcu_status s = solve_one(ctx->workers[w], idx[q]);
+                if (s) {
+                    std::lock_guard<std::mutex> g(emu);
+                    if (first == TCU_OK) {
+                        first = s;
+                        msg = "cluster " + std::to_string(idx[q]) + ": " + g_last_error;
+                    }
+                    stop = true;
+                }
+            }
+        });
+    for (auto& t : threads) t.join();
+    for (int w = 0; w < K; ++w) {
+        ctx->fallbacks += ctx->workers[w]->fallbacks - fb0[w];
+        ctx->launches += ctx->workers[w]->launches - ln0[w];
+    }
+    if (first) return fail(first, msg);
     return TCU_OK;
 }
 

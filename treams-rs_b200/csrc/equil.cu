@@ -15,7 +15,8 @@
 // [ln 2, 2 ln 2); sweeps stop after one that moves no factor by more than 2 (at most 64). A sum
 // that is not normal leaves the max scales alone; so do factors beyond 2^+-256. Two passes over
 // the matrix per sweep: column sums (CTA per column) and row sums (threads over rows, partial
-// per column chunk, fixed-order reduction).
+// per column chunk, fixed-order reduction). The sweeps read the unscaled A with the max scales
+// applied on the fly, and A is scaled once at the end: 3 + 2 sweeps passes over the matrix.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -119,40 +120,43 @@ __device__ __forceinline__ void bal_advance(double& factor, double sum, int* fla
     if (step < 0.5 || step > 2.0) atomicOr(flags, BAL_COARSE);
 }
 
+// The sweeps run on R A C without forming it: |a_ij| r_i c_j with the max scales r, c.
 template <typename C>
-__global__ void bal_col_kernel(const C* __restrict__ A, int n, const double* __restrict__ x, double* __restrict__ y,
+__global__ void bal_col_kernel(const C* __restrict__ A, int n, const double* __restrict__ r,
+                               const double* __restrict__ c, const double* __restrict__ x, double* __restrict__ y,
                                int* flags) {
     __shared__ double sh[256];
     const int j = blockIdx.x;
     double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += x[i] * mag(A[(size_t)j * n + i]);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += x[i] * r[i] * mag(A[(size_t)j * n + i]);
     sh[threadIdx.x] = s;
     __syncthreads();
     for (int w = blockDim.x / 2; w > 0; w >>= 1) {
         if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) bal_advance(y[j], sh[0], flags);
+    if (threadIdx.x == 0) bal_advance(y[j], sh[0] * c[j], flags);
 }
 
 template <typename C>
-__global__ void bal_row_partial(const C* __restrict__ A, int n, const double* __restrict__ y,
-                                double* __restrict__ partial) {
+__global__ void bal_row_partial(const C* __restrict__ A, int n, const double* __restrict__ c,
+                                const double* __restrict__ y, double* __restrict__ partial) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int per = (n + EQ_CHUNKS - 1) / EQ_CHUNKS;
     const int j0 = blockIdx.y * per, j1 = min(n, j0 + per);
     double s = 0.0;
-    for (int j = j0; j < j1; ++j) s += mag(A[(size_t)j * n + i]) * y[j];
+    for (int j = j0; j < j1; ++j) s += mag(A[(size_t)j * n + i]) * (c[j] * y[j]);
     partial[(size_t)blockIdx.y * n + i] = s;
 }
 
-__global__ void bal_row_update(const double* __restrict__ partial, int n, double* __restrict__ x, int* flags) {
+__global__ void bal_row_update(const double* __restrict__ partial, int n, const double* __restrict__ r,
+                               double* __restrict__ x, int* flags) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0.0;
     for (int c = 0; c < EQ_CHUNKS; ++c) s += partial[(size_t)c * n + i];
-    bal_advance(x[i], s, flags);
+    bal_advance(x[i], s * r[i], flags);
 }
 
 // factors within 2^+-256 and normal products with the max scales, else BAL_UNFIT
@@ -180,10 +184,10 @@ __global__ void fill_kernel(double* __restrict__ v, size_t n, double value) {
     if (i < n) v[i] = value;
 }
 
-// Balancing sweeps over the max-equilibrated A (R A C, scales r and c); on success A, r and c
-// take the factors. scratch: x (n), y (n), partial (EQ_CHUNKS n), flags (one int).
+// Balancing sweeps over R A C (A unscaled, max scales r and c); on success r and c take the
+// factors (the caller then scales A once). scratch: x (n), y (n), partial (EQ_CHUNKS n), flags.
 template <typename C>
-tcu_status balance_impl(C* A, int n, double* r, double* c, double* scratch, int* sweeps_out, cudaStream_t st,
+tcu_status balance_impl(const C* A, int n, double* r, double* c, double* scratch, int* sweeps_out, cudaStream_t st,
                         long long* launches) {
     double* x = scratch;
     double* y = x + n;
@@ -195,9 +199,9 @@ tcu_status balance_impl(C* A, int n, double* r, double* c, double* scratch, int*
     int flags = 0, sweep = 0;
     for (; sweep < BAL_SWEEPS; ++sweep) {
         if (cudaMemsetAsync(d_flags, 0, sizeof(int), st) != cudaSuccess) return TCU_DEVICE_ERROR;
-        bal_col_kernel<C><<<n, 256, 0, st>>>(A, n, x, y, d_flags);
-        bal_row_partial<C><<<dim3(nb, EQ_CHUNKS), 256, 0, st>>>(A, n, y, partial);
-        bal_row_update<<<nb, 256, 0, st>>>(partial, n, x, d_flags);
+        bal_col_kernel<C><<<n, 256, 0, st>>>(A, n, r, c, x, y, d_flags);
+        bal_row_partial<C><<<dim3(nb, EQ_CHUNKS), 256, 0, st>>>(A, n, c, y, partial);
+        bal_row_update<<<nb, 256, 0, st>>>(partial, n, r, x, d_flags);
         if (launches) *launches += 3;
         if (cudaMemcpyAsync(&flags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
@@ -218,9 +222,8 @@ tcu_status balance_impl(C* A, int n, double* r, double* c, double* scratch, int*
         *sweeps_out = -(sweep + 1);
         return TCU_OK;
     }
-    apply_scales<C><<<148 * 16, 256, 0, st>>>(A, n, x, y);
     bal_fold_kernel<<<nb, 256, 0, st>>>(n, x, y, r, c);
-    if (launches) *launches += 2;
+    if (launches) *launches += 1;
     *sweeps_out = std::min(sweep + 1, BAL_SWEEPS);
     return TCU_OK;
 }
@@ -242,11 +245,14 @@ tcu_status equilibrate_impl(C* A, int n, double threshold, double* r, double* c,
     for (double v : bm) mx = std::max(mx, v);
     if (!(mx > threshold)) return TCU_OK;  // entries within the spread a unit diagonal tolerates
     col_scale<C><<<n, 256, 0, st>>>(A, n, r, c);
-    apply_scales<C><<<148 * 16, 256, 0, st>>>(A, n, r, c);
-    if (launches) *launches += 2;
-    *applied = true;
+    if (launches) ++*launches;
     int sweeps = 0;
-    return balance_impl<C>(A, n, r, c, partial, &sweeps, st, launches);
+    const tcu_status s = balance_impl<C>(A, n, r, c, partial, &sweeps, st, launches);
+    if (s) return s;
+    apply_scales<C><<<148 * 16, 256, 0, st>>>(A, n, r, c);  // R A C with the balanced (or max) scales
+    if (launches) ++*launches;
+    *applied = true;
+    return TCU_OK;
 }
 
 }  // namespace

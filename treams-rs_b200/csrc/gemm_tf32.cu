@@ -527,14 +527,14 @@ typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, v
                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 static EncodeTiled encoder() {
-    static EncodeTiled fn = nullptr;
-    if (!fn) {
+    static const EncodeTiled fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiled)p;
-    }
+            return (EncodeTiled)p;
+        return (EncodeTiled) nullptr;
+    }();
     return fn;
 }
 
@@ -561,28 +561,25 @@ constexpr size_t TI_SMEM = (size_t)(128 * 129 + 64 * 64) * sizeof(float2);
 // more than 2^20 even after equilibration, and FP16 pieces (8 exponent bits fewer) then leave
 // the FP64 refinement stalled, so every solve fell back to TF32 pieces.
 bool split_f16_default() {
-    static int on = -1;
-    if (on < 0) {
+    static const bool on = [] {
         const char* e = getenv("TCU_SPLIT");
-        on = (e && std::strcmp(e, "f16") == 0) ? 1 : 0;
-    }
-    return on == 1;
+        return e && std::strcmp(e, "f16") == 0;
+    }();
+    return on;
 }
 
 bool tf32_enabled() {
-    static int on = -1;
-    if (on < 0) {
+    static const int on = [] {
         const char* e = getenv("TCU_DISABLE_TCGEN05");
-        on = (e && e[0] == '1') ? 0 : 1;
-        if (on && !encoder()) on = 0;
-    }
+        return (e && e[0] == '1') || !encoder() ? 0 : 1;
+    }();
     if (on == 1) {
-        static std::atomic<unsigned long long> attr{0};
-        if (first_use_on_device(attr)) {
+        static PerDeviceOnce attr;
+        once_per_device(attr, [] {
             cudaFuncSetAttribute(tf32_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
             cudaFuncSetAttribute(tf32_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
             cudaFuncSetAttribute(tri_inverse_l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TI_SMEM);
-        }
+        });
     }
     return on == 1;
 }
@@ -670,12 +667,12 @@ size_t tf32_pack_bytes(int n) {
 }
 
 static int num_sms() {
-    static int sms = 0;
-    if (!sms) {
-        int dev;
+    static const int sms = [] {
+        int dev = 0, v = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v;
+    }();
     return sms;
 }
 

@@ -841,9 +841,10 @@ tcu_status LearnedProblem::loss_grad(const double* h_weights, double* loss, doub
     launch_apply_th(L, N_, d_T, m.U.as<cplx>(), n, p, m.Wt.as<cplx>(), st);
     if (nnz > 0) {
         const size_t smem = (size_t)nlm * nlm * sizeof(cplx);
-        static std::atomic<unsigned long long> attr{0};
-        if (first_use_on_device(attr))
+        static PerDeviceOnce attr;
+        once_per_device(attr, [] {
             cudaFuncSetAttribute(theta_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+        });
         theta_grad_kernel<<<(unsigned)nnz, 256, smem, st>>>((int)nnz, g.row.as<int>(), g.nbr.as<int>(), L, nlm,
                                                             g.C.as<cplx>(), m.Wt.as<cplx>(), m.R1.as<cplx>(), n, p,
                                                             m.dTH.as<double>());

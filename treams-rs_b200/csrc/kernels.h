@@ -7,6 +7,7 @@
 #include "plan.h"
 
 #include <atomic>
+#include <mutex>
 #include <vector>
 
 namespace tcu {
@@ -15,11 +16,24 @@ typedef double2 cplx;
 
 // Kernel attributes (large dynamic shared memory) are per device: each site keeps one bit per
 // device in `mask`, and this returns true the first time it runs with that device current.
-inline bool first_use_on_device(std::atomic<unsigned long long>& mask) {
+struct PerDeviceOnce {
+    std::mutex mu;
+    unsigned long long done = 0;  // bit d: done on device d
+};
+// Runs f once per process and current device; callers on other threads wait until it is done
+// (the batched solve launches from several host threads).
+template <class F>
+inline void once_per_device(PerDeviceOnce& o, F&& f) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        f();
+        return;
+    }
     const unsigned long long bit = 1ull << dev;
-    return (mask.fetch_or(bit) & bit) == 0;
+    std::lock_guard<std::mutex> g(o.mu);
+    if (o.done & bit) return;
+    f();
+    o.done |= bit;
 }
 
 // Per-stage CUDA-event timing (tcu_context_set_profiling). The API layer installs the

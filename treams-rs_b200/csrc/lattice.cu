@@ -249,24 +249,38 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
 // ---- batched periodic-array solve ----------------------------------------------------------
 // One CTA per Bloch vector, X = (I - T S)^-1 T (cluster/interaction.rs:292-315 with
 // sw/plan.rs:383-413 evaluate_periodic). The M x M operator (M = 2 lmax (lmax + 2), 96 at
-// lmax 6) lives in registers: thread (tr, tc) of a ceil(nlm/2) x ceil(nlm/3) grid owns the
-// 4 x 6 tile of rows 4 tr.., columns 6 tc.., i.e. the 2 x 2 mode blocks of destinations
-// d = 2 tr, 2 tr + 1 and sources s = 3 tc .. 3 tc + 2, assembled there from the harmonic table
-// D / N and the plan's term lists (384 threads at lmax 6: three warps per SM sub-partition
-// leave 168 registers a thread).
+// lmax 6) lives in registers: thread (tr, tc) owns the 4 x 6 tile of rows 4 tr.., columns
+// 6 tc.., i.e. the 2 x 2 mode blocks of destinations d = 2 tr, 2 tr + 1 and sources
+// s = 3 tc .. 3 tc + 2, assembled there from the harmonic table D / N and the plan's term lists.
+// A tile row is a segment of TCP = 2^ceil(log2 ceil(nlm / 3)) lanes of one warp (16 at lmax 6:
+// 24 x 16 = 384 threads, three warps per SM sub-partition, 168 registers a thread).
 //
-// The inverse comes from in-place Gauss-Jordan exchange steps without any row or column
-// interchange: step k pivots on (k, p_k), p_k the not yet pivotal column with the largest
-// |a_kj|^2 (ties to the lower column). With inv = 1 / a_kp, u_j = a_kj inv (j != p) and
-// u_p = 1 + inv, every row i != k takes a_ij -= a_ip u_j, and row k becomes u_j (j != p) and
-// inv at p. The table B then expresses the unknowns through the right-hand sides:
-// (A^-1)[p_k][k'] = B[k][p_k'], so X[p_k][col] = sum_q' B[k][p_(2 lm + q')] t_lm[q'][q]
-// for col = 2 lm + q (T is block diagonal per mode pair). Per step the owners of row k and of
-// column p publish them through shared memory, two barriers per step, 24 complex multiply-adds
-// per thread; B goes through shared memory once for the final gather. 8 M^3 real flops of
-// elimination per Bloch vector.
+// The inverse comes from in-place Gauss-Jordan exchange steps without row or column
+// interchanges, four rows at a time. Block step k0: the segment owning rows k0..k0+3 runs the
+// four exchange steps on its own rows with shuffles only (step t pivots on (k0 + t, p_t), p_t
+// the not yet pivotal column with the largest |a|^2 in row k0 + t, ties to the lower column; with
+// inv = 1 / a_(k0+t) p_t, u_j = a_(k0+t) j inv (j != p_t), u_p = 1 + inv, the other block rows
+// take a_rj -= a_rp u_j and row k0 + t becomes u_j, inv at p_t). It publishes the transformed
+// rows U (plus 1 at each row's own pivot column) and p_0..p_3; after one barrier every other row
+// takes the rank-4 update a_ij -= sum_t a_(i p_t) U_tj, its a_(i p_t) fetched by shuffles inside
+// its own segment. U and the pivots are double-buffered, so one barrier per four rows. The table
+// B then expresses the unknowns through the right-hand sides: (A^-1)[p_k][k'] = B[k][p_k'], so
+// X[p_k][col] = sum_q' B[k][p_(2 lm + q')] t_lm[q'][q] for col = 2 lm + q (T is block diagonal
+// per mode pair), gathered through shared memory. 8 M^3 real flops per Bloch vector.
 constexpr int GJ_MAXM = 96;
 constexpr int GJ_C = 6;  // tile columns (three mode pairs)
+
+__device__ __forceinline__ cplx shfl_c(unsigned mask, cplx v, int src, int width) {
+    return mk(__shfl_sync(mask, v.x, src, width), __shfl_sync(mask, v.y, src, width));
+}
+// a[c] for a runtime c < GJ_C with static register indexing
+__device__ __forceinline__ cplx pick6(const cplx* a, int c) {
+    cplx v = a[0];
+#pragma unroll
+    for (int q = 1; q < GJ_C; ++q)
+        if (c == q) v = a[q];
+    return v;
+}
 
 __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const double2* __restrict__ D,
                                                              size_t ldd, const double* __restrict__ norm,
@@ -274,18 +288,22 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
                                                              double2* __restrict__ X, int* __restrict__ status) {
     extern __shared__ double2 gj_smem[];                 // B (M x M, column-major) for the final gather
     __shared__ double2 Z[(2 * 12 + 1) * (2 * 12 + 1)];  // harmonic table, order <= 2 lmax = 12
-    __shared__ double2 rowk[GJ_MAXM], colp[GJ_MAXM];
-    __shared__ double2 s_inv;
-    __shared__ double cval[GJ_MAXM / GJ_C];
-    __shared__ int cidx[GJ_MAXM / GJ_C];
+    __shared__ double2 Ublk[2][4][GJ_MAXM];
+    __shared__ int pvt[2][4];
     __shared__ int piv[GJ_MAXM];
+    __shared__ int s_sing;
     const int nlm = P.nlm, M = 2 * nlm, TR = (nlm + 1) / 2, TC = (nlm + 2) / 3;
+    int TCP = 1;
+    while (TCP < TC) TCP *= 2;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int tr = tid / TC, tc = tid - (tid / TC) * TC;
-    const bool own = tr < TR;
+    const int tr = tid / TCP, tc = tid - (tid / TCP) * TCP;
+    const bool own = tr < TR && tc < TC;
+    const bool rowseg = tr < TR;  // this lane's segment is a tile row of the operator
     const int i0 = 4 * tr, j0 = GJ_C * tc;
+    const unsigned seg = TCP >= 32 ? 0xffffffffu : (((1u << TCP) - 1u) << (lane & ~(TCP - 1)));
     for (int kp = blockIdx.x; kp < nk; kp += gridDim.x) {
         for (int t = tid; t < P.tsize; t += blockDim.x) Z[t] = cscale(D[(size_t)kp * ldd + t], 1.0 / norm[t]);
+        if (tid == 0) s_sing = 0;
         __syncthreads();
         // A = I - T S on the tile: combo (s, d) gives rows 2d, 2d+1 of columns 2s, 2s+1
         cplx a[4][GJ_C];
@@ -316,105 +334,109 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
                 }
         }
         unsigned used = 0u;  // bit c: column j0 + c is already pivotal
-        if (own && tr == 0) {  // candidates of row 0
-            double best = -1.0;
-            int bj = 0x7fffffff;
-#pragma unroll
-            for (int c = 0; c < GJ_C; ++c)
-                if (j0 + c < M && cabs2(a[0][c]) > best) {
-                    best = cabs2(a[0][c]);
-                    bj = j0 + c;
-                }
-            cval[tc] = best;
-            cidx[tc] = bj;
-        }
-        __syncthreads();
         bool singular = false;
-        for (int k = 0; k < M; ++k) {
-            // pivot column: every warp reduces the TC candidates (largest, ties to the lower column)
-            double bv = lane < TC ? cval[lane] : -1.0;
-            int bj = lane < TC ? cidx[lane] : 0x7fffffff;
+        for (int kb = 0, buf = 0; 4 * kb < M; ++kb, buf ^= 1) {
+            const int k0 = 4 * kb, bw = min(4, M - k0);
+            if (tr == kb) {
+                // the block rows: bw exchange steps inside the segment
+                int pk[4] = {0, 0, 0, 0};
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-                const int oj = __shfl_xor_sync(0xffffffffu, bj, off);
-                if (ov > bv || (ov == bv && oj < bj)) {
-                    bv = ov;
-                    bj = oj;
-                }
-            }
-            const int p = bj;
-            if (!(bv > 0.0)) {  // no nonzero entry left in row k: singular (uniform over the CTA)
-                singular = true;
-                break;
-            }
-            if (tid == 0) piv[k] = p;
-            // publish row k, column p and 1 / a_kp
-            if (own) {
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    if (i0 + r != k) continue;
+                for (int t = 0; t < 4; ++t) {
+                    if (t >= bw) break;
+                    double best = -1.0;
+                    int bj = 0x7fffffff;
 #pragma unroll
                     for (int c = 0; c < GJ_C; ++c) {
-                        if (j0 + c >= M) continue;
-                        rowk[j0 + c] = a[r][c];
-                        if (j0 + c == p) s_inv = cinv(a[r][c]);
-                    }
-                }
-#pragma unroll
-                for (int c = 0; c < GJ_C; ++c) {
-                    if (j0 + c != p) continue;
-#pragma unroll
-                    for (int r = 0; r < 4; ++r)
-                        if (i0 + r < M) colp[i0 + r] = a[r][c];
-                }
-            }
-            __syncthreads();
-            if (own) {
-                const cplx inv = s_inv;
-                cplx nl[4];  // minus the multipliers a_ip
-#pragma unroll
-                for (int r = 0; r < 4; ++r) nl[r] = i0 + r < M ? cneg(colp[i0 + r]) : mk(0.0, 0.0);
-#pragma unroll
-                for (int c = 0; c < GJ_C; ++c) {
-                    const int j = j0 + c;
-                    if (j >= M) continue;
-                    const bool jp = j == p;
-                    const cplx rk = cmul(rowk[j], inv);
-                    const cplx u = jp ? mk(1.0 + inv.x, inv.y) : rk;
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) {
-                        if (i0 + r == k) {
-                            a[r][c] = jp ? inv : rk;
-                        } else {
-                            cfma(a[r][c], nl[r], u);
+                        const int j = j0 + c;
+                        const double v = cabs2(a[t][c]);
+                        if (own && j < M && !((used >> c) & 1u) && v > best) {
+                            best = v;
+                            bj = j;
                         }
                     }
-                    if (jp) used |= 1u << c;
-                }
-                // candidates of row k + 1 over the columns not yet pivotal
-                const int kn = k + 1;
-                if (kn < M && kn >= i0 && kn < i0 + 4) {
-                    double best = -1.0;
-                    int bjn = 0x7fffffff;
+                    for (int off = TCP / 2; off > 0; off >>= 1) {
+                        const double ov = __shfl_xor_sync(seg, best, off, TCP);
+                        const int oj = __shfl_xor_sync(seg, bj, off, TCP);
+                        if (ov > best || (ov == best && oj < bj)) {
+                            best = ov;
+                            bj = oj;
+                        }
+                    }
+                    if (!(best > 0.0)) {  // no nonzero entry left in row k0 + t: singular
+                        if (tc == 0) s_sing = 1;
+                        bj = 0;
+                    }
+                    const int p = bj, po = p / GJ_C, pc = p - po * GJ_C;
+                    pk[t] = p;
+                    cplx col[4];
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) {
-                        if (i0 + r != kn) continue;  // registers are indexed statically only
+                    for (int r = 0; r < 4; ++r) col[r] = shfl_c(seg, pick6(a[r], pc), po, TCP);
+                    const cplx inv = cinv(col[t]);
+#pragma unroll
+                    for (int c = 0; c < GJ_C; ++c) {
+                        const bool jp = j0 + c == p;
+                        const cplx rk = cmul(a[t][c], inv);
+                        const cplx u = jp ? mk(1.0 + inv.x, inv.y) : rk;
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            if (r != t) cfma(a[r][c], cneg(col[r]), u);
+                        a[t][c] = jp ? inv : rk;
+                        if (jp) used |= 1u << c;
+                    }
+                    if (tc == 0) piv[k0 + t] = p;
+                }
+                // publish U (the transformed rows, plus 1 at each row's own pivot) and the pivots
+                if (own) {
+#pragma unroll
+                    for (int t = 0; t < 4; ++t)
 #pragma unroll
                         for (int c = 0; c < GJ_C; ++c) {
                             const int j = j0 + c;
-                            const double v = cabs2(a[r][c]);
-                            if (j < M && !((used >> c) & 1u) && v > best) {
-                                best = v;
-                                bjn = j;
-                            }
+                            if (j >= M) continue;
+                            cplx v = t < bw ? a[t][c] : mk(0.0, 0.0);
+                            if (t < bw && j == pk[t]) v.x += 1.0;
+                            Ublk[buf][t][j] = v;
                         }
-                    }
-                    cval[tc] = best;
-                    cidx[tc] = bjn;
                 }
+                if (tc == 0)
+#pragma unroll
+                    for (int t = 0; t < 4; ++t) pvt[buf][t] = t < bw ? pk[t] : -1;
             }
             __syncthreads();
+            if (s_sing) {
+                singular = true;
+                break;
+            }
+            if (rowseg && tr != kb) {
+                // rank-bw update of the other rows with their entries at the pivot columns
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    if (t >= bw) break;
+                    const int p = pvt[buf][t], po = p / GJ_C, pc = p - po * GJ_C;
+                    cplx nl[4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) nl[r] = cneg(shfl_c(seg, pick6(a[r], pc), po, TCP));
+                    if (own) {
+#pragma unroll
+                        for (int c = 0; c < GJ_C; ++c) {
+                            const int j = j0 + c;
+                            if (j >= M) continue;
+                            const cplx u = Ublk[buf][t][j];
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) cfma(a[r][c], nl[r], u);
+                        }
+                    }
+                }
+                // (the pivots of this block are marked when this segment's own block comes)
+            }
+            if (rowseg && tr != kb) {
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    if (t >= bw) break;
+                    const int p = pvt[buf][t];
+                    if (p >= j0 && p < j0 + GJ_C) used |= 1u << (p - j0);
+                }
+            }
         }
         if (singular) {
             if (tid == 0) atomicExch(status, 5);
@@ -469,7 +491,9 @@ void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const do
                         double2* X, int* status, int grid, cudaStream_t st) {
     StageScope sc(ST_SMALL_LU, st);
     const int tr = (P.nlm + 1) / 2, tc = (P.nlm + 2) / 3, M = 2 * P.nlm;
-    const int threads = std::max(32, (tr * tc + 31) / 32 * 32);  // whole warps: the pivot reduction shuffles
+    int tcp = 1;
+    while (tcp < tc) tcp *= 2;  // a tile row is a power-of-two segment of lanes
+    const int threads = std::max(32, (tr * tcp + 31) / 32 * 32);
     const size_t smem = (size_t)M * M * sizeof(double2);
     cudaFuncSetAttribute(array_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     array_solve_kernel<<<grid, threads, smem, st>>>(P, D, ldd, norm, Tm, nk, X, status);

@@ -715,22 +715,23 @@ void launch_barrier_selftest(unsigned* bar, int* status, double limit_s, cudaStr
 __global__ void perm_from_piv_kernel(const int* __restrict__ piv, int* __restrict__ perm, int n);
 
 void lu_init_attributes() {
-    static std::atomic<unsigned long long> done{0};
-    if (!first_use_on_device(done)) return;
-    int dev;
-    cudaGetDevice(&dev);
-    int sms = 0;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    g_num_sms = sms;
-    cudaFuncSetAttribute(panel_kernel<double, 64, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    cudaFuncSetAttribute(panel_kernel<float, 128, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    cudaFuncSetAttribute(panel_kernel<double, 64, PANEL_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    cudaFuncSetAttribute(panel_kernel<float, 128, PANEL_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    cudaFuncSetAttribute(trsm_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(trsm_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZG_SMEM);
-    cudaFuncSetAttribute(zgemm_dmma_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZH_SMEM);
-    cudaFuncSetAttribute(perm_from_piv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    static PerDeviceOnce done;
+    once_per_device(done, [] {
+        int dev;
+        cudaGetDevice(&dev);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        g_num_sms = sms;
+        cudaFuncSetAttribute(panel_kernel<double, 64, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        cudaFuncSetAttribute(panel_kernel<float, 128, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        cudaFuncSetAttribute(panel_kernel<double, 64, PANEL_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        cudaFuncSetAttribute(panel_kernel<float, 128, PANEL_SUB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+        cudaFuncSetAttribute(trsm_kernel<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(trsm_kernel<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(zgemm_dmma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZG_SMEM);
+        cudaFuncSetAttribute(zgemm_dmma_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZH_SMEM);
+        cudaFuncSetAttribute(perm_from_piv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    });
 }
 
 size_t lu_workspace_bytes(int n, bool fp32) {
@@ -742,33 +743,30 @@ size_t lu_workspace_bytes(int n, bool fp32) {
 
 // Smallest slab of rows per panel CTA (TCU_PANEL_ROWS, default 32; the smem slab caps it).
 static int panel_rows_per_cta() {
-    static int v = 0;
-    if (!v) {
+    static const int v = [] {
         const char* e = getenv("TCU_PANEL_ROWS");
-        int x = e ? atoi(e) : 0;
-        v = (x >= 16 && x <= 200) ? x : 32;
-    }
+        const int x = e ? atoi(e) : 0;
+        return (x >= 16 && x <= 200) ? x : 32;
+    }();
     return v;
 }
 
 // FP64 trailing update: 64 x 64 complex tiles, two CTAs per SM; TCU_FP64_GEMM=big selects the
 // 128 x 64 tiles (one CTA per SM), measured 9% slower at 512 spheres (2211 vs 2029 ms of updates).
 static bool fp64_big_tiles() {
-    static int v = -1;
-    if (v < 0) {
+    static const bool v = [] {
         const char* e = getenv("TCU_FP64_GEMM");
-        v = (e && std::string(e) == "big") ? 1 : 0;
-    }
-    return v == 1;
+        return e && std::string(e) == "big";
+    }();
+    return v;
 }
 
 static bool panel_sub_enabled() {
-    static int v = -1;
-    if (v < 0) {
+    static const bool v = [] {
         const char* e = getenv("TCU_PANEL_SUB");
-        v = (e && atoi(e) == 0) ? 0 : 1;
-    }
-    return v == 1;
+        return !(e && atoi(e) == 0);
+    }();
+    return v;
 }
 
 template <typename R, int NB>

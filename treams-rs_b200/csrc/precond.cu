@@ -162,9 +162,10 @@ tcu_status make_block_jacobi(cudaStream_t st, const DevPlan& P, int N, double k0
     if (!ck(cudaMalloc((void**)&d_status, sizeof(int)))) return TCU_OUT_OF_MEMORY;
     cudaMemsetAsync(d_status, 0, sizeof(int), st);
     size_t smem = (size_t)PB_MAXMODES * PB_MAXMODES * 16 + (size_t)PB_MAXMODES * PB_PANEL * 16;
-    static std::atomic<unsigned long long> attr{0};
-    if (first_use_on_device(attr))
+    static PerDeviceOnce attr;
+    once_per_device(attr, [&] {
         cudaFuncSetAttribute(blk_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
     blk_inverse_kernel<<<p.nblocks, 512, smem, st>>>(P, k0, d_pos, d_T, p.d_bptr, p.d_bmem, p.d_dinv, d_status);
     if (launches) ++*launches;
     int hst = 0;

@@ -445,13 +445,13 @@ static void inverses_impl(const C* A, int n, double2* inv, cudaStream_t st, long
     int nb = (n + SB - 1) / SB;
     StageScope sc(ST_SOLVE, st);
     const size_t smem = (size_t)(SB * (SB + 1) + SB) * sizeof(double2);
-    static std::atomic<unsigned long long> attr{0};
-    if (first_use_on_device(attr)) {
+    static PerDeviceOnce attr;
+    once_per_device(attr, [&] {
         cudaFuncSetAttribute(tri_block_inverse_kernel<double2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(tri_block_inverse_kernel<double2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(tri_block_inverse_kernel<float2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         cudaFuncSetAttribute(tri_block_inverse_kernel<float2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    }
+    });
     cudaMemsetAsync(chain_flags(inv, n), 0, (size_t)(nb + 64) * sizeof(unsigned), st);
     tri_block_inverse_kernel<C, true><<<nb, 256, smem, st>>>(A, n, n, inv);
     tri_block_inverse_kernel<C, false><<<nb, 256, smem, st>>>(A, n, n, inv + (size_t)nb * SB * SB);
@@ -466,22 +466,22 @@ void lu_block_inverses_fp32(const float2* A, int n, double2* inv, cudaStream_t s
 
 // Persistent sweeps unless TCU_SOLVE=steps asks for one launch per block step.
 static bool chain_enabled() {
-    static int v = -1;
-    if (v < 0) {
+    static const bool v = [] {
         const char* e = getenv("TCU_SOLVE");
-        v = (e && std::string(e) == "steps") ? 0 : 1;
-    }
-    return v == 1;
+        return !(e && std::string(e) == "steps");
+    }();
+    return v;
 }
 
 template <typename C, bool LOWER, int NC>
 static bool chain_launch_nc(cudaStream_t st, const C* A, int n, const double2* dinv, const double2* rhs,
                             double2* sol, unsigned* flags, unsigned epoch, int* status) {
-    static std::atomic<unsigned long long> attr{0};
+    static PerDeviceOnce attr;
     const size_t smem = chain_smem_bytes<C>(NC);
     // a refused attribute makes the cooperative launch below fail, and the caller takes the step path
-    if (first_use_on_device(attr))
+    once_per_device(attr, [&] {
         cudaFuncSetAttribute(trsv_chain_kernel<C, LOWER, NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
     const int nb = (n + SB - 1) / SB;
     const int grid = std::min(nb, g_sms);
     size_t lda = (size_t)n;
@@ -506,11 +506,12 @@ static bool chain_launch(int nc, cudaStream_t st, const C* A, int n, const doubl
 template <typename C>
 static void solve_impl(const C* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp, int ncol,
                        cudaStream_t st, long long* launches, unsigned* epoch, int* status) {
-    if (!g_sms) {
-        int dev;
+    static PerDeviceOnce sms_once;
+    once_per_device(sms_once, [] {
+        int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-    }
+    });
     StageScope sc(ST_SOLVE, st);
     const int nb = (n + SB - 1) / SB;
     const double2* linv = inv;
