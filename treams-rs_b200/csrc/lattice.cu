@@ -262,8 +262,8 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
 // inv = 1 / a_(k0+t) p_t, u_j = a_(k0+t) j inv (j != p_t), u_p = 1 + inv, the other block rows
 // take a_rj -= a_rp u_j and row k0 + t becomes u_j, inv at p_t). It publishes the transformed
 // rows U (plus 1 at each row's own pivot column) and p_0..p_3; after one barrier every other row
-// takes the rank-4 update a_ij -= sum_t a_(i p_t) U_tj, its a_(i p_t) fetched by shuffles inside
-// its own segment. U and the pivots are double-buffered, so one barrier per four rows. The table
+// takes the rank-4 update a_ij -= sum_t a_(i p_t) U_tj with its entries a_(i p_t) from before
+// the update (staged per row in shared memory by the lanes holding them). U and the pivots are double-buffered, so one barrier per four rows. The table
 // B then expresses the unknowns through the right-hand sides: (A^-1)[p_k][k'] = B[k][p_k'], so
 // X[p_k][col] = sum_q' B[k][p_(2 lm + q')] t_lm[q'][q] for col = 2 lm + q (T is block diagonal
 // per mode pair), gathered through shared memory. 8 M^3 real flops per Bloch vector.
@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
     extern __shared__ double2 gj_smem[];                 // B (M x M, column-major) for the final gather
     __shared__ double2 Z[(2 * 12 + 1) * (2 * 12 + 1)];  // harmonic table, order <= 2 lmax = 12
     __shared__ double2 Ublk[2][4][GJ_MAXM];
+    __shared__ double2 Ls[GJ_MAXM][4];  // each row's entries at the block's pivot columns
     __shared__ int pvt[2][4];
     __shared__ int piv[GJ_MAXM];
     __shared__ int s_sing;
@@ -408,14 +409,26 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
                 break;
             }
             if (rowseg && tr != kb) {
-                // rank-bw update of the other rows with their entries at the pivot columns
+                // rank-bw update of the other rows with their entries at the pivot columns, all
+                // taken before the update changes them (staged per row in shared memory by the
+                // lanes that hold them; the segment is one warp's lanes)
 #pragma unroll
                 for (int t = 0; t < 4; ++t) {
                     if (t >= bw) break;
-                    const int p = pvt[buf][t], po = p / GJ_C, pc = p - po * GJ_C;
+                    const int p = pvt[buf][t];
+                    if (own && p >= j0 && p < j0 + GJ_C) {
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            if (i0 + r < M) Ls[i0 + r][t] = pick6(a[r], p - j0);
+                    }
+                }
+                __syncwarp(seg);
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    if (t >= bw) break;
                     cplx nl[4];
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) nl[r] = cneg(shfl_c(seg, pick6(a[r], pc), po, TCP));
+                    for (int r = 0; r < 4; ++r) nl[r] = i0 + r < M ? cneg(Ls[i0 + r][t]) : mk(0.0, 0.0);
                     if (own) {
 #pragma unroll
                         for (int c = 0; c < GJ_C; ++c) {
