@@ -249,37 +249,110 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
 // ---- batched periodic-array solve ----------------------------------------------------------
 // One CTA per Bloch vector, X = (I - T S)^-1 T (cluster/interaction.rs:292-315 with
 // sw/plan.rs:383-413 evaluate_periodic). The M x M operator (M = 2 lmax (lmax + 2), 96 at
-// lmax 6) lives in registers: thread (tr, tc) owns the 4 x 6 tile of rows 4 tr.., columns
-// 6 tc.., i.e. the 2 x 2 mode blocks of destinations d = 2 tr, 2 tr + 1 and sources
-// s = 3 tc .. 3 tc + 2, assembled there from the harmonic table D / N and the plan's term lists.
-// A tile row is a segment of TCP = 2^ceil(log2 ceil(nlm / 3)) lanes of one warp (16 at lmax 6:
-// 24 x 16 = 384 threads, three warps per SM sub-partition, 168 registers a thread).
+// lmax 6) lives in registers: warp w owns the rows 8 w .. 8 w + 7 and lane l the columns
+// 3 l .. 3 l + 2 of them (an 8 x 3 tile per lane; 12 warps and 168 registers a thread at
+// lmax 6), assembled there from the harmonic table D / N and the plan's term lists.
 //
 // The inverse comes from in-place Gauss-Jordan exchange steps without row or column
-// interchanges, four rows at a time. Block step k0: the segment owning rows k0..k0+3 runs the
-// four exchange steps on its own rows with shuffles only (step t pivots on (k0 + t, p_t), p_t
-// the not yet pivotal column with the largest |a|^2 in row k0 + t, ties to the lower column; with
-// inv = 1 / a_(k0+t) p_t, u_j = a_(k0+t) j inv (j != p_t), u_p = 1 + inv, the other block rows
-// take a_rj -= a_rp u_j and row k0 + t becomes u_j, inv at p_t). It publishes the transformed
-// rows U (plus 1 at each row's own pivot column) and p_0..p_3; after one barrier every other row
-// takes the rank-4 update a_ij -= sum_t a_(i p_t) U_tj with its entries a_(i p_t) from before
-// the update (staged per row in shared memory by the lanes holding them). U and the pivots are double-buffered, so one barrier per four rows. The table
-// B then expresses the unknowns through the right-hand sides: (A^-1)[p_k][k'] = B[k][p_k'], so
-// X[p_k][col] = sum_q' B[k][p_(2 lm + q')] t_lm[q'][q] for col = 2 lm + q (T is block diagonal
-// per mode pair), gathered through shared memory. 8 M^3 real flops per Bloch vector.
+// interchanges, eight rows (one warp) at a time. Block step k0: the warp owning rows
+// k0..k0+7 runs the eight exchange steps on its own rows with warp collectives only (step t
+// pivots on (k0 + t, p_t), p_t the not yet pivotal column with the largest |a|^2 in row
+// k0 + t, ties to the lower column; with inv = 1 / a_(k0+t) p_t, u_j = a_(k0+t) j inv (j != p_t)
+// and u_p = 1 + inv, the other block rows take a_rj -= a_rp u_j and row k0 + t becomes u_j,
+// inv at p_t). It publishes the transformed rows U (plus 1 at each row's own pivot column) and
+// p_0..p_7; after one barrier every other row takes the rank-8 update
+// a_ij -= sum_t a_(i p_t) U_tj with its entries a_(i p_t) from before the update (staged per row
+// in shared memory by the lanes holding them). U and the pivots are double-buffered: one barrier
+// per eight rows, and a pivot warp never shares its instructions with another block's update.
+// The table B then expresses the unknowns through the right-hand sides:
+// (A^-1)[p_k][k'] = B[k][p_k'], so X[p_k][col] = sum_q' B[k][p_(2 lm + q')] t_lm[q'][q] for
+// col = 2 lm + q (T is block diagonal per mode pair), gathered through shared memory.
+// 8 M^3 real flops per Bloch vector.
 constexpr int GJ_MAXM = 96;
-constexpr int GJ_C = 6;  // tile columns (three mode pairs)
+constexpr int GJ_R = 8;  // tile rows (a warp's rows)
+constexpr int GJ_C = 3;  // tile columns (a lane's columns)
 
-__device__ __forceinline__ cplx shfl_c(unsigned mask, cplx v, int src, int width) {
-    return mk(__shfl_sync(mask, v.x, src, width), __shfl_sync(mask, v.y, src, width));
+__device__ __forceinline__ cplx shfl_c(cplx v, int src) {
+    return mk(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
 // a[c] for a runtime c < GJ_C with static register indexing
-__device__ __forceinline__ cplx pick6(const cplx* a, int c) {
+__device__ __forceinline__ cplx pick3(const cplx* a, int c) {
     cplx v = a[0];
 #pragma unroll
     for (int q = 1; q < GJ_C; ++q)
         if (c == q) v = a[q];
     return v;
+}
+
+// Entries of combo (d, s) = (4 tr + dd, j0 / 2 + ss) of A = I - T S that fall in the tile
+// (rows 2d, 2d+1; columns 2s, 2s+1), unrolled by template so that the tile stays in registers.
+template <int dd, int ss>
+__device__ __forceinline__ void gj_assemble(cplx (&a)[GJ_R][GJ_C], const DevPlan& P, const double2* Z,
+                                            const double2* __restrict__ Tm, int tr, int j0, int nlm) {
+    const int d = (GJ_R / 2) * tr + dd, sidx = (j0 >> 1) + ss;
+    if (d >= nlm || sidx >= nlm || 2 * sidx >= j0 + GJ_C) return;
+    int lam = 1;
+    while ((lam + 1) * (lam + 1) - 1 <= d) ++lam;
+    const double2* t4 = Tm + (lam - 1) * 4;
+    cplx Aa, Bb;
+    plan_combo_sums(P, sidx * nlm + d, Z, Aa, Bb);
+    const cplx cp = cadd(Aa, Bb), cn = csub(Aa, Bb);
+    const double one = sidx == d ? 1.0 : 0.0;
+    const cplx a00 = csub(mk(one, 0.0), cmul(t4[0], cp)), a10 = cneg(cmul(t4[2], cp)),
+               a01 = cneg(cmul(t4[1], cn)), a11 = csub(mk(one, 0.0), cmul(t4[3], cn));
+    const int c0 = 2 * sidx - j0;  // tile column of column 2s (-1 .. 2)
+#pragma unroll
+    for (int c = 0; c < GJ_C; ++c) {  // selects, not branches: the tile stays in registers
+        const bool e = c == c0, o = c == c0 + 1;
+        a[2 * dd][c] = e ? a00 : (o ? a01 : a[2 * dd][c]);
+        a[2 * dd + 1][c] = e ? a10 : (o ? a11 : a[2 * dd + 1][c]);
+    }
+}
+
+// Exchange step t of a block (rows of one warp): pivot search by two redux.sync, the pivot
+// column broadcast by shuffles, 1 / a_kp = conj(a_kp) / |a_kp|^2, and the update of the
+// warp's rows.
+template <int t>
+__device__ __forceinline__ void gj_block_step(cplx (&a)[GJ_R][GJ_C], int (&pk)[GJ_R], int bw, bool own, int j0,
+                                              int M, unsigned& used, int* piv, int k0, int lane, int& s_sing) {
+    pk[t] = -1;
+    if (t >= bw) return;
+    // pivot: largest |a|^2 (as an FP32 key, + 1 so that 0 means no candidate) over the
+    // columns not yet pivotal, ties to the lower column
+    unsigned key = 0u, bj = 0xffffffffu;
+#pragma unroll
+    for (int c = 0; c < GJ_C; ++c) {
+        const int j = j0 + c;
+        const unsigned kk = __float_as_uint((float)cabs2(a[t][c])) + 1u;
+        if (own && j < M && !((used >> c) & 1u) && kk > key) {
+            key = kk;
+            bj = (unsigned)j;
+        }
+    }
+    const unsigned kmax = __reduce_max_sync(0xffffffffu, key);
+    const unsigned jmin = __reduce_min_sync(0xffffffffu, key == kmax ? bj : 0xffffffffu);
+    const int p = kmax ? (int)jmin : 0, po = p / GJ_C, pc = p - po * GJ_C;
+    pk[t] = p;
+    cplx col[GJ_R];
+#pragma unroll
+    for (int r = 0; r < GJ_R; ++r) col[r] = shfl_c(pick3(a[r], pc), po);
+    // an exact zero pivot (or no candidate) is singular
+    const double den = cabs2(col[t]);
+    if ((!(den > 0.0) || !kmax) && lane == 0) s_sing = 1;
+    const double rden = __drcp_rn(den);
+    const cplx inv = mk(col[t].x * rden, -col[t].y * rden);
+#pragma unroll
+    for (int c = 0; c < GJ_C; ++c) {
+        const bool jp = j0 + c == p;
+        const cplx rk = cmul(a[t][c], inv);
+        const cplx u = jp ? mk(1.0 + inv.x, inv.y) : rk;
+#pragma unroll
+        for (int r = 0; r < GJ_R; ++r)
+            if (r != t) cfma(a[r][c], cneg(col[r]), u);
+        a[t][c] = jp ? inv : rk;
+        if (jp) used |= 1u << c;
+    }
+    if (lane == 0) piv[k0 + t] = p;
 }
 
 __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const double2* __restrict__ D,
@@ -288,147 +361,98 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
                                                              double2* __restrict__ X, int* __restrict__ status) {
     extern __shared__ double2 gj_smem[];                 // B (M x M, column-major) for the final gather
     __shared__ double2 Z[(2 * 12 + 1) * (2 * 12 + 1)];  // harmonic table, order <= 2 lmax = 12
-    __shared__ double2 Ublk[2][4][GJ_MAXM];
-    __shared__ double2 Ls[GJ_MAXM][4];  // each row's entries at the block's pivot columns
-    __shared__ int pvt[2][4];
+    __shared__ double2 Ublk[2][GJ_R][GJ_MAXM];
+    __shared__ double2 Ls[GJ_MAXM][GJ_R];  // each row's entries at the block's pivot columns
+    __shared__ int pvt[2][GJ_R];
     __shared__ int piv[GJ_MAXM];
     __shared__ int s_sing;
-    const int nlm = P.nlm, M = 2 * nlm, TR = (nlm + 1) / 2, TC = (nlm + 2) / 3;
-    int TCP = 1;
-    while (TCP < TC) TCP *= 2;
+    const int nlm = P.nlm, M = 2 * nlm, TR = (M + GJ_R - 1) / GJ_R, TC = (M + GJ_C - 1) / GJ_C;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int tr = tid / TCP, tc = tid - (tid / TCP) * TCP;
+    const int tr = tid >> 5, tc = lane;  // warp = tile row, lane = tile column
     const bool own = tr < TR && tc < TC;
-    const bool rowseg = tr < TR;  // this lane's segment is a tile row of the operator
-    const int i0 = 4 * tr, j0 = GJ_C * tc;
-    const unsigned seg = TCP >= 32 ? 0xffffffffu : (((1u << TCP) - 1u) << (lane & ~(TCP - 1)));
+    const bool rowwarp = tr < TR;
+    const int i0 = GJ_R * tr, j0 = GJ_C * tc;
     for (int kp = blockIdx.x; kp < nk; kp += gridDim.x) {
         for (int t = tid; t < P.tsize; t += blockDim.x) Z[t] = cscale(D[(size_t)kp * ldd + t], 1.0 / norm[t]);
         if (tid == 0) s_sing = 0;
         __syncthreads();
-        // A = I - T S on the tile: combo (s, d) gives rows 2d, 2d+1 of columns 2s, 2s+1
-        cplx a[4][GJ_C];
+        // A = I - T S on the tile: combo (s, d) gives rows 2d, 2d+1 of columns 2s, 2s+1; the
+        // tile's rows hold d = 4 tr .. 4 tr + 3, its columns touch s = j0 / 2 and (j0 + 2) / 2
+        cplx a[GJ_R][GJ_C];
 #pragma unroll
-        for (int r = 0; r < 4; ++r)
+        for (int r = 0; r < GJ_R; ++r)
 #pragma unroll
             for (int c = 0; c < GJ_C; ++c) a[r][c] = mk(0.0, 0.0);
         if (own) {
-#pragma unroll
-            for (int dd = 0; dd < 2; ++dd)
-#pragma unroll
-                for (int ss = 0; ss < GJ_C / 2; ++ss) {
-                    const int d = 2 * tr + dd, sidx = (GJ_C / 2) * tc + ss;
-                    if (d >= nlm || sidx >= nlm) continue;
-                    int lam = 1;
-                    while ((lam + 1) * (lam + 1) - 1 <= d) ++lam;
-                    const double2* t4 = Tm + (lam - 1) * 4;
-                    cplx Aa, Bb;
-                    plan_combo_sums(P, sidx * nlm + d, Z, Aa, Bb);
-                    const cplx cp = cadd(Aa, Bb), cn = csub(Aa, Bb);
-                    const double one = sidx == d ? 1.0 : 0.0;
-                    const cplx a00 = cmul(t4[0], cp), a10 = cmul(t4[2], cp), a01 = cmul(t4[1], cn),
-                               a11 = cmul(t4[3], cn);
-                    a[2 * dd][2 * ss] = mk(one - a00.x, -a00.y);
-                    a[2 * dd + 1][2 * ss] = cneg(a10);
-                    a[2 * dd][2 * ss + 1] = cneg(a01);
-                    a[2 * dd + 1][2 * ss + 1] = mk(one - a11.x, -a11.y);
-                }
+            gj_assemble<0, 0>(a, P, Z, Tm, tr, j0, nlm);
+            gj_assemble<0, 1>(a, P, Z, Tm, tr, j0, nlm);
+            gj_assemble<1, 0>(a, P, Z, Tm, tr, j0, nlm);
+            gj_assemble<1, 1>(a, P, Z, Tm, tr, j0, nlm);
+            gj_assemble<2, 0>(a, P, Z, Tm, tr, j0, nlm);
+            gj_assemble<2, 1>(a, P, Z, Tm, tr, j0, nlm);
+            gj_assemble<3, 0>(a, P, Z, Tm, tr, j0, nlm);
+            gj_assemble<3, 1>(a, P, Z, Tm, tr, j0, nlm);
         }
         unsigned used = 0u;  // bit c: column j0 + c is already pivotal
         bool singular = false;
-        for (int kb = 0, buf = 0; 4 * kb < M; ++kb, buf ^= 1) {
-            const int k0 = 4 * kb, bw = min(4, M - k0);
+        for (int kb = 0, buf = 0; GJ_R * kb < M; ++kb, buf ^= 1) {
+            const int k0 = GJ_R * kb, bw = min(GJ_R, M - k0);
             if (tr == kb) {
-                // the block rows: bw exchange steps inside the segment
-                int pk[4] = {0, 0, 0, 0};
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    if (t >= bw) break;
-                    double best = -1.0;
-                    int bj = 0x7fffffff;
-#pragma unroll
-                    for (int c = 0; c < GJ_C; ++c) {
-                        const int j = j0 + c;
-                        const double v = cabs2(a[t][c]);
-                        if (own && j < M && !((used >> c) & 1u) && v > best) {
-                            best = v;
-                            bj = j;
-                        }
-                    }
-                    for (int off = TCP / 2; off > 0; off >>= 1) {
-                        const double ov = __shfl_xor_sync(seg, best, off, TCP);
-                        const int oj = __shfl_xor_sync(seg, bj, off, TCP);
-                        if (ov > best || (ov == best && oj < bj)) {
-                            best = ov;
-                            bj = oj;
-                        }
-                    }
-                    if (!(best > 0.0)) {  // no nonzero entry left in row k0 + t: singular
-                        if (tc == 0) s_sing = 1;
-                        bj = 0;
-                    }
-                    const int p = bj, po = p / GJ_C, pc = p - po * GJ_C;
-                    pk[t] = p;
-                    cplx col[4];
-#pragma unroll
-                    for (int r = 0; r < 4; ++r) col[r] = shfl_c(seg, pick6(a[r], pc), po, TCP);
-                    const cplx inv = cinv(col[t]);
-#pragma unroll
-                    for (int c = 0; c < GJ_C; ++c) {
-                        const bool jp = j0 + c == p;
-                        const cplx rk = cmul(a[t][c], inv);
-                        const cplx u = jp ? mk(1.0 + inv.x, inv.y) : rk;
-#pragma unroll
-                        for (int r = 0; r < 4; ++r)
-                            if (r != t) cfma(a[r][c], cneg(col[r]), u);
-                        a[t][c] = jp ? inv : rk;
-                        if (jp) used |= 1u << c;
-                    }
-                    if (tc == 0) piv[k0 + t] = p;
-                }
+                // the block rows: bw exchange steps inside the warp (unrolled by template so that
+                // the tile stays in registers)
+                int pk[GJ_R];
+                gj_block_step<0>(a, pk, bw, own, j0, M, used, piv, k0, lane, s_sing);
+                gj_block_step<1>(a, pk, bw, own, j0, M, used, piv, k0, lane, s_sing);
+                gj_block_step<2>(a, pk, bw, own, j0, M, used, piv, k0, lane, s_sing);
+                gj_block_step<3>(a, pk, bw, own, j0, M, used, piv, k0, lane, s_sing);
+                gj_block_step<4>(a, pk, bw, own, j0, M, used, piv, k0, lane, s_sing);
+                gj_block_step<5>(a, pk, bw, own, j0, M, used, piv, k0, lane, s_sing);
+                gj_block_step<6>(a, pk, bw, own, j0, M, used, piv, k0, lane, s_sing);
+                gj_block_step<7>(a, pk, bw, own, j0, M, used, piv, k0, lane, s_sing);
                 // publish U (the transformed rows, plus 1 at each row's own pivot) and the pivots
                 if (own) {
 #pragma unroll
-                    for (int t = 0; t < 4; ++t)
+                    for (int t = 0; t < GJ_R; ++t)
 #pragma unroll
                         for (int c = 0; c < GJ_C; ++c) {
                             const int j = j0 + c;
                             if (j >= M) continue;
                             cplx v = t < bw ? a[t][c] : mk(0.0, 0.0);
-                            if (t < bw && j == pk[t]) v.x += 1.0;
+                            if (j == pk[t]) v.x += 1.0;
                             Ublk[buf][t][j] = v;
                         }
                 }
-                if (tc == 0)
+                if (lane == 0)
 #pragma unroll
-                    for (int t = 0; t < 4; ++t) pvt[buf][t] = t < bw ? pk[t] : -1;
+                    for (int t = 0; t < GJ_R; ++t) pvt[buf][t] = pk[t];
             }
             __syncthreads();
             if (s_sing) {
                 singular = true;
                 break;
             }
-            if (rowseg && tr != kb) {
+            if (rowwarp && tr != kb) {
                 // rank-bw update of the other rows with their entries at the pivot columns, all
                 // taken before the update changes them (staged per row in shared memory by the
-                // lanes that hold them; the segment is one warp's lanes)
+                // lanes that hold them)
 #pragma unroll
-                for (int t = 0; t < 4; ++t) {
+                for (int t = 0; t < GJ_R; ++t) {
                     if (t >= bw) break;
                     const int p = pvt[buf][t];
                     if (own && p >= j0 && p < j0 + GJ_C) {
 #pragma unroll
-                        for (int r = 0; r < 4; ++r)
-                            if (i0 + r < M) Ls[i0 + r][t] = pick6(a[r], p - j0);
+                        for (int r = 0; r < GJ_R; ++r)
+                            if (i0 + r < M) Ls[i0 + r][t] = pick3(a[r], p - j0);
+                        used |= 1u << (p - j0);
                     }
                 }
-                __syncwarp(seg);
+                __syncwarp();
 #pragma unroll
-                for (int t = 0; t < 4; ++t) {
+                for (int t = 0; t < GJ_R; ++t) {
                     if (t >= bw) break;
-                    cplx nl[4];
+                    cplx nl[GJ_R];
 #pragma unroll
-                    for (int r = 0; r < 4; ++r) nl[r] = i0 + r < M ? cneg(Ls[i0 + r][t]) : mk(0.0, 0.0);
+                    for (int r = 0; r < GJ_R; ++r) nl[r] = i0 + r < M ? cneg(Ls[i0 + r][t]) : mk(0.0, 0.0);
                     if (own) {
 #pragma unroll
                         for (int c = 0; c < GJ_C; ++c) {
@@ -436,18 +460,9 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
                             if (j >= M) continue;
                             const cplx u = Ublk[buf][t][j];
 #pragma unroll
-                            for (int r = 0; r < 4; ++r) cfma(a[r][c], nl[r], u);
+                            for (int r = 0; r < GJ_R; ++r) cfma(a[r][c], nl[r], u);
                         }
                     }
-                }
-                // (the pivots of this block are marked when this segment's own block comes)
-            }
-            if (rowseg && tr != kb) {
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    if (t >= bw) break;
-                    const int p = pvt[buf][t];
-                    if (p >= j0 && p < j0 + GJ_C) used |= 1u << (p - j0);
                 }
             }
         }
@@ -460,7 +475,7 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
         double2* Bs = gj_smem;
         if (own) {
 #pragma unroll
-            for (int r = 0; r < 4; ++r)
+            for (int r = 0; r < GJ_R; ++r)
 #pragma unroll
                 for (int c = 0; c < GJ_C; ++c)
                     if (i0 + r < M && j0 + c < M) Bs[(size_t)(j0 + c) * M + i0 + r] = a[r][c];
@@ -503,10 +518,8 @@ void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st) {
 void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const double* norm, const double2* Tm, int nk,
                         double2* X, int* status, int grid, cudaStream_t st) {
     StageScope sc(ST_SMALL_LU, st);
-    const int tr = (P.nlm + 1) / 2, tc = (P.nlm + 2) / 3, M = 2 * P.nlm;
-    int tcp = 1;
-    while (tcp < tc) tcp *= 2;  // a tile row is a power-of-two segment of lanes
-    const int threads = std::max(32, (tr * tcp + 31) / 32 * 32);
+    const int M = 2 * P.nlm;
+    const int threads = 32 * ((M + GJ_R - 1) / GJ_R);  // a warp per eight rows
     const size_t smem = (size_t)M * M * sizeof(double2);
     cudaFuncSetAttribute(array_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     array_solve_kernel<<<grid, threads, smem, st>>>(P, D, ldd, norm, Tm, nk, X, status);
