@@ -15,8 +15,9 @@
 // [ln 2, 2 ln 2); sweeps stop after one that moves no factor by more than 2 (at most 64). A sum
 // that is not normal leaves the max scales alone; so do factors beyond 2^+-256. Two passes over
 // the matrix per sweep: column sums (CTA per column) and row sums (threads over rows, partial
-// per column chunk, fixed-order reduction). The sweeps read the unscaled A with the max scales
-// applied on the fly, and A is scaled once at the end: 3 + 2 sweeps passes over the matrix.
+// per column chunk, fixed-order reduction). The column maxima and the sweeps read a bfloat16
+// mirror of |a_ij| (written by the row-maxima pass) with the max scales applied on the fly, and A
+// is scaled once at the end: three passes over A plus (1 + 2 sweeps) over the 2-byte mirror.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -31,21 +32,40 @@ namespace tcu {
 namespace {
 
 constexpr int EQ_CHUNKS = 32;
+// bfloat16 magnitude mirror at the end of the scratch, 256-byte aligned
+inline size_t mirror_offset(int n) { return ((size_t)(EQ_CHUNKS + 2) * n + (n + 255) / 256 + 1 + 31) / 32 * 32; }
+inline size_t mirror_doubles(int n) { return ((size_t)n * n * 2 + 255) / 256 * 32; }
 
 template <typename C>
 __device__ __forceinline__ double mag(C v) {
     return fmax(fabs((double)v.x), fabs((double)v.y));
 }
+// Magnitude mirror: the column and balancing passes read |a_ij| as bfloat16 (8-bit mantissa,
+// the FP32 exponent range), a quarter of the complex64 bytes and an eighth of complex128. The
+// scales are powers of two chosen from magnitude sums; a sum off by < 0.5 % moves a choice only
+// when the sum sits at a boundary, and the scaling stays exact either way.
+__device__ __forceinline__ uint16_t to_bf16(double m) {
+    const unsigned b = __float_as_uint((float)m);
+    if ((b & 0x7f800000u) == 0x7f800000u) return (uint16_t)(b >> 16);  // inf, NaN
+    return (uint16_t)((b + 0x7fffu + ((b >> 16) & 1u)) >> 16);       // round to nearest even
+}
+__device__ __forceinline__ double mag(uint16_t v) { return (double)__uint_as_float((unsigned)v << 16); }
 
+// row maxima, and the bfloat16 magnitude mirror M (column-major like A)
 template <typename C>
-__global__ void row_max_partial(const C* __restrict__ A, int n, double* __restrict__ partial) {
+__global__ void row_max_partial(const C* __restrict__ A, int n, double* __restrict__ partial,
+                                uint16_t* __restrict__ mirror) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int chunk = blockIdx.y;
     if (i >= n) return;
     const int per = (n + EQ_CHUNKS - 1) / EQ_CHUNKS;
     const int j0 = chunk * per, j1 = min(n, j0 + per);
     double m = 0.0;
-    for (int j = j0; j < j1; ++j) m = fmax(m, mag(A[(size_t)j * n + i]));
+    for (int j = j0; j < j1; ++j) {
+        const double v = mag(A[(size_t)j * n + i]);
+        mirror[(size_t)j * n + i] = to_bf16(v);
+        m = fmax(m, v);
+    }
     partial[(size_t)chunk * n + i] = m;
 }
 
@@ -233,7 +253,8 @@ tcu_status equilibrate_impl(C* A, int n, double threshold, double* r, double* c,
                             cudaStream_t st, long long* launches) {
     *applied = false;
     const int nb = (n + 255) / 256;
-    row_max_partial<C><<<dim3(nb, EQ_CHUNKS), 256, 0, st>>>(A, n, partial);
+    uint16_t* mirror = reinterpret_cast<uint16_t*>(partial + mirror_offset(n));
+    row_max_partial<C><<<dim3(nb, EQ_CHUNKS), 256, 0, st>>>(A, n, partial, mirror);
     double* block_max = partial + (size_t)EQ_CHUNKS * n;
     row_scale<<<nb, 256, 0, st>>>(partial, n, r, block_max);
     if (launches) *launches += 2;
@@ -244,10 +265,10 @@ tcu_status equilibrate_impl(C* A, int n, double threshold, double* r, double* c,
     double mx = 0.0;
     for (double v : bm) mx = std::max(mx, v);
     if (!(mx > threshold)) return TCU_OK;  // entries within the spread a unit diagonal tolerates
-    col_scale<C><<<n, 256, 0, st>>>(A, n, r, c);
+    col_scale<uint16_t><<<n, 256, 0, st>>>(mirror, n, r, c);
     if (launches) ++*launches;
     int sweeps = 0;
-    const tcu_status s = balance_impl<C>(A, n, r, c, partial, &sweeps, st, launches);
+    const tcu_status s = balance_impl<uint16_t>(mirror, n, r, c, partial, &sweeps, st, launches);
     if (s) return s;
     apply_scales<C><<<148 * 16, 256, 0, st>>>(A, n, r, c);  // R A C with the balanced (or max) scales
     if (launches) ++*launches;
@@ -257,7 +278,7 @@ tcu_status equilibrate_impl(C* A, int n, double threshold, double* r, double* c,
 
 }  // namespace
 
-size_t equilibrate_scratch_doubles(int n) { return (size_t)(EQ_CHUNKS + 2) * n + (n + 255) / 256 + 1; }
+size_t equilibrate_scratch_doubles(int n) { return mirror_offset(n) + mirror_doubles(n); }
 
 tcu_status equilibrate(void* A, bool fp32, int n, double threshold, double* r, double* c, double* partial,
                        bool* applied, cudaStream_t st, long long* launches) {

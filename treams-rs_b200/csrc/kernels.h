@@ -191,6 +191,7 @@ struct LuWork {
     void* pack = nullptr;      // packed GEMM operands (mixed path)
     size_t pack_bytes = 0;
     bool f16_pieces = false;   // mixed path: FP16 (true) or TF32 (false) pieces of the 3-pass split
+    int panel_rows = 0;        // least rows per panel CTA (0: TCU_PANEL_ROWS or 32)
 };
 // FP16 pieces when the environment asks for them (TCU_SPLIT=f16), else TF32 pieces
 bool split_f16_default();

@@ -774,7 +774,7 @@ static int run_panel(typename Cx<R>::T* A, int n, int k0, int w, LuWork& wk, cud
     typedef typename Cx<R>::T C;
     int rows = n - k0;
     // at least panel_rows_per_cta() rows per CTA: fewer CTAs arrive at each column's barrier
-    const int per = panel_rows_per_cta();
+    const int per = wk.panel_rows > 0 ? wk.panel_rows : panel_rows_per_cta();
     int P = std::min(g_num_sms, std::max(1, (rows + per - 1) / per));
     int chunk = (rows + P - 1) / P;
     // 16-column sub-blocks when their pivot rows fit next to the slab (TCU_PANEL_SUB=0 turns
