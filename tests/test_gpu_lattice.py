@@ -97,6 +97,18 @@ def test_array_solve_small_lmax_lossy(ctx):
         assert np.max(np.abs(X[i] - ref)) <= 1e-10 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("lmax", [1, 2, 4, 5])
+def test_array_solve_every_operator_size(ctx, lmax):
+    # M = 6, 16, 48, 70: one to nine warps of eight rows, partial row blocks (M = 6, 70) and
+    # partial column tiles (M = 16, 70) of the register-resident Gauss-Jordan kernel
+    lat = np.array([[0.9, 0.0], [0.3, 0.8]])
+    kps = np.array([[0.5, 0.1], [-1.2, 2.0], [0.0, 0.0]])
+    X = tl.array_solve_batch(lmax, 2.5, 0.25, 3.0 + 0.4j, lat, kps, ctx=ctx)
+    for i in range(len(kps)):
+        ref = oracle.array_solve(lmax, 2.5, 0.25, 3.0 + 0.4j, lat, kps[i])
+        assert np.max(np.abs(X[i] - ref)) <= 1e-10 * np.max(np.abs(ref)), (lmax, i)
+
+
 def test_array_solve_rejects_touching_spheres(ctx):
     with pytest.raises(ValueError, match="overlap"):
         tl.array_solve_batch(2, 2.0, 0.6, 4.0, np.eye(2), np.array([[0.1, 0.2]]), ctx=ctx)

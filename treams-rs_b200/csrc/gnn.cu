@@ -421,8 +421,7 @@ void features(int N, const double* pos, const double* radii, const double* eps, 
         double s1 = 0.0, s3 = 0.0;
         for (int e = g.ptr[i]; e < g.ptr[i + 1]; ++e) {
             const int j = g.nbr[e];
-            const double d = std::hypot(std::hypot(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1]),
-                                        pos[3 * i + 2] - pos[3 * j + 2]);
+            const double d = std::sqrt(dist2(pos, i, j));
             const double kd = k * d;
             s1 += 1.0 / kd;
             s3 += 1.0 / (kd * kd * kd);

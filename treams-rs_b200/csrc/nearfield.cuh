@@ -112,77 +112,101 @@ struct Graph {
     std::vector<uint8_t> same;
 };
 
+// squared distance of sphere centres (plain arithmetic: centres are finite and well inside the
+// double range, validated on entry)
+inline double dist2(const double* pos, int i, int j) {
+    const double dx = pos[3 * i] - pos[3 * j], dy = pos[3 * i + 1] - pos[3 * j + 1], dz = pos[3 * i + 2] - pos[3 * j + 2];
+    return dx * dx + dy * dy + dz * dz;
+}
+
 // Neighbours within `reach` (sorted by index) and blocks of at most `per_block` spheres.
+// Cells of side `reach`; spheres sorted by cell, each cell's range found in a dense table
+// (or by binary search when the grid is much larger than the cluster); neighbour lists are
+// written straight into CSR.
 Graph build_graph(int N, const double* pos, double reach, int per_block) {
     Graph g;
+    const double reach2 = reach * reach;
     double lo[3] = {1e300, 1e300, 1e300};
     for (int i = 0; i < N; ++i)
         for (int a = 0; a < 3; ++a) lo[a] = std::min(lo[a], pos[3 * i + a]);
-    auto cell = [&](int i, int a) { return (long)std::floor((pos[3 * i + a] - lo[a]) / reach); };
+    std::vector<long> cc(3 * (size_t)N);
+    long dim = 1;
+    for (int i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a) {
+            cc[3 * i + a] = (long)std::floor((pos[3 * i + a] - lo[a]) / reach);
+            dim = std::max(dim, cc[3 * i + a] + 2);
+        }
     std::vector<std::pair<uint64_t, int>> order(N);
     for (int i = 0; i < N; ++i)
-        order[i] = {spread3(cell(i, 0)) | spread3(cell(i, 1)) << 1 | spread3(cell(i, 2)) << 2, i};
+        order[i] = {spread3(cc[3 * i]) | spread3(cc[3 * i + 1]) << 1 | spread3(cc[3 * i + 2]) << 2, i};
     std::sort(order.begin(), order.end());
-    // cell lists in Morton order: spheres sharing a cell are contiguous
-    std::vector<std::vector<int>> nb(N);
-    {
-        long dim = 1;
-        for (int i = 0; i < N; ++i)
-            for (int a = 0; a < 3; ++a) dim = std::max(dim, cell(i, a) + 2);
-        std::vector<std::pair<long, int>> byc(N);
-        for (int i = 0; i < N; ++i) byc[i] = {(cell(i, 0) * dim + cell(i, 1)) * dim + cell(i, 2), i};
-        std::sort(byc.begin(), byc.end());
-        for (int i = 0; i < N; ++i) {
-            long cx = cell(i, 0), cy = cell(i, 1), cz = cell(i, 2);
-            for (long dx = -1; dx <= 1; ++dx)
-                for (long dy = -1; dy <= 1; ++dy)
-                    for (long dz = -1; dz <= 1; ++dz) {
-                        long x = cx + dx, y = cy + dy, z = cz + dz;
-                        if (x < 0 || y < 0 || z < 0) continue;
-                        long key = (x * dim + y) * dim + z;
-                        auto it = std::lower_bound(byc.begin(), byc.end(), std::make_pair(key, -1));
-                        for (; it != byc.end() && it->first == key; ++it) {
-                            int j = it->second;
-                            if (j == i) continue;
-                            double d = std::hypot(std::hypot(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1]),
-                                                  pos[3 * i + 2] - pos[3 * j + 2]);
-                            if (d <= reach) nb[i].push_back(j);
-                        }
+    auto key_of = [&](long x, long y, long z) { return (x * dim + y) * dim + z; };
+    std::vector<std::pair<long, int>> byc(N);
+    for (int i = 0; i < N; ++i) byc[i] = {key_of(cc[3 * i], cc[3 * i + 1], cc[3 * i + 2]), i};
+    std::sort(byc.begin(), byc.end());
+    const bool dense = dim <= 4096 && dim * dim * dim <= 8L * N + 4096;
+    std::vector<int> cstart;
+    if (dense) {
+        cstart.assign((size_t)(dim * dim * dim) + 1, 0);
+        for (const auto& e : byc) ++cstart[(size_t)e.first + 1];
+        for (size_t k = 1; k < cstart.size(); ++k) cstart[k] += cstart[k - 1];
+    }
+    g.ptr.assign(N + 1, 0);
+    std::vector<int> tmp;
+    for (int i = 0; i < N; ++i) {
+        tmp.clear();
+        const long cx = cc[3 * i], cy = cc[3 * i + 1], cz = cc[3 * i + 2];
+        for (long dx = -1; dx <= 1; ++dx)
+            for (long dy = -1; dy <= 1; ++dy)
+                for (long dz = -1; dz <= 1; ++dz) {
+                    const long x = cx + dx, y = cy + dy, z = cz + dz;
+                    if (x < 0 || y < 0 || z < 0 || x >= dim || y >= dim || z >= dim) continue;
+                    const long key = key_of(x, y, z);
+                    size_t b0, b1;
+                    if (dense) {
+                        b0 = (size_t)cstart[(size_t)key];
+                        b1 = (size_t)cstart[(size_t)key + 1];
+                    } else {
+                        b0 = std::lower_bound(byc.begin(), byc.end(), std::make_pair(key, -1)) - byc.begin();
+                        b1 = b0;
+                        while (b1 < byc.size() && byc[b1].first == key) ++b1;
                     }
-            std::sort(nb[i].begin(), nb[i].end());
-        }
+                    for (size_t q = b0; q < b1; ++q) {
+                        const int j = byc[q].second;
+                        if (j != i && dist2(pos, i, j) <= reach2) tmp.push_back(j);
+                    }
+                }
+        std::sort(tmp.begin(), tmp.end());
+        g.nbr.insert(g.nbr.end(), tmp.begin(), tmp.end());
+        g.row_of.insert(g.row_of.end(), tmp.size(), i);
+        g.ptr[i + 1] = (int)g.nbr.size();
     }
     // blocks: each free sphere in Morton order takes its nearest free neighbours
     g.block_of.assign(N, -1);
     g.bptr.push_back(0);
+    std::vector<std::pair<double, int>> cand;
     for (auto& o : order) {
         int i = o.second;
         if (g.block_of[i] >= 0) continue;
         int b = (int)g.bptr.size() - 1;
         g.block_of[i] = b;
         g.bmem.push_back(i);
-        std::vector<std::pair<double, int>> cand;
-        for (int j : nb[i])
-            if (g.block_of[j] < 0)
-                cand.push_back({std::hypot(std::hypot(pos[3 * i] - pos[3 * j], pos[3 * i + 1] - pos[3 * j + 1]),
-                                           pos[3 * i + 2] - pos[3 * j + 2]),
-                                j});
-        std::sort(cand.begin(), cand.end());
-        for (size_t c = 0; c < cand.size() && (int)(g.bmem.size() - g.bptr.back()) < per_block; ++c) {
-            g.block_of[cand[c].second] = b;
-            g.bmem.push_back(cand[c].second);
+        if (per_block > 1) {
+            cand.clear();
+            for (int e = g.ptr[i]; e < g.ptr[i + 1]; ++e) {
+                const int j = g.nbr[e];
+                if (g.block_of[j] < 0) cand.push_back({dist2(pos, i, j), j});
+            }
+            std::sort(cand.begin(), cand.end());
+            for (size_t c = 0; c < cand.size() && (int)(g.bmem.size() - g.bptr.back()) < per_block; ++c) {
+                g.block_of[cand[c].second] = b;
+                g.bmem.push_back(cand[c].second);
+            }
         }
         g.bptr.push_back((int)g.bmem.size());
     }
-    g.ptr.assign(N + 1, 0);
-    for (int i = 0; i < N; ++i) {
-        g.ptr[i + 1] = g.ptr[i] + (int)nb[i].size();
-        for (int j : nb[i]) {
-            g.nbr.push_back(j);
-            g.row_of.push_back(i);
-            g.same.push_back(g.block_of[i] == g.block_of[j] ? 1 : 0);
-        }
-    }
+    g.same.resize(g.nbr.size());
+    for (size_t e = 0; e < g.nbr.size(); ++e) g.same[e] = g.block_of[g.row_of[e]] == g.block_of[g.nbr[e]] ? 1 : 0;
     return g;
 }
 
