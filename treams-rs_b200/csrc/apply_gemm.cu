@@ -39,6 +39,13 @@ struct GemmShape {
     int DI, TR, TC, RG, CG, KJ;
 };
 
+// The product restricted to the first nsrc source lm and the first ndst destination lm (the
+// table then needs degrees p <= order = l_max(src) + l_max(dst)); input vectors hold ldin and
+// output vectors ldout complex entries per sphere. The full operator: nsrc = ndst = nlm.
+struct SubOp {
+    int nsrc, ndst, order, ldin, ldout;
+};
+
 // Tile shapes per lmax: G rows DI * tsize <= TR * RG, columns 2 nlm <= TC * CG
 GemmShape gemm_shape(int L) {
     switch (L) {
@@ -49,21 +56,28 @@ GemmShape gemm_shape(int L) {
     }
 }
 
-size_t gemm_smem(const DevPlan& P, const GemmShape& s) {
+// The dipole-source (and dipole-to-dipole) products: G is (DI (order+1)^2) x 6, about 200 rows
+GemmShape sub_shape(int tsz) {
+    const int DI = std::max(1, 200 / tsz);
+    return {DI, 4, 2, (DI * tsz + 3) / 4, 3, 16};
+}
+
+size_t gemm_smem(const SubOp& o, const GemmShape& s) {
+    const size_t tsz = (size_t)(o.order + 1) * (o.order + 1);
     const size_t rows = (size_t)s.TR * s.RG, cols = (size_t)s.TC * s.CG, npair = (size_t)s.DI * s.KJ;
-    const size_t chunk = ((size_t)s.KJ * rows + (size_t)s.KJ * cols + npair * (P.order + 1)) * sizeof(cplx) +
+    const size_t chunk = ((size_t)s.KJ * rows + (size_t)s.KJ * cols + npair * (o.order + 1)) * sizeof(cplx) +
                          npair * sizeof(double4);
-    const size_t g = (size_t)s.DI * P.tsize * 2 * P.nlm * sizeof(cplx);
+    const size_t g = (size_t)s.DI * tsz * 2 * o.nsrc * sizeof(cplx);
     return chunk > g ? chunk : g;
 }
 
 template <int TR, int TC>
 __global__ void __launch_bounds__(512, 1)
-    apply_gemm_kernel(DevPlan P, int N, double k, const double* __restrict__ pos, const cplx* __restrict__ T,
+    apply_gemm_kernel(DevPlan P, SubOp O, int N, double k, const double* __restrict__ pos, const cplx* __restrict__ T,
                       const cplx* __restrict__ x, size_t ldx, const cplx* __restrict__ zadd, double alpha, double beta,
                       bool singular, cplx* __restrict__ y, int DI, int RG, int CG, int KJ) {
     extern __shared__ __align__(16) unsigned char ag_smem[];
-    const int nlm = P.nlm, M = 2 * nlm, ts = P.tsize, order = P.order, ord1 = order + 1;
+    const int nlm = P.nlm, M = 2 * O.nsrc, order = O.order, ord1 = order + 1, ts = ord1 * ord1;
     const int ROWS = TR * RG, COLS = TC * CG, npair = DI * KJ;
     cplx* Zs = reinterpret_cast<cplx*>(ag_smem);                     // KJ x ROWS (source-major)
     cplx* Xs = Zs + (size_t)KJ * ROWS;                               // KJ x COLS
@@ -74,7 +88,7 @@ __global__ void __launch_bounds__(512, 1)
     const int rg = tid / CG, cg = tid - (tid / CG) * CG;
     const bool worker = rg < RG;
     const int i0 = blockIdx.x * DI;
-    const size_t coff = (size_t)blockIdx.y * ldx;
+    const size_t coff = (size_t)blockIdx.y * ldx;  // column offset, input and output alike
     const cplx* xc = x + coff;
 
     cplx acc[TR][TC];
@@ -114,7 +128,7 @@ __global__ void __launch_bounds__(512, 1)
         }
         for (int t = tid; t < KJ * COLS; t += nthr) {
             const int jj = t / COLS, col = t - jj * COLS, j = j0 + jj;
-            Xs[t] = (col < M && j < N) ? xc[(size_t)j * M + col] : mk(0.0, 0.0);
+            Xs[t] = (col < M && j < N) ? xc[(size_t)j * O.ldin + col] : mk(0.0, 0.0);
         }
         __syncthreads();
         // B) per (pair, order m >= 0): column m of the table, entries deg = m..order at
@@ -185,12 +199,13 @@ __global__ void __launch_bounds__(512, 1)
     }
     __syncthreads();
     // term lists of the plan, Mie block and epilogue: thread per (destination, d)
-    for (int it = tid; it < DI * nlm; it += nthr) {
-        const int il = it / nlm, d = it - il * nlm, i = i0 + il;
+    const int ndst = O.ndst;
+    for (int it = tid; it < DI * ndst; it += nthr) {
+        const int il = it / ndst, d = it - il * ndst, i = i0 + il;
         if (i >= N) continue;
         const cplx* G = Gs + (size_t)il * ts * M;
         cplx sp = mk(0.0, 0.0), sn = mk(0.0, 0.0);
-        for (int s = 0; s < nlm; ++s) {
+        for (int s = 0; s < O.nsrc; ++s) {
             const int2 cb = __ldg(&P.combo[s * nlm + d]);
             int t = cb.x;
             const int na = cb.y & 0xffff, nb = cb.y >> 16;

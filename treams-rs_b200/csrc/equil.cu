@@ -33,7 +33,7 @@ namespace {
 
 constexpr int EQ_CHUNKS = 32;
 // bfloat16 magnitude mirror at the end of the scratch, 256-byte aligned
-inline size_t mirror_offset(int n) { return ((size_t)(EQ_CHUNKS + 2) * n + (n + 255) / 256 + 1 + 31) / 32 * 32; }
+inline size_t mirror_offset(int n) { return ((size_t)(EQ_CHUNKS + 4) * n + (n + 255) / 256 + 1 + 31) / 32 * 32; }
 inline size_t mirror_doubles(int n) { return ((size_t)n * n * 2 + 255) / 256 * 32; }
 
 template <typename C>
@@ -140,43 +140,76 @@ __device__ __forceinline__ void bal_advance(double& factor, double sum, int* fla
     if (step < 0.5 || step > 2.0) atomicOr(flags, BAL_COARSE);
 }
 
-// The sweeps run on R A C without forming it: |a_ij| r_i c_j with the max scales r, c.
-template <typename C>
-__global__ void bal_col_kernel(const C* __restrict__ A, int n, const double* __restrict__ r,
-                               const double* __restrict__ c, const double* __restrict__ x, double* __restrict__ y,
+// The sweeps run on R A C without forming it: |a_ij| r_i c_j with the max scales r, c, read
+// from the bfloat16 mirror M two rows (one 4-byte word; n is even) at a time. Row weights
+// w_i = x_i r_i and column weights cy_j = c_j y_j are kept beside the factors.
+__device__ __forceinline__ double lo16(uint32_t v) { return (double)__uint_as_float(v << 16); }
+__device__ __forceinline__ double hi16(uint32_t v) { return (double)__uint_as_float(v & 0xffff0000u); }
+
+// column sums: a warp per column, fixed-order warp reduction
+__global__ void bal_col_kernel(const uint16_t* __restrict__ Mg, int n, const double* __restrict__ w,
+                               const double* __restrict__ c, double* __restrict__ y, double* __restrict__ cy,
                                int* flags) {
-    __shared__ double sh[256];
-    const int j = blockIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (j >= n) return;
+    const uint32_t* col = reinterpret_cast<const uint32_t*>(Mg + (size_t)j * n);
     double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += x[i] * r[i] * mag(A[(size_t)j * n + i]);
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-        __syncthreads();
+    for (int q = lane; q < n / 2; q += 32) {
+        const uint32_t v = col[q];
+        s = fma(w[2 * q], lo16(v), s);
+        s = fma(w[2 * q + 1], hi16(v), s);
     }
-    if (threadIdx.x == 0) bal_advance(y[j], sh[0] * c[j], flags);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) {
+        double yy = y[j];
+        bal_advance(yy, s * c[j], flags);
+        y[j] = yy;
+        cy[j] = c[j] * yy;
+    }
 }
 
-template <typename C>
-__global__ void bal_row_partial(const C* __restrict__ A, int n, const double* __restrict__ c,
-                                const double* __restrict__ y, double* __restrict__ partial) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+// row sums over a chunk of columns: a thread per pair of rows, 4-byte loads coalesced over the warp
+__global__ void bal_row_partial(const uint16_t* __restrict__ Mg, int n, const double* __restrict__ cy,
+                                double* __restrict__ partial) {
+    const int i2 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (2 * i2 >= n) return;
     const int per = (n + EQ_CHUNKS - 1) / EQ_CHUNKS;
     const int j0 = blockIdx.y * per, j1 = min(n, j0 + per);
-    double s = 0.0;
-    for (int j = j0; j < j1; ++j) s += mag(A[(size_t)j * n + i]) * (c[j] * y[j]);
-    partial[(size_t)blockIdx.y * n + i] = s;
+    double s0 = 0.0, s1 = 0.0;
+    for (int j = j0; j < j1; ++j) {
+        const uint32_t v = reinterpret_cast<const uint32_t*>(Mg + (size_t)j * n)[i2];
+        const double wj = cy[j];
+        s0 = fma(lo16(v), wj, s0);
+        s1 = fma(hi16(v), wj, s1);
+    }
+    partial[(size_t)blockIdx.y * n + 2 * i2] = s0;
+    partial[(size_t)blockIdx.y * n + 2 * i2 + 1] = s1;
 }
 
 __global__ void bal_row_update(const double* __restrict__ partial, int n, const double* __restrict__ r,
-                               double* __restrict__ x, int* flags) {
+                               double* __restrict__ x, double* __restrict__ w, int* flags) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double s = 0.0;
     for (int c = 0; c < EQ_CHUNKS; ++c) s += partial[(size_t)c * n + i];
-    bal_advance(x[i], s * r[i], flags);
+    double xx = x[i];
+    bal_advance(xx, s * r[i], flags);
+    x[i] = xx;
+    w[i] = xx * r[i];
+}
+
+// x = y = 1, w = r, cy = c
+__global__ void bal_init_kernel(int n, const double* __restrict__ r, const double* __restrict__ c,
+                                double* __restrict__ x, double* __restrict__ y, double* __restrict__ w,
+                                double* __restrict__ cy) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x[i] = 1.0;
+    y[i] = 1.0;
+    w[i] = r[i];
+    cy[i] = c[i];
 }
 
 // factors within 2^+-256 and normal products with the max scales, else BAL_UNFIT
@@ -199,29 +232,27 @@ __global__ void bal_fold_kernel(int n, const double* __restrict__ x, const doubl
     c[i] *= y[i];
 }
 
-__global__ void fill_kernel(double* __restrict__ v, size_t n, double value) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) v[i] = value;
-}
 
-// Balancing sweeps over R A C (A unscaled, max scales r and c); on success r and c take the
-// factors (the caller then scales A once). scratch: x (n), y (n), partial (EQ_CHUNKS n), flags.
-template <typename C>
-tcu_status balance_impl(const C* A, int n, double* r, double* c, double* scratch, int* sweeps_out, cudaStream_t st,
-                        long long* launches) {
+// Balancing sweeps over R A C (A unscaled, mirror Mg of |A|, max scales r and c); on success r
+// and c take the factors (the caller then scales A once). scratch: x, y, w, cy (n each),
+// partial (EQ_CHUNKS n), flags.
+tcu_status balance_impl(const uint16_t* Mg, int n, double* r, double* c, double* scratch, int* sweeps_out,
+                        cudaStream_t st, long long* launches) {
     double* x = scratch;
     double* y = x + n;
-    double* partial = y + n;
+    double* w = y + n;
+    double* cy = w + n;
+    double* partial = cy + n;
     int* d_flags = reinterpret_cast<int*>(partial + (size_t)EQ_CHUNKS * n);
-    const int nb = (n + 255) / 256;
-    fill_kernel<<<(2 * n + 255) / 256, 256, 0, st>>>(x, 2 * (size_t)n, 1.0);
+    const int nb = (n + 255) / 256, nb2 = (n / 2 + 255) / 256;
+    bal_init_kernel<<<nb, 256, 0, st>>>(n, r, c, x, y, w, cy);
     if (launches) ++*launches;
     int flags = 0, sweep = 0;
     for (; sweep < BAL_SWEEPS; ++sweep) {
         if (cudaMemsetAsync(d_flags, 0, sizeof(int), st) != cudaSuccess) return TCU_DEVICE_ERROR;
-        bal_col_kernel<C><<<n, 256, 0, st>>>(A, n, r, c, x, y, d_flags);
-        bal_row_partial<C><<<dim3(nb, EQ_CHUNKS), 256, 0, st>>>(A, n, c, y, partial);
-        bal_row_update<<<nb, 256, 0, st>>>(partial, n, r, x, d_flags);
+        bal_col_kernel<<<(n + 7) / 8, 256, 0, st>>>(Mg, n, w, c, y, cy, d_flags);
+        bal_row_partial<<<dim3(nb2, EQ_CHUNKS), 256, 0, st>>>(Mg, n, cy, partial);
+        bal_row_update<<<nb, 256, 0, st>>>(partial, n, r, x, w, d_flags);
         if (launches) *launches += 3;
         if (cudaMemcpyAsync(&flags, d_flags, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
             cudaStreamSynchronize(st) != cudaSuccess)
@@ -268,7 +299,7 @@ tcu_status equilibrate_impl(C* A, int n, double threshold, double* r, double* c,
     col_scale<uint16_t><<<n, 256, 0, st>>>(mirror, n, r, c);
     if (launches) ++*launches;
     int sweeps = 0;
-    const tcu_status s = balance_impl<uint16_t>(mirror, n, r, c, partial, &sweeps, st, launches);
+    const tcu_status s = (n % 2 == 0) ? balance_impl(mirror, n, r, c, partial, &sweeps, st, launches) : TCU_OK;
     if (s) return s;
     apply_scales<C><<<148 * 16, 256, 0, st>>>(A, n, r, c);  // R A C with the balanced (or max) scales
     if (launches) ++*launches;
