@@ -1,4 +1,6 @@
-// Matrix-free operator x - T C x in product form, for lmax 2..5.
+// Matrix-free operator x - T C x in product form, for lmax 2..5, and its dipole blocks (any
+// lmax): the columns of the dipole sources (the coarse correction of the two-level
+// preconditioner) and the dipole-to-dipole block (its coarse operator).
 //
 // The coupling of destination sphere i is, per destination mode d and helicity,
 //   (C x)_i[d, +] = sum_{j != i} sum_s (A_ij(s,d) + B_ij(s,d)) x_j[2s]
@@ -223,8 +225,9 @@ __global__ void __launch_bounds__(512, 1)
                 cfma(sn, cneg(w), ge[1]);
             }
         }
-        const size_t row = (size_t)i * M + 2 * d;
-        const cplx x0 = xc[row], x1 = xc[row + 1];
+        // the input at (i, d) exists for source lm only (d < nsrc), the output for d < ndst
+        const size_t row = (size_t)i * O.ldout + 2 * d, rin = (size_t)i * O.ldin + 2 * d;
+        const cplx x0 = d < O.nsrc ? xc[rin] : mk(0.0, 0.0), x1 = d < O.nsrc ? xc[rin + 1] : mk(0.0, 0.0);
         cplx y0, y1;
         if (singular) {
             cplx tc0 = sp, tc1 = sn;  // T null: the coupling alone
@@ -257,32 +260,36 @@ bool apply_gemm_supported(const DevPlan& P) {
     return !(e && strcmp(e, "terms") == 0);
 }
 
+template <int TR, int TC>
+static void launch_shape(const DevPlan& P, const SubOp& O, const GemmShape& s, int N, double k, const double* pos,
+                         const cplx* T, const cplx* x, size_t ldx, int ncol, const cplx* zadd, double alpha,
+                         double beta, bool singular, cplx* y, cudaStream_t st) {
+    const dim3 grid((unsigned)((N + s.DI - 1) / s.DI), (unsigned)ncol);
+    apply_gemm_kernel<TR, TC><<<grid, s.RG * s.CG, gemm_smem(O, s), st>>>(P, O, N, k, pos, T, x, ldx, zadd, alpha,
+                                                                          beta, singular, y, s.DI, s.RG, s.CG, s.KJ);
+}
+
 void launch_apply_gemm(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                        int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y,
                        cudaStream_t st) {
     if (N <= 0 || ncol <= 0) return;
     const GemmShape s = gemm_shape(P.L);
-    const size_t smem = gemm_smem(P, s);
-    const dim3 grid((unsigned)((N + s.DI - 1) / s.DI), (unsigned)ncol);
-    const int threads = s.RG * s.CG;
+    const SubOp O{P.nlm, P.nlm, P.order, 2 * P.nlm, 2 * P.nlm};
     switch (P.L) {
-        case 2:
-            apply_gemm_kernel<4, 2><<<grid, threads, smem, st>>>(P, N, k, pos, T, x, ldx, zadd, alpha, beta, singular,
-                                                                 y, s.DI, s.RG, s.CG, s.KJ);
-            break;
-        case 3:
-            apply_gemm_kernel<4, 3><<<grid, threads, smem, st>>>(P, N, k, pos, T, x, ldx, zadd, alpha, beta, singular,
-                                                                 y, s.DI, s.RG, s.CG, s.KJ);
-            break;
-        case 4:
-            apply_gemm_kernel<4, 4><<<grid, threads, smem, st>>>(P, N, k, pos, T, x, ldx, zadd, alpha, beta, singular,
-                                                                 y, s.DI, s.RG, s.CG, s.KJ);
-            break;
-        default:
-            apply_gemm_kernel<4, 5><<<grid, threads, smem, st>>>(P, N, k, pos, T, x, ldx, zadd, alpha, beta, singular,
-                                                                 y, s.DI, s.RG, s.CG, s.KJ);
-            break;
+        case 2: launch_shape<4, 2>(P, O, s, N, k, pos, T, x, ldx, ncol, zadd, alpha, beta, singular, y, st); break;
+        case 3: launch_shape<4, 3>(P, O, s, N, k, pos, T, x, ldx, ncol, zadd, alpha, beta, singular, y, st); break;
+        case 4: launch_shape<4, 4>(P, O, s, N, k, pos, T, x, ldx, ncol, zadd, alpha, beta, singular, y, st); break;
+        default: launch_shape<4, 5>(P, O, s, N, k, pos, T, x, ldx, ncol, zadd, alpha, beta, singular, y, st); break;
     }
+}
+
+void launch_apply_dipole(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* z,
+                         bool dipole_rows, const cplx* zadd, double alpha, double beta, cplx* y, cudaStream_t st) {
+    if (N <= 0) return;
+    const int ndst = dipole_rows ? 3 : P.nlm;
+    const SubOp O{3, ndst, 1 + (dipole_rows ? 1 : P.L), 6, 2 * ndst};
+    const GemmShape s = sub_shape((O.order + 1) * (O.order + 1));
+    launch_shape<4, 2>(P, O, s, N, k, pos, T, z, 0, 1, zadd, alpha, beta, true, y, st);
 }
 
 void apply_gemm_init_attributes() {

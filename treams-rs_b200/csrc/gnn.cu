@@ -335,71 +335,7 @@ __global__ void coarse_scatter_add_kernel(int N, int M, const cplx* __restrict__
     const size_t o = (size_t)(t / 6) * M + t % 6;
     out[o] = cadd(out[o], vc[t]);
 }
-constexpr int CG_CHUNK = 512;  // columns per partial sum of the coarse-column product
-__global__ void __launch_bounds__(256) coarse_gemv_partial_kernel(size_t n, int nc, const float2* __restrict__ A,
-                                                                  const cplx* __restrict__ vc, cplx* __restrict__ part) {
-    __shared__ cplx xs[CG_CHUNK];
-    const int c0 = blockIdx.y * CG_CHUNK, cnt = min(CG_CHUNK, nc - c0);
-    for (int c = threadIdx.x; c < cnt; c += blockDim.x) xs[c] = vc[c0 + c];
-    __syncthreads();
-    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    cplx acc = mk(0.0, 0.0);
-    const float2* a = A + (size_t)c0 * n + r;
-#pragma unroll 8
-    for (int c = 0; c < cnt; ++c) {
-        const float2 v = __ldcs(a + (size_t)c * n);
-        cfma(acc, mk(v.x, v.y), xs[c]);
-    }
-    part[(size_t)blockIdx.y * n + r] = acc;
-}
-__global__ void coarse_gemv_final_kernel(size_t n, int nchunk, const cplx* __restrict__ part, const cplx* __restrict__ v,
-                                         cplx* __restrict__ r1) {
-    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n) return;
-    cplx s = mk(0.0, 0.0);
-    for (int k = 0; k < nchunk; ++k) s = cadd(s, part[(size_t)k * n + r]);
-    r1[r] = csub(v[r], s);
-}
-
 unsigned blocks_for(size_t count, int threads) { return (unsigned)((count + threads - 1) / threads); }
-
-// Acc (nc x nc, complex64) = the dipole rows of A[:, c]: row i*6+q of Acc is row i*M+q of A[:, c]
-__global__ void coarse_rows_kernel(int N, int M, size_t n, const float2* __restrict__ Acols, float2* __restrict__ Acc) {
-    const size_t nc = (size_t)6 * N;
-    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nc * nc) return;
-    const size_t col = t / nc, r = t - col * nc;
-    Acc[t] = Acols[col * n + (r / 6) * M + r % 6];
-}
-
-// y = A x (A m x k complex64 column-major, FP64 accumulation), partial sums over column chunks
-__global__ void __launch_bounds__(256) c64_gemv_partial_kernel(size_t m, int k, const float2* __restrict__ A,
-                                                               const cplx* __restrict__ x, cplx* __restrict__ part) {
-    __shared__ cplx xs[CG_CHUNK];
-    const int c0 = blockIdx.y * CG_CHUNK, cnt = min(CG_CHUNK, k - c0);
-    for (int c = threadIdx.x; c < cnt; c += blockDim.x) xs[c] = x[c0 + c];
-    __syncthreads();
-    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= m) return;
-    cplx acc = mk(0.0, 0.0);
-    const float2* a = A + (size_t)c0 * m + r;
-#pragma unroll 8
-    for (int c = 0; c < cnt; ++c) {
-        const float2 v = __ldcs(a + (size_t)c * m);
-        cfma(acc, mk(v.x, v.y), xs[c]);
-    }
-    part[(size_t)blockIdx.y * m + r] = acc;
-}
-__global__ void c64_gemv_final_kernel(size_t m, int nchunk, const cplx* __restrict__ part, cplx* __restrict__ y) {
-    const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= m) return;
-    cplx s = mk(0.0, 0.0);
-    for (int k = 0; k < nchunk; ++k) s = cadd(s, part[(size_t)k * m + r]);
-    y[r] = s;
-}
-
-
 
 // ---- shared set-up -------------------------------------------------------------------------
 // Node and edge features of the network (the tests restate them).
@@ -528,40 +464,44 @@ struct GraphData {
     }
 };
 
-// The coarse dipole system: A[:, c] (complex64, n x 6N) and the LU of A_cc.
-// Inexact coarse solve for large dipole systems: restarted GMRES on A_cc (complex64 operator,
-// FP64 vectors and Krylov basis, Gram-Schmidt twice with fixed-order dot products, Givens
-// rotations on the host) to a relative residual of rtol or max_it iterations, from x = 0. The
-// outer GMRES is flexible, so a preconditioner that varies from one application to the next
-// is allowed. Cheaper than factoring A_cc once its dimension reaches a few thousand: a few
-// streaming products of 8 nc^2 bytes per outer iteration instead of (8/3) nc^3 flops of LU.
+// The coarse dipole system, matrix-free. Its operator A_cc = R (I - T C) P (P puts a 6N dipole
+// vector on the dipole modes, R takes them) and the columns A P of the correction are the
+// dipole blocks of the operator in product form (launch_apply_dipole): no dense dipole
+// columns are assembled or stored.
+// Inexact coarse solve for large dipole systems: restarted GMRES on A_cc (FP64 vectors and
+// Krylov basis, Gram-Schmidt twice with fixed-order dot products, Givens rotations on the
+// host) to a relative residual of rtol or max_it iterations, from x = 0. The outer GMRES is
+// flexible, so a preconditioner that varies from one application to the next is allowed.
+// Cheaper than factoring A_cc once its dimension reaches a few thousand.
 class IterativeCoarse : public CoarseSolve {
    public:
-    int nc = 0, m = 0, max_it = 0, nchunk = 0;
+    int N = 0, nc = 0, m = 0, max_it = 0;
     long long inner_iterations = 0;  // over all applications
-    double rtol = 1e-3;
-    DevArray Acc, V, w, part, h, small, dpart;
+    double rtol = 1e-3, k0 = 0.0;
+    const DevPlan* plan = nullptr;
+    const double* pos = nullptr;
+    const cplx* T = nullptr;
+    DevArray V, w, h, small, dpart;
     long long* launches = nullptr;
-    bool build(int N, int M, size_t n, const float2* Acols, int restart, int max_iterations, double tol,
-               cudaStream_t st) {
+    bool build(const DevPlan& P, int N_, double k, const double* d_pos, const cplx* d_T, int restart,
+               int max_iterations, double tol) {
+        plan = &P;
+        N = N_;
+        k0 = k;
+        pos = d_pos;
+        T = d_T;
         nc = 6 * N;
         m = restart;
         max_it = max_iterations;
         rtol = tol;
-        nchunk = (nc + CG_CHUNK - 1) / CG_CHUNK;
-        if (!Acc.alloc((size_t)nc * nc * sizeof(float2)) || !V.alloc((size_t)(m + 1) * nc * sizeof(cplx)) ||
-            !w.alloc((size_t)nc * sizeof(cplx)) || !part.alloc((size_t)nc * nchunk * sizeof(cplx)) ||
-            !h.alloc((size_t)(m + 1) * sizeof(cplx)) || !small.alloc(64 * sizeof(double)) ||
-            !dpart.alloc((size_t)std::max(m + 1, 8) * 256 * sizeof(cplx)))
-            return false;
-        coarse_rows_kernel<<<blocks_for((size_t)nc * nc, 256), 256, 0, st>>>(N, M, n, Acols, Acc.as<float2>());
-        return true;
+        return V.alloc((size_t)(m + 1) * nc * sizeof(cplx)) && w.alloc((size_t)nc * sizeof(cplx)) &&
+               h.alloc((size_t)(m + 1) * sizeof(cplx)) && small.alloc(64 * sizeof(double)) &&
+               dpart.alloc((size_t)std::max(m + 1, 8) * 256 * sizeof(cplx));
     }
+    // y = A_cc x = x - R T C P x
     void matvec(const cplx* x, cplx* y, cudaStream_t st) {
-        dim3 grid(blocks_for(nc, 256), nchunk);
-        c64_gemv_partial_kernel<<<grid, 256, 0, st>>>(nc, nc, Acc.as<float2>(), x, part.as<cplx>());
-        c64_gemv_final_kernel<<<blocks_for(nc, 256), 256, 0, st>>>(nc, nchunk, part.as<cplx>(), y);
-        if (launches) *launches += 2;
+        launch_apply_dipole(*plan, N, k0, pos, T, x, true, nullptr, 1.0, -1.0, y, st);
+        if (launches) ++*launches;
     }
     tcu_status solve(double2* v, cudaStream_t st) override {
         // r0 = v (x0 = 0); V0 = v / |v|
@@ -632,44 +572,45 @@ class IterativeCoarse : public CoarseSolve {
 };
 
 struct Coarse {
-    int N = 0, M = 0, nc = 0, nchunk = 0;
+    int N = 0, M = 0, nc = 0;
     size_t n = 0;
-    DevArray Acols, vc, part;
+    double k0 = 0.0;
+    const DevPlan* plan = nullptr;
+    const double* pos = nullptr;
+    const cplx* T = nullptr;
+    DevArray vc;
     std::unique_ptr<CoarseSolve> solver;
-    bool build(cudaStream_t st, const DevPlan& P, int N_, double k0, const double* d_pos, const cplx* d_T,
-               std::unique_ptr<CoarseSolve> s, long long* launches) {
+    bool build(const DevPlan& P, int N_, double k, const double* d_pos, const cplx* d_T, std::unique_ptr<CoarseSolve> s,
+               long long* launches) {
+        plan = &P;
         N = N_;
         M = 2 * P.nlm;
         n = (size_t)N * M;
         nc = 6 * N;
-        nchunk = (nc + CG_CHUNK - 1) / CG_CHUNK;
+        k0 = k;
+        pos = d_pos;
+        T = d_T;
         solver = std::move(s);
-        if (!Acols.alloc(n * (size_t)nc * sizeof(float2)) || !vc.alloc((size_t)nc * sizeof(cplx)) ||
-            !part.alloc(n * (size_t)nchunk * sizeof(cplx)))
-            return false;
-        launch_assemble_sources(P, N, k0, d_pos, d_T, Acols.as<float2>(), n, 3, st);
-        if (launches) ++*launches;
-        if (!solver) {  // no factor given: an inexact GMRES on the dipole rows of A[:, c]
+        if (!vc.alloc((size_t)nc * sizeof(cplx))) return false;
+        if (!solver) {  // no factor given: an inexact GMRES on the dipole block
             auto it = std::make_unique<IterativeCoarse>();
             it->launches = launches;
             // relative tolerance of the inner solve: 3e-2 (the 4096-sphere workload measured 300,
             // 291, 256 and 269 ms at 1e-3, 1e-2, 3e-2 and 1e-1), or TCU_COARSE_RTOL
             const char* e = getenv("TCU_COARSE_RTOL");
             const double rtol = (e && atof(e) > 0.0 && atof(e) < 1.0) ? atof(e) : 3e-2;
-            if (!it->build(N, M, n, Acols.as<float2>(), 30, 30, rtol, st)) return false;
+            if (!it->build(P, N, k, d_pos, d_T, 30, 30, rtol)) return false;
             solver = std::move(it);
         }
         return true;
     }
-    // z_c = A_cc^-1 v_c (into vc) and r1 = v - A[:, c] z_c
+    // z_c = A_cc^-1 v_c (into vc) and r1 = v - A P z_c = v - P z_c + T C P z_c
     tcu_status correct(const cplx* v, cplx* r1, cudaStream_t st, long long* launches) {
         coarse_gather_kernel<<<blocks_for(nc, 256), 256, 0, st>>>(N, M, v, vc.as<cplx>());
         tcu_status s = solver->solve(vc.as<cplx>(), st);
         if (s) return s;
-        dim3 grid(blocks_for(n, 256), nchunk);
-        coarse_gemv_partial_kernel<<<grid, 256, 0, st>>>(n, nc, Acols.as<float2>(), vc.as<cplx>(), part.as<cplx>());
-        coarse_gemv_final_kernel<<<blocks_for(n, 256), 256, 0, st>>>(n, nchunk, part.as<cplx>(), v, r1);
-        if (launches) *launches += 3;
+        launch_apply_dipole(*plan, N, k0, pos, T, vc.as<cplx>(), false, v, -1.0, 1.0, r1, st);
+        if (launches) *launches += 2;
         return TCU_OK;
     }
     void add_coarse(cplx* out, cudaStream_t st, long long* launches) {
@@ -714,7 +655,7 @@ tcu_status make_two_level(cudaStream_t st, bool learned, const DevPlan& P, int L
     for (int i = 0; i < N; ++i) rmax = std::max(rmax, h_radii[i]);
     const double cutoff = 2.0 * (reach > 0.0 ? reach : LEARNED_REACH) * rmax;
     if (!pre->graph.build(st, P, L, N, k0, d_pos, h_pos, h_radii, h_eps, cutoff, launches)) return TCU_OUT_OF_MEMORY;
-    if (!pre->coarse.build(st, P, N, k0, d_pos, d_T, std::move(coarse), launches)) return TCU_OUT_OF_MEMORY;
+    if (!pre->coarse.build(P, N, k0, d_pos, d_T, std::move(coarse), launches)) return TCU_OUT_OF_MEMORY;
     if (!pre->r1.alloc(pre->graph.n * sizeof(cplx)) || !pre->noskip.alloc(std::max<size_t>(pre->graph.nnz, 1)))
         return TCU_OUT_OF_MEMORY;
     cudaMemsetAsync(pre->noskip.p, 0, std::max<size_t>(pre->graph.nnz, 1), st);
@@ -759,7 +700,7 @@ tcu_status LearnedProblem::build(cudaStream_t st, const DevPlan& P, int L_, int 
     for (int i = 0; i < N; ++i) rmax = std::max(rmax, h_radii[i]);
     const double cutoff = 2.0 * (reach > 0.0 ? reach : LEARNED_REACH) * rmax;
     if (!m.graph.build(st, P, L, N, k0, d_pos, h_pos, h_radii, h_eps, cutoff, launches)) return TCU_OUT_OF_MEMORY;
-    if (!m.coarse.build(st, P, N, k0, d_pos, d_T, std::move(cs), launches)) return TCU_OUT_OF_MEMORY;
+    if (!m.coarse.build(P, N, k0, d_pos, d_T, std::move(cs), launches)) return TCU_OUT_OF_MEMORY;
     n = m.graph.n;
     m.p = nprobe;
     const size_t vb = n * (size_t)nprobe * sizeof(cplx), nnz = m.graph.nnz;

@@ -102,10 +102,6 @@ struct StageScope {
 // pairs.cu
 void launch_assemble(const DevPlan& P, int N, double k, const double* pos, const cplx* T, void* out, size_t ld,
                      bool fp32, cudaStream_t st);
-// columns of I - T C for the first nsrc source lm of every sphere only (2 nsrc columns per
-// sphere, complex64, rows of all modes; ld >= N M)
-void launch_assemble_sources(const DevPlan& P, int N, double k, const double* pos, const cplx* T, float2* out,
-                             size_t ld, int nsrc, cudaStream_t st);
 void launch_apply(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                   int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st);
 size_t apply_smem_bytes(const DevPlan& P, int ncol);
@@ -114,6 +110,11 @@ bool apply_gemm_supported(const DevPlan& P);
 void launch_apply_gemm(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* x, size_t ldx,
                        int ncol, const cplx* zadd, double alpha, double beta, bool singular, cplx* y, cudaStream_t st);
 void apply_gemm_init_attributes();
+// Dipole blocks of the operator in product form, one vector: z holds the 6 dipole modes of every
+// sphere; y = zadd + alpha (z on the dipole modes) + beta T (C P z), on all modes (y: n) or, with
+// dipole_rows, on the dipole modes only (y: 6N). P z is z on the dipole modes, zero elsewhere.
+void launch_apply_dipole(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* z,
+                         bool dipole_rows, const cplx* zadd, double alpha, double beta, cplx* y, cudaStream_t st);
 void launch_block(const DevPlan& P, double k, const double* d, bool singular, bool helicity, cplx* out,
                   cudaStream_t st);
 void launch_mie(int L, double k0, int N, const double* radii, const cplx* eps, cplx* T, int* status, cudaStream_t st);

@@ -625,15 +625,6 @@ void launch_assemble(const DevPlan& P, int N, double k, const double* pos, const
         assemble_kernel<double2><<<grid, 256, smem, st>>>(P, N, k, pos, T, (double2*)out, ld, pairs, P.nlm);
 }
 
-void launch_assemble_sources(const DevPlan& P, int N, double k, const double* pos, const cplx* T, float2* out,
-                             size_t ld, int nsrc, cudaStream_t st) {
-    StageScope sc(ST_ASSEMBLE, st);
-    int pairs = assemble_pairs_per_cta(P.nlm);
-    dim3 grid(N, (N + pairs - 1) / pairs);
-    size_t smem = (size_t)pairs * P.tsize * sizeof(cplx);
-    assemble_kernel<float2><<<grid, 256, smem, st>>>(P, N, k, pos, T, out, ld, pairs, nsrc);
-}
-
 static size_t apply2_smem(const DevPlan& P, int ncol) {
     const size_t main = ((size_t)AP_Q * P.tsize + (size_t)AP_Q * ncol * (2 * P.nlm + 1)) * sizeof(cplx);
     const size_t red = (size_t)AP_Q * P.nlm * 2 * ncol * sizeof(cplx);
