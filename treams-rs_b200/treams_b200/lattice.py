@@ -31,7 +31,8 @@ def array_solve_batch(lmax: int, k0: float, radius: float, eps: complex, lattice
     kp = np.ascontiguousarray(kpars, np.float64).reshape(-1, 2)
     e = np.array([complex(eps)], np.complex128)
     M = 2 * lmax * (lmax + 2)
-    out = np.zeros((kp.shape[0], M, M), np.complex128)
+    out = np.empty((kp.shape[0], M, M), np.complex128)  # every entry is written by the library
     _check(lib().tcu_array_solve_batch(ctx.handle, lmax, float(k0), float(radius), _p(e), _p(a), kp.shape[0], _p(kp),
                                        float(eta), _p(out)))
-    return np.ascontiguousarray(np.transpose(out, (0, 2, 1)))
+    # the library writes each X column-major; the transposed view indexes X[k][row, col]
+    return np.transpose(out, (0, 2, 1))
