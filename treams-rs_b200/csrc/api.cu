@@ -315,7 +315,7 @@ void apply_op(tcu_context* ctx, const DevPlan* P, int N, double k0, const double
 
 tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const double* radii_h, const double* eps_h,
                        const double* pos_h, const double* radii_d, const double* eps_d, const double* pos_d,
-                       int precision, tcu_factor** out, bool f16_pieces = true) {
+                       int precision, tcu_factor** out, bool reduced = true) {
     if (!out) return fail(TCU_INVALID_INPUT, "null output handle");
     *out = nullptr;
     if (precision != TCU_FP64 && precision != TCU_MIXED) return fail(TCU_INVALID_INPUT, "unknown precision");
@@ -334,7 +334,10 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
     f->n = n;
     f->precision = precision;
     f->k0 = k0;
-    f->wk.f16_pieces = f16_pieces && split_f16_default();
+    // reduced: the piece formats the environment may ask for (FP16 pieces, two-pass TF32);
+    // the refinement's fallback factor takes the three-pass TF32 split instead
+    f->wk.f16_pieces = reduced && split_f16_default();
+    f->wk.two_pass = reduced && !f->wk.f16_pieces && split_two_pass_default();
     f->wk.panel_rows = ctx->panel_rows;
     auto cleanup = [&]() {
         for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
@@ -498,10 +501,11 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
     sweeps = 1;
     if ((s = residual())) return s;
     {
-        // iterative refinement in FP64: up to 10 sweeps on mixed factors, 2 on FP64 factors
+        // iterative refinement in FP64: up to 10 sweeps on mixed factors (20 with two-pass updates), 2 on
+        // FP64 factors
         const double tol = ctx->refine_target;
         double prev = INFINITY;
-        const int max_sweeps = f->precision == TCU_MIXED ? 10 : 2;
+        const int max_sweeps = f->precision == TCU_MIXED ? (f->wk.two_pass ? 20 : 10) : 2;
         for (int it = 0; it < max_sweeps; ++it) {
             double worst = 0.0;
             for (int c = 0; c < p; ++c) worst = std::max(worst, bn[c] > 0 ? rn[c] / bn[c] : rn[c]);
@@ -528,7 +532,7 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
                 CK(cudaMemcpyAsync(he.data(), f->d_eps, f->N * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
                 CK(cudaMemcpyAsync(hp.data(), f->d_pos, f->N * 24, cudaMemcpyDeviceToHost, ctx->stream), "copy");
                 if ((s = sync_status(ctx, "fallback"))) return s;
-                const bool to_tf32 = f->wk.f16_pieces;
+                const bool to_tf32 = f->wk.f16_pieces || f->wk.two_pass;
                 if ((s = factor_impl(ctx, f->L, f->k0, f->N, hr.data(), he.data(), hp.data(), nullptr, nullptr,
                                      nullptr, to_tf32 ? TCU_MIXED : TCU_FP64, &f->fallback, false)))
                     return s;
@@ -613,7 +617,7 @@ tcu_status solve_adjoint_impl(tcu_factor* f, const double* G, int p, double* Y, 
     if ((s = residual())) return s;
     const double tol = ctx->refine_target;
     double prev = INFINITY;
-    const int max_sweeps = f->precision == TCU_MIXED ? 10 : 2;
+    const int max_sweeps = f->precision == TCU_MIXED ? (f->wk.two_pass ? 20 : 10) : 2;
     auto worst_of = [&]() {
         double w = 0.0;
         for (int c = 0; c < p; ++c) w = std::max(w, bn[c] > 0 ? rn[c] / bn[c] : rn[c]);
@@ -636,7 +640,7 @@ tcu_status solve_adjoint_impl(tcu_factor* f, const double* G, int p, double* Y, 
             CK(cudaMemcpyAsync(he.data(), f->d_eps, f->N * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
             CK(cudaMemcpyAsync(hp.data(), f->d_pos, f->N * 24, cudaMemcpyDeviceToHost, ctx->stream), "copy");
             if ((s = sync_status(ctx, "fallback"))) return s;
-            const bool to_tf32 = f->wk.f16_pieces;
+            const bool to_tf32 = f->wk.f16_pieces || f->wk.two_pass;
             if ((s = factor_impl(ctx, f->L, f->k0, f->N, hr.data(), he.data(), hp.data(), nullptr, nullptr, nullptr,
                                  to_tf32 ? TCU_MIXED : TCU_FP64, &f->fallback, false)))
                 return s;

@@ -198,7 +198,7 @@ struct Tf32Args {
     const float* sB;      // FP16 pieces: scale of each row of the B operand (ncols)
 };
 
-template <bool F16>
+template <bool F16, bool TWO>
 __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_constant__ CUtensorMap mAhi,
                                                              const __grid_constant__ CUtensorMap mAlo,
                                                              const __grid_constant__ CUtensorMap mBhi,
@@ -249,11 +249,11 @@ __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_consta
                     uint32_t ph = (step / TB_STAGES) & 1;
                     if (!mbar_wait(bar(EMPTY + s), ph ^ 1, abort_flag)) break;
                     uint32_t st = tiles_smem + s * STAGE_BYTES;
-                    mbar_expect_tx(bar(s), STAGE_BYTES);
+                    mbar_expect_tx(bar(s), TWO ? STAGE_BYTES - B_BYTES : STAGE_BYTES);
                     tma_load_2d(st, &mAhi, kb * TB_K, tm * TB_M, bar(s));
                     tma_load_2d(st + A_BYTES, &mAlo, kb * TB_K, tm * TB_M, bar(s));
                     tma_load_2d(st + 2 * A_BYTES, &mBhi, kb * TB_K, tn * TB_N, bar(s));
-                    tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBlo, kb * TB_K, tn * TB_N, bar(s));
+                    if (!TWO) tma_load_2d(st + 2 * A_BYTES + B_BYTES, &mBlo, kb * TB_K, tn * TB_N, bar(s));
                 }
             }
             if (*abort_flag) {
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(192, 1) tf32_update_kernel(const __grid_consta
                         uint64_t blo = swz_desc(st + 2 * A_BYTES + B_BYTES + ks * 32);
                         uint32_t first = (kb == 0 && ks == 0) ? 0u : 1u;
                         mma_split<F16>(d, ahi, bhi, idesc, first);
-                        mma_split<F16>(d, ahi, blo, idesc, 1u);
+                        if (!TWO) mma_split<F16>(d, ahi, blo, idesc, 1u);
                         mma_split<F16>(d, alo, bhi, idesc, 1u);
                     }
                     mma_commit(bar(EMPTY + s));
@@ -560,6 +560,18 @@ constexpr size_t TI_SMEM = (size_t)(128 * 129 + 64 * 64) * sizeof(float2);
 // cluster operators measured here the entries of one row of L21 or one column of U12 span
 // more than 2^20 even after equilibration, and FP16 pieces (8 exponent bits fewer) then leave
 // the FP64 refinement stalled, so every solve fell back to TF32 pieces.
+// Two passes hi*hi + lo*hi (the B operand, U12, rounded to TF32) when TCU_SPLIT=tf32x2: a
+// third fewer tensor-core passes and no B lo loads, for an update accurate to about 2^-11
+// relative to max|A| max|B| per term; the FP64 refinement then needs more sweeps, and a stall
+// falls back to the three-pass factor.
+bool split_two_pass_default() {
+    static const bool on = [] {
+        const char* e = getenv("TCU_SPLIT");
+        return e && std::strcmp(e, "tf32x2") == 0;
+    }();
+    return on;
+}
+
 bool split_f16_default() {
     static const bool on = [] {
         const char* e = getenv("TCU_SPLIT");
@@ -576,8 +588,12 @@ bool tf32_enabled() {
     if (on == 1) {
         static PerDeviceOnce attr;
         once_per_device(attr, [] {
-            cudaFuncSetAttribute(tf32_update_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
-            cudaFuncSetAttribute(tf32_update_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TF32_SMEM);
+            cudaFuncSetAttribute(tf32_update_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TF32_SMEM);
+            cudaFuncSetAttribute(tf32_update_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TF32_SMEM);
+            cudaFuncSetAttribute(tf32_update_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TF32_SMEM);
             cudaFuncSetAttribute(tri_inverse_l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TI_SMEM);
         });
     }
@@ -688,7 +704,8 @@ static bool ensure_pack(LuWork& wk, size_t need, cudaStream_t st) {
 // C[row0 .. row0+m2) x [col0 .. col0+ncols) -= Apack (m2 x kp) * Bpack (ncols x kp)^T;
 // sA != null selects FP16 pieces (row scales sA of the A operand, sB of the B operand).
 static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, int kp, void* ahi, void* alo, void* bhi,
-                     void* blo, const float* sA, const float* sB, LuWork& wk, cudaStream_t st, long long* launches) {
+                     void* blo, const float* sA, const float* sB, LuWork& wk, cudaStream_t st, long long* launches,
+                     bool two = false) {
     const bool f16 = sA != nullptr;
     CUtensorMap mAhi, mAlo, mBhi, mBlo;
     bool ok = make_map(&mAhi, ahi, m2, kp, TB_M, f16) && make_map(&mAlo, alo, m2, kp, TB_M, f16) &&
@@ -725,9 +742,11 @@ static void run_gemm(float2* A, int n, int row0, int col0, int m2, int ncols, in
     a.sB = sB;
     int grid = std::min(num_sms(), a.tiles);
     if (f16)
-        tf32_update_kernel<true><<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
+        tf32_update_kernel<true, false><<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
+    else if (two)
+        tf32_update_kernel<false, true><<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
     else
-        tf32_update_kernel<false><<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
+        tf32_update_kernel<false, false><<<grid, 192, TF32_SMEM, st>>>(mAhi, mAlo, mBhi, mBlo, mC, a);
     *launches += 1;
 }
 
@@ -830,7 +849,8 @@ void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_
     if (f16)
         run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, h_ahi, h_alo, h_bhi, h_blo, sA, sB, wk, st, launches);
     else
-        run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, ahi, alo, bhi, blo, nullptr, nullptr, wk, st, launches);
+        run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, ahi, alo, bhi, blo, nullptr, nullptr, wk, st, launches,
+                 wk.two_pass);
 }
 
 }  // namespace tcu

@@ -192,10 +192,13 @@ struct LuWork {
     void* pack = nullptr;      // packed GEMM operands (mixed path)
     size_t pack_bytes = 0;
     bool f16_pieces = false;   // mixed path: FP16 (true) or TF32 (false) pieces of the 3-pass split
+    bool two_pass = false;     // mixed path: two-pass TF32 trailing updates (B operand rounded to TF32)
     int panel_rows = 0;        // least rows per panel CTA (0: TCU_PANEL_ROWS or 32)
 };
 // FP16 pieces when the environment asks for them (TCU_SPLIT=f16), else TF32 pieces
 bool split_f16_default();
+// Two-pass TF32 trailing updates when the environment asks for them (TCU_SPLIT=tf32x2)
+bool split_two_pass_default();
 int lu_factor_fp64(double2* A, int n, LuWork& w, cudaStream_t st, long long* launches);
 // The panel's grid barrier with one arrival missing (bar: a zeroed counter); it gives up
 // after limit_s (clamped to [0, 4] s) and records status 8.
