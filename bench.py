@@ -583,13 +583,14 @@ def _measure_impl(args, precision, steps, warmup, with_e2e, *, ctx, lib, stream,
         # the update runs inside a seconds-long step: the sustained bf16 rate under the power cap
         bf16 = pk.get("bf16_tflops_sustained") or pk.get("bf16_tflops", 1590.0)
         tensor_peak = bf16 / 2.0  # TF32 dense = half of bf16 dense
-        executed = 3.0 * flops
+        passes = 3.0 if os.environ.get("TCU_SPLIT") in ("tf32x3", "f16") else 2.0
+        executed = passes * flops
         achieved = executed / (gemm[1] / 1e3) / 1e12 if gemm[1] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": tensor_peak, "unit": "TFLOP/s",
                 "frac": achieved / tensor_peak if achieved else None,
                 "traffic": TF32_TRAFFIC["ratio"] * update_launch_bytes(n, nb),
                 "traffic_note": TF32_TRAFFIC["note"],
-                "kernel": "tf32_update_kernel: split-TF32 tcgen05 trailing update (3 passes executed)",
+                "kernel": f"tf32_update_kernel: split-TF32 tcgen05 trailing update ({passes:.0f} passes executed)",
                 "useful_tflops": flops / (gemm[1] / 1e3) / 1e12 if gemm[1] else None,
                 "peak_note": f"TF32 dense peak = half the sustained bf16 GEMM rate, {bf16} TFLOP/s "
                              f"(of measured: {pk.get('source')})"}

@@ -6,8 +6,10 @@
 // so that D[2mu+c][nu] is part c of (L21 U12)[mu][nu] and the 2m x n' result maps onto
 // the interleaved storage of A22 (real leading dimension 2n).
 //
-// Precision: every operand is split x = hi + lo into two 11-bit-significand pieces and three
-// passes hi*hi + hi*lo + lo*hi accumulate in FP32 in TMEM (the lo*lo term is below FP32
+// Precision: every operand is split x = hi + lo into two 11-bit-significand pieces and the
+// passes accumulate in FP32 in TMEM: by default two, hi*hi + lo*hi (the B operand rounded to
+// TF32, about 2^-11 relative per term; the FP64 refinement takes one sweep more), with
+// TCU_SPLIT=tf32x3 or f16 three, hi*hi + hi*lo + lo*hi (the lo*lo term is below FP32
 // rounding). Two piece formats:
 //   FP16 (TCU_SPLIT=f16): each row of each operand (a complex row of L21, a column of U12) is
 //     first scaled by its own power of two 2^(14 - ceil log2 max|row|) (computed in the
@@ -21,7 +23,7 @@
 // Kernel layout (persistent, one CTA per SM, 192 threads):
 //   warp 0     TMA producer: 64-byte-swizzled boxes (64-byte K rows) of the four packed
 //              operands into a 4-stage shared-memory ring (48 KB per stage), mbarrier complete_tx;
-//   warp 1     TMEM allocator and MMA issuer (one thread): 2 K-steps x 3 passes per stage
+//   warp 1     TMEM allocator and MMA issuer (one thread): 2 K-steps x 2 or 3 passes per stage
 //              into a 128 x 256 FP32 accumulator, double-buffered in TMEM (512 columns);
 //   warps 2-5  epilogue: tcgen05.ld 32 columns at a time into a shared-memory staging buffer,
 //              TMA reduce-add of -D into A22.
@@ -560,14 +562,15 @@ constexpr size_t TI_SMEM = (size_t)(128 * 129 + 64 * 64) * sizeof(float2);
 // cluster operators measured here the entries of one row of L21 or one column of U12 span
 // more than 2^20 even after equilibration, and FP16 pieces (8 exponent bits fewer) then leave
 // the FP64 refinement stalled, so every solve fell back to TF32 pieces.
-// Two passes hi*hi + lo*hi (the B operand, U12, rounded to TF32) when TCU_SPLIT=tf32x2: a
-// third fewer tensor-core passes and no B lo loads, for an update accurate to about 2^-11
-// relative to max|A| max|B| per term; the FP64 refinement then needs more sweeps, and a stall
-// falls back to the three-pass factor.
+// Two passes hi*hi + lo*hi (the B operand, U12, rounded to TF32) unless TCU_SPLIT asks for
+// three TF32 passes (tf32x3) or FP16 pieces (f16): a third fewer tensor-core passes and no B lo
+// loads, for an update accurate to about 2^-11 relative to max|A| max|B| per term. The FP64
+// refinement then takes one sweep more (512 spheres lmax 4: 3 instead of 2, factor 279 instead
+// of 320 ms), and a stall falls back to the three-pass factor.
 bool split_two_pass_default() {
     static const bool on = [] {
         const char* e = getenv("TCU_SPLIT");
-        return e && std::strcmp(e, "tf32x2") == 0;
+        return !(e && (std::strcmp(e, "tf32x3") == 0 || std::strcmp(e, "f16") == 0));
     }();
     return on;
 }

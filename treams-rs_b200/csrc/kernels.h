@@ -197,7 +197,7 @@ struct LuWork {
 };
 // FP16 pieces when the environment asks for them (TCU_SPLIT=f16), else TF32 pieces
 bool split_f16_default();
-// Two-pass TF32 trailing updates when the environment asks for them (TCU_SPLIT=tf32x2)
+// Two-pass TF32 trailing updates unless the environment asks for three passes or FP16 pieces
 bool split_two_pass_default();
 int lu_factor_fp64(double2* A, int n, LuWork& w, cudaStream_t st, long long* launches);
 // The panel's grid barrier with one arrival missing (bar: a zeroed counter); it gives up
