@@ -190,13 +190,14 @@ def iterative_workload(ctx, stream, count: int = 4096, with_cpu: bool = True) ->
     c = t.SphereCluster(w.lmax, w.k0, w.radii, w.eps, w.positions, ctx=ctx)
     B = t.plane_wave_expansion(w.lmax, w.positions, w.kvecs, w.pols, ctx=ctx)[:, 0]
     out = {"workload": f"{count} spheres r 0.2, 20% fill, eps 4+0.05i, k0 1.5, lmax 3 (n={w.n}); GMRES(50) to 1e-8",
-           "unit": "solves/s", "warmup": "one untimed solve of each kind first"}
+           "unit": "solves/s", "warmup": "one untimed solve of each kind first; ms = the faster of two timed solves"}
     kinds = ("none", "block_jacobi", "two_level", "learned")
     for kind in kinds:  # first-use costs (module loading, plan, allocations) stay out of the timing
         c.solve(B, rtol=1e-8, restart=50, max_iterations=600, preconditioner=kind)
-    for kind in kinds:
-        sol, ms, wall = _timed(stream, lambda: c.solve(B, rtol=1e-8, restart=50, max_iterations=600,
-                                                       preconditioner=kind))
+    for kind in kinds:  # the faster of two timed solves: the set-up runs partly on the host cores
+        runs = [_timed(stream, lambda: c.solve(B, rtol=1e-8, restart=50, max_iterations=600, preconditioner=kind))
+                for _ in range(2)]
+        sol, ms, wall = min(runs, key=lambda r: r[1])
         cert = sol.convergence[0]
         out[kind] = {"iterations": cert.iterations, "rel_residual": cert.residual_norm / cert.rhs_norm,
                      "ms": ms, "value": 1e3 / ms}
