@@ -681,7 +681,7 @@ __global__ void __launch_bounds__(1024) tri_inverse_l_kernel(const float2* __res
     }
 }
 size_t tf32_pack_bytes(int n) {
-    size_t kp = 256;
+    size_t kp = 512;  // two 128-column panels per trailing update
     return ((size_t)2 * n * kp + (size_t)n * kp) * 2 * 4 + (size_t)128 * 128 * 8 + 8192;
 }
 
@@ -820,8 +820,11 @@ void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t 
     }
 }
 
-void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches) {
-    int r0 = k0 + w, m = n - r0, ncols = n - r0;
+// A[r0 .. r0+m) x [c0 .. c0+ncols) -= A[r0.., k0 .. k0+w) A[k0 .. k0+w, c0..): the trailing
+// update of panel columns k0 .. k0+w restricted to a block of rows and columns.
+void launch_tf32_update_region(float2* A, int n, int k0, int w, int r0, int m, int c0, int ncols, LuWork& wk,
+                               cudaStream_t st, long long* launches) {
+    if (m <= 0 || ncols <= 0) return;
     int kp = ((2 * w + 31) / 32) * 32;  // whole 64-byte K rows of FP16 pieces (and of TF32)
     size_t need = ((size_t)2 * m * kp + (size_t)ncols * kp) * 2 * 4 + 4096;
     if (!ensure_pack(wk, need, st)) return;
@@ -838,22 +841,27 @@ void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_
         StageScope sc(ST_PACK, st);
         if (f16) {
             pack_l16_kernel<<<(m + 31) / 32, 256, 0, st>>>(A, (size_t)n, r0, k0, m, w, kp, 1.0f, h_ahi, h_alo, sA);
-            pack_u16_kernel<<<(unsigned)(((size_t)ncols * 32 + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w,
+            pack_u16_kernel<<<(unsigned)(((size_t)ncols * 32 + 255) / 256), 256, 0, st>>>(A, (size_t)n, c0, k0, ncols, w,
                                                                                          kp, h_bhi, h_blo, sB);
         } else {
             dim3 g1((m + 31) / 32, (kp / 2 + 31) / 32);
             size_t tot = (size_t)ncols * (kp / 2);
             pack_l_kernel<<<g1, 256, 0, st>>>(A, (size_t)n, r0, k0, m, w, kp, ahi, alo);
-            pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
+            pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, c0, k0, ncols, w, kp, bhi, blo);
         }
         *launches += 2;
     }
     StageScope sc(ST_GEMM, st);
     if (f16)
-        run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, h_ahi, h_alo, h_bhi, h_blo, sA, sB, wk, st, launches);
+        run_gemm(A, n, 2 * r0, c0, 2 * m, ncols, kp, h_ahi, h_alo, h_bhi, h_blo, sA, sB, wk, st, launches);
     else
-        run_gemm(A, n, 2 * r0, r0, 2 * m, ncols, kp, ahi, alo, bhi, blo, nullptr, nullptr, wk, st, launches,
+        run_gemm(A, n, 2 * r0, c0, 2 * m, ncols, kp, ahi, alo, bhi, blo, nullptr, nullptr, wk, st, launches,
                  wk.two_pass);
+}
+
+void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches) {
+    const int r0 = k0 + w;
+    launch_tf32_update_region(A, n, k0, w, r0, n - r0, r0, n - r0, wk, st, launches);
 }
 
 }  // namespace tcu

@@ -815,6 +815,20 @@ __global__ void perm_from_piv_kernel(const int* __restrict__ piv, int* __restric
 }
 
 void launch_tf32_update(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches);
+void launch_tf32_update_region(float2* A, int n, int k0, int w, int r0, int m, int c0, int ncols, LuWork& wk,
+                               cudaStream_t st, long long* launches);
+
+// Mixed path: the trailing update of two consecutive 128-column panels in one K = 256 pass over
+// A22 (TCU_LU_PAIRS=0: one update per panel). Panel a updates only panel b's columns; panel b,
+// once factored, brings its own block rows up to date with panel a, and one update with both
+// panels' L21 and U12 follows, so the trailing block is read and written once per 256 columns.
+static bool lu_pairs_enabled() {
+    static const bool v = [] {
+        const char* e = getenv("TCU_LU_PAIRS");
+        return !(e && atoi(e) == 0);
+    }();
+    return v;
+}
 void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches,
                       bool inverse_done);
 bool launch_tf32_trsm_inverse(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, cudaStream_t side,
@@ -850,6 +864,8 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
     typedef typename Cx<R>::T C;
     lu_init_attributes();
     size_t lda = n;
+    const bool pairs = sizeof(R) == 4 && tensor_cores && lu_pairs_enabled();
+    int pend_k0 = -1, pend_w = 0;  // panel a whose update right of panel b is still pending
     for (int k0 = 0; k0 < n; k0 += NB) {
         int w = std::min(NB, n - k0);
         int rc;
@@ -880,6 +896,8 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
         int cpc = 64;
         size_t smem = (size_t)NB * NB * sizeof(C);
         if (sizeof(R) == 4 && tensor_cores) {
+            if (pend_k0 >= 0)  // panel b: its block rows right of it get panel a's update first
+                launch_tf32_update_region((float2*)A, n, pend_k0, pend_w, k0, w, r0, cols, wk, st, launches);
             launch_tf32_trsm((float2*)A, n, k0, w, wk, st, launches, inverse_done);
         } else {
             StageScope sc(ST_TRSM, st);
@@ -898,7 +916,19 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
             ++*launches;
         } else {
             if (tensor_cores) {
-                launch_tf32_update((float2*)A, n, k0, w, wk, st, launches);
+                if (pend_k0 >= 0) {
+                    // both panels' L21 and U12 (K = 256) over the trailing block at once
+                    launch_tf32_update_region((float2*)A, n, pend_k0, pend_w + w, r0, cols, r0, cols, wk, st,
+                                              launches);
+                    pend_k0 = -1;
+                } else if (pairs && cols > NB) {
+                    // panel a: the next panel's columns now, the rest with panel b
+                    launch_tf32_update_region((float2*)A, n, k0, w, r0, cols, r0, NB, wk, st, launches);
+                    pend_k0 = k0;
+                    pend_w = w;
+                } else {
+                    launch_tf32_update((float2*)A, n, k0, w, wk, st, launches);
+                }
             } else {
                 StageScope sc(ST_GEMM, st);
                 cgemm_simt_kernel<<<grid, 256, 0, st>>>((float2*)A, lda, k0, w, r0, n);
