@@ -864,7 +864,8 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
     typedef typename Cx<R>::T C;
     lu_init_attributes();
     size_t lda = n;
-    const bool pairs = sizeof(R) == 4 && tensor_cores && lu_pairs_enabled();
+    // (the FP16-piece packers hold one 128-column panel, so FP16 pieces keep one update per panel)
+    const bool pairs = sizeof(R) == 4 && tensor_cores && !wk.f16_pieces && lu_pairs_enabled();
     int pend_k0 = -1, pend_w = 0;  // panel a whose update right of panel b is still pending
     for (int k0 = 0; k0 < n; k0 += NB) {
         int w = std::min(NB, n - k0);
