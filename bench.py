@@ -47,17 +47,38 @@ UNIT = "solves/s"
 # m = 11,776 launch of a 256-sphere solve: 2.395 GB measured for 2.219 GB algorithmic.
 # Traffic grows with m^2 like the algorithmic bytes, so the bench scales this ratio to the
 # average launch of the measured workload.
-TF32_TRAFFIC = {"ratio": 2.395 / 2.219,
+TF32_TRAFFIC = {"ratio": 2.275 / 2.219,
                 "note": "dram__bytes_read.sum + dram__bytes_write.sum of tf32_update_kernel per launch: "
-                        "ncu ratio to algorithmic bytes (1.08, m=11776 launch of a 256-sphere solve) "
-                        "x the average algorithmic bytes 16 m^2 of this workload's launches"}
+                        "ncu ratio to algorithmic bytes (1.03, two-pass m=11776 launch of a 256-sphere solve) "
+                        "x the average algorithmic bytes (complex64 C read + write) of this workload's "
+                        "update launches, paired K = 256 updates included"}
 
 
-def update_launch_bytes(n: int, nb: int) -> float:
+def update_launch_shapes(n: int, nb: int, pairs: bool = True) -> list:
+    """(rows, columns) of every trailing-update launch of the mixed LU, in the order the library
+    runs them: with pairs, panel a updates panel b's columns, panel b its own block rows, then
+    one update with both panels."""
+    out, pend = [], False
+    for k0 in range(0, n, nb):
+        w = min(nb, n - k0)
+        cols = n - k0 - w
+        if cols <= 0:
+            break
+        if pend:
+            out += [(w, cols), (cols, cols)]
+            pend = False
+        elif pairs and cols > nb:
+            out.append((cols, nb))
+            pend = True
+        else:
+            out.append((cols, cols))
+    return out
+
+
+def update_launch_bytes(n: int, nb: int, pairs: bool = True) -> float:
     """Average algorithmic bytes (complex64 C read + write) per trailing-update launch."""
-    sizes = [n - k0 - min(nb, n - k0) for k0 in range(0, n, nb)]
-    sizes = [m for m in sizes if m > 0]
-    return sum(16.0 * m * m for m in sizes) / len(sizes)
+    shapes = update_launch_shapes(n, nb, pairs)
+    return sum(16.0 * m * c for m, c in shapes) / len(shapes)
 
 
 # Peaks measured on this pool's B200s (STREAM-style copy, cuBLAS bf16 GEMM as a burst and as a
@@ -589,7 +610,7 @@ def _measure_impl(args, precision, steps, warmup, with_e2e, *, ctx, lib, stream,
         achieved = executed / (gemm[1] / 1e3) / 1e12 if gemm[1] else None
         roof = {"bound": "tensor", "achieved": achieved, "peak": tensor_peak, "unit": "TFLOP/s",
                 "frac": achieved / tensor_peak if achieved else None,
-                "traffic": TF32_TRAFFIC["ratio"] * update_launch_bytes(n, nb),
+                "traffic": TF32_TRAFFIC["ratio"] * update_launch_bytes(n, nb, os.environ.get("TCU_LU_PAIRS") != "0"),
                 "traffic_note": TF32_TRAFFIC["note"],
                 "kernel": f"tf32_update_kernel: split-TF32 tcgen05 trailing update ({passes:.0f} passes executed)",
                 "useful_tflops": flops / (gemm[1] / 1e3) / 1e12 if gemm[1] else None,
