@@ -66,7 +66,7 @@ GemmShape sub_shape(int tsz) {
 
 size_t gemm_smem(const SubOp& o, const GemmShape& s) {
     const size_t tsz = (size_t)(o.order + 1) * (o.order + 1);
-    const size_t rows = (size_t)s.TR * s.RG, cols = (size_t)s.TC * s.CG, npair = (size_t)s.DI * s.KJ;
+    const size_t rows = (size_t)s.TR * s.RG + 1, cols = (size_t)s.TC * s.CG, npair = (size_t)s.DI * s.KJ;
     const size_t chunk = ((size_t)s.KJ * rows + (size_t)s.KJ * cols + npair * (o.order + 1)) * sizeof(cplx) +
                          npair * sizeof(double4);
     const size_t g = (size_t)s.DI * tsz * 2 * o.nsrc * sizeof(cplx);
@@ -80,9 +80,11 @@ __global__ void __launch_bounds__(512, 1)
                       bool singular, cplx* __restrict__ y, int DI, int RG, int CG, int KJ) {
     extern __shared__ __align__(16) unsigned char ag_smem[];
     const int nlm = P.nlm, M = 2 * O.nsrc, order = O.order, ord1 = order + 1, ts = ord1 * ord1;
-    const int ROWS = TR * RG, COLS = TC * CG, npair = DI * KJ;
-    cplx* Zs = reinterpret_cast<cplx*>(ag_smem);                     // KJ x ROWS (source-major)
-    cplx* Xs = Zs + (size_t)KJ * ROWS;                               // KJ x COLS
+    // ZLD = ROWS + 1: the builder's writes of different sources (one column each) fall into
+    // different banks; the product reads consecutive rows of one column
+    const int ROWS = TR * RG, ZLD = ROWS + 1, COLS = TC * CG, npair = DI * KJ;
+    cplx* Zs = reinterpret_cast<cplx*>(ag_smem);                     // KJ x ZLD (source-major)
+    cplx* Xs = Zs + (size_t)KJ * ZLD;                                // KJ x COLS
     cplx* Rs = Xs + (size_t)KJ * COLS;                               // npair x (order + 1)
     double4* Ds = reinterpret_cast<double4*>(Rs + (size_t)npair * ord1);  // direction, state
     cplx* Gs = reinterpret_cast<cplx*>(ag_smem);                     // at the end: DI * ts x M
@@ -98,7 +100,7 @@ __global__ void __launch_bounds__(512, 1)
     for (int u = 0; u < TR; ++u)
 #pragma unroll
         for (int t = 0; t < TC; ++t) acc[u][t] = mk(0.0, 0.0);
-    for (int t = tid; t < KJ * ROWS; t += nthr) Zs[t] = mk(0.0, 0.0);  // padding rows stay zero
+    for (int t = tid; t < KJ * ZLD; t += nthr) Zs[t] = mk(0.0, 0.0);  // padding rows stay zero
 
     for (int j0 = 0; j0 < N; j0 += KJ) {
         __syncthreads();  // the previous chunk's product is done with Zs / Xs
@@ -138,7 +140,7 @@ __global__ void __launch_bounds__(512, 1)
         for (int it = tid; it < npair * ord1; it += nthr) {
             const int p = it / ord1, m = it - p * ord1;
             const int il = p / KJ, jj = p - il * KJ;
-            cplx* Zp = Zs + (size_t)jj * ROWS + (size_t)il * ts;
+            cplx* Zp = Zs + (size_t)jj * ZLD + (size_t)il * ts;
             const double4 D = Ds[p];
             if (D.w == 2.0) {
                 const cplx* rad = Rs + (size_t)p * ord1;
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(512, 1)
             for (int kk = 0; kk < KJ; ++kk) {
                 cplx a[TR], b[TC];
 #pragma unroll
-                for (int u = 0; u < TR; ++u) a[u] = zr[(size_t)kk * ROWS + u * RG];
+                for (int u = 0; u < TR; ++u) a[u] = zr[(size_t)kk * ZLD + u * RG];
 #pragma unroll
                 for (int t = 0; t < TC; ++t) b[t] = xr[(size_t)kk * COLS + t * CG];
 #pragma unroll
