@@ -100,7 +100,8 @@ tcu_status tcu_context_wait_selftest(tcu_context* ctx, double limit_seconds);
 /* Per-stage device timing with CUDA events on the context stream (off by default).
  * Stages: 0 assembly, 1 LU panel, 2 row swaps, 3 triangular block (TRSM), 4 trailing
  * update GEMM, 5 operand packing, 6 triangular solves, 7 matrix-free operator, 8 Mie,
- * 9 lattice sums, 10 batched small LU. Reading synchronises the stream. */
+ * 9 lattice sums, 10 batched small LU, 11 dipole blocks of the two-level preconditioner,
+ * 12 its near-field term. Reading synchronises the stream. */
 tcu_status tcu_context_set_profiling(tcu_context* ctx, int enabled);
 tcu_status tcu_context_stage_time(tcu_context* ctx, int stage, long long* launches, double* total_ms);
 tcu_status tcu_context_reset_stage_times(tcu_context* ctx);

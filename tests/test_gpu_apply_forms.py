@@ -1,8 +1,9 @@
-"""The matrix-free operator (I - T C) x in its two device forms against the oracle.
+"""The matrix-free operator (I - T C) x in its three device forms against the oracle.
 
 lmax 2..5 run the product form (harmonic tables of a chunk of sources times the coefficient
 block, then the plan's term lists once per destination); lmax 1 and >= 6, or TCU_APPLY=terms,
-run the per-pair term sums. 37 spheres make the destination groups and the source chunks of the
+run the per-pair term sums. TCU_APPLY=stored builds the tables of all pairs once and applies
+the FP64 tensor-core product over them (the form GMRES uses for lmax 2..5). 37 spheres make the destination groups and the source chunks of the
 product form ragged; three right-hand sides exercise the column grid. Bound: relative 1e-13 in
 the 2-norm against the oracle's FP64 operator (cluster/iterative.rs apply path).
 """
@@ -20,13 +21,13 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("lmax", [1, 2, 3, 4, 5, 6])
-@pytest.mark.parametrize("form", ["product", "terms"])
+@pytest.mark.parametrize("form", ["product", "terms", "stored"])
 def test_operator_forms_match_the_oracle(ctx, lmax, form, monkeypatch):
     import treams_b200 as t
-    if form == "terms":
-        monkeypatch.setenv("TCU_APPLY", "terms")
-    else:
+    if form == "product":
         monkeypatch.delenv("TCU_APPLY", raising=False)
+    else:
+        monkeypatch.setenv("TCU_APPLY", form)
     w = workloads.learned_cluster(seed=90 + lmax, count=37)
     n = w.radii.size * 2 * lmax * (lmax + 2)
     rng = np.random.default_rng(lmax)
@@ -46,3 +47,32 @@ def test_product_and_term_forms_agree_at_4096_spheres(ctx, monkeypatch):
     monkeypatch.setenv("TCU_APPLY", "terms")
     yt = t.cluster_apply(w.lmax, w.k0, w.radii, w.eps, w.positions, x, ctx=ctx)
     assert _rel(yp, yt) <= 1e-13
+
+
+def test_stored_and_product_forms_agree_at_4096_spheres(ctx, monkeypatch):
+    # the stored tables of the 4096-sphere workload take 14 GB of HBM
+    import treams_b200 as t
+    w = workloads.learned_cluster()
+    x = np.random.default_rng(12).standard_normal((w.n, 2)) + 0j
+    monkeypatch.delenv("TCU_APPLY", raising=False)
+    yp = t.cluster_apply(w.lmax, w.k0, w.radii, w.eps, w.positions, x, ctx=ctx)
+    monkeypatch.setenv("TCU_APPLY", "stored")
+    ys = t.cluster_apply(w.lmax, w.k0, w.radii, w.eps, w.positions, x, ctx=ctx)
+    assert _rel(ys, yp) <= 1e-13
+
+
+@pytest.mark.parametrize("lmax", [2, 3, 4, 5])
+def test_gmres_with_stored_tables_matches_the_on_the_fly_product(ctx, lmax, monkeypatch):
+    # GMRES builds the tables once per solve (default) or applies the product form every time
+    import treams_b200 as t
+    w = workloads.learned_cluster(seed=120 + lmax, count=150)
+    c = t.SphereCluster(lmax, w.k0, w.radii, w.eps, w.positions, ctx=ctx)
+    pw = t.plane_wave_expansion(lmax, w.positions, w.kvecs, w.pols, ctx=ctx)[:, 0]
+    rng = np.random.default_rng(lmax)
+    B = np.column_stack([pw, rng.standard_normal(pw.size) + 1j * rng.standard_normal(pw.size)])
+    monkeypatch.delenv("TCU_APPLY", raising=False)
+    s1 = c.solve(B, rtol=1e-12, restart=40, max_iterations=400)
+    monkeypatch.setenv("TCU_APPLY", "fly")
+    s2 = c.solve(B, rtol=1e-12, restart=40, max_iterations=400)
+    assert [q.iterations for q in s1.convergence] == [q.iterations for q in s2.convergence]
+    assert _rel(s1.value, s2.value) <= 1e-11

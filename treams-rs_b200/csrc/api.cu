@@ -36,10 +36,12 @@ tcu_status fail(tcu_status st, const std::string& msg) {
 // kept for reuse (stream-ordered on the context's stream), so repeated factorizations do
 // not pay cudaMalloc/cudaFree of multi-GB matrices. Pooled blocks are released on
 // allocation failure and when the context is destroyed.
-struct DevicePool {
+struct DevicePool : tcu::DeviceAllocator {
     std::multimap<size_t, void*> free_;
     std::map<void*, size_t> sizes_;
-    cudaError_t alloc(void** p, size_t bytes) {
+    cudaError_t alloc(void** p, size_t bytes) override { return take(p, bytes); }
+    void release(void* p) override { free(p); }
+    cudaError_t take(void** p, size_t bytes) {
         bytes = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
         auto it = free_.lower_bound(bytes);
         if (it != free_.end() && it->first <= 2 * bytes + ((size_t)1 << 20)) {
@@ -81,6 +83,7 @@ struct DevPlanStore {
 
 namespace tcu {
 thread_local Profiler* g_prof = nullptr;
+thread_local DeviceAllocator* g_call_pool = nullptr;
 void set_error_message(const char* msg) { g_last_error = msg; }
 }
 
@@ -696,9 +699,24 @@ int batch_workers() {
     return std::max(1, std::min(8, v));
 }
 
+// The stored-table operator for the applications of GMRES: lmax 2..5 in product form, unless
+// TCU_APPLY is "fly" or "terms", and only while the tables take at most half of the free device
+// memory (and at most 64 GB).
+bool use_stored_tables(const DevPlan& P, int N) {
+    if (!apply_gemm_supported(P) || !stored_tables_enabled()) return false;
+    const size_t bytes = stored_tables_bytes(P, N, STORED_FULL);
+    if (bytes == 0 || bytes > ((size_t)64 << 30)) return false;
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return bytes <= fr / 2;
+}
+
 // The dipole (lmax 1) system of a cluster: factored (complex64 from 2048 modes on, else FP64) up
 // to 6144 dipole modes; above, no factor is made (out stays empty) and the two-level
-// preconditioner solves the dipole system by an inner GMRES on its stored dipole columns.
+// preconditioner solves the dipole system by an inner GMRES on its matrix-free dipole block.
 constexpr size_t COARSE_LU_MAX = 6144;
 tcu_status make_coarse(tcu_context* ctx, double k0, size_t N, const double* radii, const double* eps,
                        const double* pos, std::unique_ptr<CoarseSolve>* out, bool factor_always = false) {
@@ -1129,7 +1147,18 @@ tcu_status tcu_cluster_apply(tcu_context* ctx, int lmax, double k0, size_t N, co
     launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
     ++ctx->launches;
     if ((s = read_status(ctx, "Mie coefficients"))) return s;
-    apply_op(ctx, P, (int)N, k0, pos, T, dx, n, p, nullptr, 1.0, -1.0, true, dy);
+    const char* form = getenv("TCU_APPLY");  // "stored": the tables once, then the stored-table product
+    if (form && strcmp(form, "stored") == 0 && apply_gemm_supported(*P)) {
+        DevBuf zbuf(ctx), xfbuf(ctx);
+        CK(zbuf.alloc(stored_tables_bytes(*P, (int)N, STORED_FULL)), "stored tables");
+        CK(xfbuf.alloc(stored_inputs_bytes(*P, (int)N, STORED_FULL, p)), "packed inputs");
+        build_stored_tables(*P, (int)N, k0, pos, STORED_FULL, (cplx*)zbuf.p, ctx->stream);
+        launch_apply_stored(*P, (int)N, STORED_FULL, (const cplx*)zbuf.p, T, dx, n, p, nullptr, 1.0, -1.0, dy, (cplx*)xfbuf.p,
+                            ctx->stream);
+        ctx->launches += 3;
+    } else {
+        apply_op(ctx, P, (int)N, k0, pos, T, dx, n, p, nullptr, 1.0, -1.0, true, dy);
+    }
     CK(cudaMemcpyAsync(y, dy, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
     return sync_status(ctx, "cluster apply");
 }
@@ -1261,6 +1290,7 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
     if (preconditioner < 0 || preconditioner > 3) return fail(TCU_INVALID_INPUT, "unknown preconditioner");
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     ProfGuard pg(ctx);
+    PoolScope ps(&ctx->pool);  // the preconditioner's buffers come from the pool, freed before return
     CK(cudaSetDevice(ctx->device), "device");
     tcu_status s = validate_spheres(lmax, k0, N, radii, eps, positions);
     if (s) return s;
@@ -1309,13 +1339,31 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
         if (s == TCU_OUT_OF_MEMORY) return fail(s, "two-level preconditioner: out of device memory");
         if (s) return fail(s, "two-level preconditioner set-up failed");
     }
+    // the harmonic tables of all pairs, built once for the applications of every column
+    DevBuf zbuf(ctx), xfbuf(ctx);
+    const cplx* Zst = nullptr;
+    if (use_stored_tables(*P, (int)N)) {
+        if (zbuf.alloc(stored_tables_bytes(*P, (int)N, STORED_FULL)) == cudaSuccess &&
+            xfbuf.alloc(stored_inputs_bytes(*P, (int)N, STORED_FULL, 1)) == cudaSuccess) {
+            build_stored_tables(*P, (int)N, k0, pos, STORED_FULL, (cplx*)zbuf.p, ctx->stream);
+            ++ctx->launches;
+            Zst = (const cplx*)zbuf.p;
+        } else {
+            cudaGetLastError();  // no room: the on-the-fly product
+        }
+    }
     tcu_status worst = TCU_OK;
     std::string msg;
     for (int c = 0; c < p; ++c) {
         tcu_certificate cert{};
         auto op = [&](const cplx* in, cplx* out) {
-            launch_apply(*P, (int)N, k0, pos, T, in, n, 1, nullptr, 1.0, -1.0, true, out, ctx->stream);
-            ++ctx->launches;
+            if (Zst) {
+                launch_apply_stored(*P, (int)N, STORED_FULL, Zst, T, in, n, 1, nullptr, 1.0, -1.0, out, (cplx*)xfbuf.p, ctx->stream);
+                ctx->launches += 2;
+            } else {
+                launch_apply(*P, (int)N, k0, pos, T, in, n, 1, nullptr, 1.0, -1.0, true, out, ctx->stream);
+                ++ctx->launches;
+            }
         };
         s = gmres_device(ctx, op, tb + c * n, n, opt, pre.get(), x + c * n, wk, &cert);
         if (certificates) certificates[c] = cert;

@@ -4,9 +4,9 @@
 //
 // Right preconditioner, applied to a vector v:
 //   1. coarse correction on the dipole modes (l = 1, the first 6 modes of every sphere):
-//      z_c = A_cc^-1 v_c with A_cc = I - T_1 C_11 factored once by the dense LU of this library,
-//      and the exact residual r1 = v - A[:, c] z_c through the stored dipole columns of A
-//      (complex64, n x 6N);
+//      z_c = A_cc^-1 v_c with A_cc = I - T_1 C_11 (factored by the dense LU of this library up
+//      to 6144 dipole modes, else solved by an inner GMRES), and the exact residual
+//      r1 = v - A P z_c through the dipole-source block of the operator (no dense columns);
 //   2. near field: y = r1 + T sum_{j in nb(i)} (Theta_ij o C_ij) r1_j over the pairs closer
 //      than the reach, where Theta_ij scales every (destination degree, source degree)
 //      sub-block of the translation block C_ij by a complex number;
@@ -392,14 +392,37 @@ std::vector<int> reverse_edges(const Graph& g) {
 
 struct DevArray {
     void* p = nullptr;
-    ~DevArray() {
-        if (p) cudaFree(p);
-    }
+    DeviceAllocator* owner = nullptr;
+    ~DevArray() { call_free(p, owner); }
     template <typename T>
     T* as() const {
         return (T*)p;
     }
-    bool alloc(size_t bytes) { return cudaMalloc(&p, std::max<size_t>(bytes, 16)) == cudaSuccess; }
+    bool alloc(size_t bytes) {
+        if (call_malloc(&p, std::max<size_t>(bytes, 16), &owner) == cudaSuccess) return true;
+        p = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+};
+
+// Stored tables of one dipole block (launch_apply_stored), built when they take at most half of
+// the free device memory; otherwise the block stays matrix-free (launch_apply_dipole).
+struct StoredDipole {
+    DevArray Z, Xf;
+    bool ready = false;
+    void build(const DevPlan& P, int N, double k, const double* d_pos, int kind, cudaStream_t st) {
+        const size_t zb = stored_tables_bytes(P, N, kind), xb = stored_inputs_bytes(P, N, kind, 1);
+        if (zb == 0 || !stored_tables_enabled()) return;
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+        if (zb + xb > fr / 2 || !Z.alloc(zb) || !Xf.alloc(xb)) return;
+        build_stored_tables(P, N, k, d_pos, kind, Z.as<cplx>(), st);
+        ready = true;
+    }
 };
 
 // Everything the network and the near field need on the device for one cluster.
@@ -457,6 +480,7 @@ struct GraphData {
     // out = zadd + T sum_e B_e x (one column)
     void near_apply(const cplx* T, const cplx* x, const cplx* zadd, cplx* out, cudaStream_t st, long long* launches,
                     const uint8_t* noskip) {
+        StageScope sc(ST_NEAR, st);
         const int Q = std::min(16, 256 / nlm);
         nf_apply_kernel<<<N, 256, (size_t)Q * nlm * 2 * sizeof(cplx), st>>>(L, nlm, ptr.as<int>(), nbr.as<int>(),
                                                                            noskip, B.as<cplx>(), T, x, zadd, out, Q);
@@ -464,10 +488,11 @@ struct GraphData {
     }
 };
 
-// The coarse dipole system, matrix-free. Its operator A_cc = R (I - T C) P (P puts a 6N dipole
-// vector on the dipole modes, R takes them) and the columns A P of the correction are the
-// dipole blocks of the operator in product form (launch_apply_dipole): no dense dipole
-// columns are assembled or stored.
+// The coarse dipole system. Its operator A_cc = R (I - T C) P (P puts a 6N dipole vector on the
+// dipole modes, R takes them) and the columns A P of the correction are the dipole blocks of
+// the operator: products over their stored harmonic tables when those fit, else in product
+// form with the tables rebuilt per application (launch_apply_dipole). No dense dipole columns
+// are assembled.
 // Inexact coarse solve for large dipole systems: restarted GMRES on A_cc (FP64 vectors and
 // Krylov basis, Gram-Schmidt twice with fixed-order dot products, Givens rotations on the
 // host) to a relative residual of rtol or max_it iterations, from x = 0. The outer GMRES is
@@ -482,6 +507,7 @@ class IterativeCoarse : public CoarseSolve {
     const double* pos = nullptr;
     const cplx* T = nullptr;
     DevArray V, w, h, small, dpart;
+    const StoredDipole* stored = nullptr;  // tables of A_cc, when built
     long long* launches = nullptr;
     bool build(const DevPlan& P, int N_, double k, const double* d_pos, const cplx* d_T, int restart,
                int max_iterations, double tol) {
@@ -500,8 +526,14 @@ class IterativeCoarse : public CoarseSolve {
     }
     // y = A_cc x = x - R T C P x
     void matvec(const cplx* x, cplx* y, cudaStream_t st) {
-        launch_apply_dipole(*plan, N, k0, pos, T, x, true, nullptr, 1.0, -1.0, y, st);
-        if (launches) ++*launches;
+        if (stored && stored->ready) {
+            launch_apply_stored(*plan, N, STORED_DIPOLE_BLOCK, stored->Z.as<cplx>(), T, x, 0, 1, nullptr, 1.0, -1.0, y,
+                                stored->Xf.as<cplx>(), st);
+            if (launches) *launches += 2;
+        } else {
+            launch_apply_dipole(*plan, N, k0, pos, T, x, true, nullptr, 1.0, -1.0, y, st);
+            if (launches) ++*launches;
+        }
     }
     tcu_status solve(double2* v, cudaStream_t st) override {
         // r0 = v (x0 = 0); V0 = v / |v|
@@ -579,9 +611,10 @@ struct Coarse {
     const double* pos = nullptr;
     const cplx* T = nullptr;
     DevArray vc;
+    StoredDipole zsrc, zcc;  // tables of the correction's dipole sources and of A_cc
     std::unique_ptr<CoarseSolve> solver;
     bool build(const DevPlan& P, int N_, double k, const double* d_pos, const cplx* d_T, std::unique_ptr<CoarseSolve> s,
-               long long* launches) {
+               cudaStream_t st, long long* launches) {
         plan = &P;
         N = N_;
         M = 2 * P.nlm;
@@ -592,9 +625,12 @@ struct Coarse {
         T = d_T;
         solver = std::move(s);
         if (!vc.alloc((size_t)nc * sizeof(cplx))) return false;
+        zsrc.build(P, N, k, d_pos, STORED_DIPOLE_SOURCES, st);
         if (!solver) {  // no factor given: an inexact GMRES on the dipole block
+            zcc.build(P, N, k, d_pos, STORED_DIPOLE_BLOCK, st);
             auto it = std::make_unique<IterativeCoarse>();
             it->launches = launches;
+            it->stored = &zcc;
             // relative tolerance of the inner solve: 3e-2 (the 4096-sphere workload measured 300,
             // 291, 256 and 269 ms at 1e-3, 1e-2, 3e-2 and 1e-1), or TCU_COARSE_RTOL
             const char* e = getenv("TCU_COARSE_RTOL");
@@ -609,8 +645,14 @@ struct Coarse {
         coarse_gather_kernel<<<blocks_for(nc, 256), 256, 0, st>>>(N, M, v, vc.as<cplx>());
         tcu_status s = solver->solve(vc.as<cplx>(), st);
         if (s) return s;
-        launch_apply_dipole(*plan, N, k0, pos, T, vc.as<cplx>(), false, v, -1.0, 1.0, r1, st);
-        if (launches) *launches += 2;
+        if (zsrc.ready) {
+            launch_apply_stored(*plan, N, STORED_DIPOLE_SOURCES, zsrc.Z.as<cplx>(), T, vc.as<cplx>(), 0, 1, v, -1.0, 1.0,
+                                r1, zsrc.Xf.as<cplx>(), st);
+            if (launches) *launches += 3;
+        } else {
+            launch_apply_dipole(*plan, N, k0, pos, T, vc.as<cplx>(), false, v, -1.0, 1.0, r1, st);
+            if (launches) *launches += 2;
+        }
         return TCU_OK;
     }
     void add_coarse(cplx* out, cudaStream_t st, long long* launches) {
@@ -655,7 +697,7 @@ tcu_status make_two_level(cudaStream_t st, bool learned, const DevPlan& P, int L
     for (int i = 0; i < N; ++i) rmax = std::max(rmax, h_radii[i]);
     const double cutoff = 2.0 * (reach > 0.0 ? reach : LEARNED_REACH) * rmax;
     if (!pre->graph.build(st, P, L, N, k0, d_pos, h_pos, h_radii, h_eps, cutoff, launches)) return TCU_OUT_OF_MEMORY;
-    if (!pre->coarse.build(P, N, k0, d_pos, d_T, std::move(coarse), launches)) return TCU_OUT_OF_MEMORY;
+    if (!pre->coarse.build(P, N, k0, d_pos, d_T, std::move(coarse), st, launches)) return TCU_OUT_OF_MEMORY;
     if (!pre->r1.alloc(pre->graph.n * sizeof(cplx)) || !pre->noskip.alloc(std::max<size_t>(pre->graph.nnz, 1)))
         return TCU_OUT_OF_MEMORY;
     cudaMemsetAsync(pre->noskip.p, 0, std::max<size_t>(pre->graph.nnz, 1), st);
@@ -700,7 +742,7 @@ tcu_status LearnedProblem::build(cudaStream_t st, const DevPlan& P, int L_, int 
     for (int i = 0; i < N; ++i) rmax = std::max(rmax, h_radii[i]);
     const double cutoff = 2.0 * (reach > 0.0 ? reach : LEARNED_REACH) * rmax;
     if (!m.graph.build(st, P, L, N, k0, d_pos, h_pos, h_radii, h_eps, cutoff, launches)) return TCU_OUT_OF_MEMORY;
-    if (!m.coarse.build(P, N, k0, d_pos, d_T, std::move(cs), launches)) return TCU_OUT_OF_MEMORY;
+    if (!m.coarse.build(P, N, k0, d_pos, d_T, std::move(cs), st, launches)) return TCU_OUT_OF_MEMORY;
     n = m.graph.n;
     m.p = nprobe;
     const size_t vb = n * (size_t)nprobe * sizeof(cplx), nnz = m.graph.nnz;

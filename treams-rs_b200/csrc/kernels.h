@@ -40,7 +40,7 @@ inline void once_per_device(PerDeviceOnce& o, F&& f) {
 // context's profiler as the calling thread's current one for the duration of a call; the
 // launch sites bracket their kernels with a StageScope.
 enum Stage { ST_ASSEMBLE = 0, ST_PANEL, ST_SWAP, ST_TRSM, ST_GEMM, ST_PACK, ST_SOLVE, ST_APPLY, ST_MIE, ST_LATTICE,
-             ST_SMALL_LU, ST_COUNT };
+             ST_SMALL_LU, ST_COARSE, ST_NEAR, ST_COUNT };
 struct Profiler {
     bool on = false;
     struct Rec {
@@ -79,6 +79,34 @@ struct Profiler {
     }
 };
 extern thread_local Profiler* g_prof;
+
+// Device memory of objects that live within one API call (preconditioners, their graphs and
+// coarse solvers): the context's caching pool while the call has installed it (PoolScope),
+// else cudaMalloc / cudaFree. Each allocation remembers where it came from.
+struct DeviceAllocator {
+    virtual cudaError_t alloc(void** p, size_t bytes) = 0;
+    virtual void release(void* p) = 0;
+
+   protected:
+    ~DeviceAllocator() = default;
+};
+extern thread_local DeviceAllocator* g_call_pool;
+struct PoolScope {
+    DeviceAllocator* prev;
+    explicit PoolScope(DeviceAllocator* a) : prev(g_call_pool) { g_call_pool = a; }
+    ~PoolScope() { g_call_pool = prev; }
+};
+inline cudaError_t call_malloc(void** p, size_t bytes, DeviceAllocator** owner) {
+    *owner = g_call_pool;
+    return *owner ? (*owner)->alloc(p, bytes) : cudaMalloc(p, bytes);
+}
+inline void call_free(void* p, DeviceAllocator* owner) {
+    if (!p) return;
+    if (owner)
+        owner->release(p);
+    else
+        cudaFree(p);
+}
 struct StageScope {
     Profiler* p;
     int stage;
@@ -115,6 +143,20 @@ void apply_gemm_init_attributes();
 // dipole_rows, on the dipole modes only (y: 6N). P z is z on the dipole modes, zero elsewhere.
 void launch_apply_dipole(const DevPlan& P, int N, double k, const double* pos, const cplx* T, const cplx* z,
                          bool dipole_rows, const cplx* zadd, double alpha, double beta, cplx* y, cudaStream_t st);
+// Stored-table form of the singular operator and of its two dipole blocks (for repeated
+// applications): the harmonic tables of all ordered pairs built once into Z
+// (stored_tables_bytes), then every application is an FP64 tensor-core product over Z plus the
+// term lists. kind: STORED_FULL (lmax 2..5) is launch_apply's operator; STORED_DIPOLE_SOURCES and
+// STORED_DIPOLE_BLOCK are launch_apply_dipole with dipole_rows false and true (input ldin 6).
+// Xf: scratch of stored_inputs_bytes for the packed inputs. Sizes are 0 where a kind does not
+// apply.
+enum StoredKind { STORED_FULL = 0, STORED_DIPOLE_SOURCES = 1, STORED_DIPOLE_BLOCK = 2 };
+bool stored_tables_enabled();  // false when TCU_APPLY is "fly" or "terms" (read at every call)
+size_t stored_tables_bytes(const DevPlan& P, int N, int kind);
+size_t stored_inputs_bytes(const DevPlan& P, int N, int kind, int ncol);
+void build_stored_tables(const DevPlan& P, int N, double k, const double* pos, int kind, cplx* Z, cudaStream_t st);
+void launch_apply_stored(const DevPlan& P, int N, int kind, const cplx* Z, const cplx* T, const cplx* x, size_t ldx,
+                         int ncol, const cplx* zadd, double alpha, double beta, cplx* y, cplx* Xf, cudaStream_t st);
 void launch_block(const DevPlan& P, double k, const double* d, bool singular, bool helicity, cplx* out,
                   cudaStream_t st);
 void launch_mie(int L, double k0, int N, const double* radii, const cplx* eps, cplx* T, int* status, cudaStream_t st);

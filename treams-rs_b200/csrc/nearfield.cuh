@@ -211,8 +211,8 @@ Graph build_graph(int N, const double* pos, double reach, int per_block) {
 }
 
 template <typename T>
-cudaError_t upload(T** d, const std::vector<T>& h, cudaStream_t st) {
-    cudaError_t e = cudaMalloc((void**)d, std::max<size_t>(h.size(), 1) * sizeof(T));
+cudaError_t upload(T** d, const std::vector<T>& h, cudaStream_t st, DeviceAllocator** owner) {
+    cudaError_t e = call_malloc((void**)d, std::max<size_t>(h.size(), 1) * sizeof(T), owner);
     if (e != cudaSuccess) return e;
     if (!h.empty()) e = cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
     return e;

@@ -113,10 +113,12 @@ class BlockJacobiPre : public Preconditioner {
     int M = 0, nblocks = 0;
     int *d_bptr = nullptr, *d_bmem = nullptr;
     cplx* d_dinv = nullptr;
+    DeviceAllocator *o_bptr = nullptr, *o_bmem = nullptr, *o_dinv = nullptr;
     long long* launches = nullptr;
     ~BlockJacobiPre() override {
-        for (void* p : {(void*)d_bptr, (void*)d_bmem, (void*)d_dinv})
-            if (p) cudaFree(p);
+        call_free(d_bptr, o_bptr);
+        call_free(d_bmem, o_bmem);
+        call_free(d_dinv, o_dinv);
     }
     void apply(const cplx* in, cplx* out, cudaStream_t st) override {
         blk_apply_kernel<<<nblocks, 128, 0, st>>>(M, d_bptr, d_bmem, d_dinv, in, out);
@@ -155,11 +157,12 @@ tcu_status make_block_jacobi(cudaStream_t st, const DevPlan& P, int N, double k0
     Graph g = build_graph(N, h_pos, 6.0 * rmax, per_block);
     p.nblocks = (int)g.bptr.size() - 1;
     auto ck = [](cudaError_t e) { return e == cudaSuccess; };
-    if (!ck(upload(&p.d_bptr, g.bptr, st)) || !ck(upload(&p.d_bmem, g.bmem, st)) ||
-        !ck(cudaMalloc((void**)&p.d_dinv, (size_t)p.nblocks * PB_MAXMODES * PB_MAXMODES * sizeof(cplx))))
+    if (!ck(upload(&p.d_bptr, g.bptr, st, &p.o_bptr)) || !ck(upload(&p.d_bmem, g.bmem, st, &p.o_bmem)) ||
+        !ck(call_malloc((void**)&p.d_dinv, (size_t)p.nblocks * PB_MAXMODES * PB_MAXMODES * sizeof(cplx), &p.o_dinv)))
         return TCU_OUT_OF_MEMORY;
     int* d_status = nullptr;
-    if (!ck(cudaMalloc((void**)&d_status, sizeof(int)))) return TCU_OUT_OF_MEMORY;
+    DeviceAllocator* o_status = nullptr;
+    if (!ck(call_malloc((void**)&d_status, sizeof(int), &o_status))) return TCU_OUT_OF_MEMORY;
     cudaMemsetAsync(d_status, 0, sizeof(int), st);
     size_t smem = (size_t)PB_MAXMODES * PB_MAXMODES * 16 + (size_t)PB_MAXMODES * PB_PANEL * 16;
     static PerDeviceOnce attr;
@@ -171,7 +174,7 @@ tcu_status make_block_jacobi(cudaStream_t st, const DevPlan& P, int N, double k0
     int hst = 0;
     cudaMemcpyAsync(&hst, d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaError_t e = cudaStreamSynchronize(st);
-    cudaFree(d_status);
+    call_free(d_status, o_status);
     if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return TCU_DEVICE_ERROR;
     if (hst == 5) return TCU_SINGULAR;
     *out = std::move(pre);

@@ -137,7 +137,8 @@ class Context:
     def launches(self) -> int:
         return lib().tcu_context_launches(self.handle)
 
-    STAGES = ("assemble", "panel", "swap", "trsm", "gemm", "pack", "solve", "apply", "mie", "lattice", "small_lu")
+    STAGES = ("assemble", "panel", "swap", "trsm", "gemm", "pack", "solve", "apply", "mie", "lattice", "small_lu",
+              "coarse", "near")
 
     def set_refinement(self, target: float = 1e-13, fallback_above: float = 1e-12) -> None:
         """Refinement stop tolerance and the residual above which mixed solves finish in FP64."""
