@@ -201,9 +201,10 @@ def _timed(stream, fn):
     return out, e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3
 
 
-def iterative_workload(ctx, stream, count: int = 4096, with_cpu: bool = True) -> dict:
+def iterative_workload(ctx, stream, count: int = 4096, with_cpu: bool = True, c128_peak=None) -> dict:
     """The 4096-sphere lmax-3 matrix-free cluster (n = 122,880): GMRES(50) to 1e-8 without,
-    with block-Jacobi and with the learned preconditioner (set-up included)."""
+    with block-Jacobi and with the learned preconditioner (set-up included). GMRES applies the
+    operator from the pair tables stored once per solve (14 GB here)."""
     import treams_b200 as t
     from treams_b200 import workloads
 
@@ -227,7 +228,34 @@ def iterative_workload(ctx, stream, count: int = 4096, with_cpu: bool = True) ->
     out["iteration_ratio_two_level_over_learned"] = out["two_level"]["iterations"] / out["learned"]["iterations"]
     out["note"] = ("two_level: coarse dipole solve (inner GMRES on the 6N dipole system above 6144 dipole modes, "
                    "else its dense LU) + near-field Neumann term; learned: the same with the graph network's "
-                   "near-field weights (Theta = 1 while no trained weights beat it); set-up included in ms")
+                   "near-field weights (Theta = 1 while no trained weights beat it); set-up included in ms; "
+                   "the operator and the two dipole blocks from harmonic tables stored once per solve")
+    # the stored-table application: device stage time of (tables + 1 application) and of
+    # (tables + 3 applications) through the ABI with TCU_APPLY=stored
+    stage = {}
+    os.environ["TCU_APPLY"] = "stored"
+    try:
+        for nc in (1, 3):
+            xs = np.random.default_rng(nc).standard_normal((w.n, nc)) + 0j
+            c.apply(xs)
+            ctx.reset_stage_times()
+            ctx.set_profiling(True)
+            c.apply(xs)
+            ctx.set_profiling(False)
+            stage[nc] = ctx.stage_times().get("apply", (0, 0.0))[1]
+    finally:
+        os.environ.pop("TCU_APPLY", None)
+    per = (stage[3] - stage[1]) / 2.0
+    pairs = w.radii.size * (w.radii.size - 1)
+    flops = 8.0 * pairs * (2 * w.lmax + 1) ** 2 * 2 * w.lmax * (w.lmax + 2)
+    tf = flops / (per / 1e3) / 1e12 if per > 0 else None
+    out["stored_operator"] = {
+        "ms_per_application": per, "table_build_ms": stage[1] - per,
+        "table_bytes": pairs * (2 * w.lmax + 1) ** 2 * 16,
+        "roofline": {"bound": "fp64 tensor (DMMA)", "achieved": tf, "peak": c128_peak, "unit": "TFLOP/s",
+                     "frac": tf / c128_peak if tf and c128_peak else None,
+                     "note": "8 (2L+1)^2 2L(L+2) useful flops per ordered pair (complex products of the table "
+                             "matrix with the coefficients); peak: measured cuBLAS complex128 GEMM rate (of measured)"}}
     # one matrix-free operator application: device time and the CPU restatement on the host cores
     x = np.ones((w.n, 1), complex)
     _, ms_apply, _ = _timed(stream, lambda: c.apply(x))
@@ -477,7 +505,8 @@ def main() -> None:
     extras = {}
     if args.extras:
         fp64_peak = yard["cublas_fp64_gemm_tflops"] if yard else None
-        extras["iterative"] = iterative_workload(ctx, stream, args.iterative_spheres, with_cpu)
+        extras["iterative"] = iterative_workload(ctx, stream, args.iterative_spheres, with_cpu,
+                                                 yard["cublas_c128_gemm_tflops"] if yard else None)
         extras["periodic"] = periodic_workload(ctx, stream, args.periodic_kpars, with_cpu, fp64_peak)
         extras["batch"] = batch_workload(ctx, stream, args.batch_clusters, with_cpu)
     if yard is not None:
