@@ -231,7 +231,12 @@ tcu_status tcu_cluster_apply_noalloc(void* stream, int lmax, double k0, size_t N
                                      const double* eps, const double* positions, int p, const double* x, double* y);
 /* Restarted GMRES on (I - T C) X = T B (cluster/iterative.rs:264-284, linalg/gmres.rs:119).
  * The preconditioner, if any, is applied on the right; certificates report the true
- * unpreconditioned residual. */
+ * unpreconditioned residual. For lmax 2..5 the harmonic tables of all N (N - 1) sphere pairs
+ * are built once per call and kept in device memory for the operator applications
+ * (N^2 (2 lmax + 1)^2 16 bytes: 14 GB at 4096 spheres and lmax 3), and the two-level
+ * preconditioners store those of their dipole blocks too; each set only while it takes at most
+ * half of the free device memory, else the tables are rebuilt per application (the results
+ * agree to rounding). The environment variable TCU_APPLY=fly turns the stored tables off. */
 tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0, size_t N, const double* radii,
                                const double* eps, const double* positions, const double* B, int p,
                                const tcu_gmres_options* options, int preconditioner, double* X,
