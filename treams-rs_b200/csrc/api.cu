@@ -127,6 +127,7 @@ struct tcu_factor {
     double2* d_inv = nullptr;  // inverses of the diagonal blocks of L and U
     LuWork wk;
     double* d_scale = nullptr;       // row scales (n) then column scales (n) when equilibrated
+    cplx* d_Z = nullptr;             // stored pair tables of the refinement's FP64 residual (lmax 2..5)
     bool scaled = false;
     tcu_factor* fallback = nullptr;  // FP64 factor of a mixed factor whose refinement stalled
     unsigned sweep_epoch = 0;        // epochs of the persistent triangular sweeps
@@ -344,7 +345,7 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
     f->wk.panel_rows = ctx->panel_rows;
     auto cleanup = [&]() {
         for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
-                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack, (void*)f->d_scale})
+                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack, (void*)f->d_scale, (void*)f->d_Z})
             ctx->pool.free(q);
     };
     tcu_status e = TCU_OK;
@@ -379,6 +380,18 @@ tcu_status factor_impl(tcu_context* ctx, int L, double k0, size_t N, const doubl
         if ((e = read_status(ctx, "Mie coefficients"))) break;
         launch_assemble(*P, (int)N, k0, f->d_pos, f->d_T, f->d_A, n, precision == TCU_MIXED, ctx->stream);
         ++ctx->launches;
+        if (apply_gemm_supported(*P) && stored_tables_enabled()) {
+            // the refinement's residuals apply the FP64 operator from stored pair tables (at most a
+            // fifth of the matrix's bytes); without room they rebuild the tables per application
+            void* z = nullptr;
+            if (ctx->pool.alloc(&z, stored_tables_bytes(*P, (int)N, STORED_FULL)) == cudaSuccess) {
+                f->d_Z = (cplx*)z;
+                build_stored_tables(*P, (int)N, k0, f->d_pos, STORED_FULL, f->d_Z, ctx->stream);
+                ++ctx->launches;
+            } else {
+                cudaGetLastError();
+            }
+        }
         {
             // equilibrate when an entry exceeds 10 (then the unit diagonal no longer bounds the
             // spread; linalg/mod.rs:137-228)
@@ -458,12 +471,14 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
                     "require finite channel-by-illumination columns matching the factorization");
     DevBuf bufs(ctx);
     size_t per = n * p;
-    CK(bufs.alloc(6 * per * sizeof(cplx)), "solve buffers");
+    const size_t xf_bytes = f->d_Z ? stored_inputs_bytes(*P, f->N, STORED_FULL, p) : 0;
+    CK(bufs.alloc(6 * per * sizeof(cplx) + xf_bytes), "solve buffers");
     cplx* b = (cplx*)bufs.p;
     cplx* tb = b + per;
     cplx* x = tb + per;
     cplx* r = x + per;
     cplx* tmp = r + per;  // 2 per
+    cplx* xf = tmp + 2 * per;  // packed inputs of the stored-table residual
     CK(cudaMemcpyAsync(b, B, per * 16, device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, ctx->stream),
        "copy rhs");
     launch_apply_t(f->L, f->N, f->d_T, b, p, tb, ctx->stream);
@@ -489,7 +504,12 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
     int sweep_status = 0;
     auto residual = [&]() -> tcu_status {
         // r = T b - (x - T C x)
-        apply_op(ctx, P, f->N, f->k0, f->d_pos, f->d_T, x, n, p, tb, -1.0, 1.0, true, r);
+        if (f->d_Z) {
+            launch_apply_stored(*P, f->N, STORED_FULL, f->d_Z, f->d_T, x, n, p, tb, -1.0, 1.0, r, xf, ctx->stream);
+            ctx->launches += 2;
+        } else {
+            apply_op(ctx, P, f->N, f->k0, f->d_pos, f->d_T, x, n, p, tb, -1.0, 1.0, true, r);
+        }
         vec_norms(r, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
         ctx->launches += 2;
         CK(cudaMemcpyAsync(rn.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "norms");
@@ -1083,7 +1103,7 @@ tcu_status tcu_factor_destroy(tcu_factor* f) {
         std::lock_guard<std::recursive_mutex> lock(f->ctx->mu);
         f->ctx->factors.erase(f);
         for (void* q : {(void*)f->d_pos, (void*)f->d_radii, (void*)f->d_eps, (void*)f->d_T, f->d_A,
-                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack, (void*)f->d_scale})
+                        (void*)f->d_inv, (void*)f->wk.piv, f->wk.pack, (void*)f->d_scale, (void*)f->d_Z})
             f->ctx->pool.free(q);
     }
     delete f;

@@ -415,7 +415,8 @@ __global__ void pack_l_kernel(const float2* __restrict__ A, size_t lda, int r0, 
     }
 }
 
-// U hi/lo (n' x kp floats, row-major): row nu = interleaved column nu of U12.
+// U hi/lo (n' x kp floats, row-major): row nu = interleaved column nu of U12. lo may be null
+// (the two-pass split reads only hi, U12 rounded to TF32).
 __global__ void pack_u_kernel(const float2* __restrict__ A, size_t lda, int r0, int k0, int ncols, int w, int kp,
                               float* __restrict__ hi, float* __restrict__ lo) {
     size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -428,7 +429,7 @@ __global__ void pack_u_kernel(const float2* __restrict__ A, size_t lda, int r0, 
     split(u.y, ih, il);
     size_t o = (size_t)nu * kp + 2 * kk;
     *(float2*)(hi + o) = make_float2(rh, ih);
-    *(float2*)(lo + o) = make_float2(rl, il);
+    if (lo) *(float2*)(lo + o) = make_float2(rl, il);
 }
 
 // x <- -x over hi and lo halves (2 count floats starting at p, contiguous)
@@ -847,7 +848,8 @@ void launch_tf32_update_region(float2* A, int n, int k0, int w, int r0, int m, i
             dim3 g1((m + 31) / 32, (kp / 2 + 31) / 32);
             size_t tot = (size_t)ncols * (kp / 2);
             pack_l_kernel<<<g1, 256, 0, st>>>(A, (size_t)n, r0, k0, m, w, kp, ahi, alo);
-            pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, c0, k0, ncols, w, kp, bhi, blo);
+            pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, c0, k0, ncols, w, kp, bhi,
+                                                                         wk.two_pass ? nullptr : blo);
         }
         *launches += 2;
     }
