@@ -1,9 +1,10 @@
 """The matrix-free operator (I - T C) x in its three device forms against the oracle.
 
 lmax 2..5 run the product form (harmonic tables of a chunk of sources times the coefficient
-block, then the plan's term lists once per destination); lmax 1 and >= 6, or TCU_APPLY=terms,
-run the per-pair term sums. TCU_APPLY=stored builds the tables of all pairs once and applies
-the FP64 tensor-core product over them (the form GMRES uses for lmax 2..5). 37 spheres make the destination groups and the source chunks of the
+block, then the plan's term lists once per destination; TCU_APPLY=fly keeps it for several
+columns too); lmax 1 and >= 6, or TCU_APPLY=terms, run the per-pair term sums. The stored form
+(the default for several columns and inside GMRES, forced by TCU_APPLY=stored) builds the
+tables of all pairs once and applies the FP64 tensor-core product over them. 37 spheres make the destination groups and the source chunks of the
 product form ragged; three right-hand sides exercise the column grid. Bound: relative 1e-13 in
 the 2-norm against the oracle's FP64 operator (cluster/iterative.rs apply path).
 """
@@ -21,10 +22,10 @@ def _rel(a, b):
 
 
 @pytest.mark.parametrize("lmax", [1, 2, 3, 4, 5, 6])
-@pytest.mark.parametrize("form", ["product", "terms", "stored"])
+@pytest.mark.parametrize("form", ["default", "fly", "terms", "stored"])
 def test_operator_forms_match_the_oracle(ctx, lmax, form, monkeypatch):
     import treams_b200 as t
-    if form == "product":
+    if form == "default":
         monkeypatch.delenv("TCU_APPLY", raising=False)
     else:
         monkeypatch.setenv("TCU_APPLY", form)
@@ -54,9 +55,9 @@ def test_stored_and_product_forms_agree_at_4096_spheres(ctx, monkeypatch):
     import treams_b200 as t
     w = workloads.learned_cluster()
     x = np.random.default_rng(12).standard_normal((w.n, 2)) + 0j
-    monkeypatch.delenv("TCU_APPLY", raising=False)
+    monkeypatch.setenv("TCU_APPLY", "fly")
     yp = t.cluster_apply(w.lmax, w.k0, w.radii, w.eps, w.positions, x, ctx=ctx)
-    monkeypatch.setenv("TCU_APPLY", "stored")
+    monkeypatch.delenv("TCU_APPLY", raising=False)
     ys = t.cluster_apply(w.lmax, w.k0, w.radii, w.eps, w.positions, x, ctx=ctx)
     assert _rel(ys, yp) <= 1e-13
 
@@ -76,3 +77,19 @@ def test_gmres_with_stored_tables_matches_the_on_the_fly_product(ctx, lmax, monk
     s2 = c.solve(B, rtol=1e-12, restart=40, max_iterations=400)
     assert [q.iterations for q in s1.convergence] == [q.iterations for q in s2.convergence]
     assert _rel(s1.value, s2.value) <= 1e-11
+
+
+@pytest.mark.parametrize("lmax", [2, 3, 4, 5])
+@pytest.mark.parametrize("pipe", ["cpasync", "tma"])
+def test_stored_product_pipelines_match_the_oracle(ctx, lmax, pipe, monkeypatch):
+    # both ways of streaming the stored tables into shared memory, forced at every lmax
+    import treams_b200 as t
+    monkeypatch.setenv("TCU_APPLY", "stored")
+    monkeypatch.setenv("TCU_STORED_PIPE", pipe)
+    w = workloads.learned_cluster(seed=140 + lmax, count=53)
+    n = w.radii.size * 2 * lmax * (lmax + 2)
+    rng = np.random.default_rng(lmax + 7)
+    x = rng.standard_normal((n, 2)) + 1j * rng.standard_normal((n, 2))
+    yg = t.cluster_apply(lmax, w.k0, w.radii, w.eps, w.positions, x, ctx=ctx)
+    yo = oracle.iterative_apply(lmax, w.k0, w.radii, w.eps, w.positions, x)
+    assert _rel(yg, yo) <= 1e-13

@@ -505,7 +505,8 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
     auto residual = [&]() -> tcu_status {
         // r = T b - (x - T C x)
         if (f->d_Z) {
-            launch_apply_stored(*P, f->N, STORED_FULL, f->d_Z, f->d_T, x, n, p, tb, -1.0, 1.0, r, xf, ctx->stream);
+            launch_apply_stored(*P, f->N, STORED_FULL, f->d_Z, f->d_T, x, n, p, tb, -1.0, 1.0, r, xf, f->wk.status,
+                                ctx->stream);
             ctx->launches += 2;
         } else {
             apply_op(ctx, P, f->N, f->k0, f->d_pos, f->d_T, x, n, p, tb, -1.0, 1.0, true, r);
@@ -516,7 +517,7 @@ tcu_status solve_impl(tcu_factor* f, const double* B, int p, double* X, tcu_cert
         CK(cudaMemcpyAsync(&sweep_status, f->wk.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "status");
         tcu_status s2 = sync_status(ctx, "residual");
         if (s2) return s2;
-        if (sweep_status == 8) return fail(TCU_TIMEOUT, "triangular sweep: a device-side wait gave up");
+        if (sweep_status == 8) return fail(TCU_TIMEOUT, "refinement: a device-side wait gave up");
         return TCU_OK;
     };
     CK(cudaMemcpyAsync(x, tb, per * 16, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
@@ -1167,20 +1168,24 @@ tcu_status tcu_cluster_apply(tcu_context* ctx, int lmax, double k0, size_t N, co
     launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
     ++ctx->launches;
     if ((s = read_status(ctx, "Mie coefficients"))) return s;
-    const char* form = getenv("TCU_APPLY");  // "stored": the tables once, then the stored-table product
-    if (form && strcmp(form, "stored") == 0 && apply_gemm_supported(*P)) {
+    // Several columns (or TCU_APPLY=stored): the pair tables once, then the stored-table
+    // product per column; one column: the product form (building the tables costs about one
+    // application, so storing them gains nothing).
+    const char* form = getenv("TCU_APPLY");
+    const bool forced = form && strcmp(form, "stored") == 0;
+    if (apply_gemm_supported(*P) && (forced || (p >= 2 && use_stored_tables(*P, (int)N)))) {
         DevBuf zbuf(ctx), xfbuf(ctx);
         CK(zbuf.alloc(stored_tables_bytes(*P, (int)N, STORED_FULL)), "stored tables");
         CK(xfbuf.alloc(stored_inputs_bytes(*P, (int)N, STORED_FULL, p)), "packed inputs");
         build_stored_tables(*P, (int)N, k0, pos, STORED_FULL, (cplx*)zbuf.p, ctx->stream);
-        launch_apply_stored(*P, (int)N, STORED_FULL, (const cplx*)zbuf.p, T, dx, n, p, nullptr, 1.0, -1.0, dy, (cplx*)xfbuf.p,
-                            ctx->stream);
+        launch_apply_stored(*P, (int)N, STORED_FULL, (const cplx*)zbuf.p, T, dx, n, p, nullptr, 1.0, -1.0, dy,
+                            (cplx*)xfbuf.p, ctx->d_status, ctx->stream);
         ctx->launches += 3;
     } else {
         apply_op(ctx, P, (int)N, k0, pos, T, dx, n, p, nullptr, 1.0, -1.0, true, dy);
     }
     CK(cudaMemcpyAsync(y, dy, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
-    return sync_status(ctx, "cluster apply");
+    return read_status(ctx, "cluster apply");
 }
 
 }  // extern "C"
@@ -1378,7 +1383,8 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
         tcu_certificate cert{};
         auto op = [&](const cplx* in, cplx* out) {
             if (Zst) {
-                launch_apply_stored(*P, (int)N, STORED_FULL, Zst, T, in, n, 1, nullptr, 1.0, -1.0, out, (cplx*)xfbuf.p, ctx->stream);
+                launch_apply_stored(*P, (int)N, STORED_FULL, Zst, T, in, n, 1, nullptr, 1.0, -1.0, out, (cplx*)xfbuf.p,
+                                    ctx->d_status, ctx->stream);
                 ctx->launches += 2;
             } else {
                 launch_apply(*P, (int)N, k0, pos, T, in, n, 1, nullptr, 1.0, -1.0, true, out, ctx->stream);
@@ -1393,7 +1399,7 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
         }
     }
     CK(cudaMemcpyAsync(X, x, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
-    s = sync_status(ctx, "GMRES");
+    s = read_status(ctx, "GMRES");
     if (s) return s;
     if (worst) return fail(worst, msg);
     return TCU_OK;

@@ -354,11 +354,10 @@ __global__ void pack_sources_kernel(const cplx* __restrict__ x, size_t ldx, int 
 }
 
 // y = zadd + alpha x + beta T C x (or the sub-operator O) from the stored tables: CTA = DI
-// destinations x one column,
-// a warp per RPW row octets with CT column octets (complex accumulators as re and im 8 x 8 FP64
-// tiles, four m8n8k4 products per complex step: re += a.re b.re + a.im (-b.im), im += a.re b.im
-// + a.im b.re, each B fragment used for RPW row octets); chunks of 16 sources through a 3-stage
-// cp.async ring; then the term lists.
+// destinations x one column, a warp per RPW row octets with CT column octets (complex
+// accumulators as re and im 8 x 8 FP64 tiles, four m8n8k4 products per complex step:
+// re += a.re b.re + a.im (-b.im), im += a.re b.im + a.im b.re, each B fragment used for RPW
+// row octets); chunks of 16 sources through a 3-stage cp.async ring; then the term lists.
 template <int CT, int RPW>
 __global__ void __launch_bounds__(256, 1)
     apply_stored_kernel(DevPlan P, SubOp O, int N, const cplx* __restrict__ Z, const cplx* __restrict__ Xf, int NC,
@@ -436,6 +435,173 @@ __global__ void __launch_bounds__(256, 1)
     __syncthreads();
     const size_t coff = (size_t)blockIdx.y * ldx;
     terms_epilogue(P, O, Gs, DI, blockIdx.x * DI, N, T, x + coff, coff, zadd, alpha, beta, true, y, tid, nthr);
+}
+
+// ---- bulk-copy pipeline of the stored product ---------------------------------------------
+constexpr int AT_STAGES = AS_STAGES;  // ring depth of the bulk-copy pipeline (2 CTAs per SM at lmax <= 4)
+
+__device__ __forceinline__ uint32_t as_smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void as_mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void as_mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void as_mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool as_mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on a phase: false after 2 s (recorded in abort_flag) or once another warp gave up.
+__device__ __forceinline__ bool as_mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    if (as_mbar_try(bar, parity)) return true;
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (unsigned it = 1;; ++it) {
+        if (as_mbar_try(bar, parity)) return true;
+        if ((it & 63u) == 0) {
+            if (*abort_flag) return false;
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            if (t - t0 > 2000000000ull) {
+                *abort_flag = 1;
+                return false;
+            }
+        }
+    }
+}
+// contiguous global -> shared copy completing on an mbarrier (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void as_bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+// The stored product with a producer warp: lane 0 of the last warp streams the 16-source chunks
+// (table slab and packed inputs, each one contiguous bulk copy) into a 3-stage ring, each stage
+// completing on its full barrier; the product warps take a stage once its full barrier flips
+// and release it through its empty barrier (one arrival per warp), so no CTA-wide barrier
+// sits in the loop. Every wait is bounded (2 s): on a timeout the kernel records status 8,
+// waits (bounded) for the copies in flight and returns without writing y.
+template <int CT, int RPW>
+__global__ void __launch_bounds__(288, 1)
+    apply_stored_tma_kernel(DevPlan P, SubOp O, int N, const cplx* __restrict__ Z, const cplx* __restrict__ Xf,
+                            int NC, int DI, int RO, const cplx* __restrict__ T, const cplx* __restrict__ x, size_t ldx,
+                            const cplx* __restrict__ zadd, double alpha, double beta, cplx* __restrict__ y,
+                            int* __restrict__ status) {
+    extern __shared__ __align__(128) unsigned char at_smem[];
+    __shared__ __align__(8) uint64_t bars[2 * AT_STAGES];
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int W = (RO + RPW - 1) / RPW;  // product warps; warp W loads
+    const int ABLK = RO * 128, BBLK = CT * 128, SBLK = ABLK + BBLK;  // complex entries per chunk
+    cplx* ring = reinterpret_cast<cplx*>(at_smem);
+    const cplx* Zb = Z + (size_t)blockIdx.x * NC * ABLK;
+    const cplx* Xb = Xf + (size_t)blockIdx.y * NC * BBLK;
+    const uint32_t full0 = as_smem_u32(bars), empty0 = full0 + 8 * AT_STAGES;
+    if (tid == 0) {
+        for (int s = 0; s < AT_STAGES; ++s) {
+            as_mbar_init(full0 + 8 * s, 1);
+            as_mbar_init(empty0 + 8 * s, W);
+        }
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    volatile int* abort_flag = &s_abort;
+    double re[RPW][CT][2], im[RPW][CT][2];
+#pragma unroll
+    for (int r = 0; r < RPW; ++r)
+#pragma unroll
+        for (int c = 0; c < CT; ++c) re[r][c][0] = re[r][c][1] = im[r][c][0] = im[r][c][1] = 0.0;
+    const int o0 = warp * RPW;
+    if (warp == W) {
+        if (lane == 0) {
+            int kc = 0;
+            for (; kc < NC; ++kc) {
+                const int s = kc % AT_STAGES;
+                if (!as_mbar_wait(empty0 + 8 * s, ((kc / AT_STAGES) & 1) ^ 1, abort_flag)) break;
+                const uint32_t dst = as_smem_u32(ring + (size_t)s * SBLK);
+                as_mbar_expect_tx(full0 + 8 * s, (uint32_t)SBLK * 16u);
+                as_bulk_load(dst, Zb + (size_t)kc * ABLK, (uint32_t)ABLK * 16u, full0 + 8 * s);
+                as_bulk_load(dst + (uint32_t)ABLK * 16u, Xb + (size_t)kc * BBLK, (uint32_t)BBLK * 16u, full0 + 8 * s);
+            }
+            if (*abort_flag) {
+                // drain: the last load issued into every stage lands before the CTA exits
+                volatile int never = 0;
+                for (int s = 0; s < AT_STAGES; ++s) {
+                    const int last = kc - 1 - ((kc - 1 - s) % AT_STAGES + AT_STAGES) % AT_STAGES;
+                    if (last >= 0) as_mbar_wait(full0 + 8 * s, (last / AT_STAGES) & 1, &never);
+                }
+            }
+        }
+    } else if (warp < W) {
+        const int nr = min(RPW, RO - o0);
+        for (int kc = 0; kc < NC; ++kc) {
+            const int s = kc % AT_STAGES;
+            if (!as_mbar_wait(full0 + 8 * s, (kc / AT_STAGES) & 1, abort_flag)) break;
+            const cplx* As = ring + (size_t)s * SBLK;
+            const cplx* Bs = As + ABLK;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                cplx a[RPW];
+#pragma unroll
+                for (int r = 0; r < RPW; ++r) a[r] = r < nr ? As[(q * RO + o0 + r) * 32 + lane] : mk(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < CT; ++c) {
+                    const cplx b = Bs[(q * CT + c) * 32 + lane];
+#pragma unroll
+                    for (int r = 0; r < RPW; ++r) {
+                        if (r < nr) {
+                            dmma(re[r][c], a[r].x, b.x);
+                            dmma(re[r][c], a[r].y, -b.y);
+                            dmma(im[r][c], a[r].x, b.y);
+                            dmma(im[r][c], a[r].y, b.x);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+            if (lane == 0) as_mbar_arrive(empty0 + 8 * s);
+        }
+    }
+    __syncthreads();  // every chunk consumed: no copy in flight, the ring is free for G
+    if (s_abort) {
+        if (tid == 0 && status) atomicExch(status, 8);
+        return;
+    }
+    cplx* Gs = reinterpret_cast<cplx*>(at_smem);
+    const int M = 2 * O.nsrc, rows = DI * (O.order + 1) * (O.order + 1);
+    if (warp < W) {
+#pragma unroll
+        for (int r = 0; r < RPW; ++r) {
+            const int row = (o0 + r) * 8 + (lane >> 2);
+            if (row < rows) {
+#pragma unroll
+                for (int c = 0; c < CT; ++c) {
+                    const int col = c * 8 + 2 * (lane & 3);
+                    if (col < M) {
+                        Gs[(size_t)row * M + col] = mk(re[r][c][0], im[r][c][0]);
+                        Gs[(size_t)row * M + col + 1] = mk(re[r][c][1], im[r][c][1]);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const size_t coff = (size_t)blockIdx.y * ldx;
+    terms_epilogue(P, O, Gs, DI, blockIdx.x * DI, N, T, x + coff, coff, zadd, alpha, beta, true, y, tid,
+                   blockDim.x);
 }
 
 }  // namespace
@@ -554,7 +720,8 @@ void build_stored_tables(const DevPlan& P, int N, double k, const double* pos, i
 }
 
 void launch_apply_stored(const DevPlan& P, int N, int kind, const cplx* Z, const cplx* T, const cplx* x, size_t ldx,
-                         int ncol, const cplx* zadd, double alpha, double beta, cplx* y, cplx* Xf, cudaStream_t st) {
+                         int ncol, const cplx* zadd, double alpha, double beta, cplx* y, cplx* Xf, int* status,
+                         cudaStream_t st) {
     if (N <= 0 || ncol <= 0 || !stored_kind_ok(P, kind)) return;
     StageScope sc(kind == STORED_FULL ? ST_APPLY : ST_COARSE, st);
     const StoredLayout l = stored_layout(P, N, kind);
@@ -564,9 +731,17 @@ void launch_apply_stored(const DevPlan& P, int N, int kind, const cplx* Z, const
     const dim3 grid((unsigned)l.nblk, (unsigned)ncol);
     const size_t smem = stored_smem(l);
     const int threads = (l.RO + l.RPW - 1) / l.RPW * 32;
+    // bulk-copy pipeline, except at 6 column octets (lmax 4) where the cp.async ring measured
+    // faster (1.43 against 1.58 ms at 1024 spheres); TCU_STORED_PIPE=cpasync or tma forces one
+    const char* pipe = getenv("TCU_STORED_PIPE");
+    const bool cpasync = pipe ? strcmp(pipe, "cpasync") == 0 : l.CT == 6;
 #define TCU_STORED(CT, RPW)                                                                                       \
-    apply_stored_kernel<CT, RPW><<<grid, threads, smem, st>>>(P, l.O, N, Z, Xf, l.NC, l.DI, l.RO, T, x, ldx, zadd, \
-                                                             alpha, beta, y)
+    if (cpasync)                                                                                                  \
+        apply_stored_kernel<CT, RPW><<<grid, threads, smem, st>>>(P, l.O, N, Z, Xf, l.NC, l.DI, l.RO, T, x, ldx,   \
+                                                                 zadd, alpha, beta, y);                            \
+    else                                                                                                          \
+        apply_stored_tma_kernel<CT, RPW><<<grid, threads + 32, smem, st>>>(P, l.O, N, Z, Xf, l.NC, l.DI, l.RO, T, \
+                                                                          x, ldx, zadd, alpha, beta, y, status)
     switch (l.CT) {
         case 1: TCU_STORED(1, 2); break;
         case 2: TCU_STORED(2, 2); break;
@@ -584,10 +759,15 @@ void apply_gemm_init_attributes() {
     cudaFuncSetAttribute(apply_gemm_kernel<4, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(table_store_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(apply_stored_kernel<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply_stored_tma_kernel<1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(apply_stored_kernel<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply_stored_tma_kernel<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(apply_stored_kernel<4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply_stored_tma_kernel<4, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(apply_stored_kernel<6, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply_stored_tma_kernel<6, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     cudaFuncSetAttribute(apply_stored_kernel<9, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(apply_stored_tma_kernel<9, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 }  // namespace tcu

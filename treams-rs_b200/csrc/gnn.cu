@@ -528,7 +528,7 @@ class IterativeCoarse : public CoarseSolve {
     void matvec(const cplx* x, cplx* y, cudaStream_t st) {
         if (stored && stored->ready) {
             launch_apply_stored(*plan, N, STORED_DIPOLE_BLOCK, stored->Z.as<cplx>(), T, x, 0, 1, nullptr, 1.0, -1.0, y,
-                                stored->Xf.as<cplx>(), st);
+                                stored->Xf.as<cplx>(), nullptr, st);
             if (launches) *launches += 2;
         } else {
             launch_apply_dipole(*plan, N, k0, pos, T, x, true, nullptr, 1.0, -1.0, y, st);
@@ -647,7 +647,7 @@ struct Coarse {
         if (s) return s;
         if (zsrc.ready) {
             launch_apply_stored(*plan, N, STORED_DIPOLE_SOURCES, zsrc.Z.as<cplx>(), T, vc.as<cplx>(), 0, 1, v, -1.0, 1.0,
-                                r1, zsrc.Xf.as<cplx>(), st);
+                                r1, zsrc.Xf.as<cplx>(), nullptr, st);
             if (launches) *launches += 3;
         } else {
             launch_apply_dipole(*plan, N, k0, pos, T, vc.as<cplx>(), false, v, -1.0, 1.0, r1, st);

@@ -155,8 +155,10 @@ bool stored_tables_enabled();  // false when TCU_APPLY is "fly" or "terms" (read
 size_t stored_tables_bytes(const DevPlan& P, int N, int kind);
 size_t stored_inputs_bytes(const DevPlan& P, int N, int kind, int ncol);
 void build_stored_tables(const DevPlan& P, int N, double k, const double* pos, int kind, cplx* Z, cudaStream_t st);
+// status (may be null) receives 8 when a bounded wait of the product gave up (y not written).
 void launch_apply_stored(const DevPlan& P, int N, int kind, const cplx* Z, const cplx* T, const cplx* x, size_t ldx,
-                         int ncol, const cplx* zadd, double alpha, double beta, cplx* y, cplx* Xf, cudaStream_t st);
+                         int ncol, const cplx* zadd, double alpha, double beta, cplx* y, cplx* Xf, int* status,
+                         cudaStream_t st);
 void launch_block(const DevPlan& P, double k, const double* d, bool singular, bool helicity, cplx* out,
                   cudaStream_t st);
 void launch_mie(int L, double k0, int N, const double* radii, const cplx* eps, cplx* T, int* status, cudaStream_t st);
