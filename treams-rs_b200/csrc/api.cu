@@ -1348,6 +1348,20 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
     if ((s = read_status(ctx, "Mie coefficients"))) return s;
     launch_apply_t(lmax, (int)N, T, b, p, tb, ctx->stream);
     ++ctx->launches;
+    // the harmonic tables of all pairs, built once for the applications of every column; launched
+    // first, so that the device builds them while the host sets up the preconditioner's graph
+    DevBuf zbuf(ctx), xfbuf(ctx);
+    const cplx* Zst = nullptr;
+    if (use_stored_tables(*P, (int)N)) {
+        if (zbuf.alloc(stored_tables_bytes(*P, (int)N, STORED_FULL)) == cudaSuccess &&
+            xfbuf.alloc(stored_inputs_bytes(*P, (int)N, STORED_FULL, 1)) == cudaSuccess) {
+            build_stored_tables(*P, (int)N, k0, pos, STORED_FULL, (cplx*)zbuf.p, ctx->stream);
+            ++ctx->launches;
+            Zst = (const cplx*)zbuf.p;
+        } else {
+            cudaGetLastError();  // no room: the on-the-fly product
+        }
+    }
     std::unique_ptr<Preconditioner> pre;
     if (preconditioner == TCU_PRECOND_BLOCK_JACOBI) {
         s = make_block_jacobi(ctx->stream, *P, (int)N, k0, pos, positions, radii, T, &pre, &ctx->launches);
@@ -1363,19 +1377,6 @@ extern "C" tcu_status tcu_iterative_solve(tcu_context* ctx, int lmax, double k0,
                            &ctx->launches);
         if (s == TCU_OUT_OF_MEMORY) return fail(s, "two-level preconditioner: out of device memory");
         if (s) return fail(s, "two-level preconditioner set-up failed");
-    }
-    // the harmonic tables of all pairs, built once for the applications of every column
-    DevBuf zbuf(ctx), xfbuf(ctx);
-    const cplx* Zst = nullptr;
-    if (use_stored_tables(*P, (int)N)) {
-        if (zbuf.alloc(stored_tables_bytes(*P, (int)N, STORED_FULL)) == cudaSuccess &&
-            xfbuf.alloc(stored_inputs_bytes(*P, (int)N, STORED_FULL, 1)) == cudaSuccess) {
-            build_stored_tables(*P, (int)N, k0, pos, STORED_FULL, (cplx*)zbuf.p, ctx->stream);
-            ++ctx->launches;
-            Zst = (const cplx*)zbuf.p;
-        } else {
-            cudaGetLastError();  // no room: the on-the-fly product
-        }
     }
     tcu_status worst = TCU_OK;
     std::string msg;

@@ -696,8 +696,9 @@ tcu_status make_two_level(cudaStream_t st, bool learned, const DevPlan& P, int L
     double rmax = 0.0;
     for (int i = 0; i < N; ++i) rmax = std::max(rmax, h_radii[i]);
     const double cutoff = 2.0 * (reach > 0.0 ? reach : LEARNED_REACH) * rmax;
-    if (!pre->graph.build(st, P, L, N, k0, d_pos, h_pos, h_radii, h_eps, cutoff, launches)) return TCU_OUT_OF_MEMORY;
+    // the coarse blocks' tables go to the device first; the host builds the graph meanwhile
     if (!pre->coarse.build(P, N, k0, d_pos, d_T, std::move(coarse), st, launches)) return TCU_OUT_OF_MEMORY;
+    if (!pre->graph.build(st, P, L, N, k0, d_pos, h_pos, h_radii, h_eps, cutoff, launches)) return TCU_OUT_OF_MEMORY;
     if (!pre->r1.alloc(pre->graph.n * sizeof(cplx)) || !pre->noskip.alloc(std::max<size_t>(pre->graph.nnz, 1)))
         return TCU_OUT_OF_MEMORY;
     cudaMemsetAsync(pre->noskip.p, 0, std::max<size_t>(pre->graph.nnz, 1), st);
