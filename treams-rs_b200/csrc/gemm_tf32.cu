@@ -779,8 +779,24 @@ bool launch_tf32_trsm_inverse(float2* A, int n, int k0, int w, LuWork& wk, cudaS
     return cudaGetLastError() == cudaSuccess;
 }
 
+// The TRSM's right-hand side A12 as TF32 pieces, packed before the main stream waits for the
+// inverse of L11 (which it does not need); launch_tf32_trsm(..., rhs_packed = true) then skips
+// it. FP16 pieces keep their packing in launch_tf32_trsm (false here).
+bool launch_tf32_trsm_rhs(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches) {
+    if (wk.f16_pieces) return false;
+    int r0 = k0 + w, ncols = n - r0, kp;
+    if (ncols <= 0 || !trsm_buffers(n, k0, w, wk, st, &kp)) return false;
+    float* bhi = (float*)wk.pack + (size_t)4 * w * kp;
+    float* blo = bhi + (size_t)ncols * kp;
+    StageScope sc(ST_TRSM, st);
+    size_t tot = (size_t)ncols * (kp / 2);
+    pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
+    ++*launches;
+    return true;
+}
+
 void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches,
-                      bool inverse_done) {
+                      bool inverse_done, bool rhs_packed) {
     int r0 = k0 + w, ncols = n - r0;
     int kp;
     float2* Nm = trsm_buffers(n, k0, w, wk, st, &kp);
@@ -813,10 +829,14 @@ void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t 
             *launches += 3;
         } else {
             pack_l_kernel<<<g1, 256, 0, st>>>(Nm, (size_t)w, 0, 0, w, w, kp, ahi, alo);
-            pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi, blo);
+            if (!rhs_packed) {
+                pack_u_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(A, (size_t)n, r0, k0, ncols, w, kp, bhi,
+                                                                             blo);
+                ++*launches;
+            }
             negate_kernel<<<(unsigned)(((size_t)4 * w * kp + 255) / 256), 256, 0, st>>>(ahi, (size_t)4 * w * kp);
             run_gemm(A, n, 2 * k0, r0, 2 * w, ncols, kp, ahi, alo, bhi, blo, nullptr, nullptr, wk, st, launches);
-            *launches += 4;
+            *launches += 3;
         }
     }
 }

@@ -829,8 +829,9 @@ static bool lu_pairs_enabled() {
     }();
     return v;
 }
+bool launch_tf32_trsm_rhs(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches);
 void launch_tf32_trsm(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, long long* launches,
-                      bool inverse_done);
+                      bool inverse_done, bool rhs_packed);
 bool launch_tf32_trsm_inverse(float2* A, int n, int k0, int w, LuWork& wk, cudaStream_t st, cudaStream_t side,
                               long long* launches);
 
@@ -888,18 +889,24 @@ static int lu_factor_impl(typename Cx<R>::T* A, int n, LuWork& wk, cudaStream_t 
             laswp_kernel<C><<<(n + 255) / 256, 256, 0, st>>>(A, lda, n, k0, w, wk.piv);
         }
         ++*launches;
+        int r0 = k0 + w;
+        int cols = n - r0;
+        // work that does not need L11's inverse runs before the main stream waits for it: panel
+        // b's block rows get panel a's update, then the TRSM's right-hand side is packed
+        bool rhs_packed = false;
+        if (sizeof(R) == 4 && tensor_cores && r0 < n) {
+            if (pend_k0 >= 0)  // panel b: its block rows right of it get panel a's update first
+                launch_tf32_update_region((float2*)A, n, pend_k0, pend_w, k0, w, r0, cols, wk, st, launches);
+            rhs_packed = launch_tf32_trsm_rhs((float2*)A, n, k0, w, wk, st, launches);
+        }
         if (inverse_done && cudaStreamWaitEvent(st, side->inverse_done, 0) != cudaSuccess) {
             cudaStreamSynchronize(side->stream);  // ordering by the host instead
         }
-        int r0 = k0 + w;
         if (r0 >= n) break;
-        int cols = n - r0;
         int cpc = 64;
         size_t smem = (size_t)NB * NB * sizeof(C);
         if (sizeof(R) == 4 && tensor_cores) {
-            if (pend_k0 >= 0)  // panel b: its block rows right of it get panel a's update first
-                launch_tf32_update_region((float2*)A, n, pend_k0, pend_w, k0, w, r0, cols, wk, st, launches);
-            launch_tf32_trsm((float2*)A, n, k0, w, wk, st, launches, inverse_done);
+            launch_tf32_trsm((float2*)A, n, k0, w, wk, st, launches, inverse_done, rhs_packed);
         } else {
             StageScope sc(ST_TRSM, st);
             trsm_kernel<R, NB><<<(cols + cpc - 1) / cpc, 256, smem, st>>>(A, lda, k0, w, n, cpc);
