@@ -77,3 +77,22 @@ def test_adjoint_is_the_conjugate_transpose_of_the_operator(ctx):
         del b
     finally:
         f.close()
+
+
+@pytest.mark.parametrize("lmax", [2, 3, 4, 5])
+def test_iterative_pullback_with_stored_tables_matches_the_on_the_fly_product(ctx, lmax, monkeypatch):
+    # adjoint GMRES applies C from the pair tables stored once per call (default) or in
+    # product form every time (TCU_APPLY=fly)
+    w = workloads.learned_cluster(seed=160 + lmax, count=120)
+    n = w.radii.size * 2 * lmax * (lmax + 2)
+    G = _cotangent(n, 2, 20 + lmax)
+    c = t.SphereCluster(lmax, w.k0, w.radii, w.eps, w.positions, ctx=ctx)
+    monkeypatch.delenv("TCU_APPLY", raising=False)
+    s1 = c.pullback_incident(G, rtol=1e-12, restart=40, max_iterations=400)
+    monkeypatch.setenv("TCU_APPLY", "fly")
+    s2 = c.pullback_incident(G, rtol=1e-12, restart=40, max_iterations=400)
+    # the two products differ by rounding only, so GMRES may stop one iteration apart at rtol 1e-12
+    for q1, q2 in zip(s1.convergence, s2.convergence):
+        assert abs(q1.iterations - q2.iterations) <= 1
+        assert q1.residual_norm <= 1e-12 * q1.rhs_norm
+    assert np.linalg.norm(s1.value - s2.value) <= 1e-9 * np.linalg.norm(s2.value)

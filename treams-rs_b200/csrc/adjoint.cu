@@ -162,18 +162,25 @@ void adjoint_solve_impl(const C* A, int n, const int* perm, const double2* inv, 
 }  // namespace
 
 void launch_apply_adjoint(const DevPlan& P, int N, double k0, const double* pos, const cplx* T, const cplx* x,
-                          size_t ldx, int ncol, cplx* y, cplx* t1, cplx* t2, cudaStream_t st, long long* launches) {
+                          size_t ldx, int ncol, cplx* y, cplx* t1, cplx* t2, cudaStream_t st, long long* launches,
+                          const cplx* Z, cplx* Xf, int* status) {
     const int L = P.L, nlm = P.nlm;
     const size_t n = (size_t)N * 2 * nlm;
     th_apply_kernel<<<nblk((size_t)N * nlm * ncol, 256), 256, 0, st>>>(N, L, T, x, ldx, ncol, t1);
     flip_conj_kernel<<<nblk(n * ncol, 256), 256, 0, st>>>(N, L, t1, nullptr, ldx, ncol, t2);
-    for (int c0 = 0; c0 < ncol; c0 += 8) {
-        const int nc = std::min(8, ncol - c0);
-        launch_apply(P, N, k0, pos, nullptr, t2 + (size_t)c0 * ldx, ldx, nc, nullptr, 0.0, 1.0, true,
-                     t1 + (size_t)c0 * ldx, st);
+    if (Z) {  // the coupling product from the stored pair tables (T null: C alone)
+        launch_apply_stored(P, N, STORED_FULL, Z, nullptr, t2, ldx, ncol, nullptr, 0.0, 1.0, t1, Xf, status, st);
+        if (launches) *launches += 2;
+    } else {
+        for (int c0 = 0; c0 < ncol; c0 += 8) {
+            const int nc = std::min(8, ncol - c0);
+            launch_apply(P, N, k0, pos, nullptr, t2 + (size_t)c0 * ldx, ldx, nc, nullptr, 0.0, 1.0, true,
+                         t1 + (size_t)c0 * ldx, st);
+        }
+        if (launches) *launches += (ncol + 7) / 8;
     }
     flip_conj_kernel<<<nblk(n * ncol, 256), 256, 0, st>>>(N, L, t1, x, ldx, ncol, y);
-    if (launches) *launches += 3 + (ncol + 7) / 8;
+    if (launches) *launches += 3;
 }
 
 void launch_apply_th(int L, int N, const cplx* T, const cplx* x, size_t ldx, int ncol, cplx* y, cudaStream_t st) {

@@ -606,13 +606,16 @@ tcu_status solve_adjoint_impl(tcu_factor* f, const double* G, int p, double* Y, 
         return fail(TCU_INVALID_INPUT, "require finite channel-by-illumination columns matching the factorization");
     DevBuf bufs(ctx);
     const size_t tmpc = adjoint_solve_tmp((int)n, p);
-    CK(bufs.alloc((5 * per + tmpc) * sizeof(cplx)), "adjoint solve buffers");
+    const size_t xfc = f->d_Z ? stored_inputs_bytes(*P, f->N, STORED_FULL, p) / sizeof(cplx) : 0;
+    CK(bufs.alloc((5 * per + tmpc + xfc) * sizeof(cplx)), "adjoint solve buffers");
     cplx* g = (cplx*)bufs.p;
     cplx* y = g + per;
     cplx* r = y + per;
     cplx* t1 = r + per;
     cplx* t2 = t1 + per;
-    cplx* tmp = t2 + per;
+    cplx* xf = t2 + per;  // packed inputs of the stored-table coupling product
+    cplx* tmp = xf + xfc;
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
     CK(cudaMemcpyAsync(g, G, per * 16, cudaMemcpyHostToDevice, ctx->stream), "copy rhs");
     std::vector<double> rn(p), bn(p);
     vec_norms(g, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
@@ -628,12 +631,13 @@ tcu_status solve_adjoint_impl(tcu_factor* f, const double* G, int p, double* Y, 
         if (f->scaled) scale_rows(v, f->d_scale, n, p, ctx->stream);  // R
     };
     auto residual = [&]() -> tcu_status {  // r = g - A^H y
-        launch_apply_adjoint(*P, f->N, f->k0, f->d_pos, f->d_T, y, n, p, r, t1, t2, ctx->stream, &ctx->launches);
+        launch_apply_adjoint(*P, f->N, f->k0, f->d_pos, f->d_T, y, n, p, r, t1, t2, ctx->stream, &ctx->launches,
+                             f->d_Z, xf, ctx->d_status);
         vec_sub(r, g, r, n, p, ctx->stream);
         vec_norms(r, n, p, ctx->d_small, ctx->d_partial, ctx->stream);
         ctx->launches += 3;
         CK(cudaMemcpyAsync(rn.data(), ctx->d_small, p * 8, cudaMemcpyDeviceToHost, ctx->stream), "norms");
-        return sync_status(ctx, "adjoint residual");
+        return read_status(ctx, "adjoint residual");
     };
     CK(cudaMemcpyAsync(y, g, per * 16, cudaMemcpyDeviceToDevice, ctx->stream), "copy");
     lu_adjoint(y);
@@ -1450,8 +1454,22 @@ extern "C" tcu_status tcu_iterative_pullback_incident(tcu_context* ctx, int lmax
     launch_mie(lmax, k0, (int)N, r, e, T, ctx->d_status, ctx->stream);
     ++ctx->launches;
     if ((s = read_status(ctx, "Mie coefficients"))) return s;
+    // the pair tables, stored once for every application of the adjoint operator
+    DevBuf zbuf(ctx), xfbuf(ctx);
+    const cplx* Zst = nullptr;
+    if (use_stored_tables(*P, (int)N)) {
+        if (zbuf.alloc(stored_tables_bytes(*P, (int)N, STORED_FULL)) == cudaSuccess &&
+            xfbuf.alloc(stored_inputs_bytes(*P, (int)N, STORED_FULL, 1)) == cudaSuccess) {
+            build_stored_tables(*P, (int)N, k0, pos, STORED_FULL, (cplx*)zbuf.p, ctx->stream);
+            ++ctx->launches;
+            Zst = (const cplx*)zbuf.p;
+        } else {
+            cudaGetLastError();  // no room: the on-the-fly product
+        }
+    }
     auto op = [&](const cplx* in, cplx* o) {
-        launch_apply_adjoint(*P, (int)N, k0, pos, T, in, n, 1, o, t1, t2, ctx->stream, &ctx->launches);
+        launch_apply_adjoint(*P, (int)N, k0, pos, T, in, n, 1, o, t1, t2, ctx->stream, &ctx->launches, Zst,
+                             (cplx*)xfbuf.p, ctx->d_status);
     };
     tcu_status worst = TCU_OK;
     std::string msg;
@@ -1467,7 +1485,7 @@ extern "C" tcu_status tcu_iterative_pullback_incident(tcu_context* ctx, int lmax
     launch_apply_th(lmax, (int)N, T, y, n, p, g, ctx->stream);  // the incident gradient T^H Y
     ++ctx->launches;
     CK(cudaMemcpyAsync(out, g, per * 16, cudaMemcpyDeviceToHost, ctx->stream), "copy");
-    s = sync_status(ctx, "adjoint GMRES");
+    s = read_status(ctx, "adjoint GMRES");
     if (s) return s;
     if (worst) return fail(worst, msg);
     return TCU_OK;

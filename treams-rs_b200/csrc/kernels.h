@@ -179,9 +179,12 @@ void launch_translate(const DevPlan& P, size_t count, const int* labels, const c
                       bool singular, cplx* out, cudaStream_t st);
 
 // adjoint.cu — y = (I - T C)^H x for ncol columns of leading dimension ldx (t1, t2: ldx x ncol
-// scratch), y = T^H x, and x <- A^-H x with the LU factors (tmp: adjoint_solve_tmp(n, ncol))
+// scratch; with stored pair tables Z (STORED_FULL) the coupling product runs over them, Xf:
+// stored_inputs_bytes for ncol columns, status as for launch_apply_stored), y = T^H x, and
+// x <- A^-H x with the LU factors (tmp: adjoint_solve_tmp(n, ncol))
 void launch_apply_adjoint(const DevPlan& P, int N, double k0, const double* pos, const cplx* T, const cplx* x,
-                          size_t ldx, int ncol, cplx* y, cplx* t1, cplx* t2, cudaStream_t st, long long* launches);
+                          size_t ldx, int ncol, cplx* y, cplx* t1, cplx* t2, cudaStream_t st, long long* launches,
+                          const cplx* Z = nullptr, cplx* Xf = nullptr, int* status = nullptr);
 void launch_apply_th(int L, int N, const cplx* T, const cplx* x, size_t ldx, int ncol, cplx* y, cudaStream_t st);
 size_t adjoint_solve_tmp(int n, int ncol);
 void lu_solve_adjoint_fp64(const double2* A, int n, const int* perm, const double2* inv, double2* x, double2* tmp,
