@@ -291,10 +291,18 @@ tcu_status tcu_learned_problem_destroy(tcu_learned_problem* p);
 tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
                               const double* kpars, double eta, double* out);
 /* The same at a shift r (lattice::sum with shift, lattice/mod.rs:283): D_lm(k, kpar, r) =
- * sum'_R h_l(k|r+R|) Y_lm(-r-R) e^{i kpar.R}, r in the lattice plane (r[2] = 0; off-plane
- * shifts are rejected), reduced into the cell on the host (lattice/ewald.rs:610-665). */
+ * sum'_R h_l(k|r+R|) Y_lm(-r-R) e^{i kpar.R}, the in-plane part of r reduced into the cell on
+ * the host (lattice/ewald.rs:610-665). Off the lattice plane (r[2] != 0) the reciprocal part
+ * takes every order of S_lmn and the t-series of F_(1/2-n)(v, t) (lattice/reciprocal.rs:22-60,
+ * lattice/reduced.rs:223); shifts with (k r_z eta)^2 > 16 are rejected (TCU_INVALID_INPUT). */
 tcu_status tcu_lsumsw2d_shift_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
                                     const double* kpars, const double* shift, double eta, double* out);
+/* The same sums at a complex wavenumber k = k[0] + i k[1] (a lossy embedding; lattice::sum takes
+ * a complex k, lattice/mod.rs:283): Re k > 0, 0 <= Im k <= Re k / 2, any shift r[3] (null: r = 0),
+ * a real split eta (0: the automatic split of cell.rs:164-175 taken at |k|). Each diffraction
+ * order is evaluated on its outgoing sheet (lattice/sheets.rs). out nk x (lmax_sum+1)^2. */
+tcu_status tcu_lsumsw2d_complex_batch(tcu_context* ctx, int lmax_sum, const double* k, const double* lattice,
+                                      size_t nk, const double* kpars, const double* shift, double eta, double* out);
 /* Periodic array of one sphere per cell: X(kpar) = (I - T S(kpar))^-1 T for nk Bloch
  * vectors (cluster/interaction.rs:292 with sw::lattice_expansion, sw/expansion.rs:418).
  * out nk x M x M (column-major per kpar). */

@@ -126,7 +126,30 @@ def test_shifted_lattice_sums_match_oracle(ctx, shift):
         assert np.max(np.abs(D[i] - ref)) <= 1e-11 * max(1.0, np.max(np.abs(ref))), (shift, i)
 
 
-def test_shifted_sums_reject_off_plane_shifts(ctx):
+@pytest.mark.parametrize("shift", [(0.3, 0.1, 0.25), (-0.45, 0.2, -0.4), (0.0, 0.0, 0.15), (2.4, -1.3, 0.6)])
+def test_off_plane_lattice_sums_match_oracle(ctx, shift):
+    # shifts off the lattice plane (spheres of a cell at different heights): every order n <= l - |m|
+    # of S_lmn and the t-series of F_(1/2-n)(v, t) (lattice/reciprocal.rs:22-60, lattice/reduced.rs:223)
+    lat = np.array([[1.0, 0.0], [0.3, 0.9]])
+    kps = np.array([[0.4, -0.7], [1.1, 0.4], [0.0, 0.0]])
+    for eta in (0.0, 0.8):
+        D = tl.lsumsw2d_batch(8, 2.7, lat, kps, eta=eta, shift=shift, ctx=ctx)
+        for i, kp in enumerate(kps):
+            ref = oracle.lsumsw2d_table(8, 2.7, lat, kp, r=shift, eta=eta)
+            assert np.max(np.abs(D[i] - ref)) <= 1e-11 * max(1.0, np.max(np.abs(ref))), (shift, eta, i)
+
+
+def test_off_plane_sums_do_not_depend_on_the_split(ctx):
+    # the exact sum does not depend on eta (tests/lattice/test_lattice.py:300-308), off the plane too
+    lat = np.array([[0.8, 0.0], [0.0, 0.8]])
+    kps = np.array([[0.5, 0.2], [-1.0, 1.5]])
+    d0 = tl.lsumsw2d_batch(10, 3.1, lat, kps, shift=(0.2, -0.1, 0.3), ctx=ctx)
+    d1 = tl.lsumsw2d_batch(10, 3.1, lat, kps, eta=0.9, shift=(0.2, -0.1, 0.3), ctx=ctx)
+    assert np.max(np.abs(d1 - d0)) <= 1e-11 * max(1.0, np.max(np.abs(d0)))
+
+
+def test_shifted_sums_reject_shifts_far_off_the_plane(ctx):
+    # (k r_z eta)^2 <= 16 keeps the alternating t-series within FP64 accuracy
     lat = np.eye(2)
-    with pytest.raises(ValueError, match="lattice plane"):
-        tl.lsumsw2d_batch(2, 2.0, lat, [[0.1, 0.2]], shift=(0.1, 0.0, 0.2), ctx=ctx)
+    with pytest.raises(ValueError, match="off the lattice plane"):
+        tl.lsumsw2d_batch(2, 2.0, lat, [[0.1, 0.2]], shift=(0.1, 0.0, 4.0), ctx=ctx)

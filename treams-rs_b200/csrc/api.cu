@@ -1502,10 +1502,13 @@ double log_fact(int n) { return std::lgamma((double)n + 1.0); }
 struct LatticeSetup {
     double eta = 0, area = 0;
     double sx = 0, sy = 0;      // in-plane shift reduced into the cell, r' = r - R0
+    double sz = 0;              // shift off the lattice plane
     double R0x = 0, R0y = 0;    // the lattice vector taken off (Bloch phase e^{-i kpar.R0})
     bool at_origin = true;      // r' = 0: the self term, and no R = 0 real-space term
+    double t = 0;               // (k r_z eta)^2 of the t-series off the plane
+    int J = 0;                  // its last term
     std::vector<double2> R, G;
-    std::vector<double> norm, reflection, coef;
+    std::vector<double> norm, reflection, coef, coefz;
     std::vector<double2> pref;
     double2 self0{0, 0};
 };
@@ -1541,7 +1544,27 @@ tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const
         S.R0y = c0 * a1y + c1 * a2y;
         S.sx = shift[0] - S.R0x;
         S.sy = shift[1] - S.R0y;
-        S.at_origin = S.sx == 0.0 && S.sy == 0.0;
+        S.sz = shift[2];
+        S.at_origin = S.sx == 0.0 && S.sy == 0.0 && S.sz == 0.0;
+    }
+    // off the plane: F_(1/2-n)(v, t) = sum_j (t/2)^j / j! F_(1/2-n-j)(v, 0) (lattice/reduced.rs:223),
+    // terms until (t/2)^j / j! falls below 1e-18 of the largest; the alternating limits cancel
+    // to about e^(-t/2) of the largest term, so t is bounded to keep FP64 accuracy
+    double zabs = 0.0;
+    if (S.sz != 0.0) {
+        zabs = std::fabs(k * S.sz);
+        S.t = (zabs * eta) * (zabs * eta);
+        if (!(S.t <= 16.0))
+            return fail(TCU_INVALID_INPUT,
+                        "shift too far off the lattice plane for the device lattice sums (require (k r_z eta)^2 <= 16)");
+        double term = 1.0, big = 1.0;
+        int J = 1;
+        for (; J < LS_TMAX; ++J) {
+            term *= 0.5 * S.t / J;
+            big = std::max(big, term);
+            if (J > 0.5 * S.t && term < 1e-18 * big) break;
+        }
+        S.J = J;
     }
     const double ke = k * eta;
     // real space: Gaussian factor e^{-(k eta)^2 R^2/2 + c} below e^-46 times the polynomial growth
@@ -1562,13 +1585,15 @@ tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const
                 double x = n1 * a1x + n2 * a2x, y = n1 * a1y + n2 * a2y;
                 if (std::hypot(x + S.sx, y + S.sy) <= Rc) S.R.push_back(make_double2(x, y));
             }
-    // reciprocal: e^{-v} (q/k)^lsum (2 eta^2)^n below e^-46
+    // reciprocal: e^{-v} (q/k)^lsum (2 eta^2)^n below e^-46 (off the plane also times the
+    // growth e^(t/2) of the t-series terms and the powers of k r_z)
     const double b1x = 2 * M_PI * a2y / det, b1y = -2 * M_PI * a2x / det;
     const double b2x = -2 * M_PI * a1y / det, b2y = 2 * M_PI * a1x / det;
-    double x2 = 1.0 + 2.0 * eta * eta * 46.0;
+    const double budget = 46.0 + 0.5 * S.t + lsum * std::log(std::max(1.0, zabs));
+    double x2 = 1.0 + 2.0 * eta * eta * budget;
     for (int it = 0; it < 30; ++it)
         x2 = 1.0 + 2.0 * eta * eta *
-                       (46.0 + 0.5 * lsum * std::log(std::max(1.0, x2)) +
+                       (budget + 0.5 * lsum * std::log(std::max(1.0, x2)) +
                         (lsum / 2) * std::log(std::max(1.0, 2.0 * eta * eta)) + std::log(std::max(1.0, 1.0 / eta)));
     double kmax = 0.0;
     for (size_t i = 0; i < nk; ++i) kmax = std::max(kmax, std::hypot(kpars[2 * i], kpars[2 * i + 1]));
@@ -1598,6 +1623,20 @@ tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const
                 for (int n = 0; n <= (l - am) / 2; ++n)
                     S.coef[(size_t)lm * LS_NMAX + n] =
                         std::exp(-log_fact(n) - log_fact((l + am - 2 * n) / 2) - log_fact((l - am - 2 * n) / 2));
+            if (S.sz != 0.0) {
+                // S_lmn off the plane (reciprocal.rs:22-60): coefficient of beta^(2p), p = (l-|m|-s)/2,
+                // (-k r_z)^(2n-s) / ((2n-s)! (s-n)! ((l+|m|-s)/2)! ((l-|m|-s)/2)!), n <= s <= min(l-|m|, 2n)
+                if (S.coefz.empty()) S.coefz.assign((size_t)T * LS_PMAX * LS_FMAX, 0.0);
+                const double mz = -k * S.sz;
+                for (int n = 0; n <= l - am; ++n)
+                    for (int sidx = n; sidx <= std::min(l - am, 2 * n); ++sidx) {
+                        if ((l - am - sidx) % 2) continue;
+                        const int p = (l - am - sidx) / 2;
+                        S.coefz[((size_t)lm * LS_PMAX + p) * LS_FMAX + n] =
+                            std::pow(mz, 2 * n - sidx) * std::exp(-log_fact(2 * n - sidx) - log_fact(sidx - n) -
+                                                                  log_fact(p + am) - log_fact(p));
+                    }
+            }
             // sqrt(2l+1) (-i)^m sqrt((l+m)!(l-m)!) / (A k^2 (-2)^l)   (reciprocal.rs:320-330)
             double mag = std::sqrt(2.0 * l + 1.0) * std::exp(0.5 * (log_fact(l + m) + log_fact(l - m))) /
                          (S.area * k * k * std::pow(-2.0, l));
@@ -1627,11 +1666,13 @@ tcu_status lattice_sums_device(tcu_context* ctx, int lsum, double k, const Latti
                                const double2* d_kpar, double2* d_out, Arena* scratch_arena, DevBuf& scratch) {
     (void)scratch_arena;
     const int T = (lsum + 1) * (lsum + 1);
-    if (lattice_sum_smem(lsum, (int)S.R.size()) > 200 * 1024 || S.G.size() > (1u << 20))
+    const bool offplane = !S.coefz.empty();
+    if (lattice_sum_smem(lsum, (int)S.R.size(), offplane) > 200 * 1024 || S.G.size() > (1u << 20))
         return fail(TCU_INVALID_INPUT, "lattice too elongated for the device lattice sums");
     Arena ar;
     size_t oR = ar.add(S.R.size() * 16), oG = ar.add(S.G.size() * 16), oN = ar.add(T * 8), oRf = ar.add(T * 8),
-           oC = ar.add((size_t)T * LS_NMAX * 8), oP = ar.add(T * 16), oTab = ar.add(S.R.size() * T * 16);
+           oC = ar.add((size_t)T * LS_NMAX * 8), oP = ar.add(T * 16), oTab = ar.add(S.R.size() * T * 16),
+           oZ = ar.add(S.coefz.size() * 8);
     CK(scratch.alloc(ar.total), "lattice scratch");
     void* b = scratch.p;
     CK(cudaMemcpyAsync(ar.at<void>(b, oR), S.R.data(), S.R.size() * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
@@ -1641,9 +1682,13 @@ tcu_status lattice_sums_device(tcu_context* ctx, int lsum, double k, const Latti
     CK(cudaMemcpyAsync(ar.at<void>(b, oC), S.coef.data(), (size_t)T * LS_NMAX * 8, cudaMemcpyHostToDevice, ctx->stream),
        "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oP), S.pref.data(), T * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    if (offplane)
+        CK(cudaMemcpyAsync(ar.at<void>(b, oZ), S.coefz.data(), S.coefz.size() * 8, cudaMemcpyHostToDevice,
+                           ctx->stream),
+           "copy");
     CK(cudaMemsetAsync(ctx->d_status, 0, 4, ctx->stream), "status");
     double2* tab = ar.at<double2>(b, oTab);
-    launch_real_table(lsum, k, S.eta, (int)S.R.size(), ar.at<double2>(b, oR), S.sx, S.sy, ar.at<double>(b, oN),
+    launch_real_table(lsum, k, S.eta, (int)S.R.size(), ar.at<double2>(b, oR), S.sx, S.sy, S.sz, ar.at<double>(b, oN),
                       ar.at<double>(b, oRf), tab, ctx->stream);
     ++ctx->launches;
     LatticeSumArgs a;
@@ -1662,6 +1707,10 @@ tcu_status lattice_sums_device(tcu_context* ctx, int lsum, double k, const Latti
     a.sy = S.sy;
     a.R0x = S.R0x;
     a.R0y = S.R0y;
+    a.offplane = offplane ? 1 : 0;
+    a.J = S.J;
+    a.t = S.t;
+    a.coefz = offplane ? ar.at<double>(b, oZ) : nullptr;
     a.nk = (int)nk;
     a.kpar = d_kpar;
     a.out = d_out;
@@ -1724,8 +1773,6 @@ extern "C" tcu_status tcu_lsumsw2d_shift_batch(tcu_context* ctx, int lmax_sum, d
                                                double* out) {
     if (!ctx || !out || !shift) return fail(TCU_INVALID_INPUT, "null context, shift or output");
     if (!finite_all(shift, 3)) return fail(TCU_INVALID_INPUT, "the shift must be finite");
-    if (shift[2] != 0.0)
-        return fail(TCU_INVALID_INPUT, "the device lattice sums take shifts in the lattice plane (r_z = 0)");
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
     ProfGuard pg(ctx);
@@ -1749,6 +1796,247 @@ extern "C" tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double 
                                          const double* kpars, double eta, double* out) {
     const double zero[3] = {0.0, 0.0, 0.0};
     return tcu_lsumsw2d_shift_batch(ctx, lmax_sum, k, lattice, nk, kpars, zero, eta, out);
+}
+
+namespace {
+
+// Host set-up of the complex-wavenumber sums: the split, the shift reduced into the cell, the
+// lattice points of both parts within their cutoffs, the S_lmn coefficients with the powers of
+// -k r_z folded in, the prefactors and the self term.
+struct LatticeSetupCk {
+    double eta = 0, area = 0;
+    double sx = 0, sy = 0, sz = 0, R0x = 0, R0y = 0;
+    bool at_origin = true;
+    std::complex<double> t{0, 0};
+    int J = 0;
+    std::vector<double2> R, G, coef, pref;
+    std::vector<double> norm, reflection;
+    double2 self0{0, 0};
+};
+
+tcu_status lattice_setup_ck(int lsum, std::complex<double> k, const double* lat, size_t nk, const double* kpars,
+                            double eta_in, const double* shift, LatticeSetupCk& S) {
+    typedef std::complex<double> Z;
+    if (lsum < 0 || lsum > LS_MAXL) return fail(TCU_INVALID_INPUT, "require 0 <= lmax_sum <= 14");
+    if (!std::isfinite(k.real()) || !std::isfinite(k.imag()) || !(k.real() > 0.0) || k.imag() < 0.0 ||
+        !(2.0 * k.imag() <= k.real()))
+        return fail(TCU_INVALID_INPUT,
+                    "the complex-wavenumber lattice sums take Re k > 0 and 0 <= Im k <= Re k / 2");
+    if (!lat || !finite_all(lat, 4) || nk == 0 || !kpars || !finite_all(kpars, 2 * nk) || !shift ||
+        !finite_all(shift, 3))
+        return fail(TCU_INVALID_INPUT, "lattice, Bloch vectors and shift must be finite");
+    const double a1x = lat[0], a1y = lat[1], a2x = lat[2], a2y = lat[3];
+    const double det = a1x * a2y - a1y * a2x;
+    S.area = std::fabs(det);
+    if (!(S.area > 0.0) || !std::isfinite(S.area)) return fail(TCU_INVALID_INPUT, "lattice is numerically singular");
+    double eta = eta_in;
+    if (!std::isfinite(eta) || eta < 0.0) return fail(TCU_INVALID_INPUT, "the device lattice sums take a real split >= 0");
+    const double kabs = std::abs(k);
+    if (eta == 0.0) {  // lattice/cell.rs:164-175 with |k| (a real split)
+        double kl = kabs * std::sqrt(S.area);
+        eta = std::sqrt(2.0 * M_PI) / kl * std::max(kl / 8.0, 1.0);
+    }
+    const double c = 0.5 / (eta * eta);
+    if (c > 8.0)
+        return fail(TCU_INVALID_INPUT,
+                    "Ewald split too small for the device lattice sums (require 1/(2 eta^2) <= 8); eta = 0 selects one");
+    S.eta = eta;
+    const double f0 = (a2y * shift[0] - a2x * shift[1]) / det, f1 = (-a1y * shift[0] + a1x * shift[1]) / det;
+    const double c0 = std::round(f0), c1 = std::round(f1);
+    S.R0x = c0 * a1x + c1 * a2x;
+    S.R0y = c0 * a1y + c1 * a2y;
+    S.sx = shift[0] - S.R0x;
+    S.sy = shift[1] - S.R0y;
+    S.sz = shift[2];
+    S.at_origin = S.sx == 0.0 && S.sy == 0.0 && S.sz == 0.0;
+    const Z ke = k * eta, ke2 = ke * ke;
+    double zabs = 0.0;
+    if (S.sz != 0.0) {
+        const Z z = k * S.sz;
+        zabs = std::abs(z);
+        S.t = (z * eta) * (z * eta);
+        if (!(std::abs(S.t) <= 16.0))
+            return fail(TCU_INVALID_INPUT,
+                        "shift too far off the lattice plane for the device lattice sums (require |k r_z eta|^2 <= 16)");
+        double term = 1.0, big = 1.0, th = 0.5 * std::abs(S.t);
+        int J = 1;
+        for (; J < LS_TMAX; ++J) {
+            term *= th / J;
+            big = std::max(big, term);
+            if (J > th && term < 1e-18 * big) break;
+        }
+        S.J = J;
+    }
+    // real space: Gaussian factor e^{-Re (k eta)^2 R^2/2 + c} below e^-46 times the polynomial growth
+    const double decay = ke2.real();
+    double Rc = std::sqrt(2.0 * (46.0 + c) / decay);
+    for (int it = 0; it < 30; ++it)
+        Rc = std::sqrt(2.0 * (46.0 + c + lsum * std::log(std::max(1.0, kabs * Rc)) +
+                              (2 * lsum + 1) * std::log(std::max(1.0, eta))) /
+                       decay);
+    const double len1 = std::hypot(a1x, a1y), len2 = std::hypot(a2x, a2y);
+    const double hdir = S.area / std::max(len1, len2);
+    const double rin = std::hypot(S.sx, S.sy);
+    long Nd = (long)std::ceil((Rc + rin) / hdir) + 1;
+    if (Nd > 64) return fail(TCU_INVALID_INPUT, "lattice too elongated for the device lattice sums");
+    for (long s = S.at_origin ? 1 : 0; s <= Nd; ++s)
+        for (long n1 = -s; n1 <= s; ++n1)
+            for (long n2 = -s; n2 <= s; ++n2) {
+                if (std::max(std::labs(n1), std::labs(n2)) != s) continue;
+                double x = n1 * a1x + n2 * a2x, y = n1 * a1y + n2 * a2y;
+                if (std::hypot(x + S.sx, y + S.sy) <= Rc) S.R.push_back(make_double2(x, y));
+            }
+    // reciprocal: e^{-Re v} with Re v = (x2 - 1)/(2 eta^2), x2 = q.q Re(1/k^2), times the growth
+    // |q/k|^lsum (2 eta^2)^n of the terms, e^(|t|/2) and the powers of |k r_z|, below e^-46
+    const double b1x = 2 * M_PI * a2y / det, b1y = -2 * M_PI * a2x / det;
+    const double b2x = -2 * M_PI * a1y / det, b2y = 2 * M_PI * a1x / det;
+    const double rek2 = (1.0 / (k * k)).real();
+    const double budget = 46.0 + 0.5 * std::abs(S.t) + lsum * std::log(std::max(1.0, zabs));
+    double x2 = 1.0 + 2.0 * eta * eta * budget;
+    for (int it = 0; it < 30; ++it)
+        x2 = 1.0 + 2.0 * eta * eta *
+                       (budget + 0.5 * lsum * std::log(std::max(1.0, x2 / (rek2 * kabs * kabs))) +
+                        lsum * std::log(std::max(1.0, 2.0 * eta * eta)) + std::log(std::max(1.0, 1.0 / eta)));
+    double kmax = 0.0;
+    for (size_t i = 0; i < nk; ++i) kmax = std::max(kmax, std::hypot(kpars[2 * i], kpars[2 * i + 1]));
+    const double qc = std::sqrt(x2 / rek2) + kmax;
+    const double blen1 = std::hypot(b1x, b1y), blen2 = std::hypot(b2x, b2y);
+    const double hrec = (4 * M_PI * M_PI / S.area) / std::max(blen1, blen2);
+    long Nr = (long)std::ceil(qc / hrec) + 1;
+    if (Nr > 64) return fail(TCU_INVALID_INPUT, "lattice or Bloch vectors out of range for the device lattice sums");
+    for (long s = 0; s <= Nr; ++s)
+        for (long n1 = -s; n1 <= s; ++n1)
+            for (long n2 = -s; n2 <= s; ++n2) {
+                if (std::max(std::labs(n1), std::labs(n2)) != s) continue;
+                double x = n1 * b1x + n2 * b2x, y = n1 * b1y + n2 * b2y;
+                if (std::hypot(x, y) <= qc) S.G.push_back(make_double2(x, y));
+            }
+    const int T = (lsum + 1) * (lsum + 1);
+    S.norm.assign(T, 0.0);
+    S.reflection.assign(T, 0.0);
+    S.coef.assign((size_t)T * LS_PMAX * LS_FMAX, make_double2(0, 0));
+    S.pref.assign(T, make_double2(0, 0));
+    const Z mz = -k * S.sz, inv_k2 = 1.0 / (k * k);
+    for (int l = 0; l <= lsum; ++l)
+        for (int m = -l; m <= l; ++m) {
+            const int lm = l * l + l + m, am = std::abs(m);
+            S.norm[lm] = std::sqrt((2 * l + 1) / (4 * M_PI)) * std::exp(0.5 * (log_fact(l - m) - log_fact(l + m)));
+            S.reflection[lm] = ((am % 2) ? -1.0 : 1.0) * std::exp(log_fact(l - am) - log_fact(l + am));
+            // S_lmn (reciprocal.rs:22-60): coefficient of beta^(2p), p = (l-|m|-s)/2, order n:
+            // (-k r_z)^(2n-s) / ((2n-s)! (s-n)! ((l+|m|-s)/2)! ((l-|m|-s)/2)!), n <= s <= min(l-|m|, 2n)
+            for (int n = 0; n <= l - am; ++n)
+                for (int sidx = n; sidx <= std::min(l - am, 2 * n); ++sidx) {
+                    if ((l - am - sidx) % 2) continue;
+                    const int zp = 2 * n - sidx, p = (l - am - sidx) / 2;
+                    if (zp > 0 && S.sz == 0.0) continue;
+                    const Z v = (zp == 0 ? Z(1.0, 0.0) : std::pow(mz, zp)) *
+                                std::exp(-log_fact(zp) - log_fact(sidx - n) - log_fact(p + am) - log_fact(p));
+                    S.coef[((size_t)lm * LS_PMAX + p) * LS_FMAX + n] = make_double2(v.real(), v.imag());
+                }
+            // sqrt(2l+1) (-i)^m sqrt((l+m)!(l-m)!) / (A k^2 (-2)^l)   (reciprocal.rs:320-330)
+            const double mag = std::sqrt(2.0 * l + 1.0) * std::exp(0.5 * (log_fact(l + m) + log_fact(l - m))) /
+                               (S.area * std::pow(-2.0, l));
+            const int ph = ((m % 4) + 4) % 4;  // (-i)^m
+            const Z mi(ph == 0 ? 1 : ph == 2 ? -1 : 0, ph == 1 ? -1 : ph == 3 ? 1 : 0);
+            const Z pr = mag * mi * inv_k2;
+            S.pref[lm] = make_double2(pr.real(), pr.imag());
+        }
+    {  // self term at l = 0 (reciprocal.rs:467-487): with a real split it does not depend on k
+        double y = c, sum = 0.0, term = 1.0;
+        for (int kk = 0; kk < 400; ++kk) {
+            if (kk > 0) term *= y / kk;
+            double add = term / (kk - 0.5);
+            sum += add;
+            if (kk > y && std::fabs(add) < 1e-18 * std::fabs(sum)) break;
+        }
+        double gre = -2.0 * std::sqrt(M_PI), gim = -sum / std::sqrt(y);
+        double f = S.norm[0] * 0.5 / std::sqrt(M_PI);
+        S.self0 = make_double2(f * gre, f * gim);
+    }
+    return TCU_OK;
+}
+
+}  // namespace
+
+extern "C" tcu_status tcu_lsumsw2d_complex_batch(tcu_context* ctx, int lmax_sum, const double* k, const double* lattice,
+                                                 size_t nk, const double* kpars, const double* shift, double eta,
+                                                 double* out) {
+    if (!ctx || !out || !k) return fail(TCU_INVALID_INPUT, "null context, wavenumber or output");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ProfGuard pg(ctx);
+    const double zero[3] = {0.0, 0.0, 0.0};
+    const std::complex<double> kc(k[0], k[1]);
+    LatticeSetupCk S;
+    tcu_status s = lattice_setup_ck(lmax_sum, kc, lattice, nk, kpars, eta, shift ? shift : zero, S);
+    if (s) return s;
+    const int T = (lmax_sum + 1) * (lmax_sum + 1);
+    if (lattice_sum_ck_smem(lmax_sum, (int)S.R.size()) > 200 * 1024 || S.G.size() > (1u << 20))
+        return fail(TCU_INVALID_INPUT, "lattice too elongated for the device lattice sums");
+    Arena ar;
+    size_t oK = ar.add(nk * 16), oO = ar.add(nk * T * 16), oR = ar.add(S.R.size() * 16), oG = ar.add(S.G.size() * 16),
+           oN = ar.add(T * 8), oRf = ar.add(T * 8), oC = ar.add(S.coef.size() * 16), oP = ar.add(T * 16),
+           oTab = ar.add(S.R.size() * T * 16);
+    DevBuf io(ctx);
+    CK(io.alloc(ar.total), "lattice-sum buffers");
+    void* b = io.p;
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(ar.at<void>(b, oK), kpars, nk * 16, cudaMemcpyHostToDevice, st), "copy");
+    if (!S.R.empty())
+        CK(cudaMemcpyAsync(ar.at<void>(b, oR), S.R.data(), S.R.size() * 16, cudaMemcpyHostToDevice, st), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oG), S.G.data(), S.G.size() * 16, cudaMemcpyHostToDevice, st), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oN), S.norm.data(), T * 8, cudaMemcpyHostToDevice, st), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oRf), S.reflection.data(), T * 8, cudaMemcpyHostToDevice, st), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oC), S.coef.data(), S.coef.size() * 16, cudaMemcpyHostToDevice, st), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oP), S.pref.data(), T * 16, cudaMemcpyHostToDevice, st), "copy");
+    CK(cudaMemsetAsync(ctx->d_status, 0, 4, st), "status");
+    double2* tab = ar.at<double2>(b, oTab);
+    const double2 kd = make_double2(k[0], k[1]);
+    if (!S.R.empty()) {
+        launch_real_table_ck(lmax_sum, kd, S.eta, (int)S.R.size(), ar.at<double2>(b, oR), S.sx, S.sy, S.sz,
+                             ar.at<double>(b, oN), ar.at<double>(b, oRf), tab, st);
+        ++ctx->launches;
+    }
+    LatticeSumCkArgs a;
+    a.lsum = lmax_sum;
+    a.k = kd;
+    a.eta = S.eta;
+    a.NR = (int)S.R.size();
+    a.R = ar.at<double2>(b, oR);
+    a.realtab = tab;
+    a.NG = (int)S.G.size();
+    a.G = ar.at<double2>(b, oG);
+    a.coef = ar.at<double2>(b, oC);
+    a.pref = ar.at<double2>(b, oP);
+    a.self0 = S.at_origin ? S.self0 : make_double2(0.0, 0.0);
+    a.sx = S.sx;
+    a.sy = S.sy;
+    a.R0x = S.R0x;
+    a.R0y = S.R0y;
+    a.J = S.J;
+    a.t = make_double2(S.t.real(), S.t.imag());
+    const std::complex<double> ksq = kc * kc;
+    a.ksq = make_double2(ksq.real(), ksq.imag());
+    // the outgoing sheets of the split (lattice/sheets.rs): arg (k eta)^2 = arg k^2 for a real eta
+    a.turn = std::arg(ksq);
+    const double angle = std::fabs(a.turn) + 0.5;
+    a.has_near = angle < M_PI / 2 ? 1 : 0;
+    a.near = a.has_near ? std::pow(std::tan(angle), 2) : 0.0;
+    a.nk = (int)nk;
+    a.kpar = ar.at<double2>(b, oK);
+    a.out = ar.at<double2>(b, oO);
+    a.ldo = T;
+    a.status = ctx->d_status;
+    launch_lattice_sum_ck(a, (int)std::min<size_t>(nk, 148 * 8), st);
+    ++ctx->launches;
+    int stw = 0;
+    CK(cudaMemcpyAsync(&stw, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, st), "status");
+    if ((s = sync_status(ctx, "lattice sums"))) return s;
+    if (stw == 9)
+        return fail(TCU_INVALID_INPUT, "lattice sum is at a diffraction threshold; supply a limiting complex wavenumber");
+    if (stw) return fail(TCU_DEVICE_ERROR, "lattice sums: device status " + std::to_string(stw));
+    CK(cudaMemcpyAsync(out, ar.at<void>(b, oO), nk * T * 16, cudaMemcpyDeviceToHost, st), "copy");
+    return sync_status(ctx, "lattice sums");
 }
 
 extern "C" tcu_status tcu_array_solve_batch(tcu_context* ctx, int lmax, double k0, double radius, const double* eps,

@@ -6,8 +6,9 @@
 // computes x = C A'^-1 (R b).
 //
 // Kernels: row maxima over column chunks (threads over rows, coalesced column reads, one
-// partial per (row, chunk)) reduced in a fixed order; column maxima of R A (CTA per column);
-// one in-place scaling pass. Three passes over the matrix: HBM-bound.
+// partial per (row, chunk)) reduced in a fixed order; column maxima of R A (a warp per four
+// columns of the magnitude mirror below); one in-place scaling pass (threads over rows, column
+// chunks). HBM-bound.
 //
 // Then the balancing sweeps of linalg/mod.rs:229-310 (Sinkhorn and Knopp: unit magnitude sums
 // determine the scaled operator, whatever the units): every column factor y_j, then every row
@@ -103,16 +104,22 @@ __global__ void col_scale(const C* __restrict__ A, int n, const double* __restri
     if (threadIdx.x == 0) c[j] = sh[0] > 0.0 ? exp2(-rint(log2(sh[0]))) : 1.0;
 }
 
+// a thread per row over a chunk of columns (the grid of row_max_partial): r_i stays in a
+// register, c_j is a broadcast load, and the column loop keeps several loads in flight
 template <typename C>
 __global__ void apply_scales(C* __restrict__ A, int n, const double* __restrict__ r, const double* __restrict__ c) {
-    const size_t total = (size_t)n * n;
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-        const int i = (int)(t % n), j = (int)(t / n);
-        const double s = r[i] * c[j];
-        C v = A[t];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int per = (n + EQ_CHUNKS - 1) / EQ_CHUNKS;
+    const int j0 = blockIdx.y * per, j1 = min(n, j0 + per);
+    const double ri = r[i];
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+        const double s = ri * c[j];
+        C v = A[(size_t)j * n + i];
         v.x = (decltype(v.x))((double)v.x * s);
         v.y = (decltype(v.y))((double)v.y * s);
-        A[t] = v;
+        A[(size_t)j * n + i] = v;
     }
 }
 
@@ -120,6 +127,40 @@ __global__ void scale_rows_kernel(cplx* __restrict__ v, const double* __restrict
     const size_t total = n * (size_t)ncol;
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x)
         v[t] = cscale(v[t], s[t % n]);
+}
+
+// Column maxima of R A on the mirror (n even): a warp per BAL_COLS columns, two rows per 4-byte
+// word, the row scales loaded once for all of the warp's columns; fixed-order warp reduction.
+constexpr int BAL_COLS = 4;
+__device__ __forceinline__ double lo16(uint32_t v) { return (double)__uint_as_float(v << 16); }
+__device__ __forceinline__ double hi16(uint32_t v) { return (double)__uint_as_float(v & 0xffff0000u); }
+
+__global__ void col_scale_mirror(const uint16_t* __restrict__ Mg, int n, const double* __restrict__ r,
+                                 double* __restrict__ c) {
+    const int lane = threadIdx.x & 31;
+    const int j0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * BAL_COLS;
+    if (j0 >= n) return;
+    const uint32_t* col[BAL_COLS];
+    double m[BAL_COLS];
+#pragma unroll
+    for (int t = 0; t < BAL_COLS; ++t) {
+        col[t] = reinterpret_cast<const uint32_t*>(Mg + (size_t)min(j0 + t, n - 1) * n);
+        m[t] = 0.0;
+    }
+    for (int q = lane; q < n / 2; q += 32) {
+        const double r0 = r[2 * q], r1 = r[2 * q + 1];
+#pragma unroll
+        for (int t = 0; t < BAL_COLS; ++t) {
+            const uint32_t v = col[t][q];
+            m[t] = fmax(m[t], fmax(r0 * lo16(v), r1 * hi16(v)));
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < BAL_COLS; ++t) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) m[t] = fmax(m[t], __shfl_xor_sync(0xffffffffu, m[t], off));
+        if (lane == 0 && j0 + t < n) c[j0 + t] = m[t] > 0.0 ? exp2(-rint(log2(m[t]))) : 1.0;
+    }
 }
 
 // ---- balancing sweeps ---------------------------------------------------------------------
@@ -143,30 +184,42 @@ __device__ __forceinline__ void bal_advance(double& factor, double sum, int* fla
 // The sweeps run on R A C without forming it: |a_ij| r_i c_j with the max scales r, c, read
 // from the bfloat16 mirror M two rows (one 4-byte word; n is even) at a time. Row weights
 // w_i = x_i r_i and column weights cy_j = c_j y_j are kept beside the factors.
-__device__ __forceinline__ double lo16(uint32_t v) { return (double)__uint_as_float(v << 16); }
-__device__ __forceinline__ double hi16(uint32_t v) { return (double)__uint_as_float(v & 0xffff0000u); }
 
-// column sums: a warp per column, fixed-order warp reduction
+// column sums: a warp per BAL_COLS columns (the row weights loaded once for all of them),
+// fixed-order warp reduction per column
 __global__ void bal_col_kernel(const uint16_t* __restrict__ Mg, int n, const double* __restrict__ w,
                                const double* __restrict__ c, double* __restrict__ y, double* __restrict__ cy,
                                int* flags) {
     const int lane = threadIdx.x & 31;
-    const int j = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (j >= n) return;
-    const uint32_t* col = reinterpret_cast<const uint32_t*>(Mg + (size_t)j * n);
-    double s = 0.0;
+    const int j0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * BAL_COLS;
+    if (j0 >= n) return;
+    const uint32_t* col[BAL_COLS];
+    double s[BAL_COLS];
+#pragma unroll
+    for (int t = 0; t < BAL_COLS; ++t) {
+        col[t] = reinterpret_cast<const uint32_t*>(Mg + (size_t)min(j0 + t, n - 1) * n);
+        s[t] = 0.0;
+    }
     for (int q = lane; q < n / 2; q += 32) {
-        const uint32_t v = col[q];
-        s = fma(w[2 * q], lo16(v), s);
-        s = fma(w[2 * q + 1], hi16(v), s);
+        const double w0 = w[2 * q], w1 = w[2 * q + 1];
+#pragma unroll
+        for (int t = 0; t < BAL_COLS; ++t) {
+            const uint32_t v = col[t][q];
+            s[t] = fma(w0, lo16(v), s[t]);
+            s[t] = fma(w1, hi16(v), s[t]);
+        }
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-    if (lane == 0) {
-        double yy = y[j];
-        bal_advance(yy, s * c[j], flags);
-        y[j] = yy;
-        cy[j] = c[j] * yy;
+    for (int t = 0; t < BAL_COLS; ++t) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) s[t] += __shfl_xor_sync(0xffffffffu, s[t], off);
+        const int j = j0 + t;
+        if (lane == 0 && j < n) {
+            double yy = y[j];
+            bal_advance(yy, s[t] * c[j], flags);
+            y[j] = yy;
+            cy[j] = c[j] * yy;
+        }
     }
 }
 
@@ -178,6 +231,7 @@ __global__ void bal_row_partial(const uint16_t* __restrict__ Mg, int n, const do
     const int per = (n + EQ_CHUNKS - 1) / EQ_CHUNKS;
     const int j0 = blockIdx.y * per, j1 = min(n, j0 + per);
     double s0 = 0.0, s1 = 0.0;
+#pragma unroll 8
     for (int j = j0; j < j1; ++j) {
         const uint32_t v = reinterpret_cast<const uint32_t*>(Mg + (size_t)j * n)[i2];
         const double wj = cy[j];
@@ -250,7 +304,7 @@ tcu_status balance_impl(const uint16_t* Mg, int n, double* r, double* c, double*
     int flags = 0, sweep = 0;
     for (; sweep < BAL_SWEEPS; ++sweep) {
         if (cudaMemsetAsync(d_flags, 0, sizeof(int), st) != cudaSuccess) return TCU_DEVICE_ERROR;
-        bal_col_kernel<<<(n + 7) / 8, 256, 0, st>>>(Mg, n, w, c, y, cy, d_flags);
+        bal_col_kernel<<<(n + 8 * BAL_COLS - 1) / (8 * BAL_COLS), 256, 0, st>>>(Mg, n, w, c, y, cy, d_flags);
         bal_row_partial<<<dim3(nb2, EQ_CHUNKS), 256, 0, st>>>(Mg, n, cy, partial);
         bal_row_update<<<nb, 256, 0, st>>>(partial, n, r, x, w, d_flags);
         if (launches) *launches += 3;
@@ -296,12 +350,15 @@ tcu_status equilibrate_impl(C* A, int n, double threshold, double* r, double* c,
     double mx = 0.0;
     for (double v : bm) mx = std::max(mx, v);
     if (!(mx > threshold)) return TCU_OK;  // entries within the spread a unit diagonal tolerates
-    col_scale<uint16_t><<<n, 256, 0, st>>>(mirror, n, r, c);
+    if (n % 2 == 0)
+        col_scale_mirror<<<(n + 8 * BAL_COLS - 1) / (8 * BAL_COLS), 256, 0, st>>>(mirror, n, r, c);
+    else
+        col_scale<uint16_t><<<n, 256, 0, st>>>(mirror, n, r, c);
     if (launches) ++*launches;
     int sweeps = 0;
     const tcu_status s = (n % 2 == 0) ? balance_impl(mirror, n, r, c, partial, &sweeps, st, launches) : TCU_OK;
     if (s) return s;
-    apply_scales<C><<<148 * 16, 256, 0, st>>>(A, n, r, c);  // R A C with the balanced (or max) scales
+    apply_scales<C><<<dim3(nb, EQ_CHUNKS), 256, 0, st>>>(A, n, r, c);  // R A C with the balanced (or max) scales
     if (launches) ++*launches;
     *applied = true;
     return TCU_OK;

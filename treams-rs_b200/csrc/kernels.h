@@ -199,9 +199,12 @@ tcu_status equilibrate(void* A, bool fp32, int n, double threshold, double* r, d
                        bool* applied, cudaStream_t st, long long* launches);
 void scale_rows(cplx* v, const double* s, size_t n, int ncol, cudaStream_t st);
 
-// lattice.cu — 2D lattice sums (in-plane shift) and the batched periodic-array solve
+// lattice.cu — 2D lattice sums (any real shift) and the batched periodic-array solve
 constexpr int LS_MAXL = 14;                // largest degree of a lattice sum
 constexpr int LS_NMAX = LS_MAXL / 2 + 1;   // reciprocal orders n per (l, m) in the plane
+constexpr int LS_FMAX = LS_MAXL + 1;       // reciprocal orders n per (l, m) off the plane
+constexpr int LS_PMAX = LS_MAXL / 2 + 1;   // powers of beta^2 in S_lmn off the plane
+constexpr int LS_TMAX = 64;                // most terms of the t-series of F_(1/2-n)(v, t)
 struct LatticeSumArgs {
     int lsum = 0;                          // degrees l <= lsum, T = (lsum+1)^2 outputs
     double k = 0, eta = 0;
@@ -215,15 +218,51 @@ struct LatticeSumArgs {
     double2 self0{0, 0};                   // self term of l = 0 (zero for a nonzero shift)
     double sx = 0, sy = 0;                 // in-plane shift r' (reciprocal phase e^{-i q.r'})
     double R0x = 0, R0y = 0;               // lattice vector taken off the shift: e^{-i kpar.R0}
+    // shift off the plane (r_z != 0): every order n <= lsum, F'_n from the t-series of
+    // F_(1/2-n)(v, t) with t = (k r_z eta)^2 (J + 1 terms), and S_lmn as a polynomial in beta^2
+    // with coefficients coefz[(lm * LS_PMAX + p) * LS_FMAX + n] (powers of -k r_z folded in)
+    int offplane = 0;
+    int J = 0;
+    double t = 0;
+    const double* coefz = nullptr;
     int nk = 0;
     const double2* kpar = nullptr;
     double2* out = nullptr;                // out[kp * ldo + l*l+l+m]
     size_t ldo = 0;
     int* status = nullptr;                 // 9: a diffraction order on its threshold
 };
-void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, double sx, double sy,
+// lattice_ck.cu — the same sums at a complex wavenumber (Im k >= 0), any shift, real split
+struct LatticeSumCkArgs {
+    int lsum = 0;
+    double2 k{0, 0};
+    double eta = 0;
+    int NR = 0;
+    const double2* R = nullptr;
+    const double2* realtab = nullptr;      // NR x T real-space terms
+    int NG = 0;
+    const double2* G = nullptr;
+    const double2* coef = nullptr;         // T x LS_PMAX x LS_FMAX: S_lmn coefficient of beta^(2p), order n
+    const double2* pref = nullptr;         // T reciprocal prefactors (1/k^2 included)
+    double2 self0{0, 0};
+    double sx = 0, sy = 0, R0x = 0, R0y = 0;
+    int J = 0;                             // t-series terms (0 in the plane)
+    double2 t{0, 0};                       // (k r_z eta)^2
+    double2 ksq{0, 0};                     // k^2
+    double turn = 0, near = 0;             // sheet split: arg (k eta)^2, tan^2 of the near sector
+    int has_near = 0;
+    int nk = 0;
+    const double2* kpar = nullptr;
+    double2* out = nullptr;
+    size_t ldo = 0;
+    int* status = nullptr;                 // 9: a diffraction order on its threshold
+};
+void launch_real_table_ck(int lsum, double2 k, double eta, int NR, const double2* R, double sx, double sy, double sz,
+                          const double* norm, const double* reflection, double2* tab, cudaStream_t st);
+size_t lattice_sum_ck_smem(int lsum, int NR);
+void launch_lattice_sum_ck(const LatticeSumCkArgs& a, int grid, cudaStream_t st);
+void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, double sx, double sy, double sz,
                        const double* norm, const double* reflection, double2* tab, cudaStream_t st);
-size_t lattice_sum_smem(int lsum, int NR);
+size_t lattice_sum_smem(int lsum, int NR, bool offplane);
 void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st);
 void launch_array_solve(const DevPlan& P, const double2* D, size_t ldd, const double* norm, const double2* Tm, int nk,
                         double2* X, int* status, int grid, cudaStream_t st);

@@ -1,5 +1,5 @@
-// 2D Ewald lattice sums of outgoing spherical waves at an in-plane shift r (real wavenumber,
-// real split) and the batched periodic-array solve X = (I - T S)^-1 T (one sphere per cell).
+// 2D Ewald lattice sums of outgoing spherical waves at a shift r (real wavenumber, real split)
+// and the batched periodic-array solve X = (I - T S)^-1 T (one sphere per cell).
 //
 // D_lm(k, kpar, r) = sum'_R h_l(k|r+R|) Y_lm(-r-R) e^{i kpar.R} (lattice/mod.rs:11-15), with r
 // first reduced into the cell (r' = r - R0, a factor e^{-i kpar.R0}; lattice/ewald.rs:610-665), is
@@ -11,7 +11,10 @@
 //               az = (q_x +- i q_y)/k, times e^{-i q.r'}             (lattice/reciprocal.rs:288-334)
 //   self term   at l = 0, for r' = 0 only                            (lattice/reciprocal.rs:467-487)
 // In the lattice plane only the n with s = 2n of S_lmn survive, so l - |m| odd sums vanish and
-// n runs to (l - |m|)/2 (reciprocal.rs:22-60).
+// n runs to (l - |m|)/2 (reciprocal.rs:22-60). Off the plane (r_z != 0) n runs to l - |m|,
+// S_lmn = sum_s (-k r_z)^(2n-s) beta^(l-|m|-s) / ((2n-s)! (s-n)! ((l+|m|-s)/2)! ((l-|m|-s)/2)!)
+// over n <= s <= min(l - |m|, 2n) with l - |m| - s even, and F_(1/2-n)(v, 0) becomes
+// F_(1/2-n)(v, t) = sum_j (t/2)^j / j! F_(1/2-n-j)(v, 0), t = (k r_z eta)^2 (reduced.rs:223).
 //
 // Device layout: the real-space terms do not depend on the Bloch vector, so one launch
 // tabulates Treal (NR x T complex, T = (lsum+1)^2) for the lattice points within the cutoff,
@@ -78,7 +81,7 @@ __device__ double scaled_gamma_low(double d, double a) {
 // One warp per lattice point: Treal_lm(R) for every l <= lsum, |m| <= l.
 __global__ void __launch_bounds__(128) real_table_kernel(int lsum, double k, double eta, int NR,
                                                          const double2* __restrict__ R, double sx, double sy,
-                                                         const double* __restrict__ norm,
+                                                         double sz, const double* __restrict__ norm,
                                                          const double* __restrict__ reflection,
                                                          double2* __restrict__ tab) {
     __shared__ double ladder[4][LS_LADDER];
@@ -90,7 +93,7 @@ __global__ void __launch_bounds__(128) real_table_kernel(int lsum, double k, dou
     const int T = (lsum + 1) * (lsum + 1);
     const double2 p = R[r];
     double dist, u[3];
-    unit_direction(-p.x - sx, -p.y - sy, 0.0, dist, u);  // rho = -r' - R
+    unit_direction(-p.x - sx, -p.y - sy, -sz, dist, u);  // rho = -r' - R
     const double a = 0.5 * (k * dist * eta) * (k * dist * eta), c = 0.5 / (eta * eta);
     // ladder[i] = R(lsum + 1/2 - i)
     const int nlad = lsum + 1 + LS_JMAX;
@@ -163,16 +166,61 @@ __device__ void reduced_limits(int nmax, double v, double eta, cplx* out) {
     }
 }
 
+// F_(1/2-n)(v, 0) on the lower side of the cut, real v != 0 (the terms of reduced_limits
+// without the factor (2 eta^2)^n / (sqrt 2 eta))
+__device__ cplx reduced_limit(int n, double v) {
+    if (v < 0.0) {
+        const double y = -v, b = 0.5 - n;
+        double s = 0.0, term = 1.0;
+        for (int kk = 0; kk < 200; ++kk) {
+            if (kk > 0) term *= y / kk;
+            double add = term / (b + kk);
+            s += add;
+            if (kk > y && fabs(add) < 1e-18 * fabs(s)) break;
+        }
+        return mk(tgamma(b) * pow(y, -b), (n & 1) ? -s : s);
+    }
+    double rr = scaled_gamma_low(0.5 - n, v);
+    if (n == 0 && v >= 2.0) rr = 1.7724538509055160273 * erfc(sqrt(v)) / sqrt(v);
+    return mk(0.0, (n & 1) ? rr : -rr);  // -i (-1)^n R
+}
+
+// Off the lattice plane (lattice/reduced.rs:223): F'_n = (2 eta^2)^n / (sqrt 2 eta) F_(1/2-n)(v, t)
+// with F_(1/2-n)(v, t) = sum_j (t/2)^j / j! F_(1/2-n-j)(v, 0), j = 0..J (tw[j] = (t/2)^j / j!),
+// n = 0..nmax. Each limit is evaluated once and added to every n it reaches, in increasing j.
+__device__ void reduced_shifted(int nmax, int J, const double* tw, double v, double eta, cplx* out) {
+    for (int n = 0; n <= nmax; ++n) out[n] = mk(0.0, 0.0);
+    for (int i = 0; i <= nmax + J; ++i) {
+        const cplx L = reduced_limit(i, v);
+        for (int n = min(nmax, i); n >= max(0, i - J); --n) cfma(out[n], mk(tw[i - n], 0.0), L);
+    }
+    double factor = 1.0 / (1.4142135623730950488 * eta);
+    const double step = 2.0 * eta * eta;
+    for (int n = 0; n <= nmax; ++n) {
+        out[n] = cscale(out[n], factor);
+        factor *= step;
+    }
+}
+
 // One CTA per Bloch vector. smem: phases NR double2, chunk arrays.
 __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
     extern __shared__ double2 ls_smem[];
+    __shared__ double tw[LS_TMAX + 1];                   // (t/2)^j / j! off the plane
+    const int nF = A.offplane ? A.lsum + 1 : A.lsum / 2 + 1;  // orders n kept per point
     double2* ph = ls_smem;                               // NR
-    double2* gF = ph + A.NR;                             // LS_CHUNK * (nmax + 1)
-    double2* gaz = gF + LS_CHUNK * (A.lsum / 2 + 1);     // LS_CHUNK
+    double2* gF = ph + A.NR;                             // LS_CHUNK * nF
+    double2* gaz = gF + LS_CHUNK * nF;                   // LS_CHUNK
     double2* gph = gaz + LS_CHUNK;                       // LS_CHUNK: e^{-i q.r'}
     double* gb2 = (double*)(gph + LS_CHUNK);             // LS_CHUNK
-    const int T = (A.lsum + 1) * (A.lsum + 1), nmax = A.lsum / 2;
+    const int T = (A.lsum + 1) * (A.lsum + 1), nmax = nF - 1;
     const int tid = threadIdx.x;
+    if (A.offplane && tid == 0) {
+        double w = 1.0;
+        for (int j = 0; j <= A.J; ++j) {
+            if (j > 0) w *= 0.5 * A.t / j;
+            tw[j] = w;
+        }
+    }
     for (int kp = blockIdx.x; kp < A.nk; kp += gridDim.x) {
         const double2 kpar = A.kpar[kp];
         for (int r = tid; r < A.NR; r += blockDim.x) {
@@ -204,9 +252,11 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
                 double v = (b2 - 1.0) / (2.0 * A.eta * A.eta);
                 if (fabs(v) <= 1e-14) {
                     atomicExch(A.status, 9);  // on a diffraction threshold (reciprocal.rs:236-241)
-                    for (int n = 0; n <= nmax; ++n) gF[tid * (nmax + 1) + n] = mk(0.0, 0.0);
+                    for (int n = 0; n <= nmax; ++n) gF[tid * nF + n] = mk(0.0, 0.0);
+                } else if (A.offplane) {
+                    reduced_shifted(nmax, A.J, tw, v, A.eta, gF + tid * nF);
                 } else {
-                    reduced_limits(nmax, v, A.eta, gF + tid * (nmax + 1));
+                    reduced_limits(nmax, v, A.eta, gF + tid * nF);
                 }
                 gb2[tid] = b2;
                 gaz[tid] = mk(qx / A.k, qy / A.k);
@@ -215,17 +265,28 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
                 gph[tid] = mk(pc, ps);
             }
             __syncthreads();
-            if (active && even) {
+            if (active && (even || A.offplane)) {
                 const int nm = (l - am) / 2;
                 const double* coef = A.coef + (size_t)lm * LS_NMAX;
                 const int cnt = min(LS_CHUNK, A.NG - g0);
                 for (int t = 0; t < cnt; ++t) {
                     const double b2 = gb2[t];
-                    const double2* F = gF + t * (nmax + 1);
+                    const double2* F = gF + t * nF;
                     cplx s = mk(0.0, 0.0);
-                    for (int n = 0; n <= nm; ++n) {  // Horner in beta^2
-                        s = cscale(s, b2);
-                        cfma(s, mk(coef[n], 0.0), F[n]);
+                    if (A.offplane) {
+                        // Horner in beta^2 over p = (l - |m| - s)/2; the orders n with n <= s <= 2n
+                        const double* cz = A.coefz + (size_t)lm * LS_PMAX * LS_FMAX;
+                        for (int p = (l - am) / 2; p >= 0; --p) {
+                            s = cscale(s, b2);
+                            const int sidx = l - am - 2 * p;
+                            for (int n = (sidx + 1) / 2; n <= sidx; ++n)
+                                cfma(s, mk(cz[p * LS_FMAX + n], 0.0), F[n]);
+                        }
+                    } else {
+                        for (int n = 0; n <= nm; ++n) {  // Horner in beta^2
+                            s = cscale(s, b2);
+                            cfma(s, mk(coef[n], 0.0), F[n]);
+                        }
                     }
                     cplx az = gaz[t];
                     if (m < 0) az.y = -az.y;
@@ -498,19 +559,20 @@ __global__ void __launch_bounds__(384, 1) array_solve_kernel(DevPlan P, const do
 
 }  // namespace
 
-void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, double sx, double sy,
+void launch_real_table(int lsum, double k, double eta, int NR, const double2* R, double sx, double sy, double sz,
                        const double* norm, const double* reflection, double2* tab, cudaStream_t st) {
     StageScope sc(ST_LATTICE, st);
-    real_table_kernel<<<(NR + 3) / 4, 128, 0, st>>>(lsum, k, eta, NR, R, sx, sy, norm, reflection, tab);
+    real_table_kernel<<<(NR + 3) / 4, 128, 0, st>>>(lsum, k, eta, NR, R, sx, sy, sz, norm, reflection, tab);
 }
 
-size_t lattice_sum_smem(int lsum, int NR) {
-    return (size_t)NR * 16 + (size_t)LS_CHUNK * (lsum / 2 + 1) * 16 + 2 * LS_CHUNK * 16 + LS_CHUNK * 8;
+size_t lattice_sum_smem(int lsum, int NR, bool offplane) {
+    const size_t nF = offplane ? lsum + 1 : lsum / 2 + 1;
+    return (size_t)NR * 16 + (size_t)LS_CHUNK * nF * 16 + 2 * LS_CHUNK * 16 + LS_CHUNK * 8;
 }
 
 void launch_lattice_sum(const LatticeSumArgs& a, int grid, cudaStream_t st) {
     StageScope sc(ST_LATTICE, st);
-    size_t smem = lattice_sum_smem(a.lsum, a.NR);
+    size_t smem = lattice_sum_smem(a.lsum, a.NR, a.offplane != 0);
     cudaFuncSetAttribute(lattice_sum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     lattice_sum_kernel<<<grid, 256, smem, st>>>(a);
 }

@@ -8,7 +8,8 @@ from ._lib import _check, _p, default_context, lib
 
 def lsumsw2d_batch(lmax_sum: int, k: float, lattice, kpars, eta: float = 0.0, shift=None, ctx=None) -> np.ndarray:
     """D_lm(k, kpar, r) for every l <= lmax_sum (table index l*l+l+m) and every Bloch vector
-    (nk, 2) (lattice.lsumsw2d, lattice::sum); shift r in the lattice plane (default 0)."""
+    (nk, 2) (lattice.lsumsw2d, lattice::sum) at a shift r (default 0; off the plane while
+    (k r_z eta)^2 <= 16)."""
     ctx = ctx or default_context()
     a = np.ascontiguousarray(lattice, np.float64).reshape(2, 2)
     kp = np.ascontiguousarray(kpars, np.float64).reshape(-1, 2)
