@@ -279,6 +279,12 @@ def periodic_workload(ctx, stream, nk: int = 4096, with_cpu: bool = True, fp64_p
 
     w = workloads.periodic_array(nk=nk)
     tl.array_solve_batch(w.lmax, w.k0, w.radius, w.eps, w.lattice, w.kpars[:8], ctx=ctx)  # warm-up
+    # the same Bloch vectors at a shift off the lattice plane, and in a lossy embedding (complex k)
+    shift = (0.1 * w.period, 0.2 * w.period, 0.3 * w.period)
+    tl.lsumsw2d_batch(12, w.k0 * (1 + 0.05j), w.lattice, w.kpars[:8], shift=shift, ctx=ctx)  # warm-up
+    _, ms_off, _ = _timed(stream, lambda: tl.lsumsw2d_batch(12, w.k0, w.lattice, w.kpars, shift=shift, ctx=ctx))
+    _, ms_ck, _ = _timed(stream, lambda: tl.lsumsw2d_batch(12, w.k0 * (1 + 0.05j), w.lattice, w.kpars, shift=shift,
+                                                           ctx=ctx))
     ctx.reset_stage_times()
     ctx.set_profiling(True)
     _, ms_sums, _ = _timed(stream, lambda: tl.lsumsw2d_batch(12, w.k0, w.lattice, w.kpars, ctx=ctx))
@@ -291,6 +297,8 @@ def periodic_workload(ctx, stream, nk: int = 4096, with_cpu: bool = True, fp64_p
     flops = nk * 8.0 * 96 ** 3
     out = {"workload": f"periodic array: period {w.period:.4f}, lmax 6, {nk} Bloch vectors", "unit": "kpar/s",
            "lattice_sums_e2e_ms": ms_sums, "array_solve_e2e_ms": ms_all,
+           "lattice_sums_off_plane_e2e_ms": ms_off, "lattice_sums_complex_k_off_plane_e2e_ms": ms_ck,
+           "lattice_sums_variants": "degrees <= 12 at the shift (0.1, 0.2, 0.3) periods, real k0 and k0 (1 + 0.05i)",
            "array_solve_e2e_value": nk / (ms_all / 1e3),
            "stages_ms": {k: v[1] for k, v in st.items()},
            "array_kernel_fp64_tflops": flops / (lu_ms / 1e3) / 1e12 if lu_ms else None,

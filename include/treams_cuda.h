@@ -294,7 +294,8 @@ tcu_status tcu_lsumsw2d_batch(tcu_context* ctx, int lmax_sum, double k, const do
  * sum'_R h_l(k|r+R|) Y_lm(-r-R) e^{i kpar.R}, the in-plane part of r reduced into the cell on
  * the host (lattice/ewald.rs:610-665). Off the lattice plane (r[2] != 0) the reciprocal part
  * takes every order of S_lmn and the t-series of F_(1/2-n)(v, t) (lattice/reciprocal.rs:22-60,
- * lattice/reduced.rs:223); shifts with (k r_z eta)^2 > 16 are rejected (TCU_INVALID_INPUT). */
+ * lattice/reduced.rs:223) with the split capped at |k r_z eta| <= 1 down to eta = 1/4 (the sum does
+ * not depend on it); shifts with (k r_z eta)^2 > 16 at that split are rejected (TCU_INVALID_INPUT). */
 tcu_status tcu_lsumsw2d_shift_batch(tcu_context* ctx, int lmax_sum, double k, const double* lattice, size_t nk,
                                     const double* kpars, const double* shift, double eta, double* out);
 /* The same sums at a complex wavenumber k = k[0] + i k[1] (a lossy embedding; lattice::sum takes

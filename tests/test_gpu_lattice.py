@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 import oracle
+from conftest import read_table
 from treams_b200 import lattice as tl
 from treams_b200 import workloads
 
@@ -149,7 +150,55 @@ def test_off_plane_sums_do_not_depend_on_the_split(ctx):
 
 
 def test_shifted_sums_reject_shifts_far_off_the_plane(ctx):
-    # (k r_z eta)^2 <= 16 keeps the alternating t-series within FP64 accuracy
+    # off the plane the split is capped at |k r_z eta| <= 1 down to eta = 1/4 (1/(2 eta^2) <= 8);
+    # beyond (k r_z eta)^2 = 16 the alternating t-series would lose FP64 accuracy: k r_z = 20 is rejected
     lat = np.eye(2)
     with pytest.raises(ValueError, match="off the lattice plane"):
-        tl.lsumsw2d_batch(2, 2.0, lat, [[0.1, 0.2]], shift=(0.1, 0.0, 4.0), ctx=ctx)
+        tl.lsumsw2d_batch(2, 2.0, lat, [[0.1, 0.2]], shift=(0.1, 0.0, 10.0), ctx=ctx)
+
+
+@pytest.mark.parametrize("k", [2.7 + 0.4j, 1.5 + 0.05j])
+@pytest.mark.parametrize("shift", [(0.0, 0.0, 0.0), (0.3, 0.1, 0.25), (0.2, -0.1, 0.0), (1.9, -2.2, -0.4)])
+def test_complex_wavenumber_lattice_sums_match_oracle(ctx, k, shift):
+    # a lossy embedding (lattice::sum at complex k, lattice/mod.rs:283): every diffraction order on
+    # its outgoing sheet (lattice/sheets.rs); the device takes a real split, the oracle its automatic
+    # complex one, and the sums do not depend on the split
+    lat = np.array([[1.0, 0.0], [0.3, 0.9]])
+    kps = np.array([[0.4, -0.7], [1.1, 0.4], [0.0, 0.0]])
+    D = tl.lsumsw2d_batch(8, k, lat, kps, shift=shift, ctx=ctx)
+    for i, kp in enumerate(kps):
+        ref = oracle.lsumsw2d_table(8, k, lat, kp, r=shift)
+        assert np.max(np.abs(D[i] - ref)) <= 1e-11 * max(1.0, np.max(np.abs(ref))), (k, shift, i)
+
+
+def _golden_full_rows():
+    rows = []
+    for key, val in read_table("lattice_sums_2d.txt"):
+        (_, l, m, dim, kr, ki, x, y, z, er, ei, a11, a12, a21, a22, b1, b2, part, jet, tol) = key
+        k = complex(float(kr), float(ki))
+        if part != "full" or float(ei) != 0.0 or not (k.real > 0 and 0 <= k.imag <= k.real / 2):
+            continue
+        rows.append(dict(l=int(l), m=int(m), k=k, r=[float(x), float(y), float(z)], eta=float(er),
+                         lattice=[[float(a11), float(a12)], [float(a21), float(a22)]], kpar=[float(b1), float(b2)],
+                         ref=complex(float(val[0]), float(val[1]))))
+    return rows
+
+
+def test_lattice_sums_match_reference_tables_on_the_device(ctx):
+    # every 2D spherical full-sum row of the reference's high-precision table that the device path
+    # takes (real split; Re k > 0, 0 <= Im k <= Re k / 2): complex k off the plane (image sums at 30
+    # digits) and real k next to diffraction thresholds (spectral sums), lattice/mod.rs:283.
+    # Tolerance 1e-11 * max(|S|, 1); 5e-11 for the rows next to thresholds of orders whose q
+    # carries the rounding of its binary64 reciprocal vector (their references use exact ones).
+    rows = _golden_full_rows()
+    assert len(rows) >= 20
+    for r in rows:
+        D = tl.lsumsw2d_batch(r["l"], r["k"], r["lattice"], [r["kpar"]], eta=r["eta"], shift=r["r"], ctx=ctx)
+        v = D[0, r["l"] * r["l"] + r["l"] + r["m"]]
+        tol = 5e-11 if r["k"].real in (6.303111309241046, 3.6954825016513464) else 1e-11
+        assert abs(v - r["ref"]) <= tol * max(1.0, abs(r["ref"])), (r, v)
+
+
+def test_complex_wavenumber_sums_reject_strong_losses(ctx):
+    with pytest.raises(ValueError, match="Im k"):
+        tl.lsumsw2d_batch(2, 2.0 + 1.5j, np.eye(2), [[0.1, 0.2]], ctx=ctx)

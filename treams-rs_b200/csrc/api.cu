@@ -1530,6 +1530,9 @@ tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const
         double kl = k * std::sqrt(S.area);
         eta = std::sqrt(2.0 * M_PI) / kl * std::max(kl / 8.0, 1.0);
     }
+    // Off the plane the t-series cancels to about e^(-|t|/2) of its largest term, so the split is
+    // capped at |t| = (k r_z eta)^2 <= 1 where 1/(2 eta^2) <= 8 allows (the sum does not depend on it)
+    if (shift && shift[2] != 0.0) eta = std::min(eta, std::max(0.25, 1.0 / std::fabs(k * shift[2])));
     const double c = 0.5 / (eta * eta);
     if (c > 8.0)
         return fail(TCU_INVALID_INPUT,
@@ -1836,6 +1839,8 @@ tcu_status lattice_setup_ck(int lsum, std::complex<double> k, const double* lat,
         double kl = kabs * std::sqrt(S.area);
         eta = std::sqrt(2.0 * M_PI) / kl * std::max(kl / 8.0, 1.0);
     }
+    // off the plane the split is capped at |k r_z eta| <= 1 where 1/(2 eta^2) <= 8 allows
+    if (shift[2] != 0.0) eta = std::min(eta, std::max(0.25, 1.0 / (kabs * std::fabs(shift[2]))));
     const double c = 0.5 / (eta * eta);
     if (c > 8.0)
         return fail(TCU_INVALID_INPUT,

@@ -65,6 +65,18 @@ TCU_HD cplx cexpz(cplx z) {
     return mk(e * c, e * s);
 }
 
+// q.q - k^2 for real q = (qx, qy) and k, with the three products and the sums compensated
+// (error-free transformations: fma for the products, two-sum for the additions): next to a
+// diffraction threshold q.q and k^2 agree in most digits, and the plain difference loses them.
+__device__ __forceinline__ double q2_minus_k2(double qx, double qy, double k) {
+    const double p1 = qx * qx, e1 = fma(qx, qx, -p1);
+    const double p2 = qy * qy, e2 = fma(qy, qy, -p2);
+    const double p3 = k * k, e3 = fma(k, k, -p3);
+    const double s1 = p1 + p2, z1 = s1 - p1, t1 = (p1 - (s1 - z1)) + (p2 - z1);
+    const double s2 = s1 - p3, z2 = s2 - s1, t2 = (s1 - (s2 - z2)) + (-p3 - z2);
+    return s2 + (((t1 + t2) + (e1 + e2)) - e3);
+}
+
 // ---- radial functions -----------------------------------------------------------------
 // Outgoing spherical Hankel functions h_0..h_last at real x > 0. For 0.5 <= x <= 1e4 the
 // upward recurrence h_{p+1} = (2p+1)/x h_p - h_{p-1} from h_-1 = e^{ix}/x, h_0 = -i e^{ix}/x

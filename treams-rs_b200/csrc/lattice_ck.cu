@@ -269,7 +269,9 @@ __global__ void __launch_bounds__(256) lattice_sum_ck_kernel(LatticeSumCkArgs A)
                 const double2 G = A.G[g];
                 const double qx = kpar.x + G.x, qy = kpar.y + G.y, q2 = qx * qx + qy * qy;
                 const cplx b2 = cscale(kinv2, q2);
-                cplx v = cscale(mk(b2.x - 1.0, b2.y), 1.0 / (2.0 * A.eta * A.eta));
+                // v = (q.q - k^2) / (2 eta^2 k^2): Re(q.q - k^2) = (q.q - Re(k)^2) + Im(k)^2 compensated
+                const cplx d = mk(q2_minus_k2(qx, qy, A.k.x) + A.k.y * A.k.y, -2.0 * A.k.x * A.k.y);
+                cplx v = cscale(cmul(d, kinv2), 1.0 / (2.0 * A.eta * A.eta));
                 if (v.y == 0.0) v.y = -0.0;  // lower side (lattice/sheets.rs:12-17)
                 if (hypot(v.x, v.y) <= 1e-14) {
                     atomicExch(A.status, 9);  // on a diffraction threshold (reciprocal.rs:236-241)

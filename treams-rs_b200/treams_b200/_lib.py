@@ -78,6 +78,7 @@ SIGNATURES = {
     "tcu_learned_problem_destroy": (c_int, [P]),
     "tcu_lsumsw2d_batch": (c_int, [P, c_int, c_double, P, c_size, P, c_double, P]),
     "tcu_lsumsw2d_shift_batch": (c_int, [P, c_int, c_double, P, c_size, P, P, c_double, P]),
+    "tcu_lsumsw2d_complex_batch": (c_int, [P, c_int, P, P, c_size, P, P, c_double, P]),
     "tcu_array_solve_batch": (c_int, [P, c_int, c_double, c_double, P, P, c_size, P, c_double, P]),
 }
 
