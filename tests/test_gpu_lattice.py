@@ -180,23 +180,22 @@ def _golden_full_rows():
             continue
         rows.append(dict(l=int(l), m=int(m), k=k, r=[float(x), float(y), float(z)], eta=float(er),
                          lattice=[[float(a11), float(a12)], [float(a21), float(a22)]], kpar=[float(b1), float(b2)],
-                         ref=complex(float(val[0]), float(val[1]))))
+                         tol=float(tol), ref=complex(float(val[0]), float(val[1]))))
     return rows
 
 
 def test_lattice_sums_match_reference_tables_on_the_device(ctx):
     # every 2D spherical full-sum row of the reference's high-precision table that the device path
     # takes (real split; Re k > 0, 0 <= Im k <= Re k / 2): complex k off the plane (image sums at 30
-    # digits) and real k next to diffraction thresholds (spectral sums), lattice/mod.rs:283.
-    # Tolerance 1e-11 * max(|S|, 1); 5e-11 for the rows next to thresholds of orders whose q
-    # carries the rounding of its binary64 reciprocal vector (their references use exact ones).
+    # digits) and real k next to diffraction thresholds (spectral sums; q.q - k^2 from compensated
+    # products with reciprocal vectors to twice FP64 precision), lattice/mod.rs:283.
+    # Tolerance max(the row's own, 1e-12) * max(|S|, 1); the rows' own are 1e-14 to 1e-12.
     rows = _golden_full_rows()
     assert len(rows) >= 20
     for r in rows:
         D = tl.lsumsw2d_batch(r["l"], r["k"], r["lattice"], [r["kpar"]], eta=r["eta"], shift=r["r"], ctx=ctx)
         v = D[0, r["l"] * r["l"] + r["l"] + r["m"]]
-        tol = 5e-11 if r["k"].real in (6.303111309241046, 3.6954825016513464) else 1e-11
-        assert abs(v - r["ref"]) <= tol * max(1.0, abs(r["ref"])), (r, v)
+        assert abs(v - r["ref"]) <= max(r["tol"], 1e-12) * max(1.0, abs(r["ref"])), (r, v)
 
 
 def test_complex_wavenumber_sums_reject_strong_losses(ctx):

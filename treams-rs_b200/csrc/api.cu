@@ -1499,6 +1499,47 @@ double log_fact(int n) { return std::lgamma((double)n + 1.0); }
 
 // Host-side set-up of one batch of lattice sums: split, lattice points within the real-space
 // cutoff, reciprocal vectors within the reciprocal cutoff, and the per-(l, m) constants.
+// Double-double arithmetic (Dekker's two-product via fma, Knuth's two-sum; Bailey's division) for
+// the reciprocal lattice vectors: next to a diffraction threshold q.q - k^2 resolves digits that a
+// binary64 reciprocal vector b = 2 pi a / det rounds away.
+struct DD {
+    double hi, lo;
+};
+DD dd_two_sum(double a, double b) {
+    const double s = a + b, z = s - a;
+    return {s, (a - (s - z)) + (b - z)};
+}
+DD dd_norm(double hi, double lo) {
+    const double s = hi + lo;
+    return {s, lo - (s - hi)};
+}
+DD dd_add(DD a, DD b) {
+    const DD s = dd_two_sum(a.hi, b.hi);
+    return dd_norm(s.hi, s.lo + a.lo + b.lo);
+}
+DD dd_mul(DD a, double b) {
+    const double p = a.hi * b;
+    return dd_norm(p, std::fma(a.hi, b, -p) + a.lo * b);
+}
+DD dd_div(DD a, DD b) {
+    const double q1 = a.hi / b.hi;
+    const DD r = dd_add(a, dd_mul(b, -q1));
+    const double q2 = r.hi / b.hi;
+    const DD r2 = dd_add(r, dd_mul(b, -q2));
+    return dd_add(dd_two_sum(q1, q2), DD{r2.hi / b.hi, 0.0});
+}
+// reciprocal vectors b1 = 2 pi (a2y, -a2x)/det, b2 = 2 pi (-a1y, a1x)/det of the binary64 lattice
+void reciprocal_dd(const double* lat, DD b[2][2]) {
+    const DD twopi{6.283185307179586, 2.4492935982947064e-16};
+    const DD p = dd_two_sum(lat[0] * lat[3], 0.0), q = dd_two_sum(lat[1] * lat[2], 0.0);
+    const DD det = dd_add(dd_add(p, DD{std::fma(lat[0], lat[3], -p.hi), 0.0}),
+                          dd_mul(dd_add(q, DD{std::fma(lat[1], lat[2], -q.hi), 0.0}), -1.0));
+    b[0][0] = dd_div(dd_mul(twopi, lat[3]), det);
+    b[0][1] = dd_div(dd_mul(twopi, -lat[2]), det);
+    b[1][0] = dd_div(dd_mul(twopi, -lat[1]), det);
+    b[1][1] = dd_div(dd_mul(twopi, lat[0]), det);
+}
+
 struct LatticeSetup {
     double eta = 0, area = 0;
     double sx = 0, sy = 0;      // in-plane shift reduced into the cell, r' = r - R0
@@ -1507,7 +1548,7 @@ struct LatticeSetup {
     bool at_origin = true;      // r' = 0: the self term, and no R = 0 real-space term
     double t = 0;               // (k r_z eta)^2 of the t-series off the plane
     int J = 0;                  // its last term
-    std::vector<double2> R, G;
+    std::vector<double2> R, G, Glo;  // Glo: low parts of the reciprocal vectors
     std::vector<double> norm, reflection, coef, coefz;
     std::vector<double2> pref;
     double2 self0{0, 0};
@@ -1605,12 +1646,18 @@ tcu_status lattice_setup(int lsum, double k, const double* lat, size_t nk, const
     const double hrec = (4 * M_PI * M_PI / S.area) / std::max(blen1, blen2);
     long Nr = (long)std::ceil(qc / hrec) + 1;
     if (Nr > 64) return fail(TCU_INVALID_INPUT, "lattice or Bloch vectors out of range for the device lattice sums");
+    DD bdd[2][2];
+    reciprocal_dd(lat, bdd);
     for (long s = 0; s <= Nr; ++s)
         for (long n1 = -s; n1 <= s; ++n1)
             for (long n2 = -s; n2 <= s; ++n2) {
                 if (std::max(std::labs(n1), std::labs(n2)) != s) continue;
-                double x = n1 * b1x + n2 * b2x, y = n1 * b1y + n2 * b2y;
-                if (std::hypot(x, y) <= qc) S.G.push_back(make_double2(x, y));
+                const DD x = dd_add(dd_mul(bdd[0][0], (double)n1), dd_mul(bdd[1][0], (double)n2));
+                const DD y = dd_add(dd_mul(bdd[0][1], (double)n1), dd_mul(bdd[1][1], (double)n2));
+                if (std::hypot(x.hi, y.hi) <= qc) {
+                    S.G.push_back(make_double2(x.hi, y.hi));
+                    S.Glo.push_back(make_double2(x.lo, y.lo));
+                }
             }
     const int T = (lsum + 1) * (lsum + 1);
     S.norm.assign(T, 0.0);
@@ -1675,11 +1722,13 @@ tcu_status lattice_sums_device(tcu_context* ctx, int lsum, double k, const Latti
     Arena ar;
     size_t oR = ar.add(S.R.size() * 16), oG = ar.add(S.G.size() * 16), oN = ar.add(T * 8), oRf = ar.add(T * 8),
            oC = ar.add((size_t)T * LS_NMAX * 8), oP = ar.add(T * 16), oTab = ar.add(S.R.size() * T * 16),
-           oZ = ar.add(S.coefz.size() * 8);
+           oZ = ar.add(S.coefz.size() * 8), oGl = ar.add(S.Glo.size() * 16);
     CK(scratch.alloc(ar.total), "lattice scratch");
     void* b = scratch.p;
     CK(cudaMemcpyAsync(ar.at<void>(b, oR), S.R.data(), S.R.size() * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oG), S.G.data(), S.G.size() * 16, cudaMemcpyHostToDevice, ctx->stream), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oGl), S.Glo.data(), S.Glo.size() * 16, cudaMemcpyHostToDevice, ctx->stream),
+       "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oN), S.norm.data(), T * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oRf), S.reflection.data(), T * 8, cudaMemcpyHostToDevice, ctx->stream), "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oC), S.coef.data(), (size_t)T * LS_NMAX * 8, cudaMemcpyHostToDevice, ctx->stream),
@@ -1703,6 +1752,7 @@ tcu_status lattice_sums_device(tcu_context* ctx, int lsum, double k, const Latti
     a.realtab = tab;
     a.NG = (int)S.G.size();
     a.G = ar.at<double2>(b, oG);
+    a.Glo = ar.at<double2>(b, oGl);
     a.coef = ar.at<double>(b, oC);
     a.pref = ar.at<double2>(b, oP);
     a.self0 = S.at_origin ? S.self0 : make_double2(0.0, 0.0);
@@ -1812,7 +1862,7 @@ struct LatticeSetupCk {
     bool at_origin = true;
     std::complex<double> t{0, 0};
     int J = 0;
-    std::vector<double2> R, G, coef, pref;
+    std::vector<double2> R, G, Glo, coef, pref;
     std::vector<double> norm, reflection;
     double2 self0{0, 0};
 };
@@ -1909,12 +1959,18 @@ tcu_status lattice_setup_ck(int lsum, std::complex<double> k, const double* lat,
     const double hrec = (4 * M_PI * M_PI / S.area) / std::max(blen1, blen2);
     long Nr = (long)std::ceil(qc / hrec) + 1;
     if (Nr > 64) return fail(TCU_INVALID_INPUT, "lattice or Bloch vectors out of range for the device lattice sums");
+    DD bdd[2][2];
+    reciprocal_dd(lat, bdd);
     for (long s = 0; s <= Nr; ++s)
         for (long n1 = -s; n1 <= s; ++n1)
             for (long n2 = -s; n2 <= s; ++n2) {
                 if (std::max(std::labs(n1), std::labs(n2)) != s) continue;
-                double x = n1 * b1x + n2 * b2x, y = n1 * b1y + n2 * b2y;
-                if (std::hypot(x, y) <= qc) S.G.push_back(make_double2(x, y));
+                const DD x = dd_add(dd_mul(bdd[0][0], (double)n1), dd_mul(bdd[1][0], (double)n2));
+                const DD y = dd_add(dd_mul(bdd[0][1], (double)n1), dd_mul(bdd[1][1], (double)n2));
+                if (std::hypot(x.hi, y.hi) <= qc) {
+                    S.G.push_back(make_double2(x.hi, y.hi));
+                    S.Glo.push_back(make_double2(x.lo, y.lo));
+                }
             }
     const int T = (lsum + 1) * (lsum + 1);
     S.norm.assign(T, 0.0);
@@ -1981,7 +2037,7 @@ extern "C" tcu_status tcu_lsumsw2d_complex_batch(tcu_context* ctx, int lmax_sum,
     Arena ar;
     size_t oK = ar.add(nk * 16), oO = ar.add(nk * T * 16), oR = ar.add(S.R.size() * 16), oG = ar.add(S.G.size() * 16),
            oN = ar.add(T * 8), oRf = ar.add(T * 8), oC = ar.add(S.coef.size() * 16), oP = ar.add(T * 16),
-           oTab = ar.add(S.R.size() * T * 16);
+           oTab = ar.add(S.R.size() * T * 16), oGl = ar.add(S.Glo.size() * 16);
     DevBuf io(ctx);
     CK(io.alloc(ar.total), "lattice-sum buffers");
     void* b = io.p;
@@ -1990,6 +2046,7 @@ extern "C" tcu_status tcu_lsumsw2d_complex_batch(tcu_context* ctx, int lmax_sum,
     if (!S.R.empty())
         CK(cudaMemcpyAsync(ar.at<void>(b, oR), S.R.data(), S.R.size() * 16, cudaMemcpyHostToDevice, st), "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oG), S.G.data(), S.G.size() * 16, cudaMemcpyHostToDevice, st), "copy");
+    CK(cudaMemcpyAsync(ar.at<void>(b, oGl), S.Glo.data(), S.Glo.size() * 16, cudaMemcpyHostToDevice, st), "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oN), S.norm.data(), T * 8, cudaMemcpyHostToDevice, st), "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oRf), S.reflection.data(), T * 8, cudaMemcpyHostToDevice, st), "copy");
     CK(cudaMemcpyAsync(ar.at<void>(b, oC), S.coef.data(), S.coef.size() * 16, cudaMemcpyHostToDevice, st), "copy");
@@ -2011,6 +2068,7 @@ extern "C" tcu_status tcu_lsumsw2d_complex_batch(tcu_context* ctx, int lmax_sum,
     a.realtab = tab;
     a.NG = (int)S.G.size();
     a.G = ar.at<double2>(b, oG);
+    a.Glo = ar.at<double2>(b, oGl);
     a.coef = ar.at<double2>(b, oC);
     a.pref = ar.at<double2>(b, oP);
     a.self0 = S.at_origin ? S.self0 : make_double2(0.0, 0.0);

@@ -65,16 +65,24 @@ TCU_HD cplx cexpz(cplx z) {
     return mk(e * c, e * s);
 }
 
-// q.q - k^2 for real q = (qx, qy) and k, with the three products and the sums compensated
-// (error-free transformations: fma for the products, two-sum for the additions): next to a
-// diffraction threshold q.q and k^2 agree in most digits, and the plain difference loses them.
-__device__ __forceinline__ double q2_minus_k2(double qx, double qy, double k) {
+// q.q - k^2 for real q = (qx + ex, qy + ey) (ex, ey: small low parts) and k, with the products
+// and the sums compensated (error-free transformations: fma for the products, two-sum for the
+// additions): next to a diffraction threshold q.q and k^2 agree in most digits, and the plain
+// difference loses them.
+__device__ __forceinline__ double q2_minus_k2(double qx, double ex, double qy, double ey, double k) {
     const double p1 = qx * qx, e1 = fma(qx, qx, -p1);
     const double p2 = qy * qy, e2 = fma(qy, qy, -p2);
     const double p3 = k * k, e3 = fma(k, k, -p3);
     const double s1 = p1 + p2, z1 = s1 - p1, t1 = (p1 - (s1 - z1)) + (p2 - z1);
     const double s2 = s1 - p3, z2 = s2 - s1, t2 = (s1 - (s2 - z2)) + (-p3 - z2);
-    return s2 + (((t1 + t2) + (e1 + e2)) - e3);
+    return s2 + ((((t1 + t2) + (e1 + e2)) - e3) + 2.0 * (qx * ex + qy * ey));
+}
+// q = kpar + G with G = Gh + Gl a reciprocal vector kept to twice the FP64 precision: the rounded
+// component and the low part (the rounding error of the sum plus Gl)
+__device__ __forceinline__ void bloch_order(double kp, double gh, double gl, double& q, double& e) {
+    q = kp + gh;
+    const double z = q - kp;
+    e = ((kp - (q - z)) + (gh - z)) + gl;
 }
 
 // ---- radial functions -----------------------------------------------------------------

@@ -213,6 +213,7 @@ struct LatticeSumArgs {
     const double2* realtab = nullptr;      // NR x T real-space terms
     int NG = 0;                            // reciprocal lattice vectors
     const double2* G = nullptr;
+    const double2* Glo = nullptr;          // their low parts (G = G + Glo to twice FP64 precision)
     const double* coef = nullptr;          // T x LS_NMAX in-plane polynomial coefficients
     const double2* pref = nullptr;         // T reciprocal prefactors
     double2 self0{0, 0};                   // self term of l = 0 (zero for a nonzero shift)
@@ -241,6 +242,7 @@ struct LatticeSumCkArgs {
     const double2* realtab = nullptr;      // NR x T real-space terms
     int NG = 0;
     const double2* G = nullptr;
+    const double2* Glo = nullptr;          // low parts of the reciprocal vectors
     const double2* coef = nullptr;         // T x LS_PMAX x LS_FMAX: S_lmn coefficient of beta^(2p), order n
     const double2* pref = nullptr;         // T reciprocal prefactors (1/k^2 included)
     double2 self0{0, 0};

@@ -246,11 +246,13 @@ __global__ void __launch_bounds__(256) lattice_sum_kernel(LatticeSumArgs A) {
             __syncthreads();
             int g = g0 + tid;
             if (tid < LS_CHUNK && g < A.NG) {
-                double2 G = A.G[g];
-                double qx = kpar.x + G.x, qy = kpar.y + G.y;
+                const double2 G = A.G[g], Gl = A.Glo[g];
+                double qx, qy, ex, ey;
+                bloch_order(kpar.x, G.x, Gl.x, qx, ex);
+                bloch_order(kpar.y, G.y, Gl.y, qy, ey);
                 double b2 = (qx * qx + qy * qy) / (A.k * A.k);
                 // v = (q.q - k^2) / (2 eta^2 k^2), the difference compensated near a threshold
-                double v = q2_minus_k2(qx, qy, A.k) / (2.0 * A.eta * A.eta * A.k * A.k);
+                double v = q2_minus_k2(qx, ex, qy, ey, A.k) / (2.0 * A.eta * A.eta * A.k * A.k);
                 if (fabs(v) <= 1e-14) {
                     atomicExch(A.status, 9);  // on a diffraction threshold (reciprocal.rs:236-241)
                     for (int n = 0; n <= nmax; ++n) gF[tid * nF + n] = mk(0.0, 0.0);

@@ -266,11 +266,14 @@ __global__ void __launch_bounds__(256) lattice_sum_ck_kernel(LatticeSumCkArgs A)
             __syncthreads();
             const int g = g0 + tid;
             if (tid < CK_CHUNK && g < A.NG) {
-                const double2 G = A.G[g];
-                const double qx = kpar.x + G.x, qy = kpar.y + G.y, q2 = qx * qx + qy * qy;
+                const double2 G = A.G[g], Gl = A.Glo[g];
+                double qx, qy, ex, ey;
+                bloch_order(kpar.x, G.x, Gl.x, qx, ex);
+                bloch_order(kpar.y, G.y, Gl.y, qy, ey);
+                const double q2 = qx * qx + qy * qy;
                 const cplx b2 = cscale(kinv2, q2);
                 // v = (q.q - k^2) / (2 eta^2 k^2): Re(q.q - k^2) = (q.q - Re(k)^2) + Im(k)^2 compensated
-                const cplx d = mk(q2_minus_k2(qx, qy, A.k.x) + A.k.y * A.k.y, -2.0 * A.k.x * A.k.y);
+                const cplx d = mk(q2_minus_k2(qx, ex, qy, ey, A.k.x) + A.k.y * A.k.y, -2.0 * A.k.x * A.k.y);
                 cplx v = cscale(cmul(d, kinv2), 1.0 / (2.0 * A.eta * A.eta));
                 if (v.y == 0.0) v.y = -0.0;  // lower side (lattice/sheets.rs:12-17)
                 if (hypot(v.x, v.y) <= 1e-14) {
