@@ -8,7 +8,7 @@ unpreconditioned), so the checks are:
     the gradient against central differences of the oracle's loss (relative 1e-6 per checked
     weight and along a random direction);
 (2) preconditioned solves against the oracle's dense FP64 solve, the FP64 residual
-    certificate as the judge (relative error 1e-8 at rtol 1e-10);
+    certificate as the criterion (relative error 1e-8 at rtol 1e-10);
 (3) what each level gains: the two-level methods need fewer iterations than block Jacobi, and
     the trained network no more than the two-level method without it.
 """
@@ -103,7 +103,7 @@ def test_block_jacobi_with_one_sphere_blocks_is_the_identity(ctx):
 def test_two_level_with_the_iterative_dipole_solve(ctx):
     # 1200 spheres: 7200 dipole modes, above the size where the dipole system is factored, so
     # the two-level preconditioner solves it by the inner GMRES (a varying preconditioner the
-    # flexible outer GMRES accepts). The FP64 residual certificate is the judge; the solution
+    # flexible outer GMRES accepts). The FP64 residual certificate is the criterion; the solution
     # agrees with block Jacobi's and keeps the two-level iteration gain.
     w = _cluster(1200, 4343)
     c = t.SphereCluster(w.lmax, w.k0, w.radii, w.eps, w.positions, ctx=ctx)
