@@ -105,9 +105,10 @@ __device__ cplx scaled_gamma_c(double d, cplx a) {
 // (lattice/reduced.rs:18-100 with lattice/sheets.rs)
 __device__ cplx reduced_limit_c(int i, cplx z, bool odd_turns) {
     const double b = 0.5 - i;
-    // (-z)^b = (-z)^(-i) sqrt(-z), principal; sqrt(-z) with -z's zero imaginary part as +0
+    // 1 / (-z)^b = (-z)^i / sqrt(-z), principal (sqrt(-z) with -z's zero imaginary part as +0);
+    // formed from the positive power, it stays finite next to a threshold at large i
     const cplx mz = cneg(z);
-    const cplx rp = cmul(cpowi_c(mz, -i), csqrt_p(mz));
+    const cplx inv_rp = cmul(cpowi_c(mz, i), cinv(csqrt_p(mz)));
     cplx g;
     if (use_fraction(z)) {
         // Gamma(b, z) = e^-z z^b CF, and z^b / (-z)^b = e^(-+ i pi b) below / above the axis
@@ -120,9 +121,9 @@ __device__ cplx reduced_limit_c(int i, cplx z, bool odd_turns) {
         const double ph = (z.y > 0.0 ? 1.0 : -1.0) * CK_PI * b;
         double s, c;
         sincos(ph, &s, &c);
-        g = csub(cscale(cinv(rp), tgamma(b)), cmul(mk(c, s), gamma_series_sum_c(b, z)));
+        g = csub(cscale(inv_rp, tgamma(b)), cmul(mk(c, s), gamma_series_sum_c(b, z)));
     }
-    if (odd_turns) g = csub(g, cscale(cinv(rp), 2.0 * tgamma(b)));
+    if (odd_turns) g = csub(g, cscale(inv_rp, 2.0 * tgamma(b)));
     if (z.y > 0.0) g = cneg(g);
     return g;
 }
